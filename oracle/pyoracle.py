@@ -1,0 +1,408 @@
+"""ctypes binding of the CPU oracle (``oracle/lib/libkira_oracle.so``).
+
+Test infrastructure only: the parity checker for the CUDA library and the timed
+CPU baseline of ``bench.py``. The product package never imports this module.
+
+The C functions restate kira-ls-aligner v0.8.3:
+``src/alignment/bitpacked.rs``, ``src/alignment/myers.rs``,
+``src/alignment/mod.rs:1331-2135``, ``src/alignment/sw_int8_vnni.rs``,
+``src/alignment/mod.rs:688-776`` and ``src/alignment/router.rs:191-203``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "lib", "libkira_oracle.so")
+
+I32_MIN = -(2**31)
+# i32::MIN / 8 (exact in Rust): the abort bound that disables the abort test.
+ABORT_DISABLED = -268435456
+OP_CHARS = "MIDNS"
+
+
+class OrcCfg(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in
+                ("match_score", "mismatch", "gap_open", "gap_extend", "bandwidth", "xdrop",
+                 "clip_penalty")]
+
+
+class OrcSwResult(C.Structure):
+    _fields_ = [("ref_start", C.c_uint32), ("ref_end", C.c_uint32), ("read_start", C.c_int32),
+                ("read_end", C.c_int32), ("score", C.c_int32), ("n_cigar", C.c_uint32),
+                ("early_abort", C.c_uint32), ("pad", C.c_uint32), ("cells", C.c_uint64)]
+
+
+class OrcVerifyParams(C.Structure):
+    _fields_ = [("cfg", OrcCfg), ("sieve_threshold", C.c_int32), ("myers_k", C.c_int32),
+                ("abort_score", C.c_int32), ("adaptive", C.c_int32), ("max_drift", C.c_int32),
+                ("dp_xdrop", C.c_int32), ("cert_strict", C.c_int32)]
+
+
+class OrcVerifyResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("sieve_shift", C.c_int32), ("sieve_mism", C.c_int32),
+                ("sieve_second", C.c_int32), ("myers_dist", C.c_int32), ("myers_end", C.c_int32),
+                ("sw", OrcSwResult)]
+
+
+def build() -> None:
+    subprocess.check_call(["make", "-s", "-C", _HERE, "all"])
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        u8p = C.POINTER(C.c_uint8)
+        L.orc_pack.restype = C.c_int
+        L.orc_pack.argtypes = [C.c_char_p, C.c_size_t, u8p]
+        L.orc_shift_bits_right.argtypes = [C.c_char_p, C.c_size_t, C.c_int, u8p]
+        L.orc_pre_shift.argtypes = [C.c_char_p, C.c_size_t, u8p]
+        L.orc_mismatch_count.restype = C.c_size_t
+        L.orc_mismatch_count.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t, C.c_size_t]
+        L.orc_scan_best_with_second_raw.argtypes = [
+            C.c_char_p, C.c_size_t, C.c_size_t, C.c_int, C.c_char_p, C.c_size_t, C.c_size_t,
+            C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.orc_scan.argtypes = [C.c_char_p, C.c_size_t, C.c_size_t, C.c_int, C.c_char_p,
+                               C.c_size_t, C.c_size_t, C.c_size_t, C.POINTER(C.c_int64),
+                               C.POINTER(C.c_int64)]
+        L.orc_gpu_sieve_semantics.argtypes = [C.c_char_p, C.c_uint32, C.c_char_p, C.c_uint32,
+                                              C.c_uint32, C.POINTER(C.c_int32),
+                                              C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.orc_byte_scan.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.c_size_t,
+                                    C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.orc_myers.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.c_size_t, C.c_int,
+                                C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.orc_banded_sw.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.c_int32,
+                                    C.POINTER(OrcCfg), C.c_int32, C.c_int, C.c_int32, C.c_int32,
+                                    C.POINTER(OrcSwResult), C.POINTER(C.c_uint32), C.c_uint32]
+        pp = C.POINTER(C.c_char_p)
+        for name in ("orc_sw_batch_avx2", "orc_sw_batch_int8"):
+            f = getattr(L, name)
+            f.argtypes = [C.c_int, pp, pp, C.c_size_t, C.c_size_t, C.POINTER(C.c_int32),
+                          C.POINTER(C.c_int32), C.POINTER(OrcCfg), C.c_int, C.c_int32, C.c_int32,
+                          C.POINTER(OrcSwResult), C.POINTER(C.c_uint32), C.c_uint32]
+        L.orc_sw_full_window_model.argtypes = [C.c_int, pp, pp, C.c_size_t, C.c_size_t,
+                                               C.POINTER(C.c_int32), C.POINTER(OrcCfg), C.c_int,
+                                               C.POINTER(OrcSwResult), C.POINTER(C.c_uint32),
+                                               C.c_uint32]
+        L.orc_int8_path_viable.argtypes = [C.c_size_t, C.POINTER(OrcCfg)]
+        L.orc_align_batch_simd.argtypes = [C.c_int, pp, C.POINTER(C.c_uint32), pp,
+                                           C.POINTER(C.c_uint32), C.POINTER(C.c_int32),
+                                           C.POINTER(C.c_int32), C.POINTER(OrcCfg), C.c_int,
+                                           C.c_int, C.c_int, C.c_int32, C.c_int32,
+                                           C.POINTER(OrcSwResult), C.POINTER(C.c_uint32),
+                                           C.c_uint32]
+        L.orc_spectral_certified.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t, C.c_size_t,
+                                             C.c_int64, C.c_size_t, C.c_int]
+        L.orc_spectral_max_mismatches.restype = C.c_size_t
+        L.orc_spectral_max_mismatches.argtypes = [C.c_size_t]
+        L.orc_myers_reject_bound.restype = C.c_size_t
+        L.orc_myers_reject_bound.argtypes = [C.c_size_t]
+        L.orc_verify_pair.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t,
+                                      C.POINTER(OrcVerifyParams), C.POINTER(OrcVerifyResult),
+                                      C.POINTER(C.c_uint32), C.c_uint32]
+        vp = C.c_void_p
+        L.orc_verify_batch.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, vp,
+                                       C.POINTER(OrcVerifyParams), C.c_int, vp, vp, C.c_uint32]
+        L.orc_banded_sw_batch.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, vp, vp,
+                                          C.POINTER(OrcCfg), C.c_int32, C.c_int, C.c_int32,
+                                          C.c_int32, C.c_int, vp, vp, C.c_uint32]
+        L.orc_sw_avx2_batch.argtypes = [C.c_uint32, vp, vp, C.c_uint32, vp, vp, C.c_uint32,
+                                        C.POINTER(OrcCfg), C.c_int, vp, vp, C.c_uint32]
+        L.orc_myers_batch.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, vp, C.c_uint32, C.c_int,
+                                      vp, vp]
+        L.orc_sieve_batch.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, vp, C.c_int, vp, vp, vp]
+        _lib = L
+    return _lib
+
+
+# ---------------------------------------------------------------------------
+# Python-shaped wrappers (mirror the reference function shapes)
+# ---------------------------------------------------------------------------
+
+def cfg(match_score=1, mismatch=4, gap_open=6, gap_extend=1, bandwidth=33, xdrop=100,
+        clip_penalty=5) -> OrcCfg:
+    return OrcCfg(match_score, mismatch, gap_open, gap_extend, bandwidth, xdrop, clip_penalty)
+
+
+def pack(seq: bytes):
+    """PackedDna::pack (bitpacked.rs:37-45) -> (bits, len, valid)."""
+    out = (C.c_uint8 * max(1, (len(seq) + 3) // 4))()
+    valid = lib().orc_pack(seq, len(seq), out)
+    return bytes(out)[: (len(seq) + 3) // 4], len(seq), bool(valid)
+
+
+def shift_bits_right(bits: bytes, off: int) -> bytes:
+    out = (C.c_uint8 * max(1, len(bits)))()
+    lib().orc_shift_bits_right(bits, len(bits), off, out)
+    return bytes(out)[: len(bits)]
+
+
+def pre_shift(bits: bytes):
+    n = len(bits)
+    out = (C.c_uint8 * max(1, 4 * n))()
+    lib().orc_pre_shift(bits, n, out)
+    raw = bytes(out)
+    return [raw[p * n:(p + 1) * n] for p in range(4)]
+
+
+def scan_best_with_second(read: bytes, text: bytes):
+    """scan_best_with_second over PackedDna of both sequences -> None | (shift, mism, second|None)."""
+    rb, rl, rv = pack(read)
+    tb, tl, _ = pack(text)
+    ph = b"".join(pre_shift(tb))
+    s, m, sec = C.c_int64(), C.c_int64(), C.c_int64()
+    ok = lib().orc_scan_best_with_second_raw(rb, len(rb), rl, int(rv), ph, len(tb), tl,
+                                             C.byref(s), C.byref(m), C.byref(sec))
+    if not ok:
+        return None
+    return s.value, m.value, (None if sec.value < 0 else sec.value)
+
+
+def scan(read: bytes, text: bytes, max_mism: int):
+    """bitpacked::scan (bitpacked.rs:122-133) -> None | (shift, mism)."""
+    rb, rl, rv = pack(read)
+    tb, tl, _ = pack(text)
+    ph = b"".join(pre_shift(tb))
+    s, m = C.c_int64(), C.c_int64()
+    ok = lib().orc_scan(rb, len(rb), rl, int(rv), ph, len(tb), tl, max_mism, C.byref(s),
+                        C.byref(m))
+    return (s.value, m.value) if ok else None
+
+
+def gpu_sieve_semantics(read_bits: bytes, read_nucs: int, ref_bits: bytes, ref_nucs: int,
+                        max_mism: int):
+    s, m, sec = C.c_int32(), C.c_int32(), C.c_int32()
+    lib().orc_gpu_sieve_semantics(read_bits, read_nucs, ref_bits, ref_nucs, max_mism,
+                                  C.byref(s), C.byref(m), C.byref(sec))
+    return s.value, m.value, sec.value
+
+
+def byte_scan(read: bytes, win: bytes, max_mism: int):
+    s, m = C.c_int64(), C.c_int64()
+    ok = lib().orc_byte_scan(read, len(read), win, len(win), max_mism, C.byref(s), C.byref(m))
+    return (s.value, m.value) if ok else None
+
+
+def bounded_edit_distance(pattern: bytes, text: bytes, max_k: int, path: int = 0):
+    """myers::bounded_edit_distance (myers.rs:47-70) -> None | (dist, end)."""
+    d, e = C.c_uint64(), C.c_uint64()
+    ok = lib().orc_myers(pattern, len(pattern), text, len(text), max_k, path, C.byref(d),
+                         C.byref(e))
+    return (d.value, e.value) if ok else None
+
+
+@dataclass
+class SwRes:
+    ref_start: int
+    ref_end: int
+    read_start: int
+    read_end: int
+    score: int
+    cigar: list  # [(len, op_char)]
+    early_abort: bool
+    cells: int = 0
+
+    def key(self):
+        return (self.ref_start, self.ref_end, self.read_start, self.read_end, self.score,
+                tuple(self.cigar), self.early_abort)
+
+    def cigar_str(self) -> str:
+        return "".join(f"{n}{c}" for n, c in self.cigar)
+
+
+def decode_cigar(words) -> list:
+    return [(int(w) >> 4, OP_CHARS[int(w) & 0xF]) for w in words]
+
+
+def _swres(r: OrcSwResult, cig) -> SwRes:
+    return SwRes(r.ref_start, r.ref_end, r.read_start, r.read_end, r.score,
+                 decode_cigar(cig[: r.n_cigar]), bool(r.early_abort), r.cells)
+
+
+def banded_sw(read: bytes, ref: bytes, offset: int, c: OrcCfg, abort_score=ABORT_DISABLED,
+              adaptive=True, max_drift=16, dp_xdrop=None) -> SwRes:
+    """banded_sw_with (mod.rs:1370-1650)."""
+    cap = len(read) + len(ref) + 2
+    cig = (C.c_uint32 * cap)()
+    out = OrcSwResult()
+    lib().orc_banded_sw(read, len(read), ref, len(ref), offset, C.byref(c), abort_score,
+                        int(adaptive), max_drift, c.xdrop if dp_xdrop is None else dp_xdrop,
+                        C.byref(out), cig, cap)
+    return _swres(out, cig)
+
+
+def _ptrs(seqs):
+    arr = (C.c_char_p * len(seqs))()
+    for i, s in enumerate(seqs):
+        arr[i] = s
+    return arr
+
+
+def sw_batch(kind: str, reads, wins, c: OrcCfg, aborts=None, offsets=None, adaptive=True,
+             max_drift=16, dp_xdrop=None):
+    """Full-window batch kernels: kind in {"avx2", "int8", "model16", "model8"}."""
+    n = len(reads)
+    q, r = len(reads[0]), len(wins[0])
+    cap = q + r + 2
+    cig = (C.c_uint32 * (cap * n))()
+    outs = (OrcSwResult * n)()
+    ab = (C.c_int32 * n)(*(aborts if aborts is not None else [ABORT_DISABLED] * n))
+    off = (C.c_int32 * n)(*(offsets if offsets is not None else [0] * n))
+    L = lib()
+    xd = c.xdrop if dp_xdrop is None else dp_xdrop
+    if kind == "avx2":
+        rc = L.orc_sw_batch_avx2(n, _ptrs(reads), _ptrs(wins), q, r, ab, off, C.byref(c),
+                                 int(adaptive), max_drift, xd, outs, cig, cap)
+    elif kind == "int8":
+        rc = L.orc_sw_batch_int8(n, _ptrs(reads), _ptrs(wins), q, r, ab, off, C.byref(c),
+                                 int(adaptive), max_drift, xd, outs, cig, cap)
+    else:
+        bits = 16 if kind == "model16" else 8
+        rc = L.orc_sw_full_window_model(n, _ptrs(reads), _ptrs(wins), q, r, ab, C.byref(c), bits,
+                                        outs, cig, cap)
+    res = [_swres(outs[k], cig[k * cap:(k + 1) * cap]) for k in range(n)]
+    return rc, res
+
+
+SIMD_SCALAR, SIMD_AVX2, SIMD_VNNI, SIMD_NEON = 0, 1, 2, 3
+
+
+def align_batch_simd(reads, wins, c: OrcCfg, mode: int, detected: int, aborts=None,
+                     offsets=None, adaptive=True, max_drift=16, dp_xdrop=None):
+    """align_batch_simd (mod.rs:1111-1169) SW results (before build_alignment)."""
+    n = len(reads)
+    if n == 0:
+        return []
+    cap = max(len(x) for x in reads) + max(len(x) for x in wins) + 2
+    cig = (C.c_uint32 * (cap * n))()
+    outs = (OrcSwResult * n)()
+    ab = (C.c_int32 * n)(*(aborts if aborts is not None else [ABORT_DISABLED] * n))
+    off = (C.c_int32 * n)(*(offsets if offsets is not None else [0] * n))
+    rl = (C.c_uint32 * n)(*[len(x) for x in reads])
+    wl = (C.c_uint32 * n)(*[len(x) for x in wins])
+    lib().orc_align_batch_simd(n, _ptrs(reads), rl, _ptrs(wins), wl, ab, off, C.byref(c), mode,
+                               detected, int(adaptive), max_drift,
+                               c.xdrop if dp_xdrop is None else dp_xdrop, outs, cig, cap)
+    return [_swres(outs[k], cig[k * cap:(k + 1) * cap]) for k in range(n)]
+
+
+def int8_path_viable(read_len: int, c: OrcCfg) -> bool:
+    return bool(lib().orc_int8_path_viable(read_len, C.byref(c)))
+
+
+def cpu_has_avx2() -> bool:
+    return bool(lib().orc_cpu_has_avx2())
+
+
+def cpu_has_avx_vnni() -> bool:
+    return bool(lib().orc_cpu_has_avx_vnni())
+
+
+def spectral_certified(read: bytes, ref_aligned: bytes, mism: int, second, max_mism: int,
+                       strict=False) -> bool:
+    return bool(lib().orc_spectral_certified(read, ref_aligned, len(read), mism,
+                                             -1 if second is None else second, max_mism,
+                                             int(strict)))
+
+
+def spectral_max_mismatches(n: int) -> int:
+    return lib().orc_spectral_max_mismatches(n)
+
+
+def myers_reject_bound(n: int) -> int:
+    return lib().orc_myers_reject_bound(n)
+
+
+def verify_params(c: OrcCfg, sieve_threshold=12, myers_k=8, abort_score=ABORT_DISABLED,
+                  adaptive=True, max_drift=16, dp_xdrop=None, cert_strict=False):
+    return OrcVerifyParams(c, sieve_threshold, myers_k, abort_score, int(adaptive), max_drift,
+                           c.xdrop if dp_xdrop is None else dp_xdrop, int(cert_strict))
+
+
+def verify_pair(read: bytes, win: bytes, p: OrcVerifyParams):
+    cap = len(read) + len(win) + 2
+    cig = (C.c_uint32 * cap)()
+    out = OrcVerifyResult()
+    lib().orc_verify_pair(read, len(read), win, len(win), C.byref(p), C.byref(out), cig, cap)
+    return out, decode_cigar(cig[: out.sw.n_cigar])
+
+
+VERIFY_DTYPE = np.dtype([("status", "<i4"), ("sieve_shift", "<i4"), ("sieve_mism", "<i4"),
+                         ("sieve_second", "<i4"), ("myers_dist", "<i4"), ("myers_end", "<i4"),
+                         ("ref_start", "<u4"), ("ref_end", "<u4"), ("read_start", "<i4"),
+                         ("read_end", "<i4"), ("score", "<i4"), ("n_cigar", "<u4"),
+                         ("early_abort", "<u4"), ("pad", "<u4"), ("cells", "<u8")])
+SW_DTYPE = np.dtype([("ref_start", "<u4"), ("ref_end", "<u4"), ("read_start", "<i4"),
+                     ("read_end", "<i4"), ("score", "<i4"), ("n_cigar", "<u4"),
+                     ("early_abort", "<u4"), ("pad", "<u4"), ("cells", "<u8")])
+assert VERIFY_DTYPE.itemsize == C.sizeof(OrcVerifyResult)
+assert SW_DTYPE.itemsize == C.sizeof(OrcSwResult)
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def verify_batch(reads, read_off, read_len, wins, win_off, win_len, p: OrcVerifyParams,
+                 nthreads: int, cap_per_pair: int):
+    """Threaded composed verification over flat arrays (numpy)."""
+    n = len(read_off)
+    out = np.zeros(n, VERIFY_DTYPE)
+    cig = np.zeros(n * cap_per_pair, np.uint32)
+    lib().orc_verify_batch(n, _p(reads), _p(read_off), _p(read_len), _p(wins), _p(win_off),
+                           _p(win_len), C.byref(p), nthreads, _p(out), _p(cig), cap_per_pair)
+    return out, cig.reshape(n, cap_per_pair)
+
+
+def banded_sw_batch(reads, read_off, read_len, wins, win_off, win_len, offsets, c: OrcCfg,
+                    nthreads: int, cap_per_pair: int, abort_score=ABORT_DISABLED, adaptive=True,
+                    max_drift=16, dp_xdrop=None):
+    n = len(read_off)
+    out = np.zeros(n, SW_DTYPE)
+    cig = np.zeros(n * cap_per_pair, np.uint32)
+    lib().orc_banded_sw_batch(n, _p(reads), _p(read_off), _p(read_len), _p(wins), _p(win_off),
+                              _p(win_len), _p(offsets), C.byref(c), abort_score, int(adaptive),
+                              max_drift, c.xdrop if dp_xdrop is None else dp_xdrop, nthreads,
+                              _p(out), _p(cig), cap_per_pair)
+    return out, cig.reshape(n, cap_per_pair)
+
+
+def sw_avx2_batch(reads, read_off, q, wins, win_off, r, c: OrcCfg, nthreads: int,
+                  cap_per_pair: int):
+    n = len(read_off)
+    out = np.zeros(n, SW_DTYPE)
+    cig = np.zeros(n * cap_per_pair, np.uint32)
+    lib().orc_sw_avx2_batch(n, _p(reads), _p(read_off), q, _p(wins), _p(win_off), r, C.byref(c),
+                            nthreads, _p(out), _p(cig), cap_per_pair)
+    return out, cig.reshape(n, cap_per_pair)
+
+
+def myers_batch(reads, read_off, read_len, wins, win_off, win_len, max_k, nthreads):
+    n = len(read_off)
+    dist = np.zeros(n, np.int64)
+    end = np.zeros(n, np.int64)
+    lib().orc_myers_batch(n, _p(reads), _p(read_off), _p(read_len), _p(wins), _p(win_off),
+                          _p(win_len), max_k, nthreads, _p(dist), _p(end))
+    return dist, end
+
+
+def sieve_batch(reads, read_off, read_len, wins, win_off, win_len, nthreads):
+    n = len(read_off)
+    s = np.zeros(n, np.int32)
+    m = np.zeros(n, np.int32)
+    sec = np.zeros(n, np.int32)
+    lib().orc_sieve_batch(n, _p(reads), _p(read_off), _p(read_len), _p(wins), _p(win_off),
+                          _p(win_len), nthreads, _p(s), _p(m), _p(sec))
+    return s, m, sec
