@@ -1,0 +1,358 @@
+"""Benchmark of the composed verification path (sieve -> certificate -> Myers ->
+banded SW with CIGAR) on the batched short-read workload: 2M (read x window)
+pairs, 150 bp reads, 250 bp windows, 8 candidates per read, band 33, scoring
++1/-4/-6/-1, sieve threshold 12, Myers k 8; seeded synthetic data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0. `value` = pairs/s with inputs resident in HBM
+(kira_gpu_verify_dev, CUDA events on the launching stream, L2 flushed between
+steps); `e2e` = pairs/s through the host API (kira_gpu_verify_batch) with pinned
+host inputs, H2D + D2H inside the timed region. Multi-GPU: one process per GPU,
+each rank verifies its own 2M-pair shard (weak scaling, no data-path collective),
+time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "batched_2M_150x250_band33"
+METRIC = "pairs/s (composed sieve+Myers+banded-SW verification, bit-exact)"
+UNIT = "pairs/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--reads", type=int, default=250_000, help="reads per rank (x8 pairs)")
+    ap.add_argument("--cpu-sample", type=int, default=20_000, help="pairs in the CPU sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(w, nthreads: int, sample: int, repeat_min_s: float = 10.0):
+    """The oracle port of the reference CPU path on a bounded sample of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    arena, woffs = w.windows_arena()
+    idx = np.arange(min(sample, w.n_pairs))
+    op = O.verify_params(O.cfg(1, 4, 6, 1, 33, 100, 5), 12, 8)
+    args = (w.reads, w.read_off[idx].copy(), w.read_len[idx].copy(), arena, woffs[idx].copy(),
+            w.win_len[idx].copy())
+    done, t0 = 0, time.perf_counter()
+    while True:
+        O.verify_batch(*args, op, nthreads, 8)
+        done += len(idx)
+        el = time.perf_counter() - t0
+        if el >= repeat_min_s:
+            break
+    return done / el, el, len(idx)
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference CPU path (oracle port, all host threads)."""
+    if rank != 0:
+        return
+    from kira_ls_aligner_b200 import synth
+    w = synth.batched(n_reads=max(args.reads // 10, 1000))
+    nthreads = os.cpu_count() or 1
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    arena, woffs = w.windows_arena()
+    n = min(args.cpu_sample, w.n_pairs)
+    op = O.verify_params(O.cfg(1, 4, 6, 1, 33, 100, 5), 12, 8)
+    a = (w.reads, w.read_off[:n].copy(), w.read_len[:n].copy(), arena, woffs[:n].copy(),
+         w.win_len[:n].copy())
+    for _ in range(args.warmup):
+        O.verify_batch(*a, op, nthreads, 8)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        O.verify_batch(*a, op, nthreads, 8)
+        times.append(time.perf_counter() - t)
+    v = n * len(times) / sum(times)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "pairs_per_step": n, "threads": nthreads},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
+                         "sample": f"{n} pairs of the batched workload per step"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, local, world, dist)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+def run_ours(args, rank, local, world, dist):
+    import torch
+
+    from kira_ls_aligner_b200 import GpuContext, VerifyParams, _abi, synth
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = synth.batched(seed=0xB200 + rank, n_reads=args.reads)
+    n = w.n_pairs
+    params = VerifyParams(sieve_threshold=12, myers_k=8)
+    ctx = GpuContext(local)
+    L = _abi.lib()
+    ctx.ref_upload(w.reference)
+
+    # Device-resident inputs and outputs.
+    t_reads = torch.from_numpy(np.concatenate([w.reads, np.zeros(16, np.uint8)])).to(dev)
+    t_roff = torch.from_numpy(w.read_off.view(np.int64)).to(dev)
+    t_rlen = torch.from_numpy(w.read_len.view(np.int32)).to(dev)
+    t_woff = torch.from_numpy(w.win_off.view(np.int64)).to(dev)
+    t_wlen = torch.from_numpy(w.win_len.view(np.int32)).to(dev)
+    cap = 4 * n
+    t_res = torch.empty(n * 32, dtype=torch.uint8, device=dev)
+    t_ops = torch.empty(cap, dtype=torch.int32, device=dev)
+    t_used = torch.zeros(1, dtype=torch.int64, device=dev)
+    t_cells = torch.zeros(1, dtype=torch.int64, device=dev)
+    pc = _abi.Pairs()
+    pc.n = n
+    pc.max_read_len, pc.max_win_len = int(w.read_len.max()), int(w.win_len.max())
+    pc.read_seq, pc.read_seq_bytes = t_reads.data_ptr(), int(w.reads.nbytes)
+    pc.read_off, pc.read_len = t_roff.data_ptr(), t_rlen.data_ptr()
+    pc.win_seq, pc.win_off, pc.win_len = None, t_woff.data_ptr(), t_wlen.data_ptr()
+    vp = params.to_c()
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        rc = L.kira_gpu_verify_dev(ctx.handle, C.byref(pc), C.byref(vp), t_res.data_ptr(),
+                                   t_ops.data_ptr(), cap, t_used.data_ptr(), None,
+                                   t_cells.data_ptr(), C.c_void_p(stream.cuda_stream))
+        ctx.check(rc)
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    L.kira_gpu_profile(ctx.handle, 1)
+    stage_ms = np.zeros(len(_abi.STAGES))
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    total_ms = 0.0
+    t_cells.zero_()
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        buf = (C.c_float * 8)()
+        k = L.kira_gpu_stage_times(ctx.handle, buf, 8)
+        stage_ms[:k] += np.array(buf[:k])
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    L.kira_gpu_profile(ctx.handle, 0)
+    cells = int(t_cells.item())
+    if dist is not None:
+        tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ms_per_step = total_ms / args.steps
+    value = n * world * args.steps / (total_ms / 1e3)
+    gcups = cells * world / (total_ms / 1e3) / 1e9
+
+    # Outcome summary of one step (for the record; parity is checked by the tests).
+    res = np.frombuffer(t_res.cpu().numpy().tobytes(), _abi.SW_RESULT_DTYPE)
+    statuses = np.bincount(res["status"], minlength=4).tolist()
+
+    # e2e through the host API with pinned host inputs.
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(a).pin_memory()
+        h_reads = pin(np.concatenate([w.reads, np.zeros(16, np.uint8)]))
+        h_roff, h_rlen = pin(w.read_off.view(np.int64)), pin(w.read_len.view(np.int32))
+        h_woff, h_wlen = pin(w.win_off.view(np.int64)), pin(w.win_len.view(np.int32))
+        res_h = torch.empty(n * 32, dtype=torch.uint8).pin_memory()
+        ops_h = torch.empty(cap, dtype=torch.int32).pin_memory()
+        cb = _abi.CigarBuf(ops_h.data_ptr(), cap, 0)
+        hpc = _abi.Pairs()
+        hpc.n = n
+        hpc.read_seq, hpc.read_seq_bytes = h_reads.data_ptr(), int(w.reads.nbytes)
+        hpc.read_off, hpc.read_len = h_roff.data_ptr(), h_rlen.data_ptr()
+        hpc.win_seq, hpc.win_off, hpc.win_len = None, h_woff.data_ptr(), h_wlen.data_ptr()
+        cells_h = C.c_uint64()
+
+        def e2e_step():
+            ctx.check(L.kira_gpu_verify_batch(ctx.handle, C.byref(hpc), C.byref(vp),
+                                              res_h.data_ptr(), C.byref(cb), None,
+                                              C.byref(cells_h)))
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        el = time.perf_counter() - t0
+        if dist is not None:
+            tt = torch.tensor([el], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            el = float(tt.item())
+        h2d = int(w.reads.nbytes) + n * (8 + 4 + 8 + 4)
+        d2h = n * 32 + 4 * int(cb.used) + 8 + 8 + 16
+        e2e = {"value": n * world * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * el / args.steps}
+
+    # Roofline of the dominant stage.
+    peak, peak_kind = measured_peaks()
+    dom = int(np.argmax(stage_ms))
+    dom_ms = stage_ms[dom] / args.steps
+    n_sw = statuses[3]
+    n_my = statuses[2] + statuses[3]
+    q, wl = 150, 250
+    alg_bytes = {  # algorithmic bytes per launch of each stage (ASCII sequences in HBM)
+        0: n * (q + wl + 24 + 32),
+        1: n_my * (q + wl + 8) + n_sw * 4,
+        2: n_sw * (q + wl + 16) + cells // max(args.steps, 1) // 2,
+        3: n_sw * (32 + 16) + cells // max(args.steps, 1) // 2 // 50,
+        4: n * (32 + 8) + 4 * n,
+    }[dom]
+    achieved = alg_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": _abi.STAGES[dom], "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs",
+                "stage_ms_per_step": {s: round(float(t) / args.steps, 4)
+                                      for s, t in zip(_abi.STAGES, stage_ms)}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        nthreads = os.cpu_count() or 1
+        v, el, ns = cpu_baseline(w, nthreads, args.cpu_sample)
+        cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": f"first {ns} pairs of the workload, repeated for {el:.1f} s"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded; no public dataset)",
+            "config": {"workload": WORKLOAD, "pairs_per_gpu": n, "read_len": 150,
+                       "window_len": 250, "candidates_per_read": 8, "band": 33,
+                       "sieve_threshold": 12, "myers_k": 8, "reference_bp": int(len(w.reference)),
+                       "l2": "flushed between steps (256 MB write)",
+                       "parallelism": f"replicas x{world} (pairs sharded, no collective)"},
+            "gcups": gcups, "cells_per_step": cells // args.steps,
+            "status_counts": {"certified": statuses[1], "myers_reject": statuses[2],
+                              "sw": statuses[3]},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": 8 * args.steps,
+        }
+        print(json.dumps(out))
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,242 @@
+/*
+ * kira_gpu.h -- C ABI of the B200 (sm_100a) candidate-verification library.
+ *
+ * Replaces the GPU backend and the CPU DP kernels of kira-ls-aligner's
+ * verification/extension hot path:
+ *   - the 2-bit multi-shift Hamming sieve   (src/alignment/bitpacked.rs,
+ *                                            src/cuda/spectral.cu, src/cuda/backend.rs)
+ *   - Myers bounded edit distance            (src/alignment/myers.rs)
+ *   - banded affine Smith-Waterman + CIGAR   (src/alignment/mod.rs:1331-1771)
+ *   - full-window batch SW (align_batch_simd) (src/alignment/mod.rs:1111-1169,1846-2135,
+ *                                            src/alignment/sw_int8_vnni.rs)
+ *
+ * Conventions
+ *   - Every entry point returns an int status (kira_status). 0 is success.
+ *   - Host buffers passed to the non-"_dev" entry points are borrowed for the
+ *     duration of the call; results are written into caller-owned buffers.
+ *   - The library owns all device memory it allocates (grow-only arena per ctx).
+ *   - One kira_ctx per host thread; a ctx is not thread-safe (like CudaBackend,
+ *     which is pinned to its thread: src/cuda/backend.rs:264-269).
+ *   - Sequences are ASCII bytes exactly as the Rust API receives them; byte
+ *     equality (SW), case-insensitive ACGT (Myers) and the 2-bit code with the
+ *     valid flag (sieve) follow the reference functions bit for bit.
+ *   - CIGAR ops are packed BAM-style: (len << 4) | op, op 0=M 1=I 2=D 3=N 4=S.
+ */
+#ifndef KIRA_GPU_H
+#define KIRA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KIRA_GPU_ABI_VERSION 1
+
+/* Status codes; the first five map onto CudaError (src/cuda/mod.rs:18-34). */
+enum kira_status {
+  KIRA_OK = 0,
+  KIRA_ERR_NOT_BUILT = 1,     /* CudaError::NotBuilt */
+  KIRA_ERR_DRIVER = 2,        /* CudaError::Driver */
+  KIRA_ERR_RUNTIME = 3,       /* CudaError::Runtime */
+  KIRA_ERR_NO_DEVICE = 4,     /* CudaError::NoDevice */
+  KIRA_ERR_READ_TOO_LONG = 5, /* CudaError::ReadTooLong */
+  KIRA_ERR_TIMEOUT = 6,       /* a bounded wait expired */
+  KIRA_ERR_INVALID = 7,       /* argument outside the supported domain */
+  KIRA_ERR_OOM = 8,           /* device memory exhausted / admission refused */
+  KIRA_ERR_CAPACITY = 9       /* caller's output buffer too small (see *_used) */
+};
+
+/* Per-pair status of the composed verification. */
+enum kira_pair_status {
+  KIRA_PAIR_PENDING = 0,
+  KIRA_PAIR_CERTIFIED = 1,    /* ungapped hit accepted by the certificate */
+  KIRA_PAIR_MYERS_REJECT = 2, /* bounded edit distance above k */
+  KIRA_PAIR_SW = 3            /* banded SW alignment */
+};
+
+/* Maximum packed read length of the sieve drop-in (src/cuda/mod.rs:35-37). */
+#define KIRA_READ_BYTES_MAX 64
+
+typedef struct kira_ctx kira_ctx;
+
+/* ---------------------------------------------------------------- context */
+
+/* cuda::is_available (src/cuda/mod.rs:39-49). 1 when a CUDA device is usable. */
+int kira_gpu_is_available(void);
+
+/* CudaBackend::new (src/cuda/backend.rs:61-93): bind `device`, create the
+ * ctx's stream and arena. */
+int kira_gpu_init(int device, kira_ctx** out);
+
+/* CudaBackend drop / release_buffers (src/cuda/backend.rs:251-261). */
+void kira_gpu_destroy(kira_ctx* ctx);
+
+/* Text of the last error on this ctx (the String inside CudaError). Returns the
+ * full length; writes at most len-1 bytes plus a NUL. */
+int kira_gpu_last_error(const kira_ctx* ctx, char* buf, size_t len);
+
+/* Bytes of device memory the ctx arena currently holds. */
+uint64_t kira_gpu_arena_bytes(const kira_ctx* ctx);
+
+/* ------------------------------------------------------- sieve (drop-in) */
+
+/* CudaJob (src/cuda/backend.rs:13-26). Only phase 0 of ref_shifted is read:
+ * the kernel derives the other three bit phases in registers, so the 4x
+ * pre-shifted host copies (bitpacked.rs:95-119) are not needed. */
+typedef struct kira_sieve_job {
+  const uint8_t* read_packed; /* 2-bit packed, (read_nucs + 3) / 4 bytes */
+  uint32_t read_bytes;        /* length of read_packed */
+  uint32_t read_nucs;
+  const uint8_t* ref_packed;  /* ref_shifted[0] */
+  uint32_t ref_bytes;         /* length of ref_packed, >= (ref_nucs + 3) / 4 */
+  uint32_t ref_nucs;
+  uint32_t max_mismatches;
+} kira_sieve_job;
+
+/* CudaResult (src/cuda/backend.rs:28-35): shift -1 / mismatches INT32_MAX when
+ * the best hit is above min(max_mismatches, read_nucs); second_mismatches is
+ * INT32_MAX for None. */
+typedef struct kira_sieve_result {
+  int32_t shift;
+  int32_t mismatches;
+  int32_t second_mismatches;
+} kira_sieve_result;
+
+/* CudaBackend::run_batch (src/cuda/backend.rs:95-249). Returns
+ * KIRA_ERR_READ_TOO_LONG when a read exceeds KIRA_READ_BYTES_MAX packed bytes. */
+int kira_gpu_sieve_batch(kira_ctx* ctx, const kira_sieve_job* jobs, uint32_t n,
+                         kira_sieve_result* out);
+
+/* ------------------------------------------------ pairs and configuration */
+
+/* A batch of (read x window) pairs. Reads and windows are ASCII arenas; pair p
+ * uses read_seq[read_off[p] .. +read_len[p]] and win_seq[win_off[p] .. +win_len[p]].
+ * Pairs may share a read (candidate windows of one read). win_seq == NULL selects
+ * the device-resident reference (kira_gpu_ref_upload); win_off is then a
+ * reference coordinate. Optional per-pair arrays may be NULL. */
+typedef struct kira_pairs {
+  uint32_t n;
+  uint32_t max_read_len;      /* upper bound of read_len[]; 0 -> computed (host API only) */
+  uint32_t max_win_len;       /* upper bound of win_len[];  0 -> computed (host API only) */
+  uint32_t max_bandwidth;     /* upper bound of bandwidth[]; 0 -> computed (host API only) */
+  const uint8_t* read_seq;
+  uint64_t read_seq_bytes;
+  const uint64_t* read_off;
+  const uint32_t* read_len;
+  const uint8_t* win_seq;
+  uint64_t win_seq_bytes;
+  const uint64_t* win_off;
+  const uint32_t* win_len;
+  const int32_t* band_offset; /* banded_sw `offset` (mod.rs:1331-1337); NULL -> 0 */
+  const int32_t* abort_score; /* NULL -> disabled (i32::MIN / 8) */
+  const int32_t* bandwidth;   /* per-pair half-width; NULL -> cfg.bandwidth */
+} kira_pairs;
+
+/* AlignmentConfig (src/alignment/mod.rs:24-35) plus the hot-path knobs that the
+ * reference reads from the environment once (mod.rs:1256-1329). */
+typedef struct kira_sw_cfg {
+  int32_t match_score;
+  int32_t mismatch;
+  int32_t gap_open;
+  int32_t gap_extend;
+  int32_t bandwidth;    /* half-width; rows cover centre +- bandwidth */
+  int32_t xdrop;
+  int32_t clip_penalty;
+  int32_t adaptive;     /* KIRA_ADAPTIVE_BAND, default 1 */
+  int32_t max_drift;    /* KIRA_ADAPTIVE_MAX_DRIFT, default 16 */
+  int32_t dp_xdrop;     /* KIRA_DP_XDROP; < 0 -> use xdrop */
+} kira_sw_cfg;
+
+/* SwPublicResult (src/alignment/mod.rs:910-920) in window coordinates; the
+ * CIGAR is ops[cigar_off .. cigar_off + n_cigar) of the call's CIGAR buffer. */
+typedef struct kira_sw_result {
+  int32_t score;
+  uint32_t ref_start;
+  uint32_t ref_end;
+  int32_t read_start;
+  int32_t read_end;
+  uint32_t cigar_off;
+  uint32_t n_cigar;
+  uint8_t status;      /* kira_pair_status (verify) or KIRA_PAIR_SW */
+  uint8_t early_abort;
+  uint16_t reserved;
+} kira_sw_result;
+
+/* Caller-owned CIGAR output: ops[cap]; *used receives the number of ops the
+ * call produced. KIRA_ERR_CAPACITY when used > cap (nothing past cap written). */
+typedef struct kira_cigar_buf {
+  uint32_t* ops;
+  uint64_t cap;
+  uint64_t used;
+} kira_cigar_buf;
+
+/* Opt-in stage timing (CUDA events on the work stream). After a verification
+ * call has completed, kira_gpu_stage_times fills ms[] with the durations of:
+ * 0 sieve + certificate, 1 Myers, 2 banded-SW DP, 3 traceback, 4 CIGAR
+ * compaction, and returns how many were filled. */
+int kira_gpu_profile(kira_ctx* ctx, int enable);
+int kira_gpu_stage_times(kira_ctx* ctx, float* ms, int max_stages);
+
+/* Upload the reference as ASCII bases (Index::ref_bases, src/index/mod.rs:1098);
+ * it stays resident until the next upload or kira_gpu_destroy. */
+int kira_gpu_ref_upload(kira_ctx* ctx, const uint8_t* seq, uint64_t len);
+
+/* ------------------------------------------------------------ Myers */
+
+/* myers::bounded_edit_distance (src/alignment/myers.rs:47-70) per pair:
+ * dist[p] = -1 for None. Patterns up to 2048 bases. */
+int kira_gpu_myers_batch(kira_ctx* ctx, const kira_pairs* pairs, uint32_t max_k, int32_t* dist,
+                         int32_t* end_pos);
+
+/* ------------------------------------------------------- banded SW */
+
+/* banded_sw_public (src/alignment/mod.rs:890-908) per pair. Requires gap_open,
+ * gap_extend, mismatch >= 0, bandwidth <= 1023 and read_len * match_score < 2^21.
+ * cells (optional) receives the executed band cells. */
+int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg* cfg,
+                       kira_sw_result* out, kira_cigar_buf* cigar, uint64_t* cells);
+
+/* ------------------------------------------- composed verification */
+
+/* Parameters of the composed path (sieve -> certificate -> Myers -> banded SW). */
+typedef struct kira_verify_params {
+  kira_sw_cfg sw;
+  int32_t sieve_threshold; /* certificate mismatch bound; < 0 -> spectral_max_mismatches */
+  int32_t myers_k;         /* < 0 -> myers_reject_bound(read_len) */
+  int32_t cert_strict;     /* KIRA_CERT_STRICT */
+  int32_t reserved;
+} kira_verify_params;
+
+/* Optional per-stage detail. */
+typedef struct kira_verify_detail {
+  int32_t sieve_shift;  /* -1 when the packed scan returned None */
+  int32_t sieve_mism;   /* INT32_MAX when None */
+  int32_t sieve_second; /* INT32_MAX when None */
+  int32_t myers_dist;   /* -1 when rejected or not run */
+  int32_t myers_end;
+} kira_verify_detail;
+
+/* For every pair: packed_scan_scratch + spectral_hit_is_certified
+ * (mod.rs:594-762) -> ungapped qM when certified; else bounded_edit_distance
+ * (myers.rs:47) with k -> KIRA_PAIR_MYERS_REJECT on None; else banded_sw
+ * (mod.rs:1331) with offset = the sieve's best shift (0 without a hit). */
+int kira_gpu_verify_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_verify_params* p,
+                          kira_sw_result* out, kira_cigar_buf* cigar, kira_verify_detail* detail,
+                          uint64_t* cells);
+
+/* Device-pointer form of kira_gpu_verify_batch: every pointer in `pairs` and the
+ * outputs are device pointers; work is enqueued on `stream` (a cudaStream_t) and
+ * the call returns without synchronising. Arena allocations must be readable up
+ * to the next 16-byte boundary past their last byte. cigar_ops receives the
+ * packed CIGAR (capacity cigar_cap ops); *cigar_used_dev (device) the op count. */
+int kira_gpu_verify_dev(kira_ctx* ctx, const kira_pairs* pairs, const kira_verify_params* p,
+                        kira_sw_result* out, uint32_t* cigar_ops, uint64_t cigar_cap,
+                        uint64_t* cigar_used_dev, kira_verify_detail* detail,
+                        unsigned long long* cells_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KIRA_GPU_H */

@@ -1,0 +1,127 @@
+"""ctypes binding of libkira_gpu.so (include/kira_gpu.h).
+
+Loading is strict: if the library is missing or cannot be loaded the import
+raises, so no caller can silently run anything but the CUDA path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libkira_gpu.so")
+
+KIRA_OK = 0
+STATUS_NAMES = {
+    0: "OK", 1: "NotBuilt", 2: "Driver", 3: "Runtime", 4: "NoDevice", 5: "ReadTooLong",
+    6: "Timeout", 7: "Invalid", 8: "OutOfMemory", 9: "Capacity",
+}
+PAIR_PENDING, PAIR_CERTIFIED, PAIR_MYERS_REJECT, PAIR_SW = 0, 1, 2, 3
+READ_BYTES_MAX = 64
+ABORT_DISABLED = -268435456  # i32::MIN / 8
+INT32_MAX = 2**31 - 1
+
+# Every symbol include/kira_gpu.h declares.
+EXPORTS = (
+    "kira_gpu_is_available", "kira_gpu_init", "kira_gpu_destroy", "kira_gpu_last_error",
+    "kira_gpu_arena_bytes", "kira_gpu_sieve_batch", "kira_gpu_ref_upload",
+    "kira_gpu_myers_batch", "kira_gpu_bsw_batch", "kira_gpu_verify_batch",
+    "kira_gpu_verify_dev", "kira_gpu_profile", "kira_gpu_stage_times",
+)
+STAGES = ("sieve_certify", "myers", "bsw_dp", "bsw_traceback", "cigar_compact")
+
+
+class SieveJob(C.Structure):
+    _fields_ = [("read_packed", C.c_void_p), ("read_bytes", C.c_uint32),
+                ("read_nucs", C.c_uint32), ("ref_packed", C.c_void_p),
+                ("ref_bytes", C.c_uint32), ("ref_nucs", C.c_uint32),
+                ("max_mismatches", C.c_uint32)]
+
+
+class SieveResult(C.Structure):
+    _fields_ = [("shift", C.c_int32), ("mismatches", C.c_int32),
+                ("second_mismatches", C.c_int32)]
+
+
+class Pairs(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("max_read_len", C.c_uint32), ("max_win_len", C.c_uint32),
+                ("max_bandwidth", C.c_uint32), ("read_seq", C.c_void_p),
+                ("read_seq_bytes", C.c_uint64), ("read_off", C.c_void_p),
+                ("read_len", C.c_void_p), ("win_seq", C.c_void_p),
+                ("win_seq_bytes", C.c_uint64), ("win_off", C.c_void_p),
+                ("win_len", C.c_void_p), ("band_offset", C.c_void_p),
+                ("abort_score", C.c_void_p), ("bandwidth", C.c_void_p)]
+
+
+class SwCfg(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in
+                ("match_score", "mismatch", "gap_open", "gap_extend", "bandwidth", "xdrop",
+                 "clip_penalty", "adaptive", "max_drift", "dp_xdrop")]
+
+
+class VerifyParams(C.Structure):
+    _fields_ = [("sw", SwCfg), ("sieve_threshold", C.c_int32), ("myers_k", C.c_int32),
+                ("cert_strict", C.c_int32), ("reserved", C.c_int32)]
+
+
+class CigarBuf(C.Structure):
+    _fields_ = [("ops", C.c_void_p), ("cap", C.c_uint64), ("used", C.c_uint64)]
+
+
+SW_RESULT_DTYPE = np.dtype([("score", "<i4"), ("ref_start", "<u4"), ("ref_end", "<u4"),
+                            ("read_start", "<i4"), ("read_end", "<i4"), ("cigar_off", "<u4"),
+                            ("n_cigar", "<u4"), ("status", "u1"), ("early_abort", "u1"),
+                            ("reserved", "<u2")])
+DETAIL_DTYPE = np.dtype([("sieve_shift", "<i4"), ("sieve_mism", "<i4"),
+                         ("sieve_second", "<i4"), ("myers_dist", "<i4"), ("myers_end", "<i4")])
+assert SW_RESULT_DTYPE.itemsize == 32 and DETAIL_DTYPE.itemsize == 20
+
+_lib = None
+
+
+def lib():
+    """Load libkira_gpu.so; raises when it is missing (no fallback path exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m kira_ls_aligner_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.kira_gpu_is_available.restype = C.c_int
+    L.kira_gpu_init.argtypes = [C.c_int, C.POINTER(vp)]
+    L.kira_gpu_destroy.argtypes = [vp]
+    L.kira_gpu_destroy.restype = None
+    L.kira_gpu_last_error.argtypes = [vp, C.c_char_p, C.c_size_t]
+    L.kira_gpu_arena_bytes.argtypes = [vp]
+    L.kira_gpu_arena_bytes.restype = C.c_uint64
+    L.kira_gpu_sieve_batch.argtypes = [vp, C.POINTER(SieveJob), C.c_uint32,
+                                       C.POINTER(SieveResult)]
+    L.kira_gpu_ref_upload.argtypes = [vp, vp, C.c_uint64]
+    L.kira_gpu_myers_batch.argtypes = [vp, C.POINTER(Pairs), C.c_uint32, vp, vp]
+    L.kira_gpu_bsw_batch.argtypes = [vp, C.POINTER(Pairs), C.POINTER(SwCfg), vp,
+                                     C.POINTER(CigarBuf), C.POINTER(C.c_uint64)]
+    L.kira_gpu_verify_batch.argtypes = [vp, C.POINTER(Pairs), C.POINTER(VerifyParams), vp,
+                                        C.POINTER(CigarBuf), vp, C.POINTER(C.c_uint64)]
+    L.kira_gpu_verify_dev.argtypes = [vp, C.POINTER(Pairs), C.POINTER(VerifyParams), vp, vp,
+                                      C.c_uint64, vp, vp, vp, vp]
+    L.kira_gpu_profile.argtypes = [vp, C.c_int]
+    L.kira_gpu_stage_times.argtypes = [vp, C.POINTER(C.c_float), C.c_int]
+    for name in EXPORTS:
+        getattr(L, name).restype = getattr(L, name).restype or C.c_int
+    L.kira_gpu_destroy.restype = None
+    L.kira_gpu_arena_bytes.restype = C.c_uint64
+    _lib = L
+    return L
+
+
+def ptr(a) -> int | None:
+    """Address of a numpy array / torch tensor (None for None)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data

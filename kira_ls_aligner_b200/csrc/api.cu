@@ -1,0 +1,625 @@
+// api.cu -- the extern "C" entry points of libkira_gpu (include/kira_gpu.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "kira_gpu.h"
+
+using namespace kira;
+
+namespace {
+
+enum BufId {
+  B_READ_SEQ, B_WIN_SEQ, B_READ_OFF, B_READ_LEN, B_WIN_OFF, B_WIN_LEN, B_BAND_OFF, B_ABORT,
+  B_BANDW, B_OUT, B_DETAIL, B_CIGAR_OUT, B_NCIG, B_CIG_OFF, B_CHUNK_SUMS, B_SW_OFFSET,
+  B_MYERS_LIST, B_SW_LIST, B_COUNTERS, B_ENDS, B_TRACE, B_META, B_CIG_SLOTS, B_ITEM_OF_PAIR,
+  B_DIST, B_END, B_SIEVE_OUT, B_SIEVE_JOBS, B_CELLS, B_TOTAL, B_COUNT
+};
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+constexpr int kStages = 5;  // sieve+certificate, Myers, SW DP, SW traceback, CIGAR compaction
+
+struct kira_ctx {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  bool profile = false;
+  cudaEvent_t ev[kStages + 1] = {};
+  int ev_recorded = 0;
+  uint8_t* ref_dev = nullptr;
+  uint64_t ref_len = 0;
+  DevBuf bufs[B_COUNT];
+};
+
+namespace {
+
+int fail(kira_ctx* ctx, int code, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    ctx->last_error = buf;
+  }
+  return code;
+}
+
+int cuda_fail(kira_ctx* ctx, cudaError_t e, const char* what) {
+  const int code = (e == cudaErrorMemoryAllocation) ? KIRA_ERR_OOM : KIRA_ERR_RUNTIME;
+  return fail(ctx, code, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// Grow-only device buffer (ensure_capacity_*, src/cuda/backend.rs:271-308);
+// 16 bytes of slack so vector loads may read to the next 16-byte boundary.
+void* dbuf(kira_ctx* ctx, BufId id, size_t bytes, cudaError_t* err) {
+  DevBuf& b = ctx->bufs[id];
+  const size_t need = bytes + 16;
+  if (b.bytes >= need) return b.p;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  const size_t cap = std::max(need, b.bytes * 2);
+  cudaError_t e = cudaMalloc(&b.p, cap);
+  if (e != cudaSuccess) {
+    *err = e;
+    b.p = nullptr;
+    return nullptr;
+  }
+  b.bytes = cap;
+  return b.p;
+}
+
+#define KIRA_DBUF(var, type, id, count)                                           \
+  type* var = (type*)dbuf(ctx, id, sizeof(type) * (size_t)(count), &cerr);        \
+  if (!var) return cuda_fail(ctx, cerr, "device allocation (" #id ")");
+
+#define KIRA_CUDA(call)                                   \
+  do {                                                    \
+    cudaError_t _e = (call);                              \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call); \
+  } while (0)
+
+SwParams resolve(const kira_sw_cfg& c) {
+  SwParams s;
+  s.match = c.match_score;
+  s.mismatch = c.mismatch;
+  s.gap_open = c.gap_open;
+  s.gap_extend = c.gap_extend;
+  s.band = std::max(c.bandwidth, 1);
+  s.dp_xdrop = c.dp_xdrop >= 0 ? c.dp_xdrop : c.xdrop;
+  s.clip = c.clip_penalty;
+  s.adaptive = c.adaptive ? 1 : 0;
+  s.max_drift = std::max(c.max_drift, 0);
+  const int64_t g = (int64_t)c.gap_open + c.gap_extend;
+  s.gof = g > INT32_MAX ? INT32_MAX : (int32_t)g;
+  return s;
+}
+
+// Domain of the GPU banded SW (exactness conditions of the F prefix scan and of
+// the packed row-argmax key).
+int check_sw_cfg(kira_ctx* ctx, const kira_sw_cfg& c, uint32_t max_q, uint32_t max_band) {
+  if (c.gap_open < 0 || c.gap_extend < 0)
+    return fail(ctx, KIRA_ERR_INVALID, "gap_open and gap_extend must be >= 0");
+  if ((int64_t)c.gap_open + c.gap_extend > (1 << 24) || c.gap_extend > (1 << 16))
+    return fail(ctx, KIRA_ERR_INVALID, "gap costs above the supported range");
+  const int64_t step = std::max<int64_t>({(int64_t)c.match_score, -(int64_t)c.mismatch, 0});
+  if ((int64_t)max_q * step >= (1 << 21))
+    return fail(ctx, KIRA_ERR_INVALID, "read_len * max cell gain must be < 2^21");
+  if (std::abs((int64_t)c.match_score) > (1 << 20) || std::abs((int64_t)c.mismatch) > (1 << 20))
+    return fail(ctx, KIRA_ERR_INVALID, "match/mismatch above the supported range");
+  const int need = 2 * (int)std::max<uint32_t>(max_band, 1) + 1;
+  if (need > kBswShapes[kNumBswShapes - 1].g * kBswShapes[kNumBswShapes - 1].k)
+    return fail(ctx, KIRA_ERR_INVALID, "bandwidth %u above the supported maximum", max_band);
+  return KIRA_OK;
+}
+
+int pick_shape(uint32_t max_band) {
+  const int need = 2 * (int)std::max<uint32_t>(max_band, 1) + 1;
+  for (int s = 0; s < kNumBswShapes; ++s)
+    if (kBswShapes[s].g * kBswShapes[s].k >= need) return s;
+  return -1;
+}
+
+struct Maxes {
+  uint32_t q = 0, w = 0, band = 0;
+};
+
+Maxes host_maxes(const kira_pairs& P, int32_t cfg_band) {
+  Maxes m;
+  for (uint32_t i = 0; i < P.n; ++i) {
+    m.q = std::max(m.q, P.read_len[i]);
+    m.w = std::max(m.w, P.win_len[i]);
+    const int32_t b = P.bandwidth ? P.bandwidth[i] : cfg_band;
+    m.band = std::max(m.band, (uint32_t)std::max(b, 1));
+  }
+  return m;
+}
+
+// Copies the host batch into the ctx arena and returns its device view.
+int upload_pairs(kira_ctx* ctx, const kira_pairs& P, DevPairs& D) {
+  cudaError_t cerr = cudaSuccess;
+  cudaStream_t st = ctx->stream;
+  const uint32_t n = P.n;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (P.read_off[i] + P.read_len[i] > P.read_seq_bytes)
+      return fail(ctx, KIRA_ERR_INVALID, "pair %u: read outside read_seq", i);
+    const uint64_t wlim = P.win_seq ? P.win_seq_bytes : ctx->ref_len;
+    if (P.win_off[i] + P.win_len[i] > wlim)
+      return fail(ctx, KIRA_ERR_INVALID, "pair %u: window outside %s", i,
+                  P.win_seq ? "win_seq" : "the resident reference");
+  }
+  KIRA_DBUF(rs, uint8_t, B_READ_SEQ, P.read_seq_bytes);
+  KIRA_CUDA(cudaMemcpyAsync(rs, P.read_seq, P.read_seq_bytes, cudaMemcpyHostToDevice, st));
+  const uint8_t* ws = ctx->ref_dev;
+  if (P.win_seq) {
+    KIRA_DBUF(w, uint8_t, B_WIN_SEQ, P.win_seq_bytes);
+    KIRA_CUDA(cudaMemcpyAsync(w, P.win_seq, P.win_seq_bytes, cudaMemcpyHostToDevice, st));
+    ws = w;
+  }
+  KIRA_DBUF(ro, uint64_t, B_READ_OFF, n);
+  KIRA_DBUF(rl, uint32_t, B_READ_LEN, n);
+  KIRA_DBUF(wo, uint64_t, B_WIN_OFF, n);
+  KIRA_DBUF(wl, uint32_t, B_WIN_LEN, n);
+  KIRA_CUDA(cudaMemcpyAsync(ro, P.read_off, 8ull * n, cudaMemcpyHostToDevice, st));
+  KIRA_CUDA(cudaMemcpyAsync(rl, P.read_len, 4ull * n, cudaMemcpyHostToDevice, st));
+  KIRA_CUDA(cudaMemcpyAsync(wo, P.win_off, 8ull * n, cudaMemcpyHostToDevice, st));
+  KIRA_CUDA(cudaMemcpyAsync(wl, P.win_len, 4ull * n, cudaMemcpyHostToDevice, st));
+  D = DevPairs{n, rs, ro, rl, ws, wo, wl, nullptr, nullptr, nullptr};
+  if (P.band_offset) {
+    KIRA_DBUF(b, int32_t, B_BAND_OFF, n);
+    KIRA_CUDA(cudaMemcpyAsync(b, P.band_offset, 4ull * n, cudaMemcpyHostToDevice, st));
+    D.band_offset = b;
+  }
+  if (P.abort_score) {
+    KIRA_DBUF(b, int32_t, B_ABORT, n);
+    KIRA_CUDA(cudaMemcpyAsync(b, P.abort_score, 4ull * n, cudaMemcpyHostToDevice, st));
+    D.abort_score = b;
+  }
+  if (P.bandwidth) {
+    KIRA_DBUF(b, int32_t, B_BANDW, n);
+    KIRA_CUDA(cudaMemcpyAsync(b, P.bandwidth, 4ull * n, cudaMemcpyHostToDevice, st));
+    D.bandwidth = b;
+  }
+  return KIRA_OK;
+}
+
+// Scratch of the banded SW stage for up to `items` items.
+int prepare_bsw(kira_ctx* ctx, uint32_t n_pairs, uint32_t items, const Maxes& mx, int shape,
+                BswLaunch& B) {
+  cudaError_t cerr = cudaSuccess;
+  const BswShapeInfo sh = kBswShapes[shape];
+  const uint32_t lane_bytes = (uint32_t)(sh.k + 1) / 2;
+  const uint32_t row_stride = (uint32_t)sh.g * lane_bytes;
+  const uint64_t slot = (((uint64_t)(mx.q + 1) * row_stride) + 15) & ~15ull;
+  const uint32_t meta_stride = mx.q + 1;
+  const uint32_t slot_cap = mx.q + mx.w + 2;
+  KIRA_DBUF(trace, uint8_t, B_TRACE, slot * std::max<uint32_t>(items, 1));
+  KIRA_DBUF(meta, uint32_t, B_META, (uint64_t)meta_stride * std::max<uint32_t>(items, 1));
+  KIRA_DBUF(ends, DpEnd, B_ENDS, std::max<uint32_t>(items, 1));
+  KIRA_DBUF(slots, uint32_t, B_CIG_SLOTS, (uint64_t)slot_cap * std::max<uint32_t>(items, 1));
+  KIRA_DBUF(iop, uint32_t, B_ITEM_OF_PAIR, std::max<uint32_t>(n_pairs, 1));
+  B.tg = TraceGeom{trace, meta, slot, row_stride, lane_bytes, (uint32_t)sh.k, meta_stride};
+  B.ends = ends;
+  B.cig_slots = slots;
+  B.slot_cap = slot_cap;
+  B.item_of_pair = iop;
+  B.max_q = mx.q;
+  return KIRA_OK;
+}
+
+// CIGAR scan + compaction over all pairs; writes the total op count to total_dev.
+int finish_cigars(kira_ctx* ctx, uint32_t n, kira_sw_result* out, const uint32_t* ncig,
+                  const BswLaunch& B, uint32_t* ops, uint64_t cap, uint64_t* total_dev,
+                  cudaStream_t st) {
+  cudaError_t cerr = cudaSuccess;
+  KIRA_DBUF(off, uint32_t, B_CIG_OFF, std::max<uint32_t>(n, 1));
+  KIRA_DBUF(sums, uint32_t, B_CHUNK_SUMS, n / 4096 + 2);
+  KIRA_CUDA(launch_cigar_scan(ncig, n, off, sums, total_dev, st));
+  CompactLaunch C{n, out, ncig, off, B.item_of_pair, B.cig_slots, B.slot_cap, ops, cap};
+  KIRA_CUDA(launch_cigar_compact(C, ctx->sms, st));
+  return KIRA_OK;
+}
+
+void mark(kira_ctx* ctx, int i, cudaStream_t st) {
+  if (!ctx->profile) return;
+  cudaEventRecord(ctx->ev[i], st);
+  ctx->ev_recorded = i + 1;
+}
+
+// The composed path on device buffers, enqueued on `st`.
+int verify_pipeline(kira_ctx* ctx, const DevPairs& D, const Maxes& mx, const kira_verify_params& p,
+                    kira_sw_result* out, uint32_t* ops, uint64_t cap, uint64_t* total_dev,
+                    kira_verify_detail* detail, unsigned long long* cells_dev, cudaStream_t st) {
+  cudaError_t cerr = cudaSuccess;
+  const uint32_t n = D.n;
+  if (n == 0) return KIRA_OK;
+  int rc = check_sw_cfg(ctx, p.sw, mx.q, mx.band);
+  if (rc) return rc;
+  if (mx.q > 512) return fail(ctx, KIRA_ERR_READ_TOO_LONG, "read of %u bases > 512", mx.q);
+  const int shape = pick_shape(mx.band);
+  KIRA_DBUF(ncig, uint32_t, B_NCIG, n);
+  KIRA_DBUF(swoff, int32_t, B_SW_OFFSET, n);
+  KIRA_DBUF(mlist, uint32_t, B_MYERS_LIST, n);
+  KIRA_DBUF(slist, uint32_t, B_SW_LIST, n);
+  KIRA_DBUF(counters, uint32_t, B_COUNTERS, 4);
+  KIRA_CUDA(cudaMemsetAsync(counters, 0, 16, st));
+  const SwParams sp = resolve(p.sw);
+  VerifyDev V{p.sieve_threshold, p.cert_strict, sp, out, detail, ncig, swoff, mlist, counters};
+  ctx->ev_recorded = 0;
+  mark(ctx, 0, st);
+  KIRA_CUDA(launch_verify_sieve(D, V, ctx->sms, st));
+  mark(ctx, 1, st);
+  MyersLaunch M{};
+  M.list = mlist;
+  M.count_dev = counters + 0;
+  M.k = p.myers_k;
+  M.per_pair_k = 1;
+  M.tw = std::max<uint32_t>((mx.w + 31) / 32, 1);
+  M.cascade = 1;
+  M.out = out;
+  M.detail = detail;
+  M.ncig = ncig;
+  M.sw_list = slist;
+  M.counters = counters;
+  M.flags = counters + 2;
+  KIRA_CUDA(launch_myers(D, M, n, ctx->sms, st));
+  BswLaunch B{};
+  rc = prepare_bsw(ctx, n, n, mx, shape, B);
+  mark(ctx, 2, st);
+  if (rc) return rc;
+  B.list = slist;
+  B.count_dev = counters + 1;
+  B.sp = sp;
+  B.offset = swoff;
+  B.cells = cells_dev;
+  B.out = out;
+  B.ncig = ncig;
+  B.flags = counters + 2;
+  KIRA_CUDA(launch_bsw(shape, D, B, n, ctx->sms, st, ctx->profile ? ctx->ev[3] : nullptr));
+  if (ctx->profile) ctx->ev_recorded = 4;
+  mark(ctx, 4, st);
+  rc = finish_cigars(ctx, n, out, ncig, B, ops, cap, total_dev, st);
+  mark(ctx, 5, st);
+  return rc;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int kira_gpu_is_available(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n > 0 ? 1 : 0;
+}
+
+int kira_gpu_init(int device, kira_ctx** out) {
+  if (!out) return KIRA_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return KIRA_ERR_NO_DEVICE;
+  if (device < 0 || device >= n) return KIRA_ERR_NO_DEVICE;
+  if (cudaSetDevice(device) != cudaSuccess) return KIRA_ERR_DRIVER;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return KIRA_ERR_DRIVER;
+  if (prop.major < 10) return KIRA_ERR_NO_DEVICE;  // sm_100a binary only
+  kira_ctx* ctx = new kira_ctx();
+  ctx->device = device;
+  ctx->sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return KIRA_ERR_DRIVER;
+  }
+  *out = ctx;
+  return KIRA_OK;
+}
+
+void kira_gpu_destroy(kira_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& b : ctx->bufs)
+    if (b.p) cudaFree(b.p);
+  for (auto& e : ctx->ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->ref_dev) cudaFree(ctx->ref_dev);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int kira_gpu_last_error(const kira_ctx* ctx, char* buf, size_t len) {
+  const std::string& s = ctx ? ctx->last_error : std::string();
+  if (buf && len) {
+    const size_t k = std::min(len - 1, s.size());
+    std::memcpy(buf, s.data(), k);
+    buf[k] = 0;
+  }
+  return (int)s.size();
+}
+
+uint64_t kira_gpu_arena_bytes(const kira_ctx* ctx) {
+  uint64_t t = 0;
+  if (!ctx) return 0;
+  for (const auto& b : ctx->bufs) t += b.bytes;
+  return t + ctx->ref_len;
+}
+
+int kira_gpu_sieve_batch(kira_ctx* ctx, const kira_sieve_job* jobs, uint32_t n,
+                         kira_sieve_result* out) {
+  if (!ctx) return KIRA_ERR_INVALID;
+  if (n == 0) return KIRA_OK;
+  if (!jobs || !out) return fail(ctx, KIRA_ERR_INVALID, "null jobs/out");
+  cudaSetDevice(ctx->device);
+  // backend.rs:101-116: per-job validation before any device work.
+  uint64_t rbytes = 0, wbytes = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const kira_sieve_job& j = jobs[i];
+    if (j.read_bytes > KIRA_READ_BYTES_MAX)
+      return fail(ctx, KIRA_ERR_READ_TOO_LONG,
+                  "read too long for the CUDA backend (%u > %d bytes packed)", j.read_bytes,
+                  KIRA_READ_BYTES_MAX);
+    if ((uint64_t)j.read_bytes * 4 < j.read_nucs || (uint64_t)j.ref_bytes * 4 < j.ref_nucs)
+      return fail(ctx, KIRA_ERR_INVALID, "job %u: packed buffer shorter than its length", i);
+    if (j.ref_nucs >= (1u << 20) + j.read_nucs)
+      return fail(ctx, KIRA_ERR_INVALID, "job %u: window longer than 2^20 shifts", i);
+    rbytes += j.read_bytes;
+    wbytes += j.ref_bytes;
+  }
+  std::vector<uint8_t> hr(rbytes + 1), hw(wbytes + 1);
+  std::vector<uint64_t> ro(n), wo(n);
+  std::vector<uint32_t> rn(n), wn(n), mm(n);
+  uint64_t a = 0, b = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const kira_sieve_job& j = jobs[i];
+    if (j.read_bytes) std::memcpy(hr.data() + a, j.read_packed, j.read_bytes);
+    if (j.ref_bytes) std::memcpy(hw.data() + b, j.ref_packed, j.ref_bytes);
+    ro[i] = a;
+    wo[i] = b;
+    a += j.read_bytes;
+    b += j.ref_bytes;
+    rn[i] = j.read_nucs;
+    wn[i] = j.ref_nucs;
+    mm[i] = j.max_mismatches;
+  }
+  cudaError_t cerr = cudaSuccess;
+  cudaStream_t st = ctx->stream;
+  KIRA_DBUF(drs, uint8_t, B_READ_SEQ, rbytes + 1);
+  KIRA_DBUF(dws, uint8_t, B_WIN_SEQ, wbytes + 1);
+  KIRA_DBUF(dro, uint64_t, B_READ_OFF, n);
+  KIRA_DBUF(dwo, uint64_t, B_WIN_OFF, n);
+  KIRA_DBUF(drn, uint32_t, B_READ_LEN, n);
+  KIRA_DBUF(dwn, uint32_t, B_WIN_LEN, n);
+  KIRA_DBUF(dmm, uint32_t, B_BAND_OFF, n);
+  KIRA_DBUF(dout, kira_sieve_result, B_SIEVE_OUT, n);
+  KIRA_CUDA(cudaMemcpyAsync(drs, hr.data(), rbytes + 1, cudaMemcpyHostToDevice, st));
+  KIRA_CUDA(cudaMemcpyAsync(dws, hw.data(), wbytes + 1, cudaMemcpyHostToDevice, st));
+  KIRA_CUDA(cudaMemcpyAsync(dro, ro.data(), 8ull * n, cudaMemcpyHostToDevice, st));
+  KIRA_CUDA(cudaMemcpyAsync(dwo, wo.data(), 8ull * n, cudaMemcpyHostToDevice, st));
+  KIRA_CUDA(cudaMemcpyAsync(drn, rn.data(), 4ull * n, cudaMemcpyHostToDevice, st));
+  KIRA_CUDA(cudaMemcpyAsync(dwn, wn.data(), 4ull * n, cudaMemcpyHostToDevice, st));
+  KIRA_CUDA(cudaMemcpyAsync(dmm, mm.data(), 4ull * n, cudaMemcpyHostToDevice, st));
+  SieveJobsDev J{n, drs, dro, drn, dws, dwo, dwn, dmm};
+  KIRA_CUDA(launch_sieve_dropin(J, dout, ctx->sms, st));
+  KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_sieve_result) * n, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaStreamSynchronize(st));
+  return KIRA_OK;
+}
+
+int kira_gpu_profile(kira_ctx* ctx, int enable) {
+  if (!ctx) return KIRA_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (enable && !ctx->ev[0])
+    for (auto& e : ctx->ev) KIRA_CUDA(cudaEventCreate(&e));
+  ctx->profile = enable != 0;
+  ctx->ev_recorded = 0;
+  return KIRA_OK;
+}
+
+int kira_gpu_stage_times(kira_ctx* ctx, float* ms, int max_stages) {
+  if (!ctx || !ms) return -KIRA_ERR_INVALID;
+  if (!ctx->profile || ctx->ev_recorded < 2) return 0;
+  const int n = std::min(ctx->ev_recorded - 1, max_stages);
+  for (int i = 0; i < n; ++i) {
+    if (cudaEventSynchronize(ctx->ev[i + 1]) != cudaSuccess) return -KIRA_ERR_RUNTIME;
+    if (cudaEventElapsedTime(ms + i, ctx->ev[i], ctx->ev[i + 1]) != cudaSuccess) ms[i] = -1.0f;
+  }
+  return n;
+}
+
+int kira_gpu_ref_upload(kira_ctx* ctx, const uint8_t* seq, uint64_t len) {
+  if (!ctx) return KIRA_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->ref_dev) cudaFree(ctx->ref_dev);
+  ctx->ref_dev = nullptr;
+  ctx->ref_len = 0;
+  if (len == 0) return KIRA_OK;
+  KIRA_CUDA(cudaMalloc(&ctx->ref_dev, len + 16));
+  KIRA_CUDA(cudaMemcpy(ctx->ref_dev, seq, len, cudaMemcpyHostToDevice));
+  ctx->ref_len = len;
+  return KIRA_OK;
+}
+
+int kira_gpu_myers_batch(kira_ctx* ctx, const kira_pairs* pairs, uint32_t max_k, int32_t* dist,
+                         int32_t* end_pos) {
+  if (!ctx || !pairs) return KIRA_ERR_INVALID;
+  const kira_pairs& P = *pairs;
+  if (P.n == 0) return KIRA_OK;
+  cudaSetDevice(ctx->device);
+  const Maxes mx = host_maxes(P, 1);
+  if (mx.q > 512) return fail(ctx, KIRA_ERR_INVALID, "pattern of %u bases > 512", mx.q);
+  DevPairs D;
+  int rc = upload_pairs(ctx, P, D);
+  if (rc) return rc;
+  cudaError_t cerr = cudaSuccess;
+  KIRA_DBUF(dd, int32_t, B_DIST, P.n);
+  KIRA_DBUF(de, int32_t, B_END, P.n);
+  KIRA_DBUF(counters, uint32_t, B_COUNTERS, 4);
+  KIRA_CUDA(cudaMemsetAsync(counters, 0, 16, ctx->stream));
+  MyersLaunch M{};
+  M.flags = counters + 2;
+  M.count = P.n;
+  M.k = (int32_t)max_k;
+  M.per_pair_k = 0;
+  M.tw = std::max<uint32_t>((mx.w + 31) / 32, 1);
+  M.dist = dd;
+  M.end = de;
+  cudaStream_t st = ctx->stream;
+  KIRA_CUDA(launch_myers(D, M, P.n, ctx->sms, st));
+  KIRA_CUDA(cudaMemcpyAsync(dist, dd, 4ull * P.n, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(end_pos, de, 4ull * P.n, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaStreamSynchronize(st));
+  return KIRA_OK;
+}
+
+int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg* cfg,
+                       kira_sw_result* out, kira_cigar_buf* cigar, uint64_t* cells) {
+  if (!ctx || !pairs || !cfg || !out || !cigar) return KIRA_ERR_INVALID;
+  const kira_pairs& P = *pairs;
+  cigar->used = 0;
+  if (cells) *cells = 0;
+  if (P.n == 0) return KIRA_OK;
+  cudaSetDevice(ctx->device);
+  const Maxes mx = host_maxes(P, cfg->bandwidth);
+  int rc = check_sw_cfg(ctx, *cfg, mx.q, mx.band);
+  if (rc) return rc;
+  DevPairs D;
+  rc = upload_pairs(ctx, P, D);
+  if (rc) return rc;
+  cudaError_t cerr = cudaSuccess;
+  cudaStream_t st = ctx->stream;
+  const uint32_t n = P.n;
+  KIRA_DBUF(dout, kira_sw_result, B_OUT, n);
+  KIRA_DBUF(ncig, uint32_t, B_NCIG, n);
+  KIRA_DBUF(counters, uint32_t, B_COUNTERS, 4);
+  KIRA_DBUF(cells_dev, unsigned long long, B_CELLS, 1);
+  KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
+  KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
+  KIRA_CUDA(cudaMemsetAsync(counters, 0, 16, st));
+  KIRA_CUDA(cudaMemsetAsync(cells_dev, 0, 8, st));
+  const int shape = pick_shape(mx.band);
+  BswLaunch B{};
+  rc = prepare_bsw(ctx, n, n, mx, shape, B);
+  if (rc) return rc;
+  B.count = n;
+  B.sp = resolve(*cfg);
+  B.offset = D.band_offset;
+  B.cells = cells_dev;
+  B.out = dout;
+  B.ncig = ncig;
+  B.flags = counters + 2;
+  KIRA_CUDA(launch_bsw(shape, D, B, n, ctx->sms, st));
+  rc = finish_cigars(ctx, n, dout, ncig, B, ops, cigar->cap, total_dev, st);
+  if (rc) return rc;
+  uint64_t total = 0;
+  unsigned long long hcells = 0;
+  uint32_t flags[4];
+  KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_sw_result) * n, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(&total, total_dev, 8, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(&hcells, cells_dev, 8, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(flags, counters, 16, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaStreamSynchronize(st));
+  cigar->used = total;
+  if (cells) *cells = hcells;
+  if (flags[2] & 1u) return fail(ctx, KIRA_ERR_RUNTIME, "CIGAR slot overflow");
+  if (flags[2] & 6u) return fail(ctx, KIRA_ERR_INVALID, "a pair exceeded the launch's length bounds");
+  if (total > cigar->cap)
+    return fail(ctx, KIRA_ERR_CAPACITY, "CIGAR buffer holds %llu ops, %llu needed",
+                (unsigned long long)cigar->cap, (unsigned long long)total);
+  if (total) {
+    KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * total, cudaMemcpyDeviceToHost, st));
+    KIRA_CUDA(cudaStreamSynchronize(st));
+  }
+  return KIRA_OK;
+}
+
+int kira_gpu_verify_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_verify_params* p,
+                          kira_sw_result* out, kira_cigar_buf* cigar, kira_verify_detail* detail,
+                          uint64_t* cells) {
+  if (!ctx || !pairs || !p || !out || !cigar) return KIRA_ERR_INVALID;
+  const kira_pairs& P = *pairs;
+  cigar->used = 0;
+  if (cells) *cells = 0;
+  if (P.n == 0) return KIRA_OK;
+  cudaSetDevice(ctx->device);
+  const Maxes mx = host_maxes(P, p->sw.bandwidth);
+  DevPairs D;
+  int rc = upload_pairs(ctx, P, D);
+  if (rc) return rc;
+  cudaError_t cerr = cudaSuccess;
+  cudaStream_t st = ctx->stream;
+  const uint32_t n = P.n;
+  KIRA_DBUF(dout, kira_sw_result, B_OUT, n);
+  kira_verify_detail* ddet = nullptr;
+  if (detail) {
+    KIRA_DBUF(dd, kira_verify_detail, B_DETAIL, n);
+    ddet = dd;
+  }
+  KIRA_DBUF(cells_dev, unsigned long long, B_CELLS, 1);
+  KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
+  KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
+  KIRA_CUDA(cudaMemsetAsync(cells_dev, 0, 8, st));
+  rc = verify_pipeline(ctx, D, mx, *p, dout, ops, cigar->cap, total_dev, ddet, cells_dev, st);
+  if (rc) return rc;
+  uint64_t total = 0;
+  unsigned long long hcells = 0;
+  uint32_t flags[4];
+  KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_sw_result) * n, cudaMemcpyDeviceToHost, st));
+  if (detail)
+    KIRA_CUDA(cudaMemcpyAsync(detail, ddet, sizeof(kira_verify_detail) * n,
+                              cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(&total, total_dev, 8, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(&hcells, cells_dev, 8, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(flags, ctx->bufs[B_COUNTERS].p, 16, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaStreamSynchronize(st));
+  cigar->used = total;
+  if (cells) *cells = hcells;
+  if (flags[2] & 1u) return fail(ctx, KIRA_ERR_RUNTIME, "CIGAR slot overflow");
+  if (flags[2] & 6u) return fail(ctx, KIRA_ERR_INVALID, "a pair exceeded the launch's length bounds");
+  if (total > cigar->cap)
+    return fail(ctx, KIRA_ERR_CAPACITY, "CIGAR buffer holds %llu ops, %llu needed",
+                (unsigned long long)cigar->cap, (unsigned long long)total);
+  if (total) {
+    KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * total, cudaMemcpyDeviceToHost, st));
+    KIRA_CUDA(cudaStreamSynchronize(st));
+  }
+  return KIRA_OK;
+}
+
+int kira_gpu_verify_dev(kira_ctx* ctx, const kira_pairs* pairs, const kira_verify_params* p,
+                        kira_sw_result* out, uint32_t* cigar_ops, uint64_t cigar_cap,
+                        uint64_t* cigar_used_dev, kira_verify_detail* detail,
+                        unsigned long long* cells_dev, void* stream) {
+  if (!ctx || !pairs || !p || !out || !cigar_used_dev) return KIRA_ERR_INVALID;
+  const kira_pairs& P = *pairs;
+  if (P.n == 0) return KIRA_OK;
+  if (!P.max_read_len || !P.max_win_len)
+    return fail(ctx, KIRA_ERR_INVALID, "device batches need max_read_len and max_win_len");
+  cudaSetDevice(ctx->device);
+  Maxes mx;
+  mx.q = P.max_read_len;
+  mx.w = P.max_win_len;
+  mx.band = P.bandwidth ? P.max_bandwidth : (uint32_t)std::max(p->sw.bandwidth, 1);
+  if (!mx.band) return fail(ctx, KIRA_ERR_INVALID, "per-pair bandwidth needs max_bandwidth");
+  DevPairs D{P.n, P.read_seq, P.read_off, P.read_len,
+             P.win_seq ? P.win_seq : ctx->ref_dev, P.win_off, P.win_len,
+             P.band_offset, P.abort_score, P.bandwidth};
+  return verify_pipeline(ctx, D, mx, *p, out, cigar_ops, cigar_cap, cigar_used_dev, detail,
+                         cells_dev, (cudaStream_t)stream);
+}
+
+}  // extern "C"

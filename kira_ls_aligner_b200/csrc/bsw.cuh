@@ -1,0 +1,274 @@
+// bsw.cuh -- banded affine Smith-Waterman with adaptive band, x-drop, abort,
+// clip-penalty end preference and 4-bit traceback (src/alignment/mod.rs:1370-1650).
+//
+// B200 mapping
+//   A group of G lanes (G | 32) owns one pair and sweeps its rows in order; lane
+//   g holds K consecutive cells idx = g*K .. g*K+K-1 of the row (G*K >= 2*band+1).
+//   Row i+1's band depends on row i's argmax, so rows stay sequential (exactly as
+//   the reference) and the parallelism is across the band and across pairs.
+//   Per row:
+//     1. H_diag / E from the previous row, read from a shared-memory row buffer at
+//        the band shift d = j_start(i) - j_start(i-1) (any d, so the adaptive
+//        re-centring costs nothing extra);
+//     2. F exactly, without the serial left-to-right chain: with go >= 0,
+//          F[idx] = max_{k<idx} (Hstar[k] - gof - (idx-1-k)*ge),  Hstar = max(Hdiag+s, E, 0)
+//        i.e. an exclusive prefix max of Hstar[k] - gof + k*ge, done in-lane over K
+//        cells and across lanes with log2(G) __shfl_up_sync steps;
+//     3. H, the direction with the reference priority diag >= E >= F, and the E/F
+//        extend flags (F flag from the left neighbour's final H and F);
+//     4. row max and FIRST argmax with one packed key (h << 10 | 1023 - idx)
+//        reduced by __shfl_xor_sync; best / x-drop / abort / adaptive centre are
+//        then warp-uniform scalar updates.
+//   The 4-bit trace (dir | E-ext << 2 | F-ext << 3, the reference's u8 trace code)
+//   is written to a per-item slot of an HBM trace arena, two cells per byte, and
+//   a separate kernel walks it with one thread per pair (thousands of
+//   independent walks hide the dependent-load latency).
+#pragma once
+
+#include "common.cuh"
+
+namespace kira {
+
+template <int G, int K>
+struct BswShape {
+  static constexpr int kCap = G * K;             // cells per row
+  static constexpr int kLaneBytes = (K + 1) / 2;  // trace bytes per lane per row
+  static constexpr int kRowStride = G * kLaneBytes;
+};
+
+// Shared memory per group: two H rows and two E rows of kCap ints.
+template <int G, int K>
+__device__ __forceinline__ void bsw_group_sweep(
+    const uint8_t* __restrict__ rd, uint32_t q, const uint8_t* __restrict__ wn, uint32_t w,
+    int32_t band, int32_t offset, int32_t abort_score, const SwParams& sp, int32_t* rowbuf,
+    uint8_t* __restrict__ trace, uint32_t* __restrict__ meta, uint32_t g, uint32_t gmask,
+    DpEnd& out, uint64_t& cells_out) {
+  constexpr int CAP = BswShape<G, K>::kCap;
+  constexpr int LB = BswShape<G, K>::kLaneBytes;
+  constexpr int S = BswShape<G, K>::kRowStride;
+  constexpr int32_t NEGBIG = INT32_MIN / 2;
+  int32_t* rowH[2] = {rowbuf, rowbuf + CAP};
+  int32_t* rowE[2] = {rowbuf + 2 * CAP, rowbuf + 3 * CAP};
+
+  int32_t prev_start = 1, prev_len = 0;
+  int cur = 0;
+  int32_t best = 0, bi = 0, bj = 0, bq = 0, bqj = 0;
+  uint32_t early = 0;
+  uint64_t cells = 0;
+  const int32_t drift = sp.adaptive ? sp.max_drift : 0;
+  int32_t acenter = 1 + offset;
+  const int32_t match = sp.match, mism = sp.mismatch, gof = sp.gof, ge = sp.gap_extend;
+  const int32_t wl = (int32_t)w;
+
+  for (uint32_t iu = 1; iu <= q; ++iu) {
+    const int32_t i = (int32_t)iu;
+    const int32_t sc = i + offset;
+    const int32_t center = sp.adaptive ? min(max(acenter, sc - drift), sc + drift) : sc;
+    const int32_t js = max(center - band, 1);
+    const int32_t je = min(center + band, wl);
+    if (js > je) {  // mod.rs:1437-1444: row skipped, no centre / x-drop update
+      if (g == 0) meta[i] = (1u << 11);
+      prev_len = 0;
+      prev_start = 1;
+      continue;
+    }
+    const int32_t row_len = je - js + 1;
+    cells += (uint64_t)row_len;
+    const uint32_t qb = ldb(rd, (uint64_t)(i - 1));
+    const int32_t d = js - prev_start;
+    const int32_t* pH = rowH[cur ^ 1];
+    const int32_t* pE = rowE[cur ^ 1];
+
+    int32_t hm[K], e[K], gv[K];
+    uint32_t eext = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int32_t idx = (int32_t)g * K + k;
+      const bool act = idx < row_len;
+      const int32_t j = js + idx;
+      const uint32_t rb = act ? ldb(wn, (uint64_t)(j - 1)) : 0x100u;
+      const int32_t s = (qb == rb) ? match : -mism;
+      const int32_t pd = idx + d - 1;
+      const int32_t hdiag = (pd >= 0 && pd < prev_len) ? pH[pd] : 0;
+      hm[k] = hdiag + s;
+      const int32_t pu = pd + 1;
+      const bool up = pu >= 0 && pu < prev_len;
+      const int32_t efh = up ? pH[pu] - gof : kNeg4;
+      const int32_t efe = up ? pE[pu] - ge : kNeg4;
+      e[k] = max(efh, efe);
+      eext |= (efe > efh ? 1u : 0u) << k;
+      const int32_t hs = max(max(hm[k], e[k]), 0);
+      gv[k] = act ? hs - gof + idx * ge : NEGBIG;
+    }
+    // Exclusive prefix max of gv over the row.
+    int32_t inc[K];
+    inc[0] = gv[0];
+#pragma unroll
+    for (int k = 1; k < K; ++k) inc[k] = max(inc[k - 1], gv[k]);
+    int32_t v = inc[K - 1];
+#pragma unroll
+    for (int off = 1; off < G; off <<= 1) {
+      const int32_t t = __shfl_up_sync(gmask, v, off, G);
+      if ((int)g >= off) v = max(v, t);
+    }
+    int32_t excl_lane = __shfl_up_sync(gmask, v, 1, G);
+    if (g == 0) excl_lane = NEGBIG;
+    int32_t f[K], h[K];
+    uint32_t dir[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int32_t idx = (int32_t)g * K + k;
+      const int32_t ek = k ? max(excl_lane, inc[k - 1]) : excl_lane;
+      f[k] = idx >= 1 ? ek - (idx - 1) * ge : kNeg4;
+      // mod.rs:1504-1516 priority diag >= E >= F.
+      if (hm[k] >= e[k] && hm[k] >= f[k] && hm[k] > 0) {
+        h[k] = hm[k];
+        dir[k] = 1;
+      } else if (e[k] >= f[k] && e[k] > 0) {
+        h[k] = e[k];
+        dir[k] = 2;
+      } else if (f[k] > 0) {
+        h[k] = f[k];
+        dir[k] = 3;
+      } else {
+        h[k] = 0;
+        dir[k] = 0;
+      }
+    }
+    // Left neighbour of cell k = 0 lives in lane g-1.
+    const int32_t left_h = __shfl_up_sync(gmask, h[K - 1], 1, G);
+    const int32_t left_f = __shfl_up_sync(gmask, f[K - 1], 1, G);
+    uint32_t key = 0;
+    uint32_t nib[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int32_t idx = (int32_t)g * K + k;
+      const bool act = idx < row_len;
+      const int32_t ph = k ? h[k - 1] : left_h;
+      const int32_t pf = k ? f[k - 1] : left_f;
+      const bool fext = idx >= 1 && (pf - ge) > (ph - gof);
+      nib[k] = act ? (dir[k] | (((eext >> k) & 1u) << 2) | (fext ? 8u : 0u)) : 0u;
+      if (act) {
+        const uint32_t kk = ((uint32_t)h[k] << kKeyIdxBits) | (uint32_t)(1023 - idx);
+        key = max(key, kk);
+        rowH[cur][idx] = h[k];
+        rowE[cur][idx] = e[k];
+      }
+    }
+    uint8_t* trow = trace + (size_t)i * S + (size_t)g * LB;
+#pragma unroll
+    for (int b = 0; b < LB; ++b) {
+      const uint32_t lo = nib[2 * b];
+      const uint32_t hi = (2 * b + 1 < K) ? nib[(2 * b + 1) < K ? 2 * b + 1 : 0] : 0u;
+      trow[b] = (uint8_t)(lo | (hi << 4));
+    }
+    if (g == 0) meta[i] = ((uint32_t)js << 11) | (uint32_t)row_len;
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) key = max(key, __shfl_xor_sync(gmask, key, off, G));
+    __syncwarp(gmask);
+    const int32_t row_best = (int32_t)(key >> kKeyIdxBits);
+    const int32_t row_best_j = row_best > 0 ? js + (1023 - (int32_t)(key & 1023u)) : -1;
+    if (row_best > best) {
+      best = row_best;
+      bi = i;
+      bj = row_best_j;
+    }
+    if (iu == q && row_best > bq) {
+      bq = row_best;
+      bqj = row_best_j;
+    }
+    prev_start = js;
+    prev_len = row_len;
+    cur ^= 1;
+    if (sp.adaptive) {  // mod.rs:1546-1559
+      const int32_t raw = row_best_j >= 0 ? row_best_j + 1 : acenter + 1;
+      const int32_t sn = i + 1 + offset;
+      acenter = min(max(raw, sn - drift), sn + drift);
+    }
+    if (sp.dp_xdrop > 0 && best - row_best > sp.dp_xdrop) {  // mod.rs:1561-1564
+      early = 1;
+      break;
+    }
+    if (abort_score > kAbortOff) {  // mod.rs:1565-1572
+      const int32_t remaining = (int32_t)(q - iu);
+      if (best + remaining * match < abort_score) {
+        early = 1;
+        break;
+      }
+    }
+  }
+  // Clip-penalty end preference (mod.rs:1575-1579).
+  if (bq > 0 && sat_add(bq, sp.clip) > best) {
+    best = bq;
+    bi = (int32_t)q;
+    bj = bqj;
+  }
+  out.score = best;
+  out.end_i = bi;
+  out.end_j = bj;
+  out.early_abort = early;
+  cells_out = cells;
+}
+
+// One thread per item: the traceback state machine of mod.rs:1581-1627 over the
+// item's trace slot; CIGAR runs are written in reverse order into the item's
+// CIGAR slot (the compaction kernel reverses them).
+__device__ __forceinline__ uint32_t bsw_walk(const uint8_t* __restrict__ trace,
+                                             const uint32_t* __restrict__ meta, uint32_t k_cells,
+                                             uint32_t lane_bytes, uint32_t row_stride, int32_t& i,
+                                             int32_t& j, uint32_t* __restrict__ ops,
+                                             uint32_t cap, uint32_t& overflow) {
+  int state = 0;  // 0 H, 1 E, 2 F
+  uint32_t n = 0, cur_op = 0xFFu, cur_len = 0;
+  auto push = [&](uint32_t op) {
+    if (op == cur_op) {
+      ++cur_len;
+      return;
+    }
+    if (cur_len) {
+      if (n < cap) ops[n] = (cur_len << 4) | cur_op;
+      else overflow = 1;
+      ++n;
+    }
+    cur_op = op;
+    cur_len = 1;
+  };
+  while (i > 0 && j > 0) {
+    const uint32_t m = __ldg(meta + i);
+    const int32_t rs = (int32_t)(m >> 11), rl = (int32_t)(m & 2047u);
+    const int32_t idx = j - rs;
+    if (idx < 0 || idx >= rl) break;
+    const uint32_t gi = (uint32_t)idx / k_cells, kk = (uint32_t)idx - gi * k_cells;
+    const uint32_t byte = trace[(size_t)i * row_stride + gi * lane_bytes + (kk >> 1)];
+    const uint32_t tr = (byte >> ((kk & 1u) * 4u)) & 15u;
+    if (state == 0) {
+      const uint32_t dd = tr & 3u;
+      if (dd == 0) break;
+      if (dd == 1) {
+        push(0);
+        --i;
+        --j;
+      } else if (dd == 2) {
+        state = 1;
+      } else {
+        state = 2;
+      }
+    } else if (state == 1) {
+      push(1);
+      --i;
+      state = (tr & 4u) ? 1 : 0;
+    } else {
+      push(2);
+      --j;
+      state = (tr & 8u) ? 2 : 0;
+    }
+  }
+  if (cur_len) {
+    if (n < cap) ops[n] = (cur_len << 4) | cur_op;
+    else overflow = 1;
+    ++n;
+  }
+  return n;
+}
+
+}  // namespace kira

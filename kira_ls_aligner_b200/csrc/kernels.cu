@@ -1,0 +1,534 @@
+// kernels.cu -- device kernels of libkira_gpu and their launchers.
+#include <cuda_runtime.h>
+
+#include "bsw.cuh"
+#include "internal.h"
+#include "myers.cuh"
+#include "sieve.cuh"
+
+namespace kira {
+
+// ---------------------------------------------------------------------------
+// Sieve drop-in: CudaBackend::run_batch semantics (src/cuda/backend.rs:95-249,
+// src/cuda/spectral.cu:136-213). Inputs are the packed read and the packed
+// phase-0 window of each job, concatenated in two device arenas.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) sieve_dropin_kernel(SieveJobsDev J,
+                                                           kira_sieve_result* __restrict__ out) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); p < J.n; p += warps) {
+    const uint32_t q = J.read_nucs[p], w = J.ref_nucs[p];
+    const uint8_t* rb = J.read_bits + J.read_off[p];
+    const uint8_t* wb = J.ref_bits + J.ref_off[p];
+    auto rcode = [&](uint32_t pos) { return ((ldb(rb, pos >> 2) >> ((pos & 3u) * 2u)) & 3u) | 4u; };
+    auto wcode = [&](uint32_t pos) { return ((ldb(wb, pos >> 2) >> ((pos & 3u) * 2u)) & 3u) | 4u; };
+    const SieveOut so = sieve_warp<8>(q, w, rcode, wcode, false);
+    if (lane == 0) {
+      kira_sieve_result r;
+      if (q == 0 || w < q) {  // spectral.cu:156-163
+        r.shift = -1;
+        r.mismatches = INT32_MAX;
+        r.second_mismatches = INT32_MAX;
+      } else {
+        const uint32_t limit = min(J.max_mism[p], q);  // backend.rs:185-188
+        const bool acc = so.mism <= limit;
+        r.shift = acc ? (int32_t)so.shift : -1;
+        r.mismatches = acc ? (int32_t)so.mism : INT32_MAX;
+        r.second_mismatches = so.second == kNoKey ? INT32_MAX : (int32_t)so.second;
+      }
+      out[p] = r;
+    }
+  }
+}
+
+// Number of positions i in [0, len) with a[i] != b[i], stopping once above
+// `limit` (bounded_hamming, src/alignment/mod.rs:764-776). Warp-cooperative.
+__device__ __forceinline__ uint32_t warp_bounded_hamming(const uint8_t* a, const uint8_t* b,
+                                                         uint32_t len, uint32_t limit,
+                                                         uint32_t lane) {
+  uint32_t m = 0;
+  for (uint32_t c = 0; c < len; c += 32u) {
+    const uint32_t i = c + lane;
+    const bool ne = i < len && ldb(a, i) != ldb(b, i);
+    m += __popc(__ballot_sync(0xFFFFFFFFu, ne));
+    if (m > limit) break;
+  }
+  return m;
+}
+
+// spectral_hit_is_certified (src/alignment/mod.rs:688-762), warp-cooperative.
+__device__ bool warp_certify(const uint8_t* read, const uint8_t* ref, uint32_t len, uint32_t mism,
+                             uint32_t second, uint32_t max_mism, bool strict, uint32_t lane) {
+  if (mism > max_mism) return false;
+  if (second != kNoKey && second <= mism + 1u) return false;
+  if (mism == 0) return true;
+  if (mism > 2) return false;
+  uint32_t n = 0, pos0 = 0xFFFFFFFFu, pos1 = 0xFFFFFFFFu;
+  for (uint32_t c = 0; c < len; c += 32u) {
+    const uint32_t i = c + lane;
+    const bool ne = i < len && ldb(read, i) != ldb(ref, i);
+    uint32_t b = __ballot_sync(0xFFFFFFFFu, ne);
+    while (b) {
+      const uint32_t at = c + (uint32_t)(__ffs(b) - 1);
+      if (n == 0) pos0 = at;
+      else if (n == 1) pos1 = at;
+      ++n;
+      b &= b - 1u;
+    }
+  }
+  if (n != mism) return false;
+  const uint32_t edge = min(len, 8u);
+  if (pos0 < edge || pos0 + edge >= len) return false;
+  if (n == 2 && (pos1 < edge || pos1 + edge >= len)) return false;
+  if (n == 2 && (pos1 > pos0 ? pos1 - pos0 : 0u) <= 4u) return false;
+  const uint32_t p = pos0;
+  const uint32_t suffix = len > p + 1u ? len - (p + 1u) : 0u;
+  const uint32_t min_suffix = strict ? 4u : 8u;
+  if (suffix >= min_suffix) {
+    if (warp_bounded_hamming(read + p + 1, ref + p, len - p - 1u, 1u, lane) <= 1u) return false;
+    if (warp_bounded_hamming(read + p, ref + p + 1, len - p - 1u, 1u, lane) <= 1u) return false;
+    if (strict && suffix >= 6u) {
+      if (warp_bounded_hamming(read + p + 2, ref + p, len - p - 2u, 1u, lane) <= 1u) return false;
+      if (warp_bounded_hamming(read + p, ref + p + 2, len - p - 2u, 1u, lane) <= 1u) return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ uint32_t sieve_threshold_for(int32_t thr, uint32_t q) {
+  // router::spectral_max_mismatches (src/alignment/router.rs:191-195), defaults 3 % / 2.
+  return thr < 0 ? max((q * 3u) / 100u, 2u) : (uint32_t)thr;
+}
+
+__device__ __forceinline__ uint32_t myers_k_for(int32_t k, uint32_t q) {
+  // router::myers_reject_bound (src/alignment/router.rs:199-203), defaults 15 % + 4.
+  return k < 0 ? (q * 15u) / 100u + 4u : (uint32_t)k;
+}
+
+// Stage 1 of the composed path: sieve + certificate, one warp per pair.
+__global__ void __launch_bounds__(256) verify_sieve_kernel(DevPairs P, VerifyDev V) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); p < P.n; p += warps) {
+    const uint32_t q = P.read_len[p], w = P.win_len[p];
+    const uint8_t* rd = P.read_seq + P.read_off[p];
+    const uint8_t* wn = P.win_seq + P.win_off[p];
+    auto rcode = [&](uint32_t pos) { return base_code(ldb(rd, pos)); };
+    auto wcode = [&](uint32_t pos) { return base_code(ldb(wn, pos)); };
+    const SieveOut so = sieve_warp<16>(q, w, rcode, wcode, true);
+    const uint32_t thr = sieve_threshold_for(V.sieve_threshold, q);
+    bool cert = false;
+    if (so.hit && so.mism <= thr)
+      cert = warp_certify(rd, wn + so.shift, q, so.mism, so.second, thr, V.cert_strict != 0, lane);
+    if (lane == 0) {
+      if (V.detail) {
+        kira_verify_detail dt;
+        dt.sieve_shift = so.hit ? (int32_t)so.shift : -1;
+        dt.sieve_mism = so.hit ? (int32_t)so.mism : INT32_MAX;
+        dt.sieve_second = so.hit && so.second != kNoKey ? (int32_t)so.second : INT32_MAX;
+        dt.myers_dist = -1;
+        dt.myers_end = -1;
+        V.detail[p] = dt;
+      }
+      if (cert) {  // build_certified_spectral_alignment (mod.rs:636-686)
+        kira_sw_result r;
+        r.score = (int32_t)(q - so.mism) * V.sw.match - (int32_t)so.mism * V.sw.mismatch;
+        r.ref_start = so.shift;
+        r.ref_end = so.shift + q;
+        r.read_start = 0;
+        r.read_end = (int32_t)q;
+        r.cigar_off = 0;
+        r.n_cigar = 1;
+        r.status = KIRA_PAIR_CERTIFIED;
+        r.early_abort = 0;
+        r.reserved = 0;
+        V.out[p] = r;
+        V.ncig[p] = 1;
+      } else {
+        V.sw_offset[p] = so.hit ? (int32_t)so.shift : 0;
+        const uint32_t slot = atomicAdd(V.counters + 0, 1u);
+        V.myers_list[slot] = p;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Myers over a work list (one pair per lane; 32 pairs per warp).
+// ---------------------------------------------------------------------------
+template <int L>
+__device__ void myers_warp(const DevPairs& P, const MyersLaunch& M, uint32_t base,
+                           uint32_t count, MyersSmem sm) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t item = base + lane;
+  const bool valid = item < count;
+  const uint32_t pair = valid ? (M.list ? M.list[item] : item) : 0u;
+  MyersPeq<L> peq;
+#pragma unroll
+  for (int k = 0; k < L; ++k) peq.a[k] = peq.c[k] = peq.g[k] = peq.t[k] = 0u;
+  for (uint32_t s = 0; s < 32u; ++s) {
+    const uint32_t pv = __shfl_sync(0xFFFFFFFFu, valid ? 1u : 0u, s);
+    if (!pv) continue;
+    const uint32_t pp = __shfl_sync(0xFFFFFFFFu, pair, s);
+    const uint32_t m = P.read_len[pp], n = P.win_len[pp];
+    myers_load_pattern<L>(P.read_seq + P.read_off[pp], m, s, lane, peq);
+    myers_load_text(P.win_seq + P.win_off[pp], n, s, lane, sm);
+  }
+  __syncwarp();
+  uint32_t dist = 0, endp = 0;
+  bool hit = false;
+  if (valid) {
+    const uint32_t m = P.read_len[pair], n = P.win_len[pair];
+    const uint32_t k = M.per_pair_k ? myers_k_for(M.k, m) : (uint32_t)M.k;
+    hit = myers_lane<L>(peq, m, n, k, sm.planes + (size_t)lane * sm.tw * 3u, dist, endp);
+  }
+  __syncwarp();
+  if (M.cascade) {
+    const uint32_t hits = __ballot_sync(0xFFFFFFFFu, valid && hit);
+    uint32_t base_slot = 0;
+    if (lane == 0 && hits) base_slot = atomicAdd(M.counters + 1, (uint32_t)__popc(hits));
+    base_slot = __shfl_sync(0xFFFFFFFFu, base_slot, 0);
+    if (valid) {
+      if (M.detail) {
+        M.detail[pair].myers_dist = hit ? (int32_t)dist : -1;
+        M.detail[pair].myers_end = hit ? (int32_t)endp : -1;
+      }
+      if (hit) {
+        const uint32_t rank = (uint32_t)__popc(hits & ((1u << lane) - 1u));
+        M.sw_list[base_slot + rank] = pair;
+      } else {
+        kira_sw_result r;
+        r.score = 0;
+        r.ref_start = r.ref_end = 0;
+        r.read_start = r.read_end = 0;
+        r.cigar_off = 0;
+        r.n_cigar = 0;
+        r.status = KIRA_PAIR_MYERS_REJECT;
+        r.early_abort = 0;
+        r.reserved = 0;
+        M.out[pair] = r;
+        M.ncig[pair] = 0;
+      }
+    }
+  } else if (valid) {
+    M.dist[pair] = hit ? (int32_t)dist : -1;
+    M.end[pair] = hit ? (int32_t)endp : -1;
+  }
+}
+
+__global__ void __launch_bounds__(128) myers_kernel(DevPairs P, MyersLaunch M) {
+  extern __shared__ uint32_t myers_smem[];
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp_in_block = threadIdx.x >> 5;
+  MyersSmem sm{myers_smem + (size_t)warp_in_block * 32u * M.tw * 3u, M.tw};
+  const uint32_t count = M.count_dev ? *M.count_dev : M.count;
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp_in_block) * 32u; base < count;
+       base += nwarps * 32u) {
+    const uint32_t item = base + lane;
+    uint32_t m = 0;
+    if (item < count) m = P.read_len[M.list ? M.list[item] : item];
+    uint32_t mx = m;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, off));
+    const uint32_t limbs = max((mx + 31u) / 32u, 1u);
+    switch (limbs) {
+#define KIRA_MYERS_CASE(n) \
+  case n:                  \
+    myers_warp<n>(P, M, base, count, sm); \
+    break;
+      KIRA_MYERS_CASE(1) KIRA_MYERS_CASE(2) KIRA_MYERS_CASE(3) KIRA_MYERS_CASE(4)
+      KIRA_MYERS_CASE(5) KIRA_MYERS_CASE(6) KIRA_MYERS_CASE(7) KIRA_MYERS_CASE(8)
+      KIRA_MYERS_CASE(9) KIRA_MYERS_CASE(10) KIRA_MYERS_CASE(11) KIRA_MYERS_CASE(12)
+      KIRA_MYERS_CASE(13) KIRA_MYERS_CASE(14) KIRA_MYERS_CASE(15) KIRA_MYERS_CASE(16)
+#undef KIRA_MYERS_CASE
+      default: {  // longer patterns: the host rejects them; flag and answer None
+        const uint32_t it = base + lane;
+        if (it < count) {
+          const uint32_t pair = M.list ? M.list[it] : it;
+          if (M.cascade) {
+            kira_sw_result r{};
+            r.status = KIRA_PAIR_MYERS_REJECT;
+            M.out[pair] = r;
+            M.ncig[pair] = 0;
+          } else {
+            M.dist[pair] = -1;
+            M.end[pair] = -1;
+          }
+        }
+        if (lane == 0 && M.flags) atomicOr(M.flags, 4u);
+        break;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Banded SW: DP sweep (group of G lanes per item) and traceback (thread per item)
+// ---------------------------------------------------------------------------
+template <int G, int K>
+__global__ void __launch_bounds__(256) bsw_dp_kernel(DevPairs P, BswLaunch B) {
+  extern __shared__ int32_t bsw_smem[];
+  constexpr int CAP = G * K;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t g = lane % G;
+  const uint32_t gw = lane / G;
+  const uint32_t gmask = (G == 32) ? 0xFFFFFFFFu : (((1u << G) - 1u) << (gw * G));
+  const uint32_t groups_per_block = blockDim.x / G;
+  const uint32_t group_in_block = threadIdx.x / G;
+  int32_t* rowbuf = bsw_smem + (size_t)group_in_block * 4u * CAP;
+  const uint32_t count = B.count_dev ? *B.count_dev : B.count;
+  const uint32_t ngroups = gridDim.x * groups_per_block;
+  for (uint32_t item = blockIdx.x * groups_per_block + group_in_block; item < count;
+       item += ngroups) {
+    const uint32_t pair = B.list ? B.list[item] : item;
+    const uint32_t q = P.read_len[pair], w = P.win_len[pair];
+    const int32_t band = max(P.bandwidth ? P.bandwidth[pair] : B.sp.band, 1);
+    const int32_t offset = B.offset ? B.offset[pair] : 0;
+    const int32_t abort_score = P.abort_score ? P.abort_score[pair] : kAbortOff;
+    DpEnd end;
+    uint64_t cells = 0;
+    if (q > B.max_q || 2 * band + 1 > CAP) {  // outside this launch's trace slot / row buffer
+      if (g == 0) {
+        B.ends[item] = DpEnd{0, 0, 0, 0};
+        atomicOr(B.flags, 2u);
+      }
+      continue;
+    }
+    bsw_group_sweep<G, K>(P.read_seq + P.read_off[pair], q, P.win_seq + P.win_off[pair], w, band,
+                          offset, abort_score, B.sp, rowbuf,
+                          B.tg.trace + (size_t)item * B.tg.slot_bytes,
+                          B.tg.meta + (size_t)item * B.tg.meta_stride, g, gmask, end, cells);
+    if (g == 0) {
+      B.ends[item] = end;
+      if (B.cells) atomicAdd(B.cells, (unsigned long long)cells);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
+  const uint32_t count = B.count_dev ? *B.count_dev : B.count;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t item = blockIdx.x * blockDim.x + threadIdx.x; item < count; item += stride) {
+    const uint32_t pair = B.list ? B.list[item] : item;
+    const DpEnd e = B.ends[item];
+    int32_t i = e.end_i, j = e.end_j;
+    uint32_t overflow = 0;
+    const uint32_t n = bsw_walk(B.tg.trace + (size_t)item * B.tg.slot_bytes,
+                                B.tg.meta + (size_t)item * B.tg.meta_stride, B.tg.k_cells,
+                                B.tg.lane_bytes, B.tg.row_stride, i, j,
+                                B.cig_slots + (size_t)item * B.slot_cap, B.slot_cap, overflow);
+    kira_sw_result r;
+    r.score = e.score;
+    r.ref_start = (uint32_t)j;
+    r.ref_end = (uint32_t)e.end_j;
+    r.read_start = i;
+    r.read_end = e.end_i;
+    r.cigar_off = 0;
+    r.n_cigar = n;
+    r.status = KIRA_PAIR_SW;
+    r.early_abort = (uint8_t)e.early_abort;
+    r.reserved = overflow ? 1 : 0;
+    B.out[pair] = r;
+    B.ncig[pair] = n;
+    B.item_of_pair[pair] = item;
+    if (overflow) atomicOr(B.flags, 1u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scan of per-pair CIGAR counts and compaction into the output array.
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 1024;
+constexpr int kScanPerThread = 4;
+constexpr int kScanChunk = kScanThreads * kScanPerThread;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* sh,
+                                                         uint32_t& total) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, x, off);
+    if ((int)lane >= off) x += t;
+  }
+  if (lane == 31) sh[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t nw = blockDim.x >> 5;
+    uint32_t y = lane < nw ? sh[lane] : 0u;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, y, off);
+      if ((int)lane >= off) y += t;
+    }
+    if (lane < nw) sh[lane] = y;
+  }
+  __syncthreads();
+  const uint32_t warp_prefix = warp ? sh[warp - 1] : 0u;
+  total = sh[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return warp_prefix + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_chunk_sums(const uint32_t* __restrict__ v,
+                                                                uint32_t n,
+                                                                uint32_t* __restrict__ sums) {
+  __shared__ uint32_t sh[32];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanChunk + (uint64_t)threadIdx.x * kScanPerThread;
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPerThread; ++k)
+    if (base + k < n) s += v[base + k];
+  uint32_t total;
+  block_exclusive_scan(s, sh, total);
+  if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_sums(uint32_t* __restrict__ sums,
+                                                          uint32_t nchunks,
+                                                          uint64_t* __restrict__ total_out) {
+  __shared__ uint32_t sh[32];
+  uint32_t carry = 0;
+  for (uint32_t base = 0; base < nchunks; base += kScanThreads) {
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t v = i < nchunks ? sums[i] : 0u;
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan(v, sh, total);
+    if (i < nchunks) sums[i] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0 && total_out) *total_out = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_apply(const uint32_t* __restrict__ v,
+                                                           uint32_t n,
+                                                           const uint32_t* __restrict__ sums,
+                                                           uint32_t* __restrict__ off) {
+  __shared__ uint32_t sh[32];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanChunk + (uint64_t)threadIdx.x * kScanPerThread;
+  uint32_t vals[kScanPerThread];
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPerThread; ++k) {
+    vals[k] = base + k < n ? v[base + k] : 0u;
+    s += vals[k];
+  }
+  uint32_t total;
+  uint32_t ex = block_exclusive_scan(s, sh, total) + sums[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanPerThread; ++k) {
+    if (base + k < n) off[base + k] = ex;
+    ex += vals[k];
+  }
+}
+
+// Writes cigar_off into the results and the ops into the packed output.
+__global__ void __launch_bounds__(256) cigar_compact_kernel(CompactLaunch C) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < C.n; p += stride) {
+    const uint32_t off = C.off[p];
+    const uint32_t n = C.ncig[p];
+    kira_sw_result* r = C.out + p;
+    r->cigar_off = off;
+    if ((uint64_t)off + n > C.cap) continue;
+    if (r->status == KIRA_PAIR_CERTIFIED) {
+      C.ops[off] = ((uint32_t)r->read_end << 4) | 0u;
+    } else if (r->status == KIRA_PAIR_SW) {
+      const uint32_t* src = C.slots + (size_t)C.item_of_pair[p] * C.slot_cap;
+      for (uint32_t t = 0; t < n; ++t) C.ops[off + t] = src[n - 1u - t];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+static int grid_for(uint64_t units, int per_block, int max_blocks) {
+  uint64_t b = (units + per_block - 1) / per_block;
+  if (b < 1) b = 1;
+  if (b > (uint64_t)max_blocks) b = max_blocks;
+  return (int)b;
+}
+
+cudaError_t launch_sieve_dropin(const SieveJobsDev& J, kira_sieve_result* out, int sms,
+                                cudaStream_t st) {
+  const int blocks = grid_for(J.n, 8, sms * 16);
+  sieve_dropin_kernel<<<blocks, 256, 0, st>>>(J, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_verify_sieve(const DevPairs& P, const VerifyDev& V, int sms, cudaStream_t st) {
+  const int blocks = grid_for(P.n, 8, sms * 16);
+  verify_sieve_kernel<<<blocks, 256, 0, st>>>(P, V);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_myers(const DevPairs& P, const MyersLaunch& M, uint32_t max_items, int sms,
+                         cudaStream_t st) {
+  const size_t smem = (size_t)4 * 32 * M.tw * 3 * sizeof(uint32_t);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(myers_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set = true;
+  }
+  const int blocks = grid_for(max_items, 128, sms * 8);
+  myers_kernel<<<blocks, 128, smem, st>>>(P, M);
+  return cudaGetLastError();
+}
+
+template <int G, int K>
+static cudaError_t launch_bsw_shape(const DevPairs& P, const BswLaunch& B, uint32_t max_items,
+                                    int sms, cudaStream_t st, cudaEvent_t between) {
+  constexpr int threads = 256;
+  const size_t smem = (size_t)(threads / G) * 4 * G * K * sizeof(int32_t);
+  cudaFuncSetAttribute(bsw_dp_kernel<G, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bsw_dp_kernel<G, K>, threads, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int blocks = grid_for(max_items, threads / G, sms * per_sm);
+  bsw_dp_kernel<G, K><<<blocks, threads, smem, st>>>(P, B);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (between) cudaEventRecord(between, st);
+  const int tb_blocks = grid_for(max_items, 128, sms * 16);
+  bsw_tb_kernel<<<tb_blocks, 128, 0, st>>>(P, B);
+  return cudaGetLastError();
+}
+
+const BswShapeInfo kBswShapes[] = {
+    {4, 10}, {8, 10}, {16, 10}, {32, 10}, {32, 17},
+};
+const int kNumBswShapes = sizeof(kBswShapes) / sizeof(kBswShapes[0]);
+
+cudaError_t launch_bsw(int shape, const DevPairs& P, const BswLaunch& B, uint32_t max_items,
+                       int sms, cudaStream_t st, cudaEvent_t between) {
+  switch (shape) {
+    case 0: return launch_bsw_shape<4, 10>(P, B, max_items, sms, st, between);
+    case 1: return launch_bsw_shape<8, 10>(P, B, max_items, sms, st, between);
+    case 2: return launch_bsw_shape<16, 10>(P, B, max_items, sms, st, between);
+    case 3: return launch_bsw_shape<32, 10>(P, B, max_items, sms, st, between);
+    case 4: return launch_bsw_shape<32, 17>(P, B, max_items, sms, st, between);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_cigar_scan(const uint32_t* ncig, uint32_t n, uint32_t* off, uint32_t* chunk_sums,
+                              uint64_t* total_dev, cudaStream_t st) {
+  const uint32_t chunks = (n + kScanChunk - 1) / kScanChunk;
+  if (chunks == 0) return cudaSuccess;
+  scan_chunk_sums<<<chunks, kScanThreads, 0, st>>>(ncig, n, chunk_sums);
+  scan_sums<<<1, kScanThreads, 0, st>>>(chunk_sums, chunks, total_dev);
+  scan_apply<<<chunks, kScanThreads, 0, st>>>(ncig, n, chunk_sums, off);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cigar_compact(const CompactLaunch& C, int sms, cudaStream_t st) {
+  const int blocks = grid_for(C.n, 256, sms * 8);
+  cigar_compact_kernel<<<blocks, 256, 0, st>>>(C);
+  return cudaGetLastError();
+}
+
+}  // namespace kira

@@ -1,0 +1,325 @@
+"""Host runtime over the C ABI: context, error mapping and pair batches.
+
+The classes here are the host side of the drop-in boundary; every compute call
+goes through libkira_gpu.so (there is no CPU path in this package).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi as A
+
+OP_CHARS = "MIDNS"
+
+
+# --- CudaError (src/cuda/mod.rs:17-34) --------------------------------------
+class CudaError(Exception):
+    status = -1
+
+
+class NotBuilt(CudaError):
+    status = 1
+
+
+class DriverError(CudaError):
+    status = 2
+
+
+class RuntimeFailure(CudaError):
+    status = 3
+
+
+class NoDevice(CudaError):
+    status = 4
+
+
+class ReadTooLong(CudaError):
+    status = 5
+
+    def __init__(self, msg: str, length: int = 0, maximum: int = A.READ_BYTES_MAX):
+        super().__init__(msg)
+        self.len = length
+        self.max = maximum
+
+
+class Timeout(CudaError):
+    status = 6
+
+
+class InvalidArgument(CudaError):
+    status = 7
+
+
+class OutOfMemory(CudaError):
+    status = 8
+
+
+class CapacityError(CudaError):
+    status = 9
+
+
+_ERRORS = {c.status: c for c in (NotBuilt, DriverError, RuntimeFailure, NoDevice, ReadTooLong,
+                                 Timeout, InvalidArgument, OutOfMemory, CapacityError)}
+
+
+def raise_for(rc: int, msg: str) -> None:
+    if rc == A.KIRA_OK:
+        return
+    cls = _ERRORS.get(rc, CudaError)
+    raise cls(f"[{A.STATUS_NAMES.get(rc, rc)}] {msg}")
+
+
+def is_available() -> bool:
+    """cuda::is_available (src/cuda/mod.rs:39-49)."""
+    return bool(A.lib().kira_gpu_is_available())
+
+
+# --- configuration -----------------------------------------------------------
+@dataclass
+class AlignmentConfig:
+    """AlignmentConfig (src/alignment/mod.rs:24-35) plus the DP knobs the reference
+    reads from KIRA_ADAPTIVE_BAND / KIRA_ADAPTIVE_MAX_DRIFT / KIRA_DP_XDROP."""
+    match_score: int = 1
+    mismatch: int = 4
+    gap_open: int = 6
+    gap_extend: int = 1
+    bandwidth: int = 33
+    xdrop: int = 100
+    clip_penalty: int = 5
+    adaptive: bool = True
+    max_drift: int = 16
+    dp_xdrop: int = -1
+
+    def to_c(self) -> A.SwCfg:
+        return A.SwCfg(self.match_score, self.mismatch, self.gap_open, self.gap_extend,
+                       self.bandwidth, self.xdrop, self.clip_penalty, int(self.adaptive),
+                       self.max_drift, self.dp_xdrop)
+
+
+@dataclass
+class VerifyParams:
+    cfg: AlignmentConfig = field(default_factory=AlignmentConfig)
+    sieve_threshold: int = 12
+    myers_k: int = 8
+    cert_strict: bool = False
+
+    def to_c(self) -> A.VerifyParams:
+        return A.VerifyParams(self.cfg.to_c(), self.sieve_threshold, self.myers_k,
+                              int(self.cert_strict), 0)
+
+
+# --- pair batches --------------------------------------------------------------
+@dataclass
+class PairBatch:
+    """Flat (read x window) pairs: ASCII arenas plus per-pair offsets/lengths."""
+    read_seq: np.ndarray
+    read_off: np.ndarray
+    read_len: np.ndarray
+    win_seq: np.ndarray | None
+    win_off: np.ndarray
+    win_len: np.ndarray
+    band_offset: np.ndarray | None = None
+    abort_score: np.ndarray | None = None
+    bandwidth: np.ndarray | None = None
+
+    @property
+    def n(self) -> int:
+        return int(len(self.read_off))
+
+    @classmethod
+    def from_pairs(cls, reads, wins, band_offset=None, abort_score=None, bandwidth=None):
+        """Build from equal-length lists of byte strings (a read may repeat)."""
+        uniq: dict[bytes, int] = {}
+        chunks, roff = [], []
+        pos = 0
+        for r in reads:
+            r = bytes(r)
+            if r not in uniq:
+                uniq[r] = pos
+                chunks.append(r)
+                pos += len(r)
+            roff.append(uniq[r])
+        wchunks, woff = [], []
+        wpos = 0
+        for w in wins:
+            w = bytes(w)
+            woff.append(wpos)
+            wchunks.append(w)
+            wpos += len(w)
+
+        def arr(x, dt):
+            return None if x is None else np.ascontiguousarray(np.asarray(x, dtype=dt))
+
+        return cls(np.frombuffer(b"".join(chunks) + b"\0", np.uint8).copy(),
+                   np.asarray(roff, np.uint64), np.asarray([len(r) for r in reads], np.uint32),
+                   np.frombuffer(b"".join(wchunks) + b"\0", np.uint8).copy(),
+                   np.asarray(woff, np.uint64), np.asarray([len(w) for w in wins], np.uint32),
+                   arr(band_offset, np.int32), arr(abort_score, np.int32),
+                   arr(bandwidth, np.int32))
+
+    def to_c(self) -> A.Pairs:
+        p = A.Pairs()
+        p.n = self.n
+        p.read_seq = A.ptr(self.read_seq)
+        p.read_seq_bytes = int(self.read_seq.nbytes)
+        p.read_off = A.ptr(self.read_off)
+        p.read_len = A.ptr(self.read_len)
+        p.win_seq = A.ptr(self.win_seq)
+        p.win_seq_bytes = 0 if self.win_seq is None else int(self.win_seq.nbytes)
+        p.win_off = A.ptr(self.win_off)
+        p.win_len = A.ptr(self.win_len)
+        p.band_offset = A.ptr(self.band_offset)
+        p.abort_score = A.ptr(self.abort_score)
+        p.bandwidth = A.ptr(self.bandwidth)
+        return p
+
+
+def decode_cigar(ops) -> list:
+    return [(int(w) >> 4, OP_CHARS[int(w) & 0xF]) for w in ops]
+
+
+def cigar_string(cig) -> str:
+    return "".join(f"{n}{c}" for n, c in cig)
+
+
+@dataclass
+class SwPublicResult:
+    """SwPublicResult (src/alignment/mod.rs:910-920), window coordinates."""
+    ref_start: int
+    ref_end: int
+    read_start: int
+    read_end: int
+    score: int
+    cigar: list
+    early_abort: bool
+    status: int = A.PAIR_SW
+
+    def key(self):
+        return (self.ref_start, self.ref_end, self.read_start, self.read_end, self.score,
+                tuple(self.cigar), self.early_abort)
+
+
+def results_to_list(res: np.ndarray, ops: np.ndarray) -> list:
+    out = []
+    for r in res:
+        o, n = int(r["cigar_off"]), int(r["n_cigar"])
+        out.append(SwPublicResult(int(r["ref_start"]), int(r["ref_end"]), int(r["read_start"]),
+                                  int(r["read_end"]), int(r["score"]),
+                                  decode_cigar(ops[o:o + n]), bool(r["early_abort"]),
+                                  int(r["status"])))
+    return out
+
+
+# --- context -------------------------------------------------------------------
+class GpuContext:
+    """One kira_ctx (one device, one stream, one grow-only arena)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = A.lib()
+        h = C.c_void_p()
+        rc = self._lib.kira_gpu_init(device, C.byref(h))
+        if rc != A.KIRA_OK:
+            raise_for(rc, f"kira_gpu_init(device={device}) failed")
+        self._h = h
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.kira_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def last_error(self) -> str:
+        buf = C.create_string_buffer(1024)
+        self._lib.kira_gpu_last_error(self._h, buf, 1024)
+        return buf.value.decode(errors="replace")
+
+    def check(self, rc: int) -> None:
+        if rc != A.KIRA_OK:
+            raise_for(rc, self.last_error())
+
+    def arena_bytes(self) -> int:
+        return int(self._lib.kira_gpu_arena_bytes(self._h))
+
+    # -- sieve drop-in
+    def sieve_batch(self, jobs: list) -> np.ndarray:
+        n = len(jobs)
+        arr = (A.SieveJob * max(n, 1))()
+        keep = []
+        for i, j in enumerate(jobs):
+            rb = np.frombuffer(bytes(j.read_packed) or b"\0", np.uint8)
+            wb = np.frombuffer(bytes(j.ref_shifted[0]) or b"\0", np.uint8)
+            keep += [rb, wb]
+            arr[i] = A.SieveJob(rb.ctypes.data, len(j.read_packed), j.read_nucs, wb.ctypes.data,
+                                len(j.ref_shifted[0]), j.ref_nucs, j.max_mismatches)
+        out = (A.SieveResult * max(n, 1))()
+        self.check(self._lib.kira_gpu_sieve_batch(self._h, arr, n, out))
+        return np.array([(o.shift, o.mismatches, o.second_mismatches) for o in out[:n]],
+                        dtype=np.int64).reshape(n, 3)
+
+    def ref_upload(self, seq) -> None:
+        a = np.frombuffer(bytes(seq), np.uint8) if not isinstance(seq, np.ndarray) else seq
+        self.check(self._lib.kira_gpu_ref_upload(self._h, A.ptr(a), int(a.nbytes)))
+
+    # -- Myers
+    def myers_batch(self, batch: PairBatch, max_k: int):
+        dist = np.empty(batch.n, np.int32)
+        end = np.empty(batch.n, np.int32)
+        pc = batch.to_c()
+        self.check(self._lib.kira_gpu_myers_batch(self._h, C.byref(pc), max_k, A.ptr(dist),
+                                                  A.ptr(end)))
+        return dist, end
+
+    # -- banded SW
+    def bsw_batch(self, batch: PairBatch, cfg: AlignmentConfig, cigar_cap: int | None = None):
+        n = batch.n
+        res = np.zeros(n, A.SW_RESULT_DTYPE)
+        cap = cigar_cap if cigar_cap is not None else max(16, 8 * n)
+        ops = np.zeros(cap, np.uint32)
+        cb = A.CigarBuf(A.ptr(ops), cap, 0)
+        cells = C.c_uint64()
+        pc = batch.to_c()
+        cc = cfg.to_c()
+        rc = self._lib.kira_gpu_bsw_batch(self._h, C.byref(pc), C.byref(cc), A.ptr(res),
+                                          C.byref(cb), C.byref(cells))
+        if rc == 9 and cigar_cap is None:
+            return self.bsw_batch(batch, cfg, int(cb.used) + 16)
+        self.check(rc)
+        return res, ops[: cb.used], int(cells.value)
+
+    # -- composed verification
+    def verify_batch(self, batch: PairBatch, params: VerifyParams, detail: bool = False,
+                     cigar_cap: int | None = None):
+        n = batch.n
+        res = np.zeros(n, A.SW_RESULT_DTYPE)
+        det = np.zeros(n, A.DETAIL_DTYPE) if detail else None
+        cap = cigar_cap if cigar_cap is not None else max(16, 4 * n)
+        ops = np.zeros(cap, np.uint32)
+        cb = A.CigarBuf(A.ptr(ops), cap, 0)
+        cells = C.c_uint64()
+        pc = batch.to_c()
+        vp = params.to_c()
+        rc = self._lib.kira_gpu_verify_batch(self._h, C.byref(pc), C.byref(vp), A.ptr(res),
+                                             C.byref(cb), A.ptr(det), C.byref(cells))
+        if rc == 9 and cigar_cap is None:
+            return self.verify_batch(batch, params, detail, int(cb.used) + 16)
+        self.check(rc)
+        return res, ops[: cb.used], det, int(cells.value)

@@ -1,0 +1,133 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+No public dataset is involved: references, reads and candidate windows are
+generated from fixed seeds (numpy PCG64), with the sizes and error profiles of
+the verification workloads:
+
+* ``small``   -- 1 Mbp uniform reference, 10k reads of 150 bp (1 % substitutions,
+  0.1 % indels of length 1-3, geometric), 4 windows of 250 bp per read
+  (1 true + 3 random): 40k pairs.
+* ``batched`` -- 100 Mbp reference (uniform + 5 % of 300 bp repeat families at
+  2-10 % divergence), 250k reads x 8 candidates (1 true) = 2M pairs,
+  150 / 250 bp, per-read substitution rate U[0.5 %, 2 %], 0.1 % indels.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+BASES = np.frombuffer(b"ACGT", np.uint8)
+
+
+@dataclass
+class Workload:
+    name: str
+    reference: np.ndarray      # uint8 ASCII
+    reads: np.ndarray          # uint8 ASCII arena (all reads)
+    read_off: np.ndarray       # per pair (uint64)
+    read_len: np.ndarray       # per pair (uint32)
+    win_off: np.ndarray        # per pair, reference coordinate (uint64)
+    win_len: np.ndarray        # per pair (uint32)
+    is_true: np.ndarray        # per pair: window holds the read's origin
+
+    @property
+    def n_pairs(self) -> int:
+        return int(len(self.read_off))
+
+    def windows_arena(self):
+        """Materialise windows into their own arena (host-window mode)."""
+        offs = np.zeros(self.n_pairs, np.uint64)
+        if self.n_pairs:
+            offs[1:] = np.cumsum(self.win_len[:-1].astype(np.uint64))
+        total = int(self.win_len.astype(np.uint64).sum())
+        arena = np.empty(total + 16, np.uint8)
+        idx = np.repeat(self.win_off.astype(np.int64), self.win_len) + (
+            np.arange(total) - np.repeat(offs.astype(np.int64), self.win_len))
+        arena[:total] = self.reference[idx]
+        arena[total:] = 0
+        return arena, offs
+
+
+def random_reference(rng, length: int, repeat_frac: float = 0.0, family_len: int = 300,
+                     div_lo: float = 0.02, div_hi: float = 0.10, n_families: int = 200):
+    ref = BASES[rng.integers(0, 4, length)]
+    if repeat_frac > 0:
+        copies = int(length * repeat_frac) // family_len
+        fams = BASES[rng.integers(0, 4, (n_families, family_len))]
+        starts = rng.integers(0, length - family_len, copies)
+        which = rng.integers(0, n_families, copies)
+        div = rng.uniform(div_lo, div_hi, copies)
+        for s, f, d in zip(starts, which, div):
+            seq = fams[f].copy()
+            m = rng.random(family_len) < d
+            seq[m] = BASES[(np.searchsorted(BASES, seq[m]) + rng.integers(1, 4, m.sum())) % 4]
+            ref[s:s + family_len] = seq
+    return ref
+
+
+def _mutate(rng, frag: np.ndarray, read_len: int, sub_rate: float, indel_rate: float):
+    """Substitutions + indels (length 1-3, geometric p=0.5) on a reference fragment
+    that is longer than the read; returns exactly read_len bases."""
+    out = []
+    i = 0
+    n = len(frag)
+    while len(out) < read_len and i < n:
+        if rng.random() < indel_rate:
+            ln = min(int(rng.geometric(0.5)), 3)
+            if rng.random() < 0.5:  # insertion
+                out.extend(BASES[rng.integers(0, 4, ln)].tolist())
+            else:  # deletion
+                i += ln
+            continue
+        out.append(int(frag[i]))
+        i += 1
+    while len(out) < read_len:
+        out.append(int(BASES[rng.integers(0, 4)]))
+    r = np.asarray(out[:read_len], np.uint8)
+    m = rng.random(read_len) < sub_rate
+    if m.any():
+        r[m] = BASES[(np.searchsorted(BASES, r[m]) + rng.integers(1, 4, m.sum())) % 4]
+    return r
+
+
+def make_workload(name: str, n_reads: int, ref_len: int, read_len: int = 150,
+                  win_len: int = 250, cands: int = 4, sub_lo: float = 0.01,
+                  sub_hi: float = 0.01, indel_rate: float = 0.001, repeat_frac: float = 0.0,
+                  seed: int = 0x5EED) -> Workload:
+    rng = np.random.default_rng(seed)
+    ref = random_reference(rng, ref_len, repeat_frac)
+    slack = win_len - read_len
+    origins = rng.integers(slack, ref_len - win_len - 8, n_reads)
+    sub = rng.uniform(sub_lo, sub_hi, n_reads)
+    has_indel = rng.random(n_reads) < 1.0 - (1.0 - indel_rate) ** read_len
+    reads = ref[origins[:, None] + np.arange(read_len)[None, :]]
+    m = rng.random((n_reads, read_len)) < sub[:, None]
+    reads[m] = BASES[(np.searchsorted(BASES, reads[m]) + rng.integers(1, 4, int(m.sum()))) % 4]
+    for r in np.nonzero(has_indel)[0]:
+        o = int(origins[r])
+        reads[r] = _mutate(rng, ref[o:o + read_len + 16], read_len, sub[r], indel_rate)
+    n_pairs = n_reads * cands
+    read_off = np.repeat(np.arange(n_reads, dtype=np.uint64) * read_len, cands)
+    true_slot = rng.integers(0, cands, n_reads)
+    win_off = rng.integers(0, ref_len - win_len, n_pairs).astype(np.uint64)
+    lead = rng.integers(0, slack + 1, n_reads)
+    true_idx = np.arange(n_reads) * cands + true_slot
+    win_off[true_idx] = (origins - lead).astype(np.uint64)
+    is_true = np.zeros(n_pairs, bool)
+    is_true[true_idx] = True
+    return Workload(name, ref, reads.reshape(-1), read_off,
+                    np.full(n_pairs, read_len, np.uint32), win_off,
+                    np.full(n_pairs, win_len, np.uint32), is_true)
+
+
+def small(seed: int = 0x5EED) -> Workload:
+    """1 Mbp, 10k x 150 bp reads, 4 windows of 250 bp each: 40k pairs."""
+    return make_workload("small_40k_150x250", 10_000, 1_000_000, cands=4, sub_lo=0.01,
+                         sub_hi=0.01, seed=seed)
+
+
+def batched(seed: int = 0xB200, n_reads: int = 250_000, ref_len: int = 100_000_000) -> Workload:
+    """100 Mbp + 5 % repeats, 250k reads x 8 candidates = 2M pairs of 150 / 250 bp."""
+    return make_workload("batched_2M_150x250", n_reads, ref_len, cands=8, sub_lo=0.005,
+                         sub_hi=0.02, repeat_frac=0.05, seed=seed)
