@@ -62,7 +62,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -233,6 +233,10 @@ def run_ours(args, rank, local, world, dist):
     stage_ms = np.zeros(len(_abi.STAGES))
     sampler = ClockSampler(local)
     sampler.start()
+    time.sleep(0.3)  # let the sampler attach before the timed region
+    # keep the GPU busy while the sampler attaches so its first samples see load
+    for _ in range(3):
+        step()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize(dev)

@@ -19,7 +19,8 @@ enum BufId {
   B_READ_SEQ, B_WIN_SEQ, B_READ_OFF, B_READ_LEN, B_WIN_OFF, B_WIN_LEN, B_BAND_OFF, B_ABORT,
   B_BANDW, B_OUT, B_DETAIL, B_CIGAR_OUT, B_NCIG, B_CIG_OFF, B_CHUNK_SUMS, B_SW_OFFSET,
   B_MYERS_LIST, B_SW_LIST, B_COUNTERS, B_ENDS, B_TRACE, B_META, B_CIG_SLOTS, B_ITEM_OF_PAIR,
-  B_DIST, B_END, B_SIEVE_OUT, B_SIEVE_JOBS, B_CELLS, B_TOTAL, B_COUNT
+  B_DIST, B_END, B_SIEVE_OUT, B_SIEVE_JOBS, B_CELLS, B_TOTAL, B_READ_PLANES, B_WIN_PLANES,
+  B_COUNT
 };
 
 struct DevBuf {
@@ -40,6 +41,7 @@ struct kira_ctx {
   cudaEvent_t ev[kStages + 1] = {};
   int ev_recorded = 0;
   uint8_t* ref_dev = nullptr;
+  uint4* ref_planes = nullptr;  // 2-bit + valid planes of the resident reference
   uint64_t ref_len = 0;
   DevBuf bufs[B_COUNT];
 };
@@ -178,7 +180,7 @@ int upload_pairs(kira_ctx* ctx, const kira_pairs& P, DevPairs& D) {
   KIRA_CUDA(cudaMemcpyAsync(rl, P.read_len, 4ull * n, cudaMemcpyHostToDevice, st));
   KIRA_CUDA(cudaMemcpyAsync(wo, P.win_off, 8ull * n, cudaMemcpyHostToDevice, st));
   KIRA_CUDA(cudaMemcpyAsync(wl, P.win_len, 4ull * n, cudaMemcpyHostToDevice, st));
-  D = DevPairs{n, rs, ro, rl, ws, wo, wl, nullptr, nullptr, nullptr};
+  D = DevPairs{n, rs, ro, rl, ws, wo, wl, nullptr, nullptr, nullptr, nullptr, nullptr};
   if (P.band_offset) {
     KIRA_DBUF(b, int32_t, B_BAND_OFF, n);
     KIRA_CUDA(cudaMemcpyAsync(b, P.band_offset, 4ull * n, cudaMemcpyHostToDevice, st));
@@ -193,6 +195,27 @@ int upload_pairs(kira_ctx* ctx, const kira_pairs& P, DevPairs& D) {
     KIRA_DBUF(b, int32_t, B_BANDW, n);
     KIRA_CUDA(cudaMemcpyAsync(b, P.bandwidth, 4ull * n, cudaMemcpyHostToDevice, st));
     D.bandwidth = b;
+  }
+  return KIRA_OK;
+}
+
+// Plane arenas of the batch's reads and windows (the resident reference keeps
+// the planes built at upload).
+int build_planes(kira_ctx* ctx, DevPairs& D, uint64_t read_bytes, uint64_t win_bytes,
+                 bool resident, cudaStream_t st) {
+  cudaError_t cerr = cudaSuccess;
+  const uint64_t rb = plane_blocks(read_bytes);
+  KIRA_DBUF(rp, uint4, B_READ_PLANES, rb);
+  KIRA_CUDA(launch_pack_planes(D.read_seq, read_bytes, rp, rb, ctx->sms, st));
+  D.read_planes = rp;
+  if (resident) {
+    if (!ctx->ref_planes) return fail(ctx, KIRA_ERR_INVALID, "no resident reference uploaded");
+    D.win_planes = ctx->ref_planes;
+  } else {
+    const uint64_t wb = plane_blocks(win_bytes);
+    KIRA_DBUF(wp, uint4, B_WIN_PLANES, wb);
+    KIRA_CUDA(launch_pack_planes(D.win_seq, win_bytes, wp, wb, ctx->sms, st));
+    D.win_planes = wp;
   }
   return KIRA_OK;
 }
@@ -241,9 +264,10 @@ void mark(kira_ctx* ctx, int i, cudaStream_t st) {
 }
 
 // The composed path on device buffers, enqueued on `st`.
-int verify_pipeline(kira_ctx* ctx, const DevPairs& D, const Maxes& mx, const kira_verify_params& p,
-                    kira_sw_result* out, uint32_t* ops, uint64_t cap, uint64_t* total_dev,
-                    kira_verify_detail* detail, unsigned long long* cells_dev, cudaStream_t st) {
+int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verify_params& p,
+                    uint64_t read_bytes, uint64_t win_bytes, bool resident, kira_sw_result* out,
+                    uint32_t* ops, uint64_t cap, uint64_t* total_dev, kira_verify_detail* detail,
+                    unsigned long long* cells_dev, cudaStream_t st) {
   cudaError_t cerr = cudaSuccess;
   const uint32_t n = D.n;
   if (n == 0) return KIRA_OK;
@@ -261,7 +285,9 @@ int verify_pipeline(kira_ctx* ctx, const DevPairs& D, const Maxes& mx, const kir
   VerifyDev V{p.sieve_threshold, p.cert_strict, sp, out, detail, ncig, swoff, mlist, counters};
   ctx->ev_recorded = 0;
   mark(ctx, 0, st);
-  KIRA_CUDA(launch_verify_sieve(D, V, ctx->sms, st));
+  rc = build_planes(ctx, D, read_bytes, win_bytes, resident, st);
+  if (rc) return rc;
+  KIRA_CUDA(launch_verify_sieve(D, V, mx.q, ctx->sms, st));
   mark(ctx, 1, st);
   MyersLaunch M{};
   M.list = mlist;
@@ -269,6 +295,7 @@ int verify_pipeline(kira_ctx* ctx, const DevPairs& D, const Maxes& mx, const kir
   M.k = p.myers_k;
   M.per_pair_k = 1;
   M.tw = std::max<uint32_t>((mx.w + 31) / 32, 1);
+  M.lmax = std::max<uint32_t>((mx.q + 31) / 32, 1);
   M.cascade = 1;
   M.out = out;
   M.detail = detail;
@@ -338,6 +365,7 @@ void kira_gpu_destroy(kira_ctx* ctx) {
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);
   if (ctx->ref_dev) cudaFree(ctx->ref_dev);
+  if (ctx->ref_planes) cudaFree(ctx->ref_planes);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -445,11 +473,17 @@ int kira_gpu_ref_upload(kira_ctx* ctx, const uint8_t* seq, uint64_t len) {
   if (!ctx) return KIRA_ERR_INVALID;
   cudaSetDevice(ctx->device);
   if (ctx->ref_dev) cudaFree(ctx->ref_dev);
+  if (ctx->ref_planes) cudaFree(ctx->ref_planes);
   ctx->ref_dev = nullptr;
+  ctx->ref_planes = nullptr;
   ctx->ref_len = 0;
   if (len == 0) return KIRA_OK;
   KIRA_CUDA(cudaMalloc(&ctx->ref_dev, len + 16));
   KIRA_CUDA(cudaMemcpy(ctx->ref_dev, seq, len, cudaMemcpyHostToDevice));
+  const uint64_t nb = plane_blocks(len);
+  KIRA_CUDA(cudaMalloc(&ctx->ref_planes, nb * sizeof(uint4)));
+  KIRA_CUDA(launch_pack_planes(ctx->ref_dev, len, ctx->ref_planes, nb, ctx->sms, ctx->stream));
+  KIRA_CUDA(cudaStreamSynchronize(ctx->stream));
   ctx->ref_len = len;
   return KIRA_OK;
 }
@@ -470,12 +504,15 @@ int kira_gpu_myers_batch(kira_ctx* ctx, const kira_pairs* pairs, uint32_t max_k,
   KIRA_DBUF(de, int32_t, B_END, P.n);
   KIRA_DBUF(counters, uint32_t, B_COUNTERS, 4);
   KIRA_CUDA(cudaMemsetAsync(counters, 0, 16, ctx->stream));
+  rc = build_planes(ctx, D, P.read_seq_bytes, P.win_seq_bytes, P.win_seq == nullptr, ctx->stream);
+  if (rc) return rc;
   MyersLaunch M{};
   M.flags = counters + 2;
   M.count = P.n;
   M.k = (int32_t)max_k;
   M.per_pair_k = 0;
   M.tw = std::max<uint32_t>((mx.w + 31) / 32, 1);
+  M.lmax = std::max<uint32_t>((mx.q + 31) / 32, 1);
   M.dist = dd;
   M.end = de;
   cudaStream_t st = ctx->stream;
@@ -573,7 +610,8 @@ int kira_gpu_verify_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_ver
   KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
   KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
   KIRA_CUDA(cudaMemsetAsync(cells_dev, 0, 8, st));
-  rc = verify_pipeline(ctx, D, mx, *p, dout, ops, cigar->cap, total_dev, ddet, cells_dev, st);
+  rc = verify_pipeline(ctx, D, mx, *p, P.read_seq_bytes, P.win_seq_bytes, P.win_seq == nullptr,
+                       dout, ops, cigar->cap, total_dev, ddet, cells_dev, st);
   if (rc) return rc;
   uint64_t total = 0;
   unsigned long long hcells = 0;
@@ -617,9 +655,10 @@ int kira_gpu_verify_dev(kira_ctx* ctx, const kira_pairs* pairs, const kira_verif
   if (!mx.band) return fail(ctx, KIRA_ERR_INVALID, "per-pair bandwidth needs max_bandwidth");
   DevPairs D{P.n, P.read_seq, P.read_off, P.read_len,
              P.win_seq ? P.win_seq : ctx->ref_dev, P.win_off, P.win_len,
-             P.band_offset, P.abort_score, P.bandwidth};
-  return verify_pipeline(ctx, D, mx, *p, out, cigar_ops, cigar_cap, cigar_used_dev, detail,
-                         cells_dev, (cudaStream_t)stream);
+             P.band_offset, P.abort_score, P.bandwidth, nullptr, nullptr};
+  return verify_pipeline(ctx, D, mx, *p, P.read_seq_bytes, P.win_seq_bytes, P.win_seq == nullptr,
+                         out, cigar_ops, cigar_cap, cigar_used_dev, detail, cells_dev,
+                         (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -36,22 +36,49 @@ struct BswShape {
   static constexpr int kRowStride = G * kLaneBytes;
 };
 
-// Shared memory per group: two H rows and two E rows of kCap ints.
+// The previous row stays in registers: ph[k] / pe[k] hold H / E of cell
+// g*K + k + sh of the previous row, where `sh` is the realignment applied so far.
+// With the band moving one column per row (d = j_start(i) - j_start(i-1) = 1,
+// the common case for a read following its diagonal) the diagonal predecessor of
+// cell idx is previous cell idx (same register) and the upper one is idx + 1 (next
+// register, or lane g+1's first register via one shuffle). Rows with d != 1
+// realign the registers through a transposed shared-memory buffer
+// ([k][warp lane]: bank-conflict-free for every shift).
+template <int G, int K>
+__device__ __forceinline__ void bsw_realign(int32_t (&ph)[K], int32_t (&pe)[K], int32_t s,
+                                            int32_t* buf, uint32_t lb, int32_t gi,
+                                            uint32_t gmask) {
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    buf[k * 32 + (int32_t)lb + gi] = ph[k];
+    buf[(K + k) * 32 + (int32_t)lb + gi] = pe[k];
+  }
+  __syncwarp(gmask);
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int32_t t = k + s;
+    const int32_t tq = t >= 0 ? t / K : -((K - 1 - t) / K);  // floor(t / K)
+    const int32_t tr = t - tq * K;
+    const int32_t src = gi + tq;
+    const bool ok = src >= 0 && src < G;  // outside: never read (masked by the bounds)
+    const int32_t a = tr * 32 + (int32_t)lb + (ok ? src : gi);
+    ph[k] = buf[a];
+    pe[k] = buf[K * 32 + a];
+  }
+  __syncwarp(gmask);
+}
+
 template <int G, int K>
 __device__ __forceinline__ void bsw_group_sweep(
     const uint8_t* __restrict__ rd, uint32_t q, const uint8_t* __restrict__ wn, uint32_t w,
     int32_t band, int32_t offset, int32_t abort_score, const SwParams& sp, int32_t* rowbuf,
-    uint8_t* __restrict__ trace, uint32_t* __restrict__ meta, uint32_t g, uint32_t gmask,
-    DpEnd& out, uint64_t& cells_out) {
-  constexpr int CAP = BswShape<G, K>::kCap;
+    uint32_t lb, uint8_t* __restrict__ trace, uint32_t* __restrict__ meta, uint32_t g,
+    uint32_t gmask, DpEnd& out, uint64_t& cells_out) {
   constexpr int LB = BswShape<G, K>::kLaneBytes;
   constexpr int S = BswShape<G, K>::kRowStride;
   constexpr int32_t NEGBIG = INT32_MIN / 2;
-  int32_t* rowH[2] = {rowbuf, rowbuf + CAP};
-  int32_t* rowE[2] = {rowbuf + 2 * CAP, rowbuf + 3 * CAP};
 
   int32_t prev_start = 1, prev_len = 0;
-  int cur = 0;
   int32_t best = 0, bi = 0, bj = 0, bq = 0, bqj = 0;
   uint32_t early = 0;
   uint64_t cells = 0;
@@ -59,6 +86,14 @@ __device__ __forceinline__ void bsw_group_sweep(
   int32_t acenter = 1 + offset;
   const int32_t match = sp.match, mism = sp.mismatch, gof = sp.gof, ge = sp.gap_extend;
   const int32_t wl = (int32_t)w;
+  const int32_t gi = (int32_t)g;
+  const int32_t base_idx = gi * K;
+  int32_t ph[K], pe[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    ph[k] = 0;
+    pe[k] = kNeg4;
+  }
 
   for (uint32_t iu = 1; iu <= q; ++iu) {
     const int32_t i = (int32_t)iu;
@@ -75,26 +110,28 @@ __device__ __forceinline__ void bsw_group_sweep(
     const int32_t row_len = je - js + 1;
     cells += (uint64_t)row_len;
     const uint32_t qb = ldb(rd, (uint64_t)(i - 1));
-    const int32_t d = js - prev_start;
-    const int32_t* pH = rowH[cur ^ 1];
-    const int32_t* pE = rowE[cur ^ 1];
+    // Previous cell of diag = idx + s with s = d - 1; realign registers unless s == 0.
+    const int32_t sft = js - prev_start - 1;
+    if (sft != 0 && prev_len > 0) bsw_realign<G, K>(ph, pe, sft, rowbuf, lb, gi, gmask);
+    const int32_t lo = -sft, hi = prev_len - sft;  // valid previous cells: lo <= idx < hi
+    const int32_t up_h1 = __shfl_down_sync(gmask, ph[0], 1, G);
+    const int32_t up_e1 = __shfl_down_sync(gmask, pe[0], 1, G);
 
     int32_t hm[K], e[K], gv[K];
     uint32_t eext = 0;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const int32_t idx = (int32_t)g * K + k;
+      const int32_t idx = base_idx + k;
       const bool act = idx < row_len;
-      const int32_t j = js + idx;
-      const uint32_t rb = act ? ldb(wn, (uint64_t)(j - 1)) : 0x100u;
+      const uint32_t rb = act ? ldb(wn, (uint64_t)(js - 1 + idx)) : 0x100u;
       const int32_t s = (qb == rb) ? match : -mism;
-      const int32_t pd = idx + d - 1;
-      const int32_t hdiag = (pd >= 0 && pd < prev_len) ? pH[pd] : 0;
+      const int32_t hdiag = (idx >= lo && idx < hi) ? ph[k] : 0;
       hm[k] = hdiag + s;
-      const int32_t pu = pd + 1;
-      const bool up = pu >= 0 && pu < prev_len;
-      const int32_t efh = up ? pH[pu] - gof : kNeg4;
-      const int32_t efe = up ? pE[pu] - ge : kNeg4;
+      const bool up = idx + 1 >= lo && idx + 1 < hi;
+      const int32_t uh = k + 1 < K ? ph[k + 1 < K ? k + 1 : 0] : up_h1;
+      const int32_t ue = k + 1 < K ? pe[k + 1 < K ? k + 1 : 0] : up_e1;
+      const int32_t efh = up ? uh - gof : kNeg4;
+      const int32_t efe = up ? ue - ge : kNeg4;
       e[k] = max(efh, efe);
       eext |= (efe > efh ? 1u : 0u) << k;
       const int32_t hs = max(max(hm[k], e[k]), 0);
@@ -144,23 +181,23 @@ __device__ __forceinline__ void bsw_group_sweep(
     for (int k = 0; k < K; ++k) {
       const int32_t idx = (int32_t)g * K + k;
       const bool act = idx < row_len;
-      const int32_t ph = k ? h[k - 1] : left_h;
-      const int32_t pf = k ? f[k - 1] : left_f;
-      const bool fext = idx >= 1 && (pf - ge) > (ph - gof);
+      const int32_t lh = k ? h[k - 1] : left_h;
+      const int32_t lf = k ? f[k - 1] : left_f;
+      const bool fext = idx >= 1 && (lf - ge) > (lh - gof);
       nib[k] = act ? (dir[k] | (((eext >> k) & 1u) << 2) | (fext ? 8u : 0u)) : 0u;
       if (act) {
         const uint32_t kk = ((uint32_t)h[k] << kKeyIdxBits) | (uint32_t)(1023 - idx);
         key = max(key, kk);
-        rowH[cur][idx] = h[k];
-        rowE[cur][idx] = e[k];
       }
+      ph[k] = h[k];
+      pe[k] = e[k];
     }
     uint8_t* trow = trace + (size_t)i * S + (size_t)g * LB;
 #pragma unroll
     for (int b = 0; b < LB; ++b) {
-      const uint32_t lo = nib[2 * b];
-      const uint32_t hi = (2 * b + 1 < K) ? nib[(2 * b + 1) < K ? 2 * b + 1 : 0] : 0u;
-      trow[b] = (uint8_t)(lo | (hi << 4));
+      const uint32_t n0 = nib[2 * b];
+      const uint32_t n1 = (2 * b + 1 < K) ? nib[(2 * b + 1) < K ? 2 * b + 1 : 0] : 0u;
+      trow[b] = (uint8_t)(n0 | (n1 << 4));
     }
     if (g == 0) meta[i] = ((uint32_t)js << 11) | (uint32_t)row_len;
 #pragma unroll
@@ -179,7 +216,6 @@ __device__ __forceinline__ void bsw_group_sweep(
     }
     prev_start = js;
     prev_len = row_len;
-    cur ^= 1;
     if (sp.adaptive) {  // mod.rs:1546-1559
       const int32_t raw = row_best_j >= 0 ? row_best_j + 1 : acenter + 1;
       const int32_t sn = i + 1 + offset;

@@ -26,6 +26,8 @@ struct DevPairs {
   const int32_t* band_offset;  // may be null
   const int32_t* abort_score;  // may be null
   const int32_t* bandwidth;    // may be null
+  const uint4* read_planes;    // planes of read_seq (sieve / Myers stages)
+  const uint4* win_planes;     // planes of win_seq
 };
 
 // Banded SW parameters resolved on the host.

@@ -40,6 +40,7 @@ struct MyersLaunch {
   int32_t k;                  // per_pair_k: k < 0 -> router bound per read
   int32_t per_pair_k;
   uint32_t tw;                // text plane words per pair in shared memory
+  uint32_t lmax;              // Peq limbs reserved per lane in shared memory
   int32_t cascade;
   // direct outputs
   int32_t* dist;
@@ -91,7 +92,11 @@ extern const int kNumBswShapes;
 
 cudaError_t launch_sieve_dropin(const SieveJobsDev& J, kira_sieve_result* out, int sms,
                                 cudaStream_t st);
-cudaError_t launch_verify_sieve(const DevPairs& P, const VerifyDev& V, int sms, cudaStream_t st);
+cudaError_t launch_pack_planes(const uint8_t* seq, uint64_t len, uint4* out, uint64_t nblocks,
+                               int sms, cudaStream_t st);
+inline uint64_t plane_blocks(uint64_t len) { return (len + 31) / 32 + 4; }
+cudaError_t launch_verify_sieve(const DevPairs& P, const VerifyDev& V, uint32_t max_q, int sms,
+                                cudaStream_t st);
 cudaError_t launch_myers(const DevPairs& P, const MyersLaunch& M, uint32_t max_items, int sms,
                          cudaStream_t st);
 cudaError_t launch_bsw(int shape, const DevPairs& P, const BswLaunch& B, uint32_t max_items,

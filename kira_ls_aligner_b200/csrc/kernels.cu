@@ -4,6 +4,7 @@
 #include "bsw.cuh"
 #include "internal.h"
 #include "myers.cuh"
+#include "planes.cuh"
 #include "sieve.cuh"
 
 namespace kira {
@@ -39,6 +40,34 @@ __global__ void __launch_bounds__(256) sieve_dropin_kernel(SieveJobsDev J,
       }
       out[p] = r;
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Plane packing: one warp builds 32 plane blocks (1 KB of bases); lane i loads
+// byte 32*i + lane of the warp's span at step i (coalesced) and __ballot_sync
+// collects the bits of block i, which lane i stores.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) pack_planes_kernel(const uint8_t* __restrict__ seq,
+                                                          uint64_t len, uint4* __restrict__ out,
+                                                          uint64_t nblocks) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t wb = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+       wb * 32u < nblocks; wb += nwarps) {
+    const uint64_t base = wb * 1024u;
+    uint4 mine = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll 4
+    for (uint32_t i = 0; i < 32u; ++i) {
+      const uint64_t p = base + (uint64_t)i * 32u + lane;
+      const uint32_t c = p < len ? base_code(ldb(seq, p)) : 0u;
+      const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, c & 1u);
+      const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, c & 2u);
+      const uint32_t bv = __ballot_sync(0xFFFFFFFFu, c & 4u);
+      if (lane == i) mine = make_uint4(b0, b1, bv, 0u);
+    }
+    const uint64_t blk = wb * 32u + lane;
+    if (blk < nblocks) out[blk] = mine;
   }
 }
 
@@ -96,6 +125,51 @@ __device__ bool warp_certify(const uint8_t* read, const uint8_t* ref, uint32_t l
   return true;
 }
 
+// spectral_hit_is_certified (src/alignment/mod.rs:688-762) for one lane's pair.
+__device__ __forceinline__ uint32_t lane_bounded_hamming(const uint8_t* a, const uint8_t* b,
+                                                         uint32_t len, uint32_t limit) {
+  uint32_t m = 0;
+  for (uint32_t i = 0; i < len; ++i) {
+    m += ldb(a, i) != ldb(b, i) ? 1u : 0u;
+    if (m > limit) break;
+  }
+  return m;
+}
+
+__device__ bool lane_certify(const uint8_t* read, const uint8_t* ref, uint32_t len, uint32_t mism,
+                             uint32_t second, uint32_t max_mism, bool strict) {
+  if (mism > max_mism) return false;
+  if (second != 0xFFFFFFFFu && second <= mism + 1u) return false;
+  if (mism == 0) return true;
+  if (mism > 2) return false;
+  uint32_t n = 0, pos0 = 0xFFFFFFFFu, pos1 = 0xFFFFFFFFu;
+  for (uint32_t i = 0; i < len; ++i) {
+    if (ldb(read, i) != ldb(ref, i)) {
+      if (n == 0) pos0 = i;
+      else if (n == 1) pos1 = i;
+      ++n;
+      if (n > mism) break;  // decided: n != mism
+    }
+  }
+  if (n != mism) return false;
+  const uint32_t edge = min(len, 8u);
+  if (pos0 < edge || pos0 + edge >= len) return false;
+  if (n == 2 && (pos1 < edge || pos1 + edge >= len)) return false;
+  if (n == 2 && (pos1 > pos0 ? pos1 - pos0 : 0u) <= 4u) return false;
+  const uint32_t p = pos0;
+  const uint32_t suffix = len > p + 1u ? len - (p + 1u) : 0u;
+  const uint32_t min_suffix = strict ? 4u : 8u;
+  if (suffix >= min_suffix) {
+    if (lane_bounded_hamming(read + p + 1, ref + p, len - p - 1u, 1u) <= 1u) return false;
+    if (lane_bounded_hamming(read + p, ref + p + 1, len - p - 1u, 1u) <= 1u) return false;
+    if (strict && suffix >= 6u) {
+      if (lane_bounded_hamming(read + p + 2, ref + p, len - p - 2u, 1u) <= 1u) return false;
+      if (lane_bounded_hamming(read + p, ref + p + 2, len - p - 2u, 1u) <= 1u) return false;
+    }
+  }
+  return true;
+}
+
 __device__ __forceinline__ uint32_t sieve_threshold_for(int32_t thr, uint32_t q) {
   // router::spectral_max_mismatches (src/alignment/router.rs:191-195), defaults 3 % / 2.
   return thr < 0 ? max((q * 3u) / 100u, 2u) : (uint32_t)thr;
@@ -106,27 +180,30 @@ __device__ __forceinline__ uint32_t myers_k_for(int32_t k, uint32_t q) {
   return k < 0 ? (q * 15u) / 100u + 4u : (uint32_t)k;
 }
 
-// Stage 1 of the composed path: sieve + certificate, one warp per pair.
+// Stage 1 of the composed path: sieve + certificate, one lane per pair.
+template <int RWMAX>
 __global__ void __launch_bounds__(256) verify_sieve_kernel(DevPairs P, VerifyDev V) {
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); p < P.n; p += warps) {
-    const uint32_t q = P.read_len[p], w = P.win_len[p];
-    const uint8_t* rd = P.read_seq + P.read_off[p];
-    const uint8_t* wn = P.win_seq + P.win_off[p];
-    auto rcode = [&](uint32_t pos) { return base_code(ldb(rd, pos)); };
-    auto wcode = [&](uint32_t pos) { return base_code(ldb(wn, pos)); };
-    const SieveOut so = sieve_warp<16>(q, w, rcode, wcode, true);
-    const uint32_t thr = sieve_threshold_for(V.sieve_threshold, q);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < P.n; base += stride) {
+    const uint32_t p = base + threadIdx.x;
+    const bool valid = p < P.n;
     bool cert = false;
-    if (so.hit && so.mism <= thr)
-      cert = warp_certify(rd, wn + so.shift, q, so.mism, so.second, thr, V.cert_strict != 0, lane);
-    if (lane == 0) {
+    LaneSieve so{false, 0, 0, 0xFFFFFFFFu};
+    uint32_t q = 0;
+    if (valid) {
+      q = P.read_len[p];
+      const uint32_t w = P.win_len[p];
+      so = sieve_lane<RWMAX>(P.read_planes, P.read_off[p], q, P.win_planes, P.win_off[p], w);
+      const uint32_t thr = sieve_threshold_for(V.sieve_threshold, q);
+      if (so.hit && so.mism <= thr)
+        cert = lane_certify(P.read_seq + P.read_off[p], P.win_seq + P.win_off[p] + so.shift, q,
+                            so.mism, so.second, thr, V.cert_strict != 0);
       if (V.detail) {
         kira_verify_detail dt;
         dt.sieve_shift = so.hit ? (int32_t)so.shift : -1;
         dt.sieve_mism = so.hit ? (int32_t)so.mism : INT32_MAX;
-        dt.sieve_second = so.hit && so.second != kNoKey ? (int32_t)so.second : INT32_MAX;
+        dt.sieve_second = so.hit && so.second != 0xFFFFFFFFu ? (int32_t)so.second : INT32_MAX;
         dt.myers_dist = -1;
         dt.myers_end = -1;
         V.detail[p] = dt;
@@ -147,10 +224,14 @@ __global__ void __launch_bounds__(256) verify_sieve_kernel(DevPairs P, VerifyDev
         V.ncig[p] = 1;
       } else {
         V.sw_offset[p] = so.hit ? (int32_t)so.shift : 0;
-        const uint32_t slot = atomicAdd(V.counters + 0, 1u);
-        V.myers_list[slot] = p;
       }
     }
+    // Warp-aggregated append of the uncertified pairs to the Myers list.
+    const uint32_t need = __ballot_sync(0xFFFFFFFFu, valid && !cert);
+    uint32_t slot0 = 0;
+    if (lane == 0 && need) slot0 = atomicAdd(V.counters + 0, (uint32_t)__popc(need));
+    slot0 = __shfl_sync(0xFFFFFFFFu, slot0, 0);
+    if (valid && !cert) V.myers_list[slot0 + __popc(need & ((1u << lane) - 1u))] = p;
   }
 }
 
@@ -164,24 +245,19 @@ __device__ void myers_warp(const DevPairs& P, const MyersLaunch& M, uint32_t bas
   const uint32_t item = base + lane;
   const bool valid = item < count;
   const uint32_t pair = valid ? (M.list ? M.list[item] : item) : 0u;
-  MyersPeq<L> peq;
-#pragma unroll
-  for (int k = 0; k < L; ++k) peq.a[k] = peq.c[k] = peq.g[k] = peq.t[k] = 0u;
-  for (uint32_t s = 0; s < 32u; ++s) {
-    const uint32_t pv = __shfl_sync(0xFFFFFFFFu, valid ? 1u : 0u, s);
-    if (!pv) continue;
-    const uint32_t pp = __shfl_sync(0xFFFFFFFFu, pair, s);
-    const uint32_t m = P.read_len[pp], n = P.win_len[pp];
-    myers_load_pattern<L>(P.read_seq + P.read_off[pp], m, s, lane, peq);
-    myers_load_text(P.win_seq + P.win_off[pp], n, s, lane, sm);
-  }
+  const uint32_t m = valid ? P.read_len[pair] : 0u;
+  if (valid) myers_build_peq<L>(P.read_planes, P.read_off[pair], m, lane, sm);
   __syncwarp();
   uint32_t dist = 0, endp = 0;
   bool hit = false;
+  const bool uniform = __all_sync(0xFFFFFFFFu, !valid || (m + 31u) / 32u == (uint32_t)L);
   if (valid) {
-    const uint32_t m = P.read_len[pair], n = P.win_len[pair];
+    const uint32_t n = P.win_len[pair];
     const uint32_t k = M.per_pair_k ? myers_k_for(M.k, m) : (uint32_t)M.k;
-    hit = myers_lane<L>(peq, m, n, k, sm.planes + (size_t)lane * sm.tw * 3u, dist, endp);
+    hit = uniform ? myers_lane<L, true>(m, n, k, sm, P.win_planes, P.win_off[pair], lane, dist,
+                                        endp)
+                  : myers_lane<L, false>(m, n, k, sm, P.win_planes, P.win_off[pair], lane, dist,
+                                         endp);
   }
   __syncwarp();
   if (M.cascade) {
@@ -217,11 +293,12 @@ __device__ void myers_warp(const DevPairs& P, const MyersLaunch& M, uint32_t bas
   }
 }
 
+template <int LMAX>
 __global__ void __launch_bounds__(128) myers_kernel(DevPairs P, MyersLaunch M) {
   extern __shared__ uint32_t myers_smem[];
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp_in_block = threadIdx.x >> 5;
-  MyersSmem sm{myers_smem + (size_t)warp_in_block * 32u * M.tw * 3u, M.tw};
+  MyersSmem sm{myers_smem + (size_t)warp_in_block * M.lmax * 160u};
   const uint32_t count = M.count_dev ? *M.count_dev : M.count;
   const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
   for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp_in_block) * 32u; base < count;
@@ -234,10 +311,12 @@ __global__ void __launch_bounds__(128) myers_kernel(DevPairs P, MyersLaunch M) {
     for (int off = 16; off > 0; off >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, off));
     const uint32_t limbs = max((mx + 31u) / 32u, 1u);
     switch (limbs) {
-#define KIRA_MYERS_CASE(n) \
-  case n:                  \
-    myers_warp<n>(P, M, base, count, sm); \
-    break;
+#define KIRA_MYERS_CASE(n)                                     \
+  case n:                                                      \
+    if (n <= LMAX) {                                           \
+      myers_warp<(n <= LMAX ? n : 1)>(P, M, base, count, sm);  \
+      break;                                                   \
+    }
       KIRA_MYERS_CASE(1) KIRA_MYERS_CASE(2) KIRA_MYERS_CASE(3) KIRA_MYERS_CASE(4)
       KIRA_MYERS_CASE(5) KIRA_MYERS_CASE(6) KIRA_MYERS_CASE(7) KIRA_MYERS_CASE(8)
       KIRA_MYERS_CASE(9) KIRA_MYERS_CASE(10) KIRA_MYERS_CASE(11) KIRA_MYERS_CASE(12)
@@ -277,7 +356,7 @@ __global__ void __launch_bounds__(256) bsw_dp_kernel(DevPairs P, BswLaunch B) {
   const uint32_t gmask = (G == 32) ? 0xFFFFFFFFu : (((1u << G) - 1u) << (gw * G));
   const uint32_t groups_per_block = blockDim.x / G;
   const uint32_t group_in_block = threadIdx.x / G;
-  int32_t* rowbuf = bsw_smem + (size_t)group_in_block * 4u * CAP;
+  int32_t* rowbuf = bsw_smem + (size_t)(threadIdx.x >> 5) * 4u * K * 32u;  // per warp
   const uint32_t count = B.count_dev ? *B.count_dev : B.count;
   const uint32_t ngroups = gridDim.x * groups_per_block;
   for (uint32_t item = blockIdx.x * groups_per_block + group_in_block; item < count;
@@ -297,7 +376,7 @@ __global__ void __launch_bounds__(256) bsw_dp_kernel(DevPairs P, BswLaunch B) {
       continue;
     }
     bsw_group_sweep<G, K>(P.read_seq + P.read_off[pair], q, P.win_seq + P.win_off[pair], w, band,
-                          offset, abort_score, B.sp, rowbuf,
+                          offset, abort_score, B.sp, rowbuf, gw * G,
                           B.tg.trace + (size_t)item * B.tg.slot_bytes,
                           B.tg.meta + (size_t)item * B.tg.meta_stride, g, gmask, end, cells);
     if (g == 0) {
@@ -459,22 +538,31 @@ cudaError_t launch_sieve_dropin(const SieveJobsDev& J, kira_sieve_result* out, i
   return cudaGetLastError();
 }
 
-cudaError_t launch_verify_sieve(const DevPairs& P, const VerifyDev& V, int sms, cudaStream_t st) {
-  const int blocks = grid_for(P.n, 8, sms * 16);
-  verify_sieve_kernel<<<blocks, 256, 0, st>>>(P, V);
+cudaError_t launch_pack_planes(const uint8_t* seq, uint64_t len, uint4* out, uint64_t nblocks,
+                               int sms, cudaStream_t st) {
+  const int blocks = grid_for((nblocks + 31) / 32, 8, sms * 16);
+  pack_planes_kernel<<<blocks, 256, 0, st>>>(seq, len, out, nblocks);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_verify_sieve(const DevPairs& P, const VerifyDev& V, uint32_t max_q, int sms,
+                                cudaStream_t st) {
+  const int blocks = grid_for(P.n, 256, sms * 8);
+  const uint32_t rw = (max_q + 31) / 32;
+  if (rw <= 5) verify_sieve_kernel<5><<<blocks, 256, 0, st>>>(P, V);
+  else if (rw <= 8) verify_sieve_kernel<8><<<blocks, 256, 0, st>>>(P, V);
+  else verify_sieve_kernel<16><<<blocks, 256, 0, st>>>(P, V);
   return cudaGetLastError();
 }
 
 cudaError_t launch_myers(const DevPairs& P, const MyersLaunch& M, uint32_t max_items, int sms,
                          cudaStream_t st) {
-  const size_t smem = (size_t)4 * 32 * M.tw * 3 * sizeof(uint32_t);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(myers_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
+  const size_t smem = (size_t)4 * M.lmax * 160 * sizeof(uint32_t);
   const int blocks = grid_for(max_items, 128, sms * 8);
-  myers_kernel<<<blocks, 128, smem, st>>>(P, M);
+  if (M.lmax <= 5) myers_kernel<5><<<blocks, 128, smem, st>>>(P, M);
+  else if (M.lmax <= 8) myers_kernel<8><<<blocks, 128, smem, st>>>(P, M);
+  else if (M.lmax <= 12) myers_kernel<12><<<blocks, 128, smem, st>>>(P, M);
+  else myers_kernel<16><<<blocks, 128, smem, st>>>(P, M);
   return cudaGetLastError();
 }
 
@@ -482,7 +570,7 @@ template <int G, int K>
 static cudaError_t launch_bsw_shape(const DevPairs& P, const BswLaunch& B, uint32_t max_items,
                                     int sms, cudaStream_t st, cudaEvent_t between) {
   constexpr int threads = 256;
-  const size_t smem = (size_t)(threads / G) * 4 * G * K * sizeof(int32_t);
+  const size_t smem = (size_t)(threads / 32) * 4 * K * 32 * sizeof(int32_t);
   cudaFuncSetAttribute(bsw_dp_kernel<G, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)smem);
   int per_sm = 0;

@@ -9,74 +9,55 @@
 //
 // B200 mapping: the bit vector is held as L 32-bit limbs in registers (the
 // reference uses 64-bit blocks; bits below m never depend on bits above m, so
-// the limb width does not change any result). A warp owns 32 pairs. Global
-// loads stay coalesced: for each pair the whole warp loads 32 consecutive bytes
-// and __ballot_sync turns them into the owning lane's Peq words (pattern) or
-// into three text planes (code bit 0, code bit 1, ACGT-valid) kept in shared
-// memory, so each lane's column loop reads one shared word per 32 columns.
+// the limb width does not change any result). One lane per pair:
+//   * pattern and text come from the 2-bit + valid plane arenas (planes.cuh):
+//     one 32-base word is two 16-byte loads and a funnel shift, no cross-lane work;
+//   * Peq lives in shared memory as [k][code][lane] with code 4 = "matches
+//     nothing" (all zero), so every per-lane read is bank-conflict-free.
+//   * Per column and limb: one LDS for Eq (instead of a 4-way select), the
+//     (Eq & VP) + VP carry chain on the PTX carry flag (add.cc / addc), and one
+//     funnel shift for each of the HP / HN shifts across limbs.
 #pragma once
 
+#include "addchain.cuh"
 #include "common.cuh"
+#include "planes.cuh"
 
 namespace kira {
 
-// Shared-memory text planes of one warp: [32 pairs][tw words][3].
+// Shared memory of one warp: Peq[k][code][lane], code 4 = "matches nothing".
 struct MyersSmem {
-  uint32_t* planes;
-  uint32_t tw;  // words per pair (ceil(max window / 32))
+  uint32_t* peq;  // [L][5][32]
 };
 
+// Builds this lane's Peq columns from the pattern's plane words (no cross-lane
+// work): eq_A = ~b1 & ~b0 & valid, ... for the bases below m.
 template <int L>
-struct MyersPeq {
-  uint32_t a[L], c[L], g[L], t[L];
-};
-
-// Loads pair p's pattern into lane p's Peq (all lanes participate).
-template <int L>
-__device__ __forceinline__ void myers_load_pattern(const uint8_t* pat, uint32_t m, uint32_t p,
-                                                   uint32_t lane, MyersPeq<L>& peq) {
+__device__ __forceinline__ void myers_build_peq(const uint4* __restrict__ planes, uint64_t pos,
+                                                uint32_t m, uint32_t lane, MyersSmem sm) {
 #pragma unroll
   for (int k = 0; k < L; ++k) {
-    const uint32_t pos = (uint32_t)k * 32u + lane;
-    const uint32_t code = pos < m ? base_code(ldb(pat, pos)) : 0u;
-    const uint32_t ba = __ballot_sync(0xFFFFFFFFu, code == 4u);
-    const uint32_t bc = __ballot_sync(0xFFFFFFFFu, code == 5u);
-    const uint32_t bg = __ballot_sync(0xFFFFFFFFu, code == 6u);
-    const uint32_t bt = __ballot_sync(0xFFFFFFFFu, code == 7u);
-    if (lane == p) {
-      peq.a[k] = ba;
-      peq.c[k] = bc;
-      peq.g[k] = bg;
-      peq.t[k] = bt;
-    }
-  }
-}
-
-// Converts pair p's text into planes in shared memory (all lanes participate).
-__device__ __forceinline__ void myers_load_text(const uint8_t* text, uint32_t n, uint32_t p,
-                                                uint32_t lane, MyersSmem sm) {
-  const uint32_t words = (n + 31u) / 32u;
-  uint32_t* dst = sm.planes + (size_t)p * sm.tw * 3u;
-  for (uint32_t x = 0; x < words; ++x) {
-    const uint32_t pos = x * 32u + lane;
-    const uint32_t code = pos < n ? base_code(ldb(text, pos)) : 0u;
-    const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, code & 1u);
-    const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, code & 2u);
-    const uint32_t bv = __ballot_sync(0xFFFFFFFFu, code & 4u);
-    if (lane == 0) {
-      dst[3 * x + 0] = b0;
-      dst[3 * x + 1] = b1;
-      dst[3 * x + 2] = bv;
-    }
+    const PlaneWord pw = plane_word_at(planes, pos + 32u * k);
+    const uint32_t base = 32u * (uint32_t)k;
+    const uint32_t lm = base < m ? low_mask(m - base) : 0u;
+    const uint32_t v = pw.v & lm;
+    uint32_t* col = sm.peq + (uint32_t)k * 160u + lane;
+    col[0] = ~pw.b1 & ~pw.b0 & v;
+    col[32] = ~pw.b1 & pw.b0 & v;
+    col[64] = pw.b1 & ~pw.b0 & v;
+    col[96] = pw.b1 & pw.b0 & v;
+    col[128] = 0u;
   }
 }
 
 // Runs the recurrence for this lane's pair. Returns true with (dist, end) on a
-// hit <= max_k. L >= ceil(m / 32); limbs above the pattern stay masked to zero.
-template <int L>
-__device__ __forceinline__ bool myers_lane(const MyersPeq<L>& peq, uint32_t m, uint32_t n,
-                                           uint32_t max_k, const uint32_t* planes,
-                                           uint32_t& dist, uint32_t& end_pos) {
+// hit <= max_k. UNIFORM: every lane of the warp has ceil(m / 32) == L (no limb
+// masks below the top limb). Otherwise limbs above the pattern stay masked to 0.
+template <int L, bool UNIFORM>
+__device__ __forceinline__ bool myers_lane(uint32_t m, uint32_t n, uint32_t max_k,
+                                           MyersSmem sm, const uint4* __restrict__ tplanes,
+                                           uint64_t tpos, uint32_t lane, uint32_t& dist,
+                                           uint32_t& end_pos) {
   if (m == 0) {  // myers.rs:50-54
     dist = 0;
     end_pos = 0;
@@ -94,47 +75,59 @@ __device__ __forceinline__ bool myers_lane(const MyersPeq<L>& peq, uint32_t m, u
   uint32_t vp[L], vn[L], lm[L];
 #pragma unroll
   for (int k = 0; k < L; ++k) {
-    lm[k] = (uint32_t)k + 1u < nl ? 0xFFFFFFFFu : ((uint32_t)k + 1u == nl ? top_mask : 0u);
+    if (UNIFORM)
+      lm[k] = k + 1 < L ? 0xFFFFFFFFu : top_mask;
+    else
+      lm[k] = (uint32_t)k + 1u < nl ? 0xFFFFFFFFu : ((uint32_t)k + 1u == nl ? top_mask : 0u);
     vp[k] = lm[k];
     vn[k] = 0u;
   }
+  const uint32_t* peq = sm.peq + lane;
   uint32_t err = m, best = m, pos = 0;
   uint32_t t0 = 0, t1 = 0, tv = 0;
   for (uint32_t j = 0; j < n; ++j) {
     const uint32_t bit = j & 31u;
     if (bit == 0u) {
-      const uint32_t x = j >> 5;
-      t0 = planes[3 * x + 0];
-      t1 = planes[3 * x + 1];
-      tv = planes[3 * x + 2];
+      const PlaneWord pw = plane_word_at(tplanes, tpos + j);
+      t0 = pw.b0;
+      t1 = pw.b1;
+      tv = pw.v;
     }
-    const bool c0 = (t0 >> bit) & 1u, c1 = (t1 >> bit) & 1u, v = (tv >> bit) & 1u;
-    uint32_t carry = 0, hin_p = 0, hin_n = 0, hp_top = 0, hn_top = 0;
+    const uint32_t code = ((tv >> bit) & 1u) ? (((t0 >> bit) & 1u) | (((t1 >> bit) & 1u) << 1))
+                                             : 4u;
+    const uint32_t* pc = peq + code * 32u;
+    uint32_t eq[L], av[L], sum[L];
 #pragma unroll
     for (int k = 0; k < L; ++k) {
-      uint32_t eq = c1 ? (c0 ? peq.t[k] : peq.g[k]) : (c0 ? peq.c[k] : peq.a[k]);
-      eq = v ? eq : 0u;
+      eq[k] = pc[k * 160];
+      av[k] = eq[k] & vp[k];
+    }
+    add_chain<L>(av, vp, sum);
+    uint32_t hp_prev = 0, hn_prev = 0, hp_top = 0, hn_top = 0;
+#pragma unroll
+    for (int k = 0; k < L; ++k) {
       const uint32_t vpk = vp[k], vnk = vn[k];
-      const uint32_t x = eq | vnk;
-      const uint64_t s = (uint64_t)(eq & vpk) + (uint64_t)vpk + (uint64_t)carry;
-      const uint32_t sum = (uint32_t)s;
-      carry = (uint32_t)(s >> 32);
-      const uint32_t d0 = (sum ^ vpk) | x;
+      const uint32_t d0 = (sum[k] ^ vpk) | eq[k] | vnk;
       const uint32_t hp = vnk | ~(d0 | vpk);
       const uint32_t hn = d0 & vpk;
-      const uint32_t hps = (hp << 1) | hin_p;
-      const uint32_t hns = (hn << 1) | hin_n;
-      hin_p = hp >> 31;
-      hin_n = hn >> 31;
+      const uint32_t hps = k ? __funnelshift_l(hp_prev, hp, 1) : (hp << 1);
+      const uint32_t hns = k ? __funnelshift_l(hn_prev, hn, 1) : (hn << 1);
+      hp_prev = hp;
+      hn_prev = hn;
       vp[k] = (hns | ~(d0 | hps)) & lm[k];
       vn[k] = (d0 & hps) & lm[k];
-      if ((uint32_t)k + 1u == nl) {
+      if (UNIFORM) {
+        if (k == L - 1) {
+          hp_top = hp;
+          hn_top = hn;
+        }
+      } else if ((uint32_t)k + 1u == nl) {
         hp_top = hp;
         hn_top = hn;
       }
     }
-    if (hp_top & high) err += 1u;
-    if (hn_top & high) err -= 1u;
+    err += (hp_top & high) ? 1u : 0u;
+    err -= (hn_top & high) ? 1u : 0u;
     if (err <= best) {
       best = err;
       pos = j + 1u;

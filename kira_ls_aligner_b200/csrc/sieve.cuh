@@ -56,34 +56,44 @@ __device__ __forceinline__ SieveOut sieve_warp_rw(uint32_t q, uint32_t w, ReadCo
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t rw = RW;
   uint32_t r0[RWMAX], r1[RWMAX];
+  uint32_t w0[RWMAX + 1], w1[RWMAX + 1];
   uint32_t bad = 0;
+  // Issue every byte load of the read and of the first window words before the
+  // ballots, so the pair pays one memory latency instead of one per word.
+  uint32_t rc[RWMAX], wc[RWMAX + 1];
 #pragma unroll
   for (int k = 0; k < RWMAX; ++k) {
-    r0[k] = 0;
-    r1[k] = 0;
-    if ((uint32_t)k < rw) {
-      uint32_t b;
-      plane_word(rcode, (uint32_t)k, q, lane, r0[k], r1[k], b);
-      bad |= b;
-    }
+    const uint32_t pos = (uint32_t)k * 32u + lane;
+    rc[k] = pos < q ? rcode(pos) : 4u;
+  }
+#pragma unroll
+  for (int k = 0; k <= RWMAX; ++k) {
+    const uint32_t pos = (uint32_t)k * 32u + lane;
+    wc[k] = pos < w ? wcode(pos) : 4u;
+  }
+#pragma unroll
+  for (int k = 0; k < RWMAX; ++k) {
+    r0[k] = __ballot_sync(0xFFFFFFFFu, rc[k] & 1u);
+    r1[k] = __ballot_sync(0xFFFFFFFFu, rc[k] & 2u);
+    bad |= __ballot_sync(0xFFFFFFFFu, !(rc[k] & 4u));
+  }
+#pragma unroll
+  for (int k = 0; k <= RWMAX; ++k) {
+    w0[k] = __ballot_sync(0xFFFFFFFFu, wc[k] & 1u);
+    w1[k] = __ballot_sync(0xFFFFFFFFu, wc[k] & 2u);
+    bad |= __ballot_sync(0xFFFFFFFFu, !(wc[k] & 4u));
   }
   const uint32_t tail = q & 31u;
   const uint32_t tail_mask = tail ? ((1u << tail) - 1u) : 0xFFFFFFFFu;
-  // Sliding window plane words w0[0..rw], w1[0..rw] for shift block r.
-  uint32_t w0[RWMAX + 1], w1[RWMAX + 1];
-#pragma unroll
-  for (int k = 0; k <= RWMAX; ++k) {
-    w0[k] = 0;
-    w1[k] = 0;
-    if ((uint32_t)k <= rw) {
-      uint32_t b;
-      plane_word(wcode, (uint32_t)k, w, lane, w0[k], w1[k], b);
-      bad |= b;
-    }
-  }
   const uint32_t n_shifts = w - q + 1u;
   const uint32_t blocks = (n_shifts + 31u) / 32u;
   uint32_t best = kNoKey, second = kNoKey;
+  // Code of the window word needed by the next slide, loaded one block ahead.
+  uint32_t next_c = 4u;
+  {
+    const uint32_t pos = (1u + rw) * 32u + lane;
+    if (blocks > 1u) next_c = pos < w ? wcode(pos) : 4u;
+  }
   for (uint32_t r = 0; r < blocks; ++r) {
     const uint32_t t = r * 32u + lane;
     uint32_t mism = 0;
@@ -114,9 +124,13 @@ __device__ __forceinline__ SieveOut sieve_warp_rw(uint32_t q, uint32_t w, ReadCo
           w1[k] = w1[k + 1];
         }
       }
-      uint32_t n0, n1, b;
-      plane_word(wcode, r + 1u + rw, w, lane, n0, n1, b);
-      bad |= b;
+      const uint32_t n0 = __ballot_sync(0xFFFFFFFFu, next_c & 1u);
+      const uint32_t n1 = __ballot_sync(0xFFFFFFFFu, next_c & 2u);
+      bad |= __ballot_sync(0xFFFFFFFFu, !(next_c & 4u));
+      if (r + 2u < blocks) {
+        const uint32_t pos = (r + 2u + rw) * 32u + lane;
+        next_c = pos < w ? wcode(pos) : 4u;
+      }
 #pragma unroll
       for (int k = 0; k <= RWMAX; ++k)
         if ((uint32_t)k == rw) {
