@@ -229,6 +229,13 @@ def run_ours(args, rank, local, world, dist):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
+    from kira_ls_aligner_b200 import autotune
+
+    def run_sync():
+        step()
+        torch.cuda.synchronize(dev)
+    tuning = autotune.tune_bsw_shape(ctx, 33, run_sync,
+                                     device_name=torch.cuda.get_device_name(dev))
     L.kira_gpu_profile(ctx.handle, 1)
     stage_ms = np.zeros(len(_abi.STAGES))
     sampler = ClockSampler(local)
@@ -349,6 +356,7 @@ def run_ours(args, rank, local, world, dist):
                        "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"replicas x{world} (pairs sharded, no collective)"},
             "gcups": gcups, "cells_per_step": cells // args.steps,
+            "autotune": tuning,
             "status_counts": {"certified": statuses[1], "myers_reject": statuses[2],
                               "sw": statuses[3]},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,

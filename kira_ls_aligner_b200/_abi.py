@@ -29,6 +29,7 @@ EXPORTS = (
     "kira_gpu_arena_bytes", "kira_gpu_sieve_batch", "kira_gpu_ref_upload",
     "kira_gpu_myers_batch", "kira_gpu_bsw_batch", "kira_gpu_verify_batch",
     "kira_gpu_verify_dev", "kira_gpu_profile", "kira_gpu_stage_times",
+    "kira_gpu_bsw_shapes", "kira_gpu_set_bsw_shape",
 )
 STAGES = ("sieve_certify", "myers", "bsw_dp", "bsw_traceback", "cigar_compact")
 
@@ -109,6 +110,8 @@ def lib():
     L.kira_gpu_verify_dev.argtypes = [vp, C.POINTER(Pairs), C.POINTER(VerifyParams), vp, vp,
                                       C.c_uint64, vp, vp, vp, vp]
     L.kira_gpu_profile.argtypes = [vp, C.c_int]
+    L.kira_gpu_bsw_shapes.argtypes = [vp, vp, C.c_int]
+    L.kira_gpu_set_bsw_shape.argtypes = [vp, C.c_uint32, C.c_int]
     L.kira_gpu_stage_times.argtypes = [vp, C.POINTER(C.c_float), C.c_int]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype or C.c_int

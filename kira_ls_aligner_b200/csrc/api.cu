@@ -32,8 +32,15 @@ struct DevBuf {
 
 constexpr int kStages = 5;  // sieve+certificate, Myers, SW DP, SW traceback, CIGAR compaction
 
+constexpr int kBandClasses = 6;  // tuned-shape table: band <= 16, 33, 64, 128, 256, 511
+
+inline int band_class(uint32_t b) {
+  return b <= 16 ? 0 : b <= 33 ? 1 : b <= 64 ? 2 : b <= 128 ? 3 : b <= 256 ? 4 : 5;
+}
+
 struct kira_ctx {
   int device = 0;
+  int tuned_shape[kBandClasses] = {-1, -1, -1, -1, -1, -1};
   int sms = 148;
   cudaStream_t stream = nullptr;
   std::string last_error;
@@ -129,11 +136,16 @@ int check_sw_cfg(kira_ctx* ctx, const kira_sw_cfg& c, uint32_t max_q, uint32_t m
   return KIRA_OK;
 }
 
-int pick_shape(uint32_t max_band) {
+int default_shape(uint32_t max_band) {
   const int need = 2 * (int)std::max<uint32_t>(max_band, 1) + 1;
   for (int s = 0; s < kNumBswShapes; ++s)
     if (kBswShapes[s].g * kBswShapes[s].k >= need) return s;
   return -1;
+}
+
+bool shape_fits(int s, uint32_t max_band) {
+  return s >= 0 && s < kNumBswShapes &&
+         kBswShapes[s].g * kBswShapes[s].k >= 2 * (int)std::max<uint32_t>(max_band, 1) + 1;
 }
 
 struct Maxes {
@@ -220,12 +232,19 @@ int build_planes(kira_ctx* ctx, DevPairs& D, uint64_t read_bytes, uint64_t win_b
   return KIRA_OK;
 }
 
+// Launch shape of the banded SW stage: the tuned choice for the band class if it
+// covers the band, else the smallest shape that does.
+int pick_shape(const kira_ctx* ctx, uint32_t max_band) {
+  const int t = ctx->tuned_shape[band_class(max_band)];
+  return shape_fits(t, max_band) ? t : default_shape(max_band);
+}
+
 // Scratch of the banded SW stage for up to `items` items.
 int prepare_bsw(kira_ctx* ctx, uint32_t n_pairs, uint32_t items, const Maxes& mx, int shape,
                 BswLaunch& B) {
   cudaError_t cerr = cudaSuccess;
   const BswShapeInfo sh = kBswShapes[shape];
-  const uint32_t lane_bytes = (uint32_t)(sh.k + 1) / 2;
+  const uint32_t lane_bytes = 4u * (uint32_t)((sh.k + 7) / 8);
   const uint32_t row_stride = (uint32_t)sh.g * lane_bytes;
   const uint64_t slot = (((uint64_t)(mx.q + 1) * row_stride) + 15) & ~15ull;
   const uint32_t meta_stride = mx.q + 1;
@@ -274,7 +293,7 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
   int rc = check_sw_cfg(ctx, p.sw, mx.q, mx.band);
   if (rc) return rc;
   if (mx.q > 512) return fail(ctx, KIRA_ERR_READ_TOO_LONG, "read of %u bases > 512", mx.q);
-  const int shape = pick_shape(mx.band);
+  const int shape = pick_shape(ctx, mx.band);
   KIRA_DBUF(ncig, uint32_t, B_NCIG, n);
   KIRA_DBUF(swoff, int32_t, B_SW_OFFSET, n);
   KIRA_DBUF(mlist, uint32_t, B_MYERS_LIST, n);
@@ -448,6 +467,23 @@ int kira_gpu_sieve_batch(kira_ctx* ctx, const kira_sieve_job* jobs, uint32_t n,
   return KIRA_OK;
 }
 
+int kira_gpu_set_bsw_shape(kira_ctx* ctx, uint32_t band, int shape) {
+  if (!ctx) return KIRA_ERR_INVALID;
+  if (shape >= 0 && !shape_fits(shape, band))
+    return fail(ctx, KIRA_ERR_INVALID, "shape %d does not cover band %u", shape, band);
+  ctx->tuned_shape[band_class(band)] = shape;
+  return KIRA_OK;
+}
+
+int kira_gpu_bsw_shapes(int* lanes, int* cells, int max_shapes) {
+  const int n = std::min(max_shapes, kNumBswShapes);
+  for (int i = 0; i < n; ++i) {
+    if (lanes) lanes[i] = kBswShapes[i].g;
+    if (cells) cells[i] = kBswShapes[i].k;
+  }
+  return kNumBswShapes;
+}
+
 int kira_gpu_profile(kira_ctx* ctx, int enable) {
   if (!ctx) return KIRA_ERR_INVALID;
   cudaSetDevice(ctx->device);
@@ -548,7 +584,7 @@ int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg
   KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
   KIRA_CUDA(cudaMemsetAsync(counters, 0, 16, st));
   KIRA_CUDA(cudaMemsetAsync(cells_dev, 0, 8, st));
-  const int shape = pick_shape(mx.band);
+  const int shape = pick_shape(ctx, mx.band);
   BswLaunch B{};
   rc = prepare_bsw(ctx, n, n, mx, shape, B);
   if (rc) return rc;

@@ -15,7 +15,9 @@
 //        i.e. an exclusive prefix max of Hstar[k] - gof + k*ge, done in-lane over K
 //        cells and across lanes with log2(G) __shfl_up_sync steps;
 //     3. H, the direction with the reference priority diag >= E >= F, and the E/F
-//        extend flags (F flag from the left neighbour's final H and F);
+//        extend flags; f_from_f > f_from_h reduces to "the prefix max of G before
+//        cell idx-1 exceeds G[idx-1]" (and never holds when go == 0), so one
+//        in-lane running max serves F, H and the flag;
 //     4. row max and FIRST argmax with one packed key (h << 10 | 1023 - idx)
 //        reduced by __shfl_xor_sync; best / x-drop / abort / adaptive centre are
 //        then warp-uniform scalar updates.
@@ -31,8 +33,9 @@ namespace kira {
 
 template <int G, int K>
 struct BswShape {
-  static constexpr int kCap = G * K;             // cells per row
-  static constexpr int kLaneBytes = (K + 1) / 2;  // trace bytes per lane per row
+  static constexpr int kCap = G * K;                    // cells per row
+  static constexpr int kWords = (K + 7) / 8;            // trace words per lane per row
+  static constexpr int kLaneBytes = 4 * kWords;         // nibble k at byte k/2, half k&1
   static constexpr int kRowStride = G * kLaneBytes;
 };
 
@@ -74,6 +77,7 @@ __device__ __forceinline__ void bsw_group_sweep(
     int32_t band, int32_t offset, int32_t abort_score, const SwParams& sp, int32_t* rowbuf,
     uint32_t lb, uint8_t* __restrict__ trace, uint32_t* __restrict__ meta, uint32_t g,
     uint32_t gmask, DpEnd& out, uint64_t& cells_out) {
+  constexpr int NW = BswShape<G, K>::kWords;
   constexpr int LB = BswShape<G, K>::kLaneBytes;
   constexpr int S = BswShape<G, K>::kRowStride;
   constexpr int32_t NEGBIG = INT32_MIN / 2;
@@ -85,6 +89,7 @@ __device__ __forceinline__ void bsw_group_sweep(
   const int32_t drift = sp.adaptive ? sp.max_drift : 0;
   int32_t acenter = 1 + offset;
   const int32_t match = sp.match, mism = sp.mismatch, gof = sp.gof, ge = sp.gap_extend;
+  const int32_t go = sp.gap_open;
   const int32_t wl = (int32_t)w;
   const int32_t gi = (int32_t)g;
   const int32_t base_idx = gi * K;
@@ -116,93 +121,74 @@ __device__ __forceinline__ void bsw_group_sweep(
     const int32_t lo = -sft, hi = prev_len - sft;  // valid previous cells: lo <= idx < hi
     const int32_t up_h1 = __shfl_down_sync(gmask, ph[0], 1, G);
     const int32_t up_e1 = __shfl_down_sync(gmask, pe[0], 1, G);
+    const uint8_t* wrow = wn + (js - 1);
 
+    // Pass 1: H_diag + s, E (with its extend flag) and the F-scan operand
+    // G[idx] = max(Hdiag+s, E, 0) - gof + idx*ge.
     int32_t hm[K], e[K], gv[K];
     uint32_t eext = 0;
+    int32_t lane_max = NEGBIG;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int32_t idx = base_idx + k;
       const bool act = idx < row_len;
-      const uint32_t rb = act ? ldb(wn, (uint64_t)(js - 1 + idx)) : 0x100u;
+      const uint32_t rb = act ? __ldg(wrow + idx) : 0x100u;
       const int32_t s = (qb == rb) ? match : -mism;
-      const int32_t hdiag = (idx >= lo && idx < hi) ? ph[k] : 0;
-      hm[k] = hdiag + s;
-      const bool up = idx + 1 >= lo && idx + 1 < hi;
+      hm[k] = ((idx >= lo && idx < hi) ? ph[k] : 0) + s;
+      const bool uv = idx + 1 >= lo && idx + 1 < hi;
       const int32_t uh = k + 1 < K ? ph[k + 1 < K ? k + 1 : 0] : up_h1;
       const int32_t ue = k + 1 < K ? pe[k + 1 < K ? k + 1 : 0] : up_e1;
-      const int32_t efh = up ? uh - gof : kNeg4;
-      const int32_t efe = up ? ue - ge : kNeg4;
-      e[k] = max(efh, efe);
-      eext |= (efe > efh ? 1u : 0u) << k;
-      const int32_t hs = max(max(hm[k], e[k]), 0);
-      gv[k] = act ? hs - gof + idx * ge : NEGBIG;
+      // max(uh - gof, ue - ge) and e_from_e > e_from_h, with gof = go + ge.
+      e[k] = uv ? __viaddmax_s32(uh, -go, ue) - ge : kNeg4;
+      eext |= (uv && ue + go > uh ? 1u : 0u) << k;
+      gv[k] = __vimax_s32_relu(hm[k], e[k]) + (idx * ge - gof);
+      lane_max = max(lane_max, gv[k]);
     }
-    // Exclusive prefix max of gv over the row.
-    int32_t inc[K];
-    inc[0] = gv[0];
-#pragma unroll
-    for (int k = 1; k < K; ++k) inc[k] = max(inc[k - 1], gv[k]);
-    int32_t v = inc[K - 1];
+    // Cross-lane scan: excl = max of G over all cells left of this lane.
+    int32_t v = lane_max;
 #pragma unroll
     for (int off = 1; off < G; off <<= 1) {
       const int32_t t = __shfl_up_sync(gmask, v, off, G);
       if ((int)g >= off) v = max(v, t);
     }
-    int32_t excl_lane = __shfl_up_sync(gmask, v, 1, G);
-    if (g == 0) excl_lane = NEGBIG;
-    int32_t f[K], h[K];
-    uint32_t dir[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int32_t idx = (int32_t)g * K + k;
-      const int32_t ek = k ? max(excl_lane, inc[k - 1]) : excl_lane;
-      f[k] = idx >= 1 ? ek - (idx - 1) * ge : kNeg4;
-      // mod.rs:1504-1516 priority diag >= E >= F.
-      if (hm[k] >= e[k] && hm[k] >= f[k] && hm[k] > 0) {
-        h[k] = hm[k];
-        dir[k] = 1;
-      } else if (e[k] >= f[k] && e[k] > 0) {
-        h[k] = e[k];
-        dir[k] = 2;
-      } else if (f[k] > 0) {
-        h[k] = f[k];
-        dir[k] = 3;
-      } else {
-        h[k] = 0;
-        dir[k] = 0;
-      }
-    }
-    // Left neighbour of cell k = 0 lives in lane g-1.
-    const int32_t left_h = __shfl_up_sync(gmask, h[K - 1], 1, G);
-    const int32_t left_f = __shfl_up_sync(gmask, f[K - 1], 1, G);
+    int32_t excl = __shfl_up_sync(gmask, v, 1, G);
+    const int32_t left_g = __shfl_up_sync(gmask, gv[K - 1], 1, G);
+    if (g == 0) excl = NEGBIG;
+    // Pass 2 (in-lane running max): F[idx] = max_{k<idx} G[k] - (idx-1)*ge,
+    // H = max(Hdiag+s, E, F, 0) with the diag >= E >= F priority (mod.rs:1504-1516),
+    // F-extend = f_from_f > f_from_h = go > 0 && max_{k<idx-1} G[k] > G[idx-1].
     uint32_t key = 0;
-    uint32_t nib[K];
+    uint32_t tw[NW];
+#pragma unroll
+    for (int x = 0; x < NW; ++x) tw[x] = 0;
+    int32_t run = excl;  // max of G over the cells before idx
+    int32_t g_prev = g == 0 ? NEGBIG : left_g;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const int32_t idx = (int32_t)g * K + k;
+      const int32_t idx = base_idx + k;
       const bool act = idx < row_len;
-      const int32_t lh = k ? h[k - 1] : left_h;
-      const int32_t lf = k ? f[k - 1] : left_f;
-      const bool fext = idx >= 1 && (lf - ge) > (lh - gof);
-      nib[k] = act ? (dir[k] | (((eext >> k) & 1u) << 2) | (fext ? 8u : 0u)) : 0u;
-      if (act) {
-        const uint32_t kk = ((uint32_t)h[k] << kKeyIdxBits) | (uint32_t)(1023 - idx);
-        key = max(key, kk);
-      }
-      ph[k] = h[k];
+      const int32_t f = idx >= 1 ? run - (idx - 1) * ge : kNeg4;
+      const int32_t h = __vimax3_s32_relu(hm[k], e[k], f);
+      const uint32_t dir = h == 0 ? 0u : (h == hm[k] ? 1u : (h == e[k] ? 2u : 3u));
+      // F-extend of cell idx: max of G strictly before idx-1 exceeds G[idx-1];
+      // run = max(that, G[idx-1]), so the test is run > G[idx-1]. With go == 0
+      // f_from_f > f_from_h would need F[idx-1] > H[idx-1] >= F[idx-1]: never.
+      const bool fext = go > 0 && idx >= 1 && run > g_prev;
+      const uint32_t nib = dir | (((eext >> k) & 1u) << 2) | (fext ? 8u : 0u);
+      tw[k / 8] |= (act ? nib : 0u) << (4 * (k % 8));
+      const uint32_t kk = ((uint32_t)h << kKeyIdxBits) | (uint32_t)(1023 - idx);
+      key = act ? max(key, kk) : key;
+      ph[k] = h;
       pe[k] = e[k];
+      g_prev = gv[k];
+      run = max(run, gv[k]);
     }
-    uint8_t* trow = trace + (size_t)i * S + (size_t)g * LB;
+    uint32_t* trow = reinterpret_cast<uint32_t*>(trace + (size_t)i * S + (size_t)g * LB);
 #pragma unroll
-    for (int b = 0; b < LB; ++b) {
-      const uint32_t n0 = nib[2 * b];
-      const uint32_t n1 = (2 * b + 1 < K) ? nib[(2 * b + 1) < K ? 2 * b + 1 : 0] : 0u;
-      trow[b] = (uint8_t)(n0 | (n1 << 4));
-    }
+    for (int x = 0; x < NW; ++x) trow[x] = tw[x];
     if (g == 0) meta[i] = ((uint32_t)js << 11) | (uint32_t)row_len;
 #pragma unroll
     for (int off = G / 2; off > 0; off >>= 1) key = max(key, __shfl_xor_sync(gmask, key, off, G));
-    __syncwarp(gmask);
     const int32_t row_best = (int32_t)(key >> kKeyIdxBits);
     const int32_t row_best_j = row_best > 0 ? js + (1023 - (int32_t)(key & 1023u)) : -1;
     if (row_best > best) {

@@ -85,7 +85,7 @@ struct CompactLaunch {
 };
 
 struct BswShapeInfo {
-  int g, k;
+  int g, k, threads, min_blocks;
 };
 extern const BswShapeInfo kBswShapes[];
 extern const int kNumBswShapes;

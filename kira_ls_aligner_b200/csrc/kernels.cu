@@ -346,8 +346,8 @@ __global__ void __launch_bounds__(128) myers_kernel(DevPairs P, MyersLaunch M) {
 // ---------------------------------------------------------------------------
 // Banded SW: DP sweep (group of G lanes per item) and traceback (thread per item)
 // ---------------------------------------------------------------------------
-template <int G, int K>
-__global__ void __launch_bounds__(256) bsw_dp_kernel(DevPairs P, BswLaunch B) {
+template <int G, int K, int T, int MINB>
+__global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B) {
   extern __shared__ int32_t bsw_smem[];
   constexpr int CAP = G * K;
   const uint32_t lane = threadIdx.x & 31u;
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(256) bsw_dp_kernel(DevPairs P, BswLaunch B) {
   const uint32_t gmask = (G == 32) ? 0xFFFFFFFFu : (((1u << G) - 1u) << (gw * G));
   const uint32_t groups_per_block = blockDim.x / G;
   const uint32_t group_in_block = threadIdx.x / G;
-  int32_t* rowbuf = bsw_smem + (size_t)(threadIdx.x >> 5) * 4u * K * 32u;  // per warp
+  int32_t* rowbuf = bsw_smem + (size_t)(threadIdx.x >> 5) * 2u * K * 32u;  // per warp
   const uint32_t count = B.count_dev ? *B.count_dev : B.count;
   const uint32_t ngroups = gridDim.x * groups_per_block;
   for (uint32_t item = blockIdx.x * groups_per_block + group_in_block; item < count;
@@ -566,18 +566,18 @@ cudaError_t launch_myers(const DevPairs& P, const MyersLaunch& M, uint32_t max_i
   return cudaGetLastError();
 }
 
-template <int G, int K>
+template <int G, int K, int T, int MINB>
 static cudaError_t launch_bsw_shape(const DevPairs& P, const BswLaunch& B, uint32_t max_items,
                                     int sms, cudaStream_t st, cudaEvent_t between) {
-  constexpr int threads = 256;
-  const size_t smem = (size_t)(threads / 32) * 4 * K * 32 * sizeof(int32_t);
-  cudaFuncSetAttribute(bsw_dp_kernel<G, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)smem);
+  constexpr int threads = T;
+  const size_t smem = (size_t)(threads / 32) * 2 * K * 32 * sizeof(int32_t);
+  auto kern = bsw_dp_kernel<G, K, T, MINB>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bsw_dp_kernel<G, K>, threads, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
   if (per_sm < 1) per_sm = 1;
   const int blocks = grid_for(max_items, threads / G, sms * per_sm);
-  bsw_dp_kernel<G, K><<<blocks, threads, smem, st>>>(P, B);
+  kern<<<blocks, threads, smem, st>>>(P, B);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (between) cudaEventRecord(between, st);
@@ -586,19 +586,25 @@ static cudaError_t launch_bsw_shape(const DevPairs& P, const BswLaunch& B, uint3
   return cudaGetLastError();
 }
 
+// Launch shapes (lanes per pair, cells per lane, threads per block, min resident
+// blocks per SM). The host picks the first shape whose G*K covers 2*band+1
+// unless a tuned choice is installed for the band (autotuner / override).
 const BswShapeInfo kBswShapes[] = {
-    {4, 10}, {8, 10}, {16, 10}, {32, 10}, {32, 17},
+    {4, 10, 256, 2},  {4, 17, 128, 4},  {4, 17, 128, 3},  {8, 10, 256, 2},
+    {8, 17, 128, 3},  {16, 17, 128, 3}, {32, 17, 128, 3},
 };
 const int kNumBswShapes = sizeof(kBswShapes) / sizeof(kBswShapes[0]);
 
 cudaError_t launch_bsw(int shape, const DevPairs& P, const BswLaunch& B, uint32_t max_items,
                        int sms, cudaStream_t st, cudaEvent_t between) {
   switch (shape) {
-    case 0: return launch_bsw_shape<4, 10>(P, B, max_items, sms, st, between);
-    case 1: return launch_bsw_shape<8, 10>(P, B, max_items, sms, st, between);
-    case 2: return launch_bsw_shape<16, 10>(P, B, max_items, sms, st, between);
-    case 3: return launch_bsw_shape<32, 10>(P, B, max_items, sms, st, between);
-    case 4: return launch_bsw_shape<32, 17>(P, B, max_items, sms, st, between);
+    case 0: return launch_bsw_shape<4, 10, 256, 2>(P, B, max_items, sms, st, between);
+    case 1: return launch_bsw_shape<4, 17, 128, 4>(P, B, max_items, sms, st, between);
+    case 2: return launch_bsw_shape<4, 17, 128, 3>(P, B, max_items, sms, st, between);
+    case 3: return launch_bsw_shape<8, 10, 256, 2>(P, B, max_items, sms, st, between);
+    case 4: return launch_bsw_shape<8, 17, 128, 3>(P, B, max_items, sms, st, between);
+    case 5: return launch_bsw_shape<16, 17, 128, 3>(P, B, max_items, sms, st, between);
+    case 6: return launch_bsw_shape<32, 17, 128, 3>(P, B, max_items, sms, st, between);
     default: return cudaErrorInvalidValue;
   }
 }
