@@ -45,7 +45,8 @@ enum kira_status {
   KIRA_ERR_TIMEOUT = 6,       /* a bounded wait expired */
   KIRA_ERR_INVALID = 7,       /* argument outside the supported domain */
   KIRA_ERR_OOM = 8,           /* device memory exhausted / admission refused */
-  KIRA_ERR_CAPACITY = 9       /* caller's output buffer too small (see *_used) */
+  KIRA_ERR_CAPACITY = 9,      /* caller's output buffer too small (see *_used) */
+  KIRA_ERR_SCRATCH_LIMIT = 10 /* batch needs more than the fixed no-alloc scratch */
 };
 
 /* Per-pair status of the composed verification. */
@@ -243,6 +244,44 @@ int kira_gpu_verify_dev(kira_ctx* ctx, const kira_pairs* pairs, const kira_verif
                         kira_sw_result* out, uint32_t* cigar_ops, uint64_t cigar_cap,
                         uint64_t* cigar_used_dev, kira_verify_detail* detail,
                         unsigned long long* cells_dev, void* stream);
+
+/* ------------------------------------------- allocation-free banded SW */
+
+/* Size of the fixed scratch array that kira_gpu_bsw_batch_noalloc uses: one
+ * file-scope device array inside the library, held on every GPU that loads the
+ * library until the process exits. */
+#define KIRA_NOALLOC_SCRATCH_BYTES (32u << 20)
+
+/* No counterpart in the reference: an extra entry point for callers that cannot
+ * allocate device memory -- code whose device memory is owned by another
+ * allocator (a serving framework's pool, a fixed arena handed down by the host
+ * application) or that cannot afford the implicit device-wide synchronisation
+ * of cudaMalloc / cudaFree on its path.
+ *
+ * Same results as kira_gpu_bsw_batch (banded_sw_public per pair), but every
+ * pointer in `pairs`, `out`, `cigar_ops` and `cigar_used` is a device pointer
+ * owned by the caller, no kira_ctx is needed, and the call allocates nothing:
+ * no cudaMalloc, cudaFree or allocating library routine. All scratch (trace
+ * arena, CIGAR slots, scan buffers, flags) lives in the library's fixed
+ * KIRA_NOALLOC_SCRATCH_BYTES device array.
+ *   - pairs->max_read_len and max_win_len (and max_bandwidth when a per-pair
+ *     bandwidth array is given) are required and must bound every pair; the
+ *     scratch a batch needs grows with n, max_read_len, max_win_len and the band.
+ *     A batch that does not fit returns KIRA_ERR_SCRATCH_LIMIT before any GPU
+ *     work: split it into smaller batches.
+ *   - Work is enqueued on `stream` (a cudaStream_t) and the call returns without
+ *     synchronising; *cigar_used (device) receives the op count, and ops beyond
+ *     cigar_cap are not written (the caller compares the two after syncing).
+ *   - The first call on a device looks up the scratch array's device address on
+ *     that device (cudaGetSymbolAddress, with the device current) and caches it;
+ *     make that first call before any stream capture.
+ *   - Every call shares the one array and it keeps the previous call's
+ *     contents. Calls that overlap on the GPU (different streams without
+ *     ordering, or several host threads) race on it: order them on one stream or
+ *     synchronise between them. */
+int kira_gpu_bsw_batch_noalloc(const kira_pairs* pairs, const kira_sw_cfg* cfg,
+                               kira_sw_result* out, uint32_t* cigar_ops, uint64_t cigar_cap,
+                               uint64_t* cigar_used, void* stream);
 
 #ifdef __cplusplus
 }

@@ -16,8 +16,10 @@ LIB_PATH = os.path.join(_PKG, "lib", "libkira_gpu.so")
 KIRA_OK = 0
 STATUS_NAMES = {
     0: "OK", 1: "NotBuilt", 2: "Driver", 3: "Runtime", 4: "NoDevice", 5: "ReadTooLong",
-    6: "Timeout", 7: "Invalid", 8: "OutOfMemory", 9: "Capacity",
+    6: "Timeout", 7: "Invalid", 8: "OutOfMemory", 9: "Capacity", 10: "ScratchLimit",
 }
+KIRA_ERR_SCRATCH_LIMIT = 10
+NOALLOC_SCRATCH_BYTES = 32 << 20
 PAIR_PENDING, PAIR_CERTIFIED, PAIR_MYERS_REJECT, PAIR_SW = 0, 1, 2, 3
 READ_BYTES_MAX = 64
 ABORT_DISABLED = -268435456  # i32::MIN / 8
@@ -29,7 +31,7 @@ EXPORTS = (
     "kira_gpu_arena_bytes", "kira_gpu_sieve_batch", "kira_gpu_ref_upload",
     "kira_gpu_myers_batch", "kira_gpu_bsw_batch", "kira_gpu_verify_batch",
     "kira_gpu_verify_dev", "kira_gpu_profile", "kira_gpu_stage_times",
-    "kira_gpu_bsw_shapes", "kira_gpu_set_bsw_shape",
+    "kira_gpu_bsw_shapes", "kira_gpu_set_bsw_shape", "kira_gpu_bsw_batch_noalloc",
 )
 STAGES = ("sieve_certify", "myers", "bsw_dp", "bsw_traceback", "cigar_compact")
 
@@ -111,6 +113,8 @@ def lib():
                                       C.c_uint64, vp, vp, vp, vp]
     L.kira_gpu_profile.argtypes = [vp, C.c_int]
     L.kira_gpu_bsw_shapes.argtypes = [vp, vp, C.c_int]
+    L.kira_gpu_bsw_batch_noalloc.argtypes = [C.POINTER(Pairs), C.POINTER(SwCfg), vp, vp,
+                                             C.c_uint64, vp, vp]
     L.kira_gpu_set_bsw_shape.argtypes = [vp, C.c_uint32, C.c_int]
     L.kira_gpu_stage_times.argtypes = [vp, C.POINTER(C.c_float), C.c_int]
     for name in EXPORTS:
