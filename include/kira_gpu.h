@@ -207,6 +207,29 @@ int kira_gpu_myers_batch(kira_ctx* ctx, const kira_pairs* pairs, uint32_t max_k,
 int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg* cfg,
                        kira_sw_result* out, kira_cigar_buf* cigar, uint64_t* cells);
 
+/* SimdMode (src/simd/mod.rs:5-12). */
+enum kira_simd_mode {
+  KIRA_SIMD_SCALAR = 0,
+  KIRA_SIMD_AVX2 = 1,
+  KIRA_SIMD_AVX_VNNI = 2,
+  KIRA_SIMD_NEON = 3
+};
+
+/* align_batch_simd (src/alignment/mod.rs:1111-1169), SW results per input before
+ * build_alignment. `mode` is the requested SimdMode, `detected` the host's
+ * simd::detect_cached(); the GPU reproduces the kernel the reference would pick:
+ *   - inputs of mixed (read, window) lengths, scalar mode, or a failed i16 fit
+ *     check -> banded_sw per input with band_offset = BatchInput::scalar_sw's
+ *     offset (mod.rs:60-72);
+ *   - AVX2 (or AVX-VNNI without the i8 path) -> full-window i16 semantics in
+ *     groups of 16 consecutive inputs (sw_batch_avx2_inner, mod.rs:1914-2135);
+ *   - AVX-VNNI with int8_path_viable and <= 32 inputs -> one group of 32
+ *     (sw_batch_int8, sw_int8_vnni.rs:141-370, identical values under viability).
+ * The group matters only for abort bounds: a group stops after the first row at
+ * which every member's bound has fired. Full-window windows up to 544 bases. */
+int kira_gpu_align_batch_simd(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg* cfg,
+                              int mode, int detected, kira_sw_result* out, kira_cigar_buf* cigar);
+
 /* ------------------------------------------- composed verification */
 
 /* Parameters of the composed path (sieve -> certificate -> Myers -> banded SW). */

@@ -20,7 +20,7 @@ enum BufId {
   B_BANDW, B_OUT, B_DETAIL, B_CIGAR_OUT, B_NCIG, B_CIG_OFF, B_CHUNK_SUMS, B_SW_OFFSET,
   B_MYERS_LIST, B_SW_LIST, B_COUNTERS, B_ENDS, B_TRACE, B_META, B_CIG_SLOTS, B_ITEM_OF_PAIR,
   B_DIST, B_END, B_SIEVE_OUT, B_SIEVE_JOBS, B_CELLS, B_TOTAL, B_READ_PLANES, B_WIN_PLANES,
-  B_COUNT
+  B_ROWKEYS, B_DONE_ROW, B_COUNT
 };
 
 struct DevBuf {
@@ -610,6 +610,114 @@ int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg
   if (cells) *cells = hcells;
   if (flags[2] & 1u) return fail(ctx, KIRA_ERR_RUNTIME, "CIGAR slot overflow");
   if (flags[2] & 6u) return fail(ctx, KIRA_ERR_INVALID, "a pair exceeded the launch's length bounds");
+  if (total > cigar->cap)
+    return fail(ctx, KIRA_ERR_CAPACITY, "CIGAR buffer holds %llu ops, %llu needed",
+                (unsigned long long)cigar->cap, (unsigned long long)total);
+  if (total) {
+    KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * total, cudaMemcpyDeviceToHost, st));
+    KIRA_CUDA(cudaStreamSynchronize(st));
+  }
+  return KIRA_OK;
+}
+
+// i16 fit check of sw_batch_avx2 (src/alignment/mod.rs:1854-1868).
+static bool i16_fits(uint32_t q, uint32_t r, const kira_sw_cfg& c) {
+  const int64_t mx = 32767;
+  const bool costs = c.match_score >= 0 && c.match_score <= mx && c.mismatch >= 0 &&
+                     c.mismatch <= mx && c.gap_open >= 0 && c.gap_extend >= 0 &&
+                     (int64_t)c.gap_open + c.gap_extend <= mx;
+  if (!costs || q > mx || r > mx) return false;
+  return (int64_t)std::min(q, r) * c.match_score <= mx;
+}
+
+// int8_path_viable (src/alignment/sw_int8_vnni.rs:47-55).
+static bool int8_viable(uint32_t q, const kira_sw_cfg& c) {
+  const int64_t ms = std::max(c.match_score, 1);
+  auto in = [](int32_t v) { return v >= 0 && v <= 32; };
+  return (int64_t)q * ms < 120 && in(c.match_score) && in(c.mismatch) && in(c.gap_open) &&
+         in(c.gap_extend);
+}
+
+int kira_gpu_align_batch_simd(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg* cfg,
+                              int mode, int detected, kira_sw_result* out, kira_cigar_buf* cigar) {
+  if (!ctx || !pairs || !cfg || !out || !cigar) return KIRA_ERR_INVALID;
+  const kira_pairs& P = *pairs;
+  cigar->used = 0;
+  if (P.n == 0) return KIRA_OK;  // mod.rs:1116-1118
+  cudaSetDevice(ctx->device);
+  const uint32_t n = P.n;
+  const uint32_t q0 = P.read_len[0], r0 = P.win_len[0];
+  bool mixed = false;
+  for (uint32_t i = 0; i < n && !mixed; ++i) mixed = P.read_len[i] != q0 || P.win_len[i] != r0;
+  // Which kernel the reference dispatch (mod.rs:1131-1149, 1824-1841) would run.
+  uint32_t group = 0;  // 0: scalar banded for every input
+  if (!mixed) {
+    if (mode == KIRA_SIMD_AVX_VNNI && detected == KIRA_SIMD_AVX_VNNI) {
+      group = (int8_viable(q0, *cfg) && n <= 32) ? 32u : 16u;
+    } else if (mode == KIRA_SIMD_AVX2 &&
+               (detected == KIRA_SIMD_AVX2 || detected == KIRA_SIMD_AVX_VNNI)) {
+      group = 16u;
+    }
+    if (group == 16u && !i16_fits(q0, r0, *cfg)) group = 0;  // per-chunk scalar fallback
+  }
+  if (group == 0) return kira_gpu_bsw_batch(ctx, pairs, cfg, out, cigar, nullptr);
+  // Full-window kernel.
+  const int cap_need = (int)r0;
+  int shape = -1;
+  for (int s = 0; s < kNumBswShapes; ++s)
+    if (kBswShapes[s].g * kBswShapes[s].k >= cap_need) {
+      shape = s;
+      break;
+    }
+  if (shape < 0)
+    return fail(ctx, KIRA_ERR_INVALID, "full-window batch: window of %u > supported 544", r0);
+  if (cfg->gap_open < 0 || cfg->gap_extend < 0)
+    return fail(ctx, KIRA_ERR_INVALID, "gap costs must be >= 0");
+  DevPairs D;
+  int rc = upload_pairs(ctx, P, D);
+  if (rc) return rc;
+  cudaError_t cerr = cudaSuccess;
+  cudaStream_t st = ctx->stream;
+  Maxes mx;
+  mx.q = q0;
+  mx.w = r0;
+  mx.band = 1;
+  KIRA_DBUF(dout, kira_sw_result, B_OUT, n);
+  KIRA_DBUF(ncig, uint32_t, B_NCIG, n);
+  KIRA_DBUF(counters, uint32_t, B_COUNTERS, 4);
+  KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
+  KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
+  KIRA_CUDA(cudaMemsetAsync(counters, 0, 16, st));
+  BswLaunch B{};
+  rc = prepare_bsw(ctx, n, n, mx, shape, B);
+  if (rc) return rc;
+  bool any_abort = false;
+  if (P.abort_score)
+    for (uint32_t i = 0; i < n && !any_abort; ++i) any_abort = P.abort_score[i] > kAbortOff;
+  B.count = n;
+  B.sp = resolve(*cfg);
+  B.out = dout;
+  B.ncig = ncig;
+  B.flags = counters + 2;
+  B.full = 1;
+  B.group = group;
+  if (any_abort) {
+    KIRA_DBUF(keys, uint32_t, B_ROWKEYS, (uint64_t)(mx.q + 1) * n);
+    KIRA_DBUF(done, uint32_t, B_DONE_ROW, n);
+    B.rowkeys = keys;
+    B.done_row = done;
+  }
+  KIRA_CUDA(launch_bsw(shape, D, B, n, ctx->sms, st));
+  rc = finish_cigars(ctx, n, dout, ncig, B, ops, cigar->cap, total_dev, st);
+  if (rc) return rc;
+  uint64_t total = 0;
+  uint32_t flags[4];
+  KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_sw_result) * n, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(&total, total_dev, 8, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(flags, counters, 16, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaStreamSynchronize(st));
+  cigar->used = total;
+  if (flags[2]) return fail(ctx, KIRA_ERR_RUNTIME, "full-window batch outside its launch shape");
   if (total > cigar->cap)
     return fail(ctx, KIRA_ERR_CAPACITY, "CIGAR buffer holds %llu ops, %llu needed",
                 (unsigned long long)cigar->cap, (unsigned long long)total);

@@ -71,12 +71,19 @@ __device__ __forceinline__ void bsw_realign(int32_t (&ph)[K], int32_t (&pe)[K], 
   __syncwarp(gmask);
 }
 
-template <int G, int K>
+// FULL = the full-window kernel of align_batch_simd (sw_batch_avx2_inner,
+// src/alignment/mod.rs:1914-2135): every row covers columns 1..w, row 0 has H = 0
+// and E = -16384, column 0 has H = 0 and F = -16384, no band, no x-drop. Within the
+// i16 fit check of sw_batch_avx2 (mod.rs:1854-1868) the saturating i16 lanes never
+// change an observable value, so exact int32 arithmetic reproduces them. The
+// per-group "every lane done" abort break is resolved afterwards from the per-row
+// keys written to `rowkeys` (bsw_full_resolve_kernel).
+template <int G, int K, bool FULL>
 __device__ __forceinline__ void bsw_group_sweep(
     const uint8_t* __restrict__ rd, uint32_t q, const uint8_t* __restrict__ wn, uint32_t w,
     int32_t band, int32_t offset, int32_t abort_score, const SwParams& sp, int32_t* rowbuf,
     uint32_t lb, uint8_t* __restrict__ trace, uint32_t* __restrict__ meta, uint32_t g,
-    uint32_t gmask, DpEnd& out, uint64_t& cells_out) {
+    uint32_t gmask, DpEnd& out, uint64_t& cells_out, uint32_t* __restrict__ rowkeys) {
   constexpr int NW = BswShape<G, K>::kWords;
   constexpr int LB = BswShape<G, K>::kLaneBytes;
   constexpr int S = BswShape<G, K>::kRowStride;
@@ -93,21 +100,23 @@ __device__ __forceinline__ void bsw_group_sweep(
   const int32_t wl = (int32_t)w;
   const int32_t gi = (int32_t)g;
   const int32_t base_idx = gi * K;
+  constexpr int32_t kNeg16 = -16384;  // row-0 E / column-0 F of the full-window kernel
   int32_t ph[K], pe[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     ph[k] = 0;
-    pe[k] = kNeg4;
+    pe[k] = FULL ? kNeg16 : kNeg4;
   }
 
   for (uint32_t iu = 1; iu <= q; ++iu) {
     const int32_t i = (int32_t)iu;
     const int32_t sc = i + offset;
     const int32_t center = sp.adaptive ? min(max(acenter, sc - drift), sc + drift) : sc;
-    const int32_t js = max(center - band, 1);
-    const int32_t je = min(center + band, wl);
+    const int32_t js = FULL ? 1 : max(center - band, 1);
+    const int32_t je = FULL ? wl : min(center + band, wl);
     if (js > je) {  // mod.rs:1437-1444: row skipped, no centre / x-drop update
       if (g == 0) meta[i] = (1u << 11);
+      if (FULL && rowkeys && g == 0) rowkeys[i] = 0;
       prev_len = 0;
       prev_start = 1;
       continue;
@@ -116,11 +125,13 @@ __device__ __forceinline__ void bsw_group_sweep(
     cells += (uint64_t)row_len;
     const uint32_t qb = ldb(rd, (uint64_t)(i - 1));
     // Previous cell of diag = idx + s with s = d - 1; realign registers unless s == 0.
-    const int32_t sft = js - prev_start - 1;
-    if (sft != 0 && prev_len > 0) bsw_realign<G, K>(ph, pe, sft, rowbuf, lb, gi, gmask);
+    // (Full window: the band never moves, diag = previous cell idx - 1, up = idx.)
+    const int32_t sft = FULL ? -1 : js - prev_start - 1;
+    if (!FULL && sft != 0 && prev_len > 0) bsw_realign<G, K>(ph, pe, sft, rowbuf, lb, gi, gmask);
     const int32_t lo = -sft, hi = prev_len - sft;  // valid previous cells: lo <= idx < hi
     const int32_t up_h1 = __shfl_down_sync(gmask, ph[0], 1, G);
     const int32_t up_e1 = __shfl_down_sync(gmask, pe[0], 1, G);
+    const int32_t diag_left = FULL ? __shfl_up_sync(gmask, ph[K - 1], 1, G) : 0;
     const uint8_t* wrow = wn + (js - 1);
 
     // Pass 1: H_diag + s, E (with its extend flag) and the F-scan operand
@@ -134,14 +145,24 @@ __device__ __forceinline__ void bsw_group_sweep(
       const bool act = idx < row_len;
       const uint32_t rb = act ? __ldg(wrow + idx) : 0x100u;
       const int32_t s = (qb == rb) ? match : -mism;
-      hm[k] = ((idx >= lo && idx < hi) ? ph[k] : 0) + s;
-      const bool uv = idx + 1 >= lo && idx + 1 < hi;
-      const int32_t uh = k + 1 < K ? ph[k + 1 < K ? k + 1 : 0] : up_h1;
-      const int32_t ue = k + 1 < K ? pe[k + 1 < K ? k + 1 : 0] : up_e1;
+      int32_t uh, ue;
+      bool uv;
+      if (FULL) {
+        const int32_t hd = k ? ph[k ? k - 1 : 0] : (g == 0 ? 0 : diag_left);
+        hm[k] = hd + s;
+        uv = true;
+        uh = ph[k];
+        ue = pe[k];
+      } else {
+        hm[k] = ((idx >= lo && idx < hi) ? ph[k] : 0) + s;
+        uv = idx + 1 >= lo && idx + 1 < hi;
+        uh = k + 1 < K ? ph[k + 1 < K ? k + 1 : 0] : up_h1;
+        ue = k + 1 < K ? pe[k + 1 < K ? k + 1 : 0] : up_e1;
+      }
       // max(uh - gof, ue - ge) and e_from_e > e_from_h, with gof = go + ge.
       e[k] = uv ? __viaddmax_s32(uh, -go, ue) - ge : kNeg4;
       eext |= (uv && ue + go > uh ? 1u : 0u) << k;
-      gv[k] = __vimax_s32_relu(hm[k], e[k]) + (idx * ge - gof);
+      gv[k] = __vimax_s32_relu(hm[k], e[k]) + ((FULL ? idx + 1 : idx) * ge - gof);
       lane_max = max(lane_max, gv[k]);
     }
     // Cross-lane scan: excl = max of G over all cells left of this lane.
@@ -153,7 +174,9 @@ __device__ __forceinline__ void bsw_group_sweep(
     }
     int32_t excl = __shfl_up_sync(gmask, v, 1, G);
     const int32_t left_g = __shfl_up_sync(gmask, gv[K - 1], 1, G);
-    if (g == 0) excl = NEGBIG;
+    // Full window: column 0 contributes G(0) = H(0) - gof = -gof and the F chain
+    // seeded by F(0) = -16384 folds in as the constant -16384 - ge.
+    if (g == 0) excl = FULL ? max(-gof, kNeg16 - ge) : NEGBIG;
     // Pass 2 (in-lane running max): F[idx] = max_{k<idx} G[k] - (idx-1)*ge,
     // H = max(Hdiag+s, E, F, 0) with the diag >= E >= F priority (mod.rs:1504-1516),
     // F-extend = f_from_f > f_from_h = go > 0 && max_{k<idx-1} G[k] > G[idx-1].
@@ -162,18 +185,18 @@ __device__ __forceinline__ void bsw_group_sweep(
 #pragma unroll
     for (int x = 0; x < NW; ++x) tw[x] = 0;
     int32_t run = excl;  // max of G over the cells before idx
-    int32_t g_prev = g == 0 ? NEGBIG : left_g;
+    int32_t g_prev = g == 0 ? (FULL ? -gof : NEGBIG) : left_g;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int32_t idx = base_idx + k;
       const bool act = idx < row_len;
-      const int32_t f = idx >= 1 ? run - (idx - 1) * ge : kNeg4;
+      const int32_t f = FULL ? run - idx * ge : (idx >= 1 ? run - (idx - 1) * ge : kNeg4);
       const int32_t h = __vimax3_s32_relu(hm[k], e[k], f);
       const uint32_t dir = h == 0 ? 0u : (h == hm[k] ? 1u : (h == e[k] ? 2u : 3u));
       // F-extend of cell idx: max of G strictly before idx-1 exceeds G[idx-1];
       // run = max(that, G[idx-1]), so the test is run > G[idx-1]. With go == 0
       // f_from_f > f_from_h would need F[idx-1] > H[idx-1] >= F[idx-1]: never.
-      const bool fext = go > 0 && idx >= 1 && run > g_prev;
+      const bool fext = go > 0 && (FULL || idx >= 1) && run > g_prev;
       const uint32_t nib = dir | (((eext >> k) & 1u) << 2) | (fext ? 8u : 0u);
       tw[k / 8] |= (act ? nib : 0u) << (4 * (k % 8));
       const uint32_t kk = ((uint32_t)h << kKeyIdxBits) | (uint32_t)(1023 - idx);
@@ -189,6 +212,7 @@ __device__ __forceinline__ void bsw_group_sweep(
     if (g == 0) meta[i] = ((uint32_t)js << 11) | (uint32_t)row_len;
 #pragma unroll
     for (int off = G / 2; off > 0; off >>= 1) key = max(key, __shfl_xor_sync(gmask, key, off, G));
+    if (FULL && rowkeys && g == 0) rowkeys[i] = key;
     const int32_t row_best = (int32_t)(key >> kKeyIdxBits);
     const int32_t row_best_j = row_best > 0 ? js + (1023 - (int32_t)(key & 1023u)) : -1;
     if (row_best > best) {
@@ -202,6 +226,7 @@ __device__ __forceinline__ void bsw_group_sweep(
     }
     prev_start = js;
     prev_len = row_len;
+    if (FULL) continue;  // no centre, x-drop or abort inside the full-window sweep
     if (sp.adaptive) {  // mod.rs:1546-1559
       const int32_t raw = row_best_j >= 0 ? row_best_j + 1 : acenter + 1;
       const int32_t sn = i + 1 + offset;

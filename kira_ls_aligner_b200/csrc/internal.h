@@ -70,6 +70,11 @@ struct BswLaunch {
   uint32_t* item_of_pair;     // per pair
   uint32_t* flags;            // bit 0: CIGAR slot overflow, bit 1: item outside the launch shape
   uint32_t max_q;             // rows per trace slot - 1
+  // full-window mode (align_batch_simd): per-row keys for the group abort rule
+  int32_t full;
+  uint32_t* rowkeys;          // [item][max_q + 1] or null when no abort bound is active
+  uint32_t* done_row;         // [item] first row whose abort test fired (0xFFFFFFFF: never)
+  uint32_t group;             // lanes per SIMD batch (16: AVX2 i16, 32: AVX-VNNI i8)
 };
 
 struct CompactLaunch {

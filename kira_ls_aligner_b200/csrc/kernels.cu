@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(128) myers_kernel(DevPairs P, MyersLaunch M) {
 // ---------------------------------------------------------------------------
 // Banded SW: DP sweep (group of G lanes per item) and traceback (thread per item)
 // ---------------------------------------------------------------------------
-template <int G, int K, int T, int MINB>
+template <int G, int K, int T, int MINB, bool FULL>
 __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B) {
   extern __shared__ int32_t bsw_smem[];
   constexpr int CAP = G * K;
@@ -368,17 +368,18 @@ __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B
     const int32_t abort_score = P.abort_score ? P.abort_score[pair] : kAbortOff;
     DpEnd end;
     uint64_t cells = 0;
-    if (q > B.max_q || 2 * band + 1 > CAP) {  // outside this launch's trace slot / row buffer
+    if (q > B.max_q || (FULL ? (int32_t)w > CAP : 2 * band + 1 > CAP)) {  // outside the shape
       if (g == 0) {
         B.ends[item] = DpEnd{0, 0, 0, 0};
         atomicOr(B.flags, 2u);
       }
       continue;
     }
-    bsw_group_sweep<G, K>(P.read_seq + P.read_off[pair], q, P.win_seq + P.win_off[pair], w, band,
-                          offset, abort_score, B.sp, rowbuf, gw * G,
-                          B.tg.trace + (size_t)item * B.tg.slot_bytes,
-                          B.tg.meta + (size_t)item * B.tg.meta_stride, g, gmask, end, cells);
+    bsw_group_sweep<G, K, FULL>(
+        P.read_seq + P.read_off[pair], q, P.win_seq + P.win_off[pair], w, band, offset,
+        abort_score, B.sp, rowbuf, gw * G, B.tg.trace + (size_t)item * B.tg.slot_bytes,
+        B.tg.meta + (size_t)item * B.tg.meta_stride, g, gmask, end, cells,
+        B.rowkeys ? B.rowkeys + (size_t)item * B.tg.meta_stride : nullptr);
     if (g == 0) {
       B.ends[item] = end;
       if (B.cells) atomicAdd(B.cells, (unsigned long long)cells);
@@ -414,6 +415,63 @@ __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
     B.item_of_pair[pair] = item;
     if (overflow) atomicOr(B.flags, 1u);
   }
+}
+
+// Full-window group abort rule of sw_batch_avx2_inner (mod.rs:2058-2081): after
+// each row a lane with an active bound is done once best + remaining * match <
+// abort; the batch stops after the first row where every lane of the group is
+// done. Pass 1 finds each item's first firing row from its per-row keys.
+__global__ void __launch_bounds__(128) bsw_full_done_kernel(DevPairs P, BswLaunch B) {
+  const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= B.count) return;
+  const uint32_t q = P.read_len[item];
+  const int32_t abort_score = P.abort_score ? P.abort_score[item] : kAbortOff;
+  uint32_t done = 0xFFFFFFFFu;
+  if (abort_score > kAbortOff) {
+    const uint32_t* keys = B.rowkeys + (size_t)item * B.tg.meta_stride;
+    int32_t best = 0;
+    for (uint32_t i = 1; i <= q; ++i) {
+      best = max(best, (int32_t)(keys[i] >> kKeyIdxBits));
+      if (best + (int32_t)(q - i) * B.sp.match < abort_score) {
+        done = i;
+        break;
+      }
+    }
+  }
+  B.done_row[item] = done;
+}
+
+// Pass 2: the group's stop row R (max of the members' firing rows, if all fire),
+// then best / end / early flag as of row R with the clip rule (mod.rs:2104-2132).
+__global__ void __launch_bounds__(128) bsw_full_resolve_kernel(DevPairs P, BswLaunch B) {
+  const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= B.count) return;
+  const uint32_t g0 = (item / B.group) * B.group;
+  const uint32_t g1 = min(g0 + B.group, B.count);
+  uint32_t stop = 0;
+  for (uint32_t t = g0; t < g1; ++t) stop = max(stop, B.done_row[t]);
+  const uint32_t q = P.read_len[item];
+  const uint32_t last = stop == 0xFFFFFFFFu ? q : min(stop, q);
+  const uint32_t* keys = B.rowkeys + (size_t)item * B.tg.meta_stride;
+  int32_t best = 0, bi = 0, bj = 0;
+  for (uint32_t i = 1; i <= last; ++i) {
+    const int32_t rb = (int32_t)(keys[i] >> kKeyIdxBits);
+    if (rb > best) {
+      best = rb;
+      bi = (int32_t)i;
+      bj = 1 + (1023 - (int32_t)(keys[i] & 1023u));
+    }
+  }
+  if (last == q && q > 0) {
+    const int32_t bq = (int32_t)(keys[q] >> kKeyIdxBits);
+    const int32_t bqj = 1 + (1023 - (int32_t)(keys[q] & 1023u));
+    if (bq > 0 && sat_add(bq, B.sp.clip) > best) {
+      best = bq;
+      bi = (int32_t)q;
+      bj = bqj;
+    }
+  }
+  B.ends[item] = DpEnd{best, bi, bj, B.done_row[item] <= last ? 1u : 0u};
 }
 
 // ---------------------------------------------------------------------------
@@ -571,7 +629,7 @@ static cudaError_t launch_bsw_shape(const DevPairs& P, const BswLaunch& B, uint3
                                     int sms, cudaStream_t st, cudaEvent_t between) {
   constexpr int threads = T;
   const size_t smem = (size_t)(threads / 32) * 2 * K * 32 * sizeof(int32_t);
-  auto kern = bsw_dp_kernel<G, K, T, MINB>;
+  auto kern = B.full ? bsw_dp_kernel<G, K, T, MINB, true> : bsw_dp_kernel<G, K, T, MINB, false>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
@@ -580,6 +638,13 @@ static cudaError_t launch_bsw_shape(const DevPairs& P, const BswLaunch& B, uint3
   kern<<<blocks, threads, smem, st>>>(P, B);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (B.full && B.rowkeys) {
+    const int rb = (int)((B.count + 127) / 128);
+    bsw_full_done_kernel<<<rb, 128, 0, st>>>(P, B);
+    bsw_full_resolve_kernel<<<rb, 128, 0, st>>>(P, B);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   if (between) cudaEventRecord(between, st);
   const int tb_blocks = grid_for(max_items, 128, sms * 16);
   bsw_tb_kernel<<<tb_blocks, 128, 0, st>>>(P, B);

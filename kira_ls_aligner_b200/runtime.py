@@ -305,6 +305,23 @@ class GpuContext:
         self.check(rc)
         return res, ops[: cb.used], int(cells.value)
 
+    # -- align_batch_simd (full-window batch SW drop-in)
+    def align_batch_simd(self, batch: PairBatch, cfg: AlignmentConfig, mode: int,
+                         detected: int, cigar_cap: int | None = None):
+        n = batch.n
+        res = np.zeros(max(n, 1), A.SW_RESULT_DTYPE)
+        cap = cigar_cap if cigar_cap is not None else max(16, 8 * n)
+        ops = np.zeros(cap, np.uint32)
+        cb = A.CigarBuf(A.ptr(ops), cap, 0)
+        pc = batch.to_c()
+        cc = cfg.to_c()
+        rc = self._lib.kira_gpu_align_batch_simd(self._h, C.byref(pc), C.byref(cc), mode,
+                                                 detected, A.ptr(res), C.byref(cb))
+        if rc == 9 and cigar_cap is None:
+            return self.align_batch_simd(batch, cfg, mode, detected, int(cb.used) + 16)
+        self.check(rc)
+        return res[:n], ops[: cb.used]
+
     # -- composed verification
     def verify_batch(self, batch: PairBatch, params: VerifyParams, detail: bool = False,
                      cigar_cap: int | None = None):
