@@ -188,6 +188,13 @@ int kira_gpu_stage_times(kira_ctx* ctx, float* ms, int max_stages);
 int kira_gpu_bsw_shapes(int* lanes, int* cells, int max_shapes);
 int kira_gpu_set_bsw_shape(kira_ctx* ctx, uint32_t band, int shape);
 
+/* kira_gpu_bsw_batch buckets pairs by band class (one tuned launch shape and trace
+ * geometry per class, longest reads first, dynamic work fetching). plain = 1
+ * selects the one-launch form instead (a single shape sized for the widest band,
+ * static order), kept as the baseline the bucketed form is measured against.
+ * Results are identical either way. */
+int kira_gpu_set_plain(kira_ctx* ctx, int plain);
+
 /* Upload the reference as ASCII bases (Index::ref_bases, src/index/mod.rs:1098);
  * it stays resident until the next upload or kira_gpu_destroy. */
 int kira_gpu_ref_upload(kira_ctx* ctx, const uint8_t* seq, uint64_t len);

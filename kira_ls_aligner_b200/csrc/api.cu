@@ -20,7 +20,7 @@ enum BufId {
   B_BANDW, B_OUT, B_DETAIL, B_CIGAR_OUT, B_NCIG, B_CIG_OFF, B_CHUNK_SUMS, B_SW_OFFSET,
   B_MYERS_LIST, B_SW_LIST, B_COUNTERS, B_ENDS, B_TRACE, B_META, B_CIG_SLOTS, B_ITEM_OF_PAIR,
   B_DIST, B_END, B_SIEVE_OUT, B_SIEVE_JOBS, B_CELLS, B_TOTAL, B_READ_PLANES, B_WIN_PLANES,
-  B_ROWKEYS, B_DONE_ROW, B_COUNT
+  B_ROWKEYS, B_DONE_ROW, B_WORK, B_COUNT
 };
 
 struct DevBuf {
@@ -41,6 +41,7 @@ inline int band_class(uint32_t b) {
 struct kira_ctx {
   int device = 0;
   int tuned_shape[kBandClasses] = {-1, -1, -1, -1, -1, -1};
+  bool plain = false;  // single-launch banded SW (no bucketing): the comparison baseline
   int sms = 148;
   cudaStream_t stream = nullptr;
   std::string last_error;
@@ -343,6 +344,94 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
   return rc;
 }
 
+// Banded SW over a host batch already uploaded to D: pairs are bucketed by band
+// class (each class gets the launch shape tuned for it and a trace geometry sized
+// for its longest read), sorted longest-first inside a class, and fetched
+// dynamically by the DP kernel's groups. One DP + one traceback launch per class.
+int bsw_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const kira_sw_cfg& cfg,
+                 kira_sw_result* dout, uint32_t* ncig, uint32_t* flags_dev,
+                 unsigned long long* cells_dev, BswLaunch& G, cudaStream_t st) {
+  cudaError_t cerr = cudaSuccess;
+  const uint32_t n = P.n;
+  std::vector<uint8_t> cls(n);
+  uint32_t cnt[kBandClasses] = {}, qmax[kBandClasses] = {}, bmax[kBandClasses] = {};
+  uint32_t qall = 0, wall = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t b = (uint32_t)std::max(P.bandwidth ? P.bandwidth[i] : cfg.bandwidth, 1);
+    const int c = band_class(b);
+    cls[i] = (uint8_t)c;
+    ++cnt[c];
+    qmax[c] = std::max(qmax[c], P.read_len[i]);
+    bmax[c] = std::max(bmax[c], b);
+    qall = std::max(qall, P.read_len[i]);
+    wall = std::max(wall, P.win_len[i]);
+  }
+  uint32_t base[kBandClasses + 1] = {};
+  for (int c = 0; c < kBandClasses; ++c) base[c + 1] = base[c] + cnt[c];
+  std::vector<uint32_t> list(n);
+  {
+    uint32_t at[kBandClasses];
+    for (int c = 0; c < kBandClasses; ++c) at[c] = base[c];
+    for (uint32_t i = 0; i < n; ++i) list[at[cls[i]]++] = i;
+    for (int c = 0; c < kBandClasses; ++c)  // longest first: the tail of a launch is short
+      std::stable_sort(list.begin() + base[c], list.begin() + base[c + 1],
+                       [&](uint32_t a, uint32_t b) { return P.read_len[a] > P.read_len[b]; });
+  }
+  int shape[kBandClasses];
+  uint64_t slot[kBandClasses] = {}, tbase[kBandClasses + 1] = {}, mbase[kBandClasses + 1] = {};
+  for (int c = 0; c < kBandClasses; ++c) {
+    shape[c] = cnt[c] ? pick_shape(ctx, bmax[c]) : -1;
+    if (cnt[c] && shape[c] < 0) return fail(ctx, KIRA_ERR_INVALID, "no shape for band %u", bmax[c]);
+    if (cnt[c]) {
+      const BswShapeInfo sh = kBswShapes[shape[c]];
+      const uint64_t rs = (uint64_t)sh.g * 4u * (uint64_t)((sh.k + 7) / 8);
+      slot[c] = (((uint64_t)(qmax[c] + 1) * rs) + 15) & ~15ull;
+    }
+    tbase[c + 1] = tbase[c] + slot[c] * cnt[c];
+    mbase[c + 1] = mbase[c] + (uint64_t)(qmax[c] + 1) * cnt[c];
+  }
+  const uint32_t cap = qall + wall + 2;
+  KIRA_DBUF(dlist, uint32_t, B_SW_LIST, n);
+  KIRA_DBUF(trace, uint8_t, B_TRACE, std::max<uint64_t>(tbase[kBandClasses], 16));
+  KIRA_DBUF(meta, uint32_t, B_META, std::max<uint64_t>(mbase[kBandClasses], 1));
+  KIRA_DBUF(ends, DpEnd, B_ENDS, n);
+  KIRA_DBUF(slots, uint32_t, B_CIG_SLOTS, (uint64_t)cap * n);
+  KIRA_DBUF(iop, uint32_t, B_ITEM_OF_PAIR, n);
+  KIRA_DBUF(work, uint32_t, B_WORK, kBandClasses);
+  KIRA_CUDA(cudaMemcpyAsync(dlist, list.data(), 4ull * n, cudaMemcpyHostToDevice, st));
+  KIRA_CUDA(cudaMemsetAsync(work, 0, 4 * kBandClasses, st));
+  const SwParams sp = resolve(cfg);
+  for (int c = 0; c < kBandClasses; ++c) {
+    if (!cnt[c]) continue;
+    const BswShapeInfo sh = kBswShapes[shape[c]];
+    const uint32_t lane_bytes = 4u * (uint32_t)((sh.k + 7) / 8);
+    BswLaunch B{};
+    B.list = dlist + base[c];
+    B.count = cnt[c];
+    B.sp = sp;
+    B.offset = D.band_offset;
+    B.tg = TraceGeom{trace + tbase[c], meta + mbase[c], slot[c], (uint32_t)sh.g * lane_bytes,
+                     lane_bytes, (uint32_t)sh.k, qmax[c] + 1};
+    B.ends = ends + base[c];
+    B.cells = cells_dev;
+    B.cig_slots = slots + (uint64_t)base[c] * cap;
+    B.slot_cap = cap;
+    B.out = dout;
+    B.ncig = ncig;
+    B.item_of_pair = iop;
+    B.flags = flags_dev;
+    B.max_q = qmax[c];
+    B.work = work + c;
+    B.item_base = base[c];
+    KIRA_CUDA(launch_bsw(shape[c], D, B, cnt[c], ctx->sms, st));
+  }
+  G = BswLaunch{};
+  G.item_of_pair = iop;
+  G.cig_slots = slots;
+  G.slot_cap = cap;
+  return KIRA_OK;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -475,6 +564,12 @@ int kira_gpu_set_bsw_shape(kira_ctx* ctx, uint32_t band, int shape) {
   return KIRA_OK;
 }
 
+int kira_gpu_set_plain(kira_ctx* ctx, int plain) {
+  if (!ctx) return KIRA_ERR_INVALID;
+  ctx->plain = plain != 0;
+  return KIRA_OK;
+}
+
 int kira_gpu_bsw_shapes(int* lanes, int* cells, int max_shapes) {
   const int n = std::min(max_shapes, kNumBswShapes);
   for (int i = 0; i < n; ++i) {
@@ -584,18 +679,23 @@ int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg
   KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
   KIRA_CUDA(cudaMemsetAsync(counters, 0, 16, st));
   KIRA_CUDA(cudaMemsetAsync(cells_dev, 0, 8, st));
-  const int shape = pick_shape(ctx, mx.band);
   BswLaunch B{};
-  rc = prepare_bsw(ctx, n, n, mx, shape, B);
-  if (rc) return rc;
-  B.count = n;
-  B.sp = resolve(*cfg);
-  B.offset = D.band_offset;
-  B.cells = cells_dev;
-  B.out = dout;
-  B.ncig = ncig;
-  B.flags = counters + 2;
-  KIRA_CUDA(launch_bsw(shape, D, B, n, ctx->sms, st));
+  if (ctx->plain) {  // one launch, one shape for the widest band, static order
+    const int shape = default_shape(mx.band);
+    rc = prepare_bsw(ctx, n, n, mx, shape, B);
+    if (rc) return rc;
+    B.count = n;
+    B.sp = resolve(*cfg);
+    B.offset = D.band_offset;
+    B.cells = cells_dev;
+    B.out = dout;
+    B.ncig = ncig;
+    B.flags = counters + 2;
+    KIRA_CUDA(launch_bsw(shape, D, B, n, ctx->sms, st));
+  } else {
+    rc = bsw_bucketed(ctx, P, D, *cfg, dout, ncig, counters + 2, cells_dev, B, st);
+    if (rc) return rc;
+  }
   rc = finish_cigars(ctx, n, dout, ncig, B, ops, cigar->cap, total_dev, st);
   if (rc) return rc;
   uint64_t total = 0;

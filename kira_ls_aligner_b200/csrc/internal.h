@@ -75,6 +75,9 @@ struct BswLaunch {
   uint32_t* rowkeys;          // [item][max_q + 1] or null when no abort bound is active
   uint32_t* done_row;         // [item] first row whose abort test fired (0xFFFFFFFF: never)
   uint32_t group;             // lanes per SIMD batch (16: AVX2 i16, 32: AVX-VNNI i8)
+  // bucketed launches
+  uint32_t* work;             // dynamic work counter (null: static grid-stride order)
+  uint32_t item_base;         // global index of this launch's first item (CIGAR slots)
 };
 
 struct CompactLaunch {

@@ -359,8 +359,14 @@ __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B
   int32_t* rowbuf = bsw_smem + (size_t)(threadIdx.x >> 5) * 2u * K * 32u;  // per warp
   const uint32_t count = B.count_dev ? *B.count_dev : B.count;
   const uint32_t ngroups = gridDim.x * groups_per_block;
-  for (uint32_t item = blockIdx.x * groups_per_block + group_in_block; item < count;
-       item += ngroups) {
+  uint32_t item = blockIdx.x * groups_per_block + group_in_block;
+  for (;;) {
+    if (B.work) {  // dynamic fetch: the group leader takes the next item
+      uint32_t t = 0;
+      if (g == 0) t = atomicAdd(B.work, 1u);
+      item = __shfl_sync(gmask, t, gw * G);
+    }
+    if (item >= count) break;
     const uint32_t pair = B.list ? B.list[item] : item;
     const uint32_t q = P.read_len[pair], w = P.win_len[pair];
     const int32_t band = max(P.bandwidth ? P.bandwidth[pair] : B.sp.band, 1);
@@ -373,6 +379,7 @@ __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B
         B.ends[item] = DpEnd{0, 0, 0, 0};
         atomicOr(B.flags, 2u);
       }
+      if (!B.work) item += ngroups;
       continue;
     }
     bsw_group_sweep<G, K, FULL>(
@@ -384,6 +391,7 @@ __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B
       B.ends[item] = end;
       if (B.cells) atomicAdd(B.cells, (unsigned long long)cells);
     }
+    if (!B.work) item += ngroups;
   }
 }
 
@@ -412,7 +420,7 @@ __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
     r.reserved = overflow ? 1 : 0;
     B.out[pair] = r;
     B.ncig[pair] = n;
-    B.item_of_pair[pair] = item;
+    B.item_of_pair[pair] = B.item_base + item;
     if (overflow) atomicOr(B.flags, 1u);
   }
 }

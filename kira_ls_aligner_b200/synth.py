@@ -131,3 +131,73 @@ def batched(seed: int = 0xB200, n_reads: int = 250_000, ref_len: int = 100_000_0
     """100 Mbp + 5 % repeats, 250k reads x 8 candidates = 2M pairs of 150 / 250 bp."""
     return make_workload("batched_2M_150x250", n_reads, ref_len, cands=8, sub_lo=0.005,
                          sub_hi=0.02, repeat_frac=0.05, seed=seed)
+
+
+def _mutate_matrix(rng, frag: np.ndarray, q: np.ndarray, rate: np.ndarray,
+                   split=(8, 1, 1)):
+    """Vectorised read simulation: frag is (n, L) source bases (L >= 2 * max q);
+    per output position an op M/S/I/D is drawn (error `rate` per read split
+    subs:ins:del); D skips one source base. Returns (n, max q) reads."""
+    n, L = frag.shape
+    qm = int(q.max())
+    tot = float(sum(split))
+    u = rng.random((n, qm))
+    r = rate[:, None]
+    sub = u < r * split[0] / tot
+    ins = (u >= r * split[0] / tot) & (u < r * (split[0] + split[1]) / tot)
+    dele = (u >= r * (split[0] + split[1]) / tot) & (u < r)
+    adv = np.where(ins, 0, np.where(dele, 2, 1)).astype(np.int32)
+    src = np.cumsum(adv, axis=1) - adv + dele  # index of the base emitted at each position
+    src = np.minimum(src, L - 1)
+    out = np.take_along_axis(frag, src, axis=1)
+    if sub.any():
+        out[sub] = BASES[(np.searchsorted(BASES, out[sub]) + rng.integers(1, 4, int(sub.sum())))
+                         % 4]
+    if ins.any():
+        out[ins] = BASES[rng.integers(0, 4, int(ins.sum()))]
+    return out
+
+
+@dataclass
+class SwWorkload:
+    """Independent (read, window, band offset, band) pairs for the banded SW."""
+    name: str
+    reads: np.ndarray
+    read_off: np.ndarray
+    read_len: np.ndarray
+    wins: np.ndarray
+    win_off: np.ndarray
+    win_len: np.ndarray
+    band_offset: np.ndarray
+    bandwidth: np.ndarray
+
+    @property
+    def n_pairs(self) -> int:
+        return int(len(self.read_off))
+
+
+def uneven(n_pairs: int = 500_000, seed: int = 0x3E3E, q_lo: int = 50, q_hi: int = 300,
+           bands=(16, 32, 64, 128), err_hi: float = 0.03, ref_len: int = 20_000_000) -> SwWorkload:
+    """Reads U[50, 300] bp, band uniform in {16, 32, 64, 128}, window = read + 2 x band
+    with the read's origin at window offset band, errors U[0, 3 %] at 8:1:1."""
+    rng = np.random.default_rng(seed)
+    ref = BASES[rng.integers(0, 4, ref_len)]
+    q = rng.integers(q_lo, q_hi + 1, n_pairs).astype(np.int64)
+    b = np.asarray(bands, np.int64)[rng.integers(0, len(bands), n_pairs)]
+    w = q + 2 * b
+    start = rng.integers(0, ref_len - int(w.max()) - q_hi - 64, n_pairs)
+    L = q_hi + 48  # deletions beyond 48 per read clamp at the fragment end
+    frag = ref[(start + b).astype(np.int32)[:, None] + np.arange(L, dtype=np.int32)[None, :]]
+    rate = rng.uniform(0.0, err_hi, n_pairs)
+    reads = _mutate_matrix(rng, frag, q, rate)
+    mask = np.arange(reads.shape[1])[None, :] < q[:, None]
+    read_arena = reads[mask]
+    read_off = np.zeros(n_pairs, np.uint64)
+    read_off[1:] = np.cumsum(q[:-1])
+    win_off = np.zeros(n_pairs, np.uint64)
+    win_off[1:] = np.cumsum(w[:-1])
+    idx = np.repeat(start, w) + (np.arange(int(w.sum())) - np.repeat(win_off.astype(np.int64), w))
+    wins = ref[idx]
+    return SwWorkload("uneven_500k_q50-300_band16-128", np.concatenate([read_arena, np.zeros(16, np.uint8)]),
+                      read_off, q.astype(np.uint32), np.concatenate([wins, np.zeros(16, np.uint8)]),
+                      win_off, w.astype(np.uint32), b.astype(np.int32), b.astype(np.int32))
