@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=20_000, help="pairs in the CPU sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--shape", type=int, default=-1,
+                    help="install this banded-SW launch shape instead of autotuning")
     ap.add_argument("--workload", choices=["batched", "uneven"], default="batched",
                     help="batched: the headline 2M-pair verification; uneven: 500k banded-SW "
                          "pairs of mixed length and band (bucketed vs one-launch path)")
@@ -184,25 +186,13 @@ def run_uneven(args, rank, local, world):
     cfg = AlignmentConfig(1, 4, 6, 1, 33, 100, 5, True, 16)
     ctx = GpuContext(local)
     L = _abi.lib()
-    # Autotune the shape of each band class on a 20k-pair sample of that class.
+    # Autotune the shape of each band class on a 20k-pair sample of that class
+    # (DP stage time from the library's stage events).
     tuned = {}
     for band in (16, 32, 64, 128):
-        idx = np.nonzero(w.bandwidth == band)[0][:20000]
-        sub = PairBatch(w.reads, w.read_off[idx].copy(), w.read_len[idx].copy(), w.wins,
-                        w.win_off[idx].copy(), w.win_len[idx].copy(),
-                        w.band_offset[idx].copy(), None, w.bandwidth[idx].copy())
-        best, times = None, {}
-        for s in autotune.covering(band):
-            ctx.check(L.kira_gpu_set_bsw_shape(ctx.handle, band, s))
-            ctx.bsw_batch(sub, cfg)
-            t = min(_timed(lambda: ctx.bsw_batch(sub, cfg)) for _ in range(3))
-            times[s] = t
-            if best is None or t < times[best]:
-                best = s
-        ctx.check(L.kira_gpu_set_bsw_shape(ctx.handle, band, best))
-        tuned[band] = {"shape": autotune.shapes()[best],
-                       "ms": {f"{autotune.shapes()[k][0]}x{autotune.shapes()[k][1]}#{k}": round(v, 3)
-                              for k, v in times.items()}}
+        sub = _subset(w, np.nonzero(w.bandwidth == band)[0][:20000])
+        tuned[band] = autotune.tune_bsw_shape(
+            ctx, band, lambda: ctx.bsw_batch(sub, cfg), device_name=torch.cuda.get_device_name(local))
     out = {}
     for mode in ("plain", "bucketed"):
         ctx.check(L.kira_gpu_set_plain(ctx.handle, 1 if mode == "plain" else 0))
@@ -210,7 +200,14 @@ def run_uneven(args, rank, local, world):
             res, ops, cells = ctx.bsw_batch(batch, cfg)
         ts = [_timed(lambda: ctx.bsw_batch(batch, cfg)) for _ in range(args.steps)]
         res, ops, cells = ctx.bsw_batch(batch, cfg)
-        out[mode] = {"pairs_per_s": n / (sum(ts) / len(ts) / 1e3),
+        ctx.check(L.kira_gpu_profile(ctx.handle, 1))
+        ctx.bsw_batch(batch, cfg)
+        buf = (C.c_float * 8)()
+        k = L.kira_gpu_stage_times(ctx.handle, buf, 8)
+        ctx.check(L.kira_gpu_profile(ctx.handle, 0))
+        stages = dict(zip(("upload", "bucketing", "bsw_dp", "bsw_traceback", "cigar_compact"),
+                          [round(float(x), 3) for x in buf[:k]]))
+        out[mode] = {"stage_ms": stages, "pairs_per_s": n / (sum(ts) / len(ts) / 1e3),
                      "ms_per_call": sum(ts) / len(ts), "gcups": cells / (sum(ts) / len(ts) / 1e3) / 1e9,
                      "cells": int(cells), "checksum": int(res["score"].astype(np.int64).sum())}
     assert out["plain"]["checksum"] == out["bucketed"]["checksum"]
@@ -227,6 +224,20 @@ def run_uneven(args, rank, local, world):
         "speedup_vs_plain": out["bucketed"]["pairs_per_s"] / out["plain"]["pairs_per_s"],
         "autotune": tuned}))
     ctx.close()
+
+
+def _subset(w, idx):
+    """A compact PairBatch of the pairs `idx` of an SwWorkload (own arenas)."""
+    from kira_ls_aligner_b200 import PairBatch
+    rl, wl = w.read_len[idx], w.win_len[idx]
+    reads = np.concatenate([w.reads[int(o):int(o) + int(n)] for o, n in zip(w.read_off[idx], rl)]
+                           + [np.zeros(16, np.uint8)])
+    wins = np.concatenate([w.wins[int(o):int(o) + int(n)] for o, n in zip(w.win_off[idx], wl)]
+                          + [np.zeros(16, np.uint8)])
+    ro = np.concatenate([[0], np.cumsum(rl[:-1], dtype=np.uint64)]).astype(np.uint64)
+    wo = np.concatenate([[0], np.cumsum(wl[:-1], dtype=np.uint64)]).astype(np.uint64)
+    return PairBatch(reads, ro, rl.copy(), wins, wo, wl.copy(), w.band_offset[idx].copy(), None,
+                     w.bandwidth[idx].copy())
 
 
 def _timed(fn) -> float:
@@ -309,8 +320,12 @@ def run_ours(args, rank, local, world, dist):
     def run_sync():
         step()
         torch.cuda.synchronize(dev)
-    tuning = autotune.tune_bsw_shape(ctx, 33, run_sync,
-                                     device_name=torch.cuda.get_device_name(dev))
+    if args.shape >= 0:
+        ctx.check(L.kira_gpu_set_bsw_shape(ctx.handle, 33, args.shape))
+        tuning = {"best": args.shape, "shape": autotune.shapes()[args.shape], "dp_ms": None}
+    else:
+        tuning = autotune.tune_bsw_shape(ctx, 33, run_sync,
+                                         device_name=torch.cuda.get_device_name(dev))
     L.kira_gpu_profile(ctx.handle, 1)
     stage_ms = np.zeros(len(_abi.STAGES))
     sampler = ClockSampler(local)

@@ -132,21 +132,39 @@ int check_sw_cfg(kira_ctx* ctx, const kira_sw_cfg& c, uint32_t max_q, uint32_t m
   if (std::abs((int64_t)c.match_score) > (1 << 20) || std::abs((int64_t)c.mismatch) > (1 << 20))
     return fail(ctx, KIRA_ERR_INVALID, "match/mismatch above the supported range");
   const int need = 2 * (int)std::max<uint32_t>(max_band, 1) + 1;
-  if (need > kBswShapes[kNumBswShapes - 1].g * kBswShapes[kNumBswShapes - 1].k)
+  int cap = 0;
+  for (int s = 0; s < kNumBswShapes; ++s) cap = std::max(cap, shape_cap(kBswShapes[s]));
+  if (need > cap)
     return fail(ctx, KIRA_ERR_INVALID, "bandwidth %u above the supported maximum", max_band);
   return KIRA_OK;
 }
 
-int default_shape(uint32_t max_band) {
+// The int32 shape of the one-launch path: the first whose row covers the band.
+int plain_shape(uint32_t max_band) {
   const int need = 2 * (int)std::max<uint32_t>(max_band, 1) + 1;
   for (int s = 0; s < kNumBswShapes; ++s)
-    if (kBswShapes[s].g * kBswShapes[s].k >= need) return s;
+    if (!kBswShapes[s].packed && shape_cap(kBswShapes[s]) >= need) return s;
   return -1;
 }
 
 bool shape_fits(int s, uint32_t max_band) {
   return s >= 0 && s < kNumBswShapes &&
-         kBswShapes[s].g * kBswShapes[s].k >= 2 * (int)std::max<uint32_t>(max_band, 1) + 1;
+         shape_cap(kBswShapes[s]) >= 2 * (int)std::max<uint32_t>(max_band, 1) + 1;
+}
+
+// A shape can run a batch when its row covers the band and, for a packed int16
+// shape, every value of the batch stays inside the exact int16 range.
+bool shape_usable(int s, uint32_t max_band, uint32_t max_q, const SwParams& sp) {
+  if (!shape_fits(s, max_band)) return false;
+  return !kBswShapes[s].packed || packed_fits(kBswShapes[s], max_q, sp);
+}
+
+// Default: the first packed shape that covers the band and fits int16, else the
+// int32 shape of the one-launch path.
+int default_shape(uint32_t max_band, uint32_t max_q, const SwParams& sp) {
+  for (int s = 0; s < kNumBswShapes; ++s)
+    if (kBswShapes[s].packed && shape_usable(s, max_band, max_q, sp)) return s;
+  return plain_shape(max_band);
 }
 
 struct Maxes {
@@ -235,9 +253,9 @@ int build_planes(kira_ctx* ctx, DevPairs& D, uint64_t read_bytes, uint64_t win_b
 
 // Launch shape of the banded SW stage: the tuned choice for the band class if it
 // covers the band, else the smallest shape that does.
-int pick_shape(const kira_ctx* ctx, uint32_t max_band) {
+int pick_shape(const kira_ctx* ctx, uint32_t max_band, uint32_t max_q, const SwParams& sp) {
   const int t = ctx->tuned_shape[band_class(max_band)];
-  return shape_fits(t, max_band) ? t : default_shape(max_band);
+  return shape_usable(t, max_band, max_q, sp) ? t : default_shape(max_band, max_q, sp);
 }
 
 // Scratch of the banded SW stage for up to `items` items.
@@ -245,8 +263,7 @@ int prepare_bsw(kira_ctx* ctx, uint32_t n_pairs, uint32_t items, const Maxes& mx
                 BswLaunch& B) {
   cudaError_t cerr = cudaSuccess;
   const BswShapeInfo sh = kBswShapes[shape];
-  const uint32_t lane_bytes = 4u * (uint32_t)((sh.k + 7) / 8);
-  const uint32_t row_stride = (uint32_t)sh.g * lane_bytes;
+  const uint32_t row_stride = shape_row_stride(sh);
   const uint64_t slot = (((uint64_t)(mx.q + 1) * row_stride) + 15) & ~15ull;
   const uint32_t meta_stride = mx.q + 1;
   const uint32_t slot_cap = mx.q + mx.w + 2;
@@ -255,7 +272,7 @@ int prepare_bsw(kira_ctx* ctx, uint32_t n_pairs, uint32_t items, const Maxes& mx
   KIRA_DBUF(ends, DpEnd, B_ENDS, std::max<uint32_t>(items, 1));
   KIRA_DBUF(slots, uint32_t, B_CIG_SLOTS, (uint64_t)slot_cap * std::max<uint32_t>(items, 1));
   KIRA_DBUF(iop, uint32_t, B_ITEM_OF_PAIR, std::max<uint32_t>(n_pairs, 1));
-  B.tg = TraceGeom{trace, meta, slot, row_stride, lane_bytes, (uint32_t)sh.k, meta_stride};
+  B.tg = shape_trace_geom(sh, trace, meta, slot, meta_stride);
   B.ends = ends;
   B.cig_slots = slots;
   B.slot_cap = slot_cap;
@@ -294,14 +311,15 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
   int rc = check_sw_cfg(ctx, p.sw, mx.q, mx.band);
   if (rc) return rc;
   if (mx.q > 512) return fail(ctx, KIRA_ERR_READ_TOO_LONG, "read of %u bases > 512", mx.q);
-  const int shape = pick_shape(ctx, mx.band);
+  const SwParams sp = resolve(p.sw);
+  const int shape = pick_shape(ctx, mx.band, mx.q, sp);
+  if (shape < 0) return fail(ctx, KIRA_ERR_INVALID, "no banded-SW shape for band %u", mx.band);
   KIRA_DBUF(ncig, uint32_t, B_NCIG, n);
   KIRA_DBUF(swoff, int32_t, B_SW_OFFSET, n);
   KIRA_DBUF(mlist, uint32_t, B_MYERS_LIST, n);
   KIRA_DBUF(slist, uint32_t, B_SW_LIST, n);
   KIRA_DBUF(counters, uint32_t, B_COUNTERS, 4);
   KIRA_CUDA(cudaMemsetAsync(counters, 0, 16, st));
-  const SwParams sp = resolve(p.sw);
   VerifyDev V{p.sieve_threshold, p.cert_strict, sp, out, detail, ncig, swoff, mlist, counters};
   ctx->ev_recorded = 0;
   mark(ctx, 0, st);
@@ -331,6 +349,7 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
   B.list = slist;
   B.count_dev = counters + 1;
   B.sp = sp;
+  B.bias = packed_bias(kBswShapes[shape], sp);
   B.offset = swoff;
   B.cells = cells_dev;
   B.out = out;
@@ -368,23 +387,33 @@ int bsw_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const ki
   }
   uint32_t base[kBandClasses + 1] = {};
   for (int c = 0; c < kBandClasses; ++c) base[c + 1] = base[c] + cnt[c];
+  // Order: band class, then read length descending (the tail of a launch is
+  // short), stable. Counting sort on (class, qall - q) when the key range is
+  // modest, else a comparison sort.
   std::vector<uint32_t> list(n);
-  {
+  const uint64_t nkeys = (uint64_t)kBandClasses * (qall + 1);
+  if (nkeys <= 4ull * n + (1u << 16)) {
+    std::vector<uint32_t> at(nkeys + 1, 0);
+    auto key = [&](uint32_t i) { return (uint64_t)cls[i] * (qall + 1) + (qall - P.read_len[i]); };
+    for (uint32_t i = 0; i < n; ++i) ++at[key(i) + 1];
+    for (uint64_t k = 0; k < nkeys; ++k) at[k + 1] += at[k];
+    for (uint32_t i = 0; i < n; ++i) list[at[key(i)]++] = i;
+  } else {
     uint32_t at[kBandClasses];
     for (int c = 0; c < kBandClasses; ++c) at[c] = base[c];
     for (uint32_t i = 0; i < n; ++i) list[at[cls[i]]++] = i;
-    for (int c = 0; c < kBandClasses; ++c)  // longest first: the tail of a launch is short
+    for (int c = 0; c < kBandClasses; ++c)
       std::stable_sort(list.begin() + base[c], list.begin() + base[c + 1],
                        [&](uint32_t a, uint32_t b) { return P.read_len[a] > P.read_len[b]; });
   }
+  const SwParams sp = resolve(cfg);
   int shape[kBandClasses];
   uint64_t slot[kBandClasses] = {}, tbase[kBandClasses + 1] = {}, mbase[kBandClasses + 1] = {};
   for (int c = 0; c < kBandClasses; ++c) {
-    shape[c] = cnt[c] ? pick_shape(ctx, bmax[c]) : -1;
+    shape[c] = cnt[c] ? pick_shape(ctx, bmax[c], qmax[c], sp) : -1;
     if (cnt[c] && shape[c] < 0) return fail(ctx, KIRA_ERR_INVALID, "no shape for band %u", bmax[c]);
     if (cnt[c]) {
-      const BswShapeInfo sh = kBswShapes[shape[c]];
-      const uint64_t rs = (uint64_t)sh.g * 4u * (uint64_t)((sh.k + 7) / 8);
+      const uint64_t rs = shape_row_stride(kBswShapes[shape[c]]);
       slot[c] = (((uint64_t)(qmax[c] + 1) * rs) + 15) & ~15ull;
     }
     tbase[c + 1] = tbase[c] + slot[c] * cnt[c];
@@ -400,18 +429,18 @@ int bsw_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const ki
   KIRA_DBUF(work, uint32_t, B_WORK, kBandClasses);
   KIRA_CUDA(cudaMemcpyAsync(dlist, list.data(), 4ull * n, cudaMemcpyHostToDevice, st));
   KIRA_CUDA(cudaMemsetAsync(work, 0, 4 * kBandClasses, st));
-  const SwParams sp = resolve(cfg);
+  BswLaunch L[kBandClasses];
   for (int c = 0; c < kBandClasses; ++c) {
     if (!cnt[c]) continue;
     const BswShapeInfo sh = kBswShapes[shape[c]];
-    const uint32_t lane_bytes = 4u * (uint32_t)((sh.k + 7) / 8);
-    BswLaunch B{};
+    BswLaunch& B = L[c];
+    B = BswLaunch{};
     B.list = dlist + base[c];
     B.count = cnt[c];
     B.sp = sp;
+    B.bias = packed_bias(sh, sp);
     B.offset = D.band_offset;
-    B.tg = TraceGeom{trace + tbase[c], meta + mbase[c], slot[c], (uint32_t)sh.g * lane_bytes,
-                     lane_bytes, (uint32_t)sh.k, qmax[c] + 1};
+    B.tg = shape_trace_geom(sh, trace + tbase[c], meta + mbase[c], slot[c], qmax[c] + 1);
     B.ends = ends + base[c];
     B.cells = cells_dev;
     B.cig_slots = slots + (uint64_t)base[c] * cap;
@@ -423,8 +452,15 @@ int bsw_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const ki
     B.max_q = qmax[c];
     B.work = work + c;
     B.item_base = base[c];
-    KIRA_CUDA(launch_bsw(shape[c], D, B, cnt[c], ctx->sms, st));
   }
+  mark(ctx, 2, st);
+  // Widest class first (longest rows), then the narrower ones fill in behind it.
+  for (int c = kBandClasses - 1; c >= 0; --c)
+    if (cnt[c]) KIRA_CUDA(launch_bsw(shape[c], D, L[c], cnt[c], ctx->sms, st, nullptr, kBswPartDp));
+  mark(ctx, 3, st);
+  for (int c = kBandClasses - 1; c >= 0; --c)
+    if (cnt[c]) KIRA_CUDA(launch_bsw(shape[c], D, L[c], cnt[c], ctx->sms, st, nullptr, kBswPartTb));
+  mark(ctx, 4, st);
   G = BswLaunch{};
   G.item_of_pair = iop;
   G.cig_slots = slots;
@@ -574,7 +610,7 @@ int kira_gpu_bsw_shapes(int* lanes, int* cells, int max_shapes) {
   const int n = std::min(max_shapes, kNumBswShapes);
   for (int i = 0; i < n; ++i) {
     if (lanes) lanes[i] = kBswShapes[i].g;
-    if (cells) cells[i] = kBswShapes[i].k;
+    if (cells) cells[i] = shape_cap(kBswShapes[i]) / kBswShapes[i].g;
   }
   return kNumBswShapes;
 }
@@ -666,10 +702,13 @@ int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg
   int rc = check_sw_cfg(ctx, *cfg, mx.q, mx.band);
   if (rc) return rc;
   DevPairs D;
+  cudaStream_t st = ctx->stream;
+  ctx->ev_recorded = 0;
+  mark(ctx, 0, st);
   rc = upload_pairs(ctx, P, D);
   if (rc) return rc;
+  mark(ctx, 1, st);
   cudaError_t cerr = cudaSuccess;
-  cudaStream_t st = ctx->stream;
   const uint32_t n = P.n;
   KIRA_DBUF(dout, kira_sw_result, B_OUT, n);
   KIRA_DBUF(ncig, uint32_t, B_NCIG, n);
@@ -681,7 +720,9 @@ int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg
   KIRA_CUDA(cudaMemsetAsync(cells_dev, 0, 8, st));
   BswLaunch B{};
   if (ctx->plain) {  // one launch, one shape for the widest band, static order
-    const int shape = default_shape(mx.band);
+    const int shape = plain_shape(mx.band);
+    if (shape < 0)
+      return fail(ctx, KIRA_ERR_INVALID, "band %u above the int32 one-launch maximum", mx.band);
     rc = prepare_bsw(ctx, n, n, mx, shape, B);
     if (rc) return rc;
     B.count = n;
@@ -691,13 +732,17 @@ int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg
     B.out = dout;
     B.ncig = ncig;
     B.flags = counters + 2;
-    KIRA_CUDA(launch_bsw(shape, D, B, n, ctx->sms, st));
+    mark(ctx, 2, st);
+    KIRA_CUDA(launch_bsw(shape, D, B, n, ctx->sms, st, ctx->profile ? ctx->ev[3] : nullptr));
+    if (ctx->profile) ctx->ev_recorded = 4;
+    mark(ctx, 4, st);
   } else {
     rc = bsw_bucketed(ctx, P, D, *cfg, dout, ncig, counters + 2, cells_dev, B, st);
     if (rc) return rc;
   }
   rc = finish_cigars(ctx, n, dout, ncig, B, ops, cigar->cap, total_dev, st);
   if (rc) return rc;
+  mark(ctx, 5, st);
   uint64_t total = 0;
   unsigned long long hcells = 0;
   uint32_t flags[4];
@@ -765,7 +810,7 @@ int kira_gpu_align_batch_simd(kira_ctx* ctx, const kira_pairs* pairs, const kira
   const int cap_need = (int)r0;
   int shape = -1;
   for (int s = 0; s < kNumBswShapes; ++s)
-    if (kBswShapes[s].g * kBswShapes[s].k >= cap_need) {
+    if (!kBswShapes[s].packed && shape_cap(kBswShapes[s]) >= cap_need) {
       shape = s;
       break;
     }

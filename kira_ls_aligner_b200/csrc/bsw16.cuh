@@ -1,0 +1,370 @@
+// bsw16.cuh -- banded affine Smith-Waterman on packed int16 lanes (two cells per
+// 32-bit register), bit-exact with the int32 sweep of bsw.cuh / banded_sw_with
+// (src/alignment/mod.rs:1370-1650) whenever the host-side range check passes.
+//
+// Layout
+//   A group of G lanes owns one pair. The row (capacity 2H cells, H = G*K) is cut
+//   in two halves: word k of lane g holds cell c = g*K + k in its low 16 bits and
+//   cell H + c in its high 16 bits, so every per-row quantity (band start, shift,
+//   argmax, x-drop) stays one scalar per pair while the DP arithmetic runs two
+//   cells per instruction with the DPX s16x2 forms (__viaddmax_s16x2,
+//   __vimax_s16x2_relu, __vibmax_s16x2).
+//
+// Biased values
+//   Every DP value v is kept as v + B (B = bias >= gof + 2H*ge + mismatch + 1), so
+//   all stored halves are non-negative and below 2^13 (checked on the host). That
+//   makes plain 32-bit IADD/IADD3 exact on packed words (no carry crosses the
+//   half boundary when each half's result stays in [0, 2^16)), and turns every
+//   comparison into the sign of a biased difference: 2^p + a - b has bit p set iff
+//   a >= b when |a - b| < 2^p. The five trace flags are produced that way at
+//   distinct bit positions (15..11) and merged with bit-select LOP3s.
+//
+// Band edges
+//   Cells outside the previous row's band read as "neutral" (H = 0, E = the
+//   biased floor 0): a diagonal predecessor out of band then contributes 0 + s
+//   (the reference's scored-restart quirk, mod.rs:1464-1480) and an upper
+//   predecessor out of band yields E = -gof instead of i32::MIN/4, which never
+//   wins a cell, never ties a nonzero H and never sets an extend flag, so H,
+//   directions and flags equal the reference's. The invariant is kept by masking
+//   the cells at and beyond the row length after each row.
+#pragma once
+
+#include "common.cuh"
+
+namespace kira {
+
+template <int G, int K>
+struct Bsw16Shape {
+  static constexpr int kHalf = G * K;                  // cells per half row
+  static constexpr int kCap = 2 * kHalf;               // cells per row
+  static constexpr int kWords = (K + 1) / 2;           // trace words per lane per row
+  static constexpr int kLaneBytes = 4 * kWords;        // one code byte per cell
+  static constexpr int kRowStride = G * kLaneBytes;
+};
+
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+  uint32_t r;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
+  return r;
+}
+
+// Bits of `y` where m is set, bits of `x` elsewhere (one LOP3).
+__device__ __forceinline__ uint32_t bsel(uint32_t x, uint32_t y, uint32_t m) {
+  return (x & ~m) | (y & m);
+}
+
+// Both halves of a packed word as the same 16-bit value (two's complement).
+__host__ __device__ __forceinline__ uint32_t pk2(int32_t v) {
+  return ((uint32_t)v & 0xFFFFu) * 0x10001u;
+}
+
+// (lo, hi) as an integer sum hi * 2^16 + lo: the form that 32-bit IADD adds per
+// half when both halves' results stay inside [0, 2^16).
+__host__ __device__ __forceinline__ uint32_t isum(int32_t lo, int32_t hi) {
+  return (uint32_t)hi * 65536u + (uint32_t)lo;
+}
+
+// Realign the packed previous row by `s` cells (cell c <- old cell c + s); old
+// cells outside [0, prev_len) become neutral. Each group stages the row as
+// 16-bit halves in its own shared-memory strip [h: 2H][e: 2H].
+template <int G, int K>
+__device__ __forceinline__ void bsw16_realign(uint32_t (&ph)[K], uint32_t (&pe)[K], int32_t s,
+                                              int32_t prev_len, uint16_t* buf, int32_t c0,
+                                              uint32_t b2, uint32_t gmask) {
+  constexpr int H = G * K;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    buf[c0 + k] = (uint16_t)(ph[k] & 0xFFFFu);
+    buf[H + c0 + k] = (uint16_t)(ph[k] >> 16);
+    buf[2 * H + c0 + k] = (uint16_t)(pe[k] & 0xFFFFu);
+    buf[3 * H + c0 + k] = (uint16_t)(pe[k] >> 16);
+  }
+  __syncwarp(gmask);
+  const uint32_t bias = b2 & 0xFFFFu;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int32_t a = c0 + k + s, b = H + c0 + k + s;
+    const bool va = a >= 0 && a < prev_len, vb = b >= 0 && b < prev_len;
+    const uint32_t hl = va ? (uint32_t)buf[a] : bias, hh = vb ? (uint32_t)buf[b] : bias;
+    const uint32_t el = va ? (uint32_t)buf[2 * H + a] : 0u, eh = vb ? (uint32_t)buf[2 * H + b] : 0u;
+    ph[k] = hl | (hh << 16);
+    pe[k] = el | (eh << 16);
+  }
+  __syncwarp(gmask);
+}
+
+// Activity masks for a row of `row_len` cells: 0xFFFF per active half.
+template <int G, int K>
+__device__ __forceinline__ void bsw16_act(uint32_t (&act)[K], int32_t row_len, int32_t c0) {
+  constexpr int H = G * K;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    act[k] = (c0 + k < row_len ? 0x0000FFFFu : 0u) | (H + c0 + k < row_len ? 0xFFFF0000u : 0u);
+}
+
+template <int G, int K>
+__device__ __forceinline__ void bsw16_group_sweep(
+    const uint8_t* __restrict__ rd, uint32_t q, const uint8_t* __restrict__ wn, uint32_t w,
+    int32_t band, int32_t offset, int32_t abort_score, const SwParams& sp, int32_t bias,
+    uint16_t* rowbuf, uint8_t* __restrict__ trace, uint32_t* __restrict__ meta, uint32_t g,
+    uint32_t gmask, DpEnd& out, uint64_t& cells_out) {
+  constexpr int H = G * K;
+  constexpr int NW = Bsw16Shape<G, K>::kWords;
+  constexpr int LB = Bsw16Shape<G, K>::kLaneBytes;
+  constexpr int S = Bsw16Shape<G, K>::kRowStride;
+  const int32_t gi = (int32_t)g;
+  const int32_t c0 = gi * K;
+  const int32_t match = sp.match, mism = sp.mismatch, gof = sp.gof, ge = sp.gap_extend;
+  // Packed constants (per-half two's complement for DPX, integer sums for IADD).
+  const uint32_t B2 = pk2(bias);
+  const uint32_t MAT2 = pk2(match), MIS2 = pk2(-mism), NGE2 = pk2(-ge);
+  const uint32_t GOFS = isum(gof, gof);
+  const uint32_t FOFS = isum(ge - gof, ge - gof);              // f = run - C_k + (ge - gof)
+  const uint32_t NZC = isum(0x8000 - bias - 1, 0x8000 - bias - 1);
+  const uint32_t C0 = isum(c0 * ge - gof, (H + c0) * ge - gof);  // C_k = idx*ge - gof
+  const uint32_t GE2S = isum(ge, ge);
+
+  int32_t prev_start = 1, prev_len = 0, act_len = -1;
+  int32_t best = 0, bi = 0, bj = 0, bq = 0, bqj = 0;
+  uint32_t early = 0;
+  uint64_t cells = 0;
+  const int32_t drift = sp.adaptive ? sp.max_drift : 0;
+  int32_t acenter = 1 + offset;
+  const int32_t wl = (int32_t)w;
+  uint32_t ph[K], pe[K], act[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    ph[k] = B2;
+    pe[k] = 0u;
+    act[k] = 0u;
+  }
+
+  for (uint32_t iu = 1; iu <= q; ++iu) {
+    const int32_t i = (int32_t)iu;
+    const int32_t sc = i + offset;
+    const int32_t center = sp.adaptive ? min(max(acenter, sc - drift), sc + drift) : sc;
+    const int32_t js = max(center - band, 1);
+    const int32_t je = min(center + band, wl);
+    if (js > je) {  // mod.rs:1437-1444: row skipped, no centre / x-drop update
+      if (g == 0) meta[i] = (1u << 11);
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        ph[k] = B2;
+        pe[k] = 0u;
+      }
+      prev_len = 0;
+      prev_start = 1;
+      continue;
+    }
+    const int32_t row_len = je - js + 1;
+    cells += (uint64_t)row_len;
+    const uint32_t qb = ldb(rd, (uint64_t)(i - 1));
+    const uint32_t qb2 = qb * 0x10001u;
+    const int32_t sft = js - prev_start - 1;
+    if (sft != 0 && prev_len > 0) bsw16_realign<G, K>(ph, pe, sft, prev_len, rowbuf, c0, B2, gmask);
+    if (row_len != act_len) {
+      bsw16_act<G, K>(act, row_len, c0);
+      act_len = row_len;
+    }
+    // Upper neighbours of the last word: the next lane's first word; for the last
+    // lane the low half continues into cell H (lane 0's high half) and the high
+    // half runs past the capacity (neutral).
+    uint32_t nh = __shfl_sync(gmask, ph[0], (gi + 1) & (G - 1), G);
+    uint32_t ne = __shfl_sync(gmask, pe[0], (gi + 1) & (G - 1), G);
+    if (gi == G - 1) {
+      nh = prmt(nh, B2, 0x5432u);
+      ne = prmt(ne, 0u, 0x5432u);
+    }
+    const uint8_t* wrow = wn + (js - 1);
+    const int32_t rl1 = row_len - 1;
+
+    // Pass 1: E (+ extend flag), H_diag + s, the diag-vs-E flag, max(Hdiag+s, E)
+    // and the F-scan operand G = max(Hdiag+s, E, 0) - gof + idx*ge.
+    uint32_t m1[K], gv[K], ev[K], code[K];
+    uint32_t lmax = 0u;
+    uint32_t ck = C0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const uint32_t uh = k + 1 < K ? ph[k + 1 < K ? k + 1 : 0] : nh;
+      const uint32_t ue = k + 1 < K ? pe[k + 1 < K ? k + 1 : 0] : ne;
+      const uint32_t t = uh - GOFS;                      // H_up - gof
+      const uint32_t e = __viaddmax_s16x2(ue, NGE2, t);  // max(E_up - ge, H_up - gof)
+      const uint32_t yee = e + 0x0FFF0FFFu - t;          // bit 12: e > t (E extended)
+      const uint32_t bl = __ldg(wrow + min(c0 + k, rl1));
+      const uint32_t bh = __ldg(wrow + min(H + c0 + k, rl1));
+      const uint32_t x = prmt(bl, bh, 0x5410u) ^ qb2;    // per half: 0 iff bases equal
+      const uint32_t ms = prmt(x + 0x7FFF7FFFu, 0u, 0xBB99u);  // 0xFFFF per mismatching half
+      const uint32_t s2 = bsel(MAT2, MIS2, ms);
+      const uint32_t hm = __viaddmax_s16x2(ph[k], s2, B2);     // max(Hdiag + s, 0)
+      const uint32_t y1 = hm + 0x40004000u - e;          // bit 14: hm >= e
+      const uint32_t mm = __vimax_s16x2_relu(hm, e);
+      const uint32_t gk = mm + ck;
+      code[k] = bsel(y1, yee, 0x10001000u);
+      m1[k] = mm;
+      gv[k] = gk;
+      ev[k] = e;
+      lmax = __vimax_s16x2_relu(lmax, gk);
+      ck += GE2S;
+    }
+    // Cross-lane inclusive max-scan of G per half; exclusive value per lane, then
+    // the high half also sees every low-half cell (they precede it in the row).
+    uint32_t v = lmax;
+#pragma unroll
+    for (int off = 1; off < G; off <<= 1) {
+      const uint32_t tt = __shfl_up_sync(gmask, v, off, G);
+      if (gi >= off) v = __vimax_s16x2_relu(v, tt);
+    }
+    uint32_t excl = __shfl_up_sync(gmask, v, 1, G);
+    if (gi == 0) excl = 0u;
+    const uint32_t tot = __shfl_sync(gmask, v, G - 1, G);
+    excl = __vimax_s16x2_relu(excl, prmt(tot, 0u, 0x1054u));
+    uint32_t gp = __shfl_sync(gmask, gv[K - 1], (gi + G - 1) & (G - 1), G);
+    if (gi == 0) gp = prmt(gp, 0u, 0x1054u);
+
+    // Pass 2: F, H, the remaining flags; neutralise inactive cells.
+    uint32_t run = excl;
+    ck = C0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const uint32_t f = run - ck + FOFS;                // max_{k<idx} G - (idx-1)*ge
+      const uint32_t h = __vimax_s16x2_relu(m1[k], f);
+      const uint32_t y2 = m1[k] + 0x20002000u - f;       // bit 13: max(hm, e) >= f
+      const uint32_t ynz = h + NZC;                      // bit 15: h > 0
+      const uint32_t yfe = gp + 0x08000800u - run;       // bit 11: F not extended
+      uint32_t c = bsel(code[k], y2, 0x20002000u);
+      c = bsel(c, ynz, 0x80008000u);
+      code[k] = bsel(c, yfe, 0x08000800u);
+      run = __vimax_s16x2_relu(run, gv[k]);
+      gp = gv[k];
+      ph[k] = bsel(B2, h, act[k]);
+      pe[k] = ev[k] & act[k];
+      ck += GE2S;
+    }
+    uint32_t* trow = reinterpret_cast<uint32_t*>(trace + (size_t)i * S + (size_t)g * LB);
+#pragma unroll
+    for (int x = 0; x < NW; ++x)
+      trow[x] = prmt(code[2 * x], code[2 * x + 1 < K ? 2 * x + 1 : 2 * x], 0x7531u);
+    if (g == 0) meta[i] = ((uint32_t)js << 11) | (uint32_t)row_len;
+
+    // Row max and its first cell: per half the first k with the max (descending
+    // scan keeps ties at the lowest k), then one 32-bit key per lane.
+    uint32_t mx = 0u;
+    int32_t ilo = 0, ihi = 0;
+#pragma unroll
+    for (int k = K - 1; k >= 0; --k) {
+      bool phi, plo;
+      mx = __vibmax_s16x2(ph[k], mx, &phi, &plo);
+      ilo = plo ? k : ilo;
+      ihi = phi ? k : ihi;
+    }
+    const uint32_t klo = ((mx & 0xFFFFu) << 11) | (uint32_t)(2047 - (c0 + ilo));
+    const uint32_t khi = ((mx >> 16) << 11) | (uint32_t)(2047 - (H + c0 + ihi));
+    uint32_t key = max(klo, khi);
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) key = max(key, __shfl_xor_sync(gmask, key, off, G));
+    const int32_t row_best = (int32_t)(key >> 11) - bias;
+    const int32_t row_best_j = row_best > 0 ? js + (2047 - (int32_t)(key & 2047u)) : -1;
+    if (row_best > best) {
+      best = row_best;
+      bi = i;
+      bj = row_best_j;
+    }
+    if (iu == q && row_best > bq) {
+      bq = row_best;
+      bqj = row_best_j;
+    }
+    prev_start = js;
+    prev_len = row_len;
+    if (sp.adaptive) {  // mod.rs:1546-1559
+      const int32_t raw = row_best_j >= 0 ? row_best_j + 1 : acenter + 1;
+      const int32_t sn = i + 1 + offset;
+      acenter = min(max(raw, sn - drift), sn + drift);
+    }
+    if (sp.dp_xdrop > 0 && best - row_best > sp.dp_xdrop) {  // mod.rs:1561-1564
+      early = 1;
+      break;
+    }
+    if (abort_score > kAbortOff) {  // mod.rs:1565-1572
+      const int32_t remaining = (int32_t)(q - iu);
+      if (best + remaining * match < abort_score) {
+        early = 1;
+        break;
+      }
+    }
+  }
+  if (bq > 0 && sat_add(bq, sp.clip) > best) {  // mod.rs:1575-1579
+    best = bq;
+    bi = (int32_t)q;
+    bj = bqj;
+  }
+  out.score = best;
+  out.end_i = bi;
+  out.end_j = bj;
+  out.early_abort = early;
+  cells_out = cells;
+}
+
+// Traceback over the packed kernel's byte codes (state machine of
+// mod.rs:1581-1627). Code byte of a cell: bit 7 H > 0, bit 6 diag >= E,
+// bit 5 max(diag, E) >= F, bit 4 E extended, bit 3 F NOT extended.
+__device__ __forceinline__ uint32_t bsw16_walk(const uint8_t* __restrict__ trace,
+                                               const uint32_t* __restrict__ meta, uint32_t k_words,
+                                               uint32_t half, uint32_t lane_bytes,
+                                               uint32_t row_stride, int32_t go, int32_t& i,
+                                               int32_t& j, uint32_t* __restrict__ ops,
+                                               uint32_t cap, uint32_t& overflow) {
+  int state = 0;  // 0 H, 1 E, 2 F
+  uint32_t n = 0, cur_op = 0xFFu, cur_len = 0;
+  auto push = [&](uint32_t op) {
+    if (op == cur_op) {
+      ++cur_len;
+      return;
+    }
+    if (cur_len) {
+      if (n < cap) ops[n] = (cur_len << 4) | cur_op;
+      else overflow = 1;
+      ++n;
+    }
+    cur_op = op;
+    cur_len = 1;
+  };
+  while (i > 0 && j > 0) {
+    const uint32_t m = __ldg(meta + i);
+    const int32_t rs = (int32_t)(m >> 11), rl = (int32_t)(m & 2047u);
+    const int32_t idx = j - rs;
+    if (idx < 0 || idx >= rl) break;
+    const uint32_t hi = (uint32_t)idx >= half ? 1u : 0u;
+    const uint32_t c = (uint32_t)idx - hi * half;
+    const uint32_t gi = c / k_words, kk = c - gi * k_words;
+    const uint32_t b = trace[(size_t)i * row_stride + gi * lane_bytes + (kk >> 1) * 4u +
+                             (kk & 1u) * 2u + hi];
+    if (state == 0) {
+      if (!(b & 0x80u)) break;  // H == 0
+      if ((b & 0x60u) == 0x60u) {
+        push(0);
+        --i;
+        --j;
+      } else if (b & 0x20u) {
+        state = 1;
+      } else {
+        state = 2;
+      }
+    } else if (state == 1) {
+      push(1);
+      --i;
+      state = (b & 0x10u) ? 1 : 0;
+    } else {
+      push(2);
+      --j;
+      state = (go > 0 && !(b & 0x08u)) ? 2 : 0;
+    }
+  }
+  if (cur_len) {
+    if (n < cap) ops[n] = (cur_len << 4) | cur_op;
+    else overflow = 1;
+    ++n;
+  }
+  return n;
+}
+
+}  // namespace kira

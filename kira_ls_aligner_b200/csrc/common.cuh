@@ -45,8 +45,9 @@ struct TraceGeom {
   uint64_t slot_bytes;
   uint32_t row_stride;
   uint32_t lane_bytes;
-  uint32_t k_cells;     // cells per lane (K)
+  uint32_t k_cells;     // cells per lane (K); packed shapes: words per lane
   uint32_t meta_stride; // words per item
+  uint32_t half;        // packed shapes: cells per half row (G*K); 0: int32 nibble trace
 };
 
 // Per-item DP result consumed by the traceback kernel.

@@ -78,6 +78,7 @@ struct BswLaunch {
   // bucketed launches
   uint32_t* work;             // dynamic work counter (null: static grid-stride order)
   uint32_t item_base;         // global index of this launch's first item (CIGAR slots)
+  int32_t bias;               // packed int16 shapes: value bias (packed_bias)
 };
 
 struct CompactLaunch {
@@ -92,11 +93,43 @@ struct CompactLaunch {
   uint64_t cap;
 };
 
+// Banded-SW launch shape: G lanes per pair, K cells (int32) or K packed words of
+// two int16 cells (packed) per lane.
 struct BswShapeInfo {
-  int g, k, threads, min_blocks;
+  int g, k, threads, min_blocks, packed;
 };
 extern const BswShapeInfo kBswShapes[];
 extern const int kNumBswShapes;
+
+inline int shape_cap(const BswShapeInfo& s) { return (s.packed ? 2 : 1) * s.g * s.k; }
+inline uint32_t shape_lane_bytes(const BswShapeInfo& s) {
+  return s.packed ? 4u * (uint32_t)((s.k + 1) / 2) : 4u * (uint32_t)((s.k + 7) / 8);
+}
+inline uint32_t shape_row_stride(const BswShapeInfo& s) {
+  return (uint32_t)s.g * shape_lane_bytes(s);
+}
+inline TraceGeom shape_trace_geom(const BswShapeInfo& s, uint8_t* trace, uint32_t* meta,
+                                  uint64_t slot_bytes, uint32_t meta_stride) {
+  return TraceGeom{trace, meta, slot_bytes, shape_row_stride(s), shape_lane_bytes(s),
+                   (uint32_t)s.k, meta_stride, s.packed ? (uint32_t)(s.g * s.k) : 0u};
+}
+
+// Bias of the packed int16 sweep: every biased DP value is >= 0 (F at the far
+// end of a row included) and the first cell's F sentinel stays below H = 0.
+inline int32_t packed_bias(const BswShapeInfo& s, const SwParams& sp) {
+  return sp.gof + shape_cap(s) * sp.gap_extend + sp.mismatch + 1;
+}
+
+// The packed sweep is exact when every biased value stays below 2^13 and every
+// difference its flags test stays below 2^11 (the F-extend flag at bit 11).
+inline bool packed_fits(const BswShapeInfo& s, uint32_t max_q, const SwParams& sp) {
+  if (!s.packed) return false;
+  if (sp.match < 0 || sp.mismatch < 0 || sp.gap_open < 0 || sp.gap_extend < 0) return false;
+  const int64_t top = (int64_t)max_q * sp.match;
+  const int64_t cap = shape_cap(s);
+  if (top + cap * sp.gap_extend + sp.gof >= 2048) return false;
+  return top + (int64_t)packed_bias(s, sp) + cap * sp.gap_extend < 8192;
+}
 
 cudaError_t launch_sieve_dropin(const SieveJobsDev& J, kira_sieve_result* out, int sms,
                                 cudaStream_t st);
@@ -107,8 +140,12 @@ cudaError_t launch_verify_sieve(const DevPairs& P, const VerifyDev& V, uint32_t 
                                 cudaStream_t st);
 cudaError_t launch_myers(const DevPairs& P, const MyersLaunch& M, uint32_t max_items, int sms,
                          cudaStream_t st);
+// Banded SW: the DP sweep (kBswPartDp) and/or the traceback (kBswPartTb); an
+// event given as `between` is recorded after the DP part.
+constexpr int kBswPartDp = 1, kBswPartTb = 2;
 cudaError_t launch_bsw(int shape, const DevPairs& P, const BswLaunch& B, uint32_t max_items,
-                       int sms, cudaStream_t st, cudaEvent_t between = nullptr);
+                       int sms, cudaStream_t st, cudaEvent_t between = nullptr,
+                       int parts = kBswPartDp | kBswPartTb);
 cudaError_t launch_cigar_scan(const uint32_t* ncig, uint32_t n, uint32_t* off,
                               uint32_t* chunk_sums, uint64_t* total_dev, cudaStream_t st);
 cudaError_t launch_cigar_compact(const CompactLaunch& C, int sms, cudaStream_t st);

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include "bsw.cuh"
+#include "bsw16.cuh"
 #include "internal.h"
 #include "myers.cuh"
 #include "planes.cuh"
@@ -395,6 +396,55 @@ __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B
   }
 }
 
+// Packed int16 sweep (bsw16.cuh); same item loop and outputs as bsw_dp_kernel.
+template <int G, int K, int T, int MINB>
+__global__ void __launch_bounds__(T, MINB) bsw16_dp_kernel(DevPairs P, BswLaunch B) {
+  extern __shared__ uint16_t bsw16_smem[];
+  constexpr int CAP = 2 * G * K;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t g = lane % G;
+  const uint32_t gw = lane / G;
+  const uint32_t gmask = (G == 32) ? 0xFFFFFFFFu : (((1u << G) - 1u) << (gw * G));
+  const uint32_t groups_per_block = blockDim.x / G;
+  const uint32_t group_in_block = threadIdx.x / G;
+  uint16_t* rowbuf = bsw16_smem + (size_t)group_in_block * 4u * G * K;  // per group
+  const uint32_t count = B.count_dev ? *B.count_dev : B.count;
+  const uint32_t ngroups = gridDim.x * groups_per_block;
+  uint32_t item = blockIdx.x * groups_per_block + group_in_block;
+  for (;;) {
+    if (B.work) {
+      uint32_t t = 0;
+      if (g == 0) t = atomicAdd(B.work, 1u);
+      item = __shfl_sync(gmask, t, gw * G);
+    }
+    if (item >= count) break;
+    const uint32_t pair = B.list ? B.list[item] : item;
+    const uint32_t q = P.read_len[pair], w = P.win_len[pair];
+    const int32_t band = max(P.bandwidth ? P.bandwidth[pair] : B.sp.band, 1);
+    const int32_t offset = B.offset ? B.offset[pair] : 0;
+    const int32_t abort_score = P.abort_score ? P.abort_score[pair] : kAbortOff;
+    DpEnd end;
+    uint64_t cells = 0;
+    if (q > B.max_q || 2 * band + 1 > CAP) {  // outside the shape
+      if (g == 0) {
+        B.ends[item] = DpEnd{0, 0, 0, 0};
+        atomicOr(B.flags, 2u);
+      }
+      if (!B.work) item += ngroups;
+      continue;
+    }
+    bsw16_group_sweep<G, K>(P.read_seq + P.read_off[pair], q, P.win_seq + P.win_off[pair], w,
+                            band, offset, abort_score, B.sp, B.bias, rowbuf,
+                            B.tg.trace + (size_t)item * B.tg.slot_bytes,
+                            B.tg.meta + (size_t)item * B.tg.meta_stride, g, gmask, end, cells);
+    if (g == 0) {
+      B.ends[item] = end;
+      if (B.cells) atomicAdd(B.cells, (unsigned long long)cells);
+    }
+    if (!B.work) item += ngroups;
+  }
+}
+
 __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
   const uint32_t count = B.count_dev ? *B.count_dev : B.count;
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -403,10 +453,14 @@ __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
     const DpEnd e = B.ends[item];
     int32_t i = e.end_i, j = e.end_j;
     uint32_t overflow = 0;
-    const uint32_t n = bsw_walk(B.tg.trace + (size_t)item * B.tg.slot_bytes,
-                                B.tg.meta + (size_t)item * B.tg.meta_stride, B.tg.k_cells,
-                                B.tg.lane_bytes, B.tg.row_stride, i, j,
-                                B.cig_slots + (size_t)item * B.slot_cap, B.slot_cap, overflow);
+    const uint8_t* tr = B.tg.trace + (size_t)item * B.tg.slot_bytes;
+    const uint32_t* mt = B.tg.meta + (size_t)item * B.tg.meta_stride;
+    uint32_t* ops = B.cig_slots + (size_t)item * B.slot_cap;
+    const uint32_t n =
+        B.tg.half ? bsw16_walk(tr, mt, B.tg.k_cells, B.tg.half, B.tg.lane_bytes, B.tg.row_stride,
+                               B.sp.gap_open, i, j, ops, B.slot_cap, overflow)
+                  : bsw_walk(tr, mt, B.tg.k_cells, B.tg.lane_bytes, B.tg.row_stride, i, j, ops,
+                             B.slot_cap, overflow);
     kira_sw_result r;
     r.score = e.score;
     r.ref_start = (uint32_t)j;
@@ -634,50 +688,91 @@ cudaError_t launch_myers(const DevPairs& P, const MyersLaunch& M, uint32_t max_i
 
 template <int G, int K, int T, int MINB>
 static cudaError_t launch_bsw_shape(const DevPairs& P, const BswLaunch& B, uint32_t max_items,
-                                    int sms, cudaStream_t st, cudaEvent_t between) {
-  constexpr int threads = T;
-  const size_t smem = (size_t)(threads / 32) * 2 * K * 32 * sizeof(int32_t);
-  auto kern = B.full ? bsw_dp_kernel<G, K, T, MINB, true> : bsw_dp_kernel<G, K, T, MINB, false>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
-  if (per_sm < 1) per_sm = 1;
-  const int blocks = grid_for(max_items, threads / G, sms * per_sm);
-  kern<<<blocks, threads, smem, st>>>(P, B);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  if (B.full && B.rowkeys) {
-    const int rb = (int)((B.count + 127) / 128);
-    bsw_full_done_kernel<<<rb, 128, 0, st>>>(P, B);
-    bsw_full_resolve_kernel<<<rb, 128, 0, st>>>(P, B);
+                                    int sms, cudaStream_t st, cudaEvent_t between, int parts) {
+  cudaError_t e = cudaSuccess;
+  if (parts & kBswPartDp) {
+    constexpr int threads = T;
+    const size_t smem = (size_t)(threads / 32) * 2 * K * 32 * sizeof(int32_t);
+    auto kern = B.full ? bsw_dp_kernel<G, K, T, MINB, true> : bsw_dp_kernel<G, K, T, MINB, false>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (per_sm < 1) per_sm = 1;
+    const int blocks = grid_for(max_items, threads / G, sms * per_sm);
+    kern<<<blocks, threads, smem, st>>>(P, B);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (B.full && B.rowkeys) {
+      const int rb = (int)((B.count + 127) / 128);
+      bsw_full_done_kernel<<<rb, 128, 0, st>>>(P, B);
+      bsw_full_resolve_kernel<<<rb, 128, 0, st>>>(P, B);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (between) cudaEventRecord(between, st);
+  if (parts & kBswPartTb) {
+    const int tb_blocks = grid_for(max_items, 128, sms * 16);
+    bsw_tb_kernel<<<tb_blocks, 128, 0, st>>>(P, B);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+template <int G, int K, int T, int MINB>
+static cudaError_t launch_bsw16_shape(const DevPairs& P, const BswLaunch& B, uint32_t max_items,
+                                      int sms, cudaStream_t st, cudaEvent_t between, int parts) {
+  cudaError_t e = cudaSuccess;
+  if (parts & kBswPartDp) {
+    const size_t smem = (size_t)T * 8u * K;  // per group 4 * G * K halves
+    auto kern = bsw16_dp_kernel<G, K, T, MINB>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, smem);
+    if (per_sm < 1) per_sm = 1;
+    const int blocks = grid_for(max_items, T / G, sms * per_sm);
+    kern<<<blocks, T, smem, st>>>(P, B);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   if (between) cudaEventRecord(between, st);
-  const int tb_blocks = grid_for(max_items, 128, sms * 16);
-  bsw_tb_kernel<<<tb_blocks, 128, 0, st>>>(P, B);
-  return cudaGetLastError();
+  if (parts & kBswPartTb) {
+    const int tb_blocks = grid_for(max_items, 128, sms * 16);
+    bsw_tb_kernel<<<tb_blocks, 128, 0, st>>>(P, B);
+    e = cudaGetLastError();
+  }
+  return e;
 }
 
 // Launch shapes (lanes per pair, cells per lane, threads per block, min resident
 // blocks per SM). The host picks the first shape whose G*K covers 2*band+1
 // unless a tuned choice is installed for the band (autotuner / override).
 const BswShapeInfo kBswShapes[] = {
-    {4, 10, 256, 2},  {4, 17, 128, 4},  {4, 17, 128, 3},  {8, 10, 256, 2},
-    {8, 17, 128, 3},  {16, 17, 128, 3}, {32, 17, 128, 3},
+    {4, 10, 256, 2, 0},  {4, 17, 128, 4, 0},  {4, 17, 128, 3, 0}, {8, 10, 256, 2, 0},
+    {8, 17, 128, 3, 0},  {16, 17, 128, 3, 0}, {32, 17, 128, 3, 0},
+    // packed int16: K words = 2K cells per lane
+    {2, 9, 256, 2, 1},   {4, 5, 256, 2, 1},   {4, 9, 256, 2, 1},  {8, 5, 256, 2, 1},
+    {8, 9, 256, 2, 1},   {16, 9, 256, 2, 1},  {32, 9, 256, 2, 1},
 };
 const int kNumBswShapes = sizeof(kBswShapes) / sizeof(kBswShapes[0]);
 
 cudaError_t launch_bsw(int shape, const DevPairs& P, const BswLaunch& B, uint32_t max_items,
-                       int sms, cudaStream_t st, cudaEvent_t between) {
+                       int sms, cudaStream_t st, cudaEvent_t between, int parts) {
   switch (shape) {
-    case 0: return launch_bsw_shape<4, 10, 256, 2>(P, B, max_items, sms, st, between);
-    case 1: return launch_bsw_shape<4, 17, 128, 4>(P, B, max_items, sms, st, between);
-    case 2: return launch_bsw_shape<4, 17, 128, 3>(P, B, max_items, sms, st, between);
-    case 3: return launch_bsw_shape<8, 10, 256, 2>(P, B, max_items, sms, st, between);
-    case 4: return launch_bsw_shape<8, 17, 128, 3>(P, B, max_items, sms, st, between);
-    case 5: return launch_bsw_shape<16, 17, 128, 3>(P, B, max_items, sms, st, between);
-    case 6: return launch_bsw_shape<32, 17, 128, 3>(P, B, max_items, sms, st, between);
+    case 0: return launch_bsw_shape<4, 10, 256, 2>(P, B, max_items, sms, st, between, parts);
+    case 1: return launch_bsw_shape<4, 17, 128, 4>(P, B, max_items, sms, st, between, parts);
+    case 2: return launch_bsw_shape<4, 17, 128, 3>(P, B, max_items, sms, st, between, parts);
+    case 3: return launch_bsw_shape<8, 10, 256, 2>(P, B, max_items, sms, st, between, parts);
+    case 4: return launch_bsw_shape<8, 17, 128, 3>(P, B, max_items, sms, st, between, parts);
+    case 5: return launch_bsw_shape<16, 17, 128, 3>(P, B, max_items, sms, st, between, parts);
+    case 6: return launch_bsw_shape<32, 17, 128, 3>(P, B, max_items, sms, st, between, parts);
+    case 7: return launch_bsw16_shape<2, 9, 256, 2>(P, B, max_items, sms, st, between, parts);
+    case 8: return launch_bsw16_shape<4, 5, 256, 2>(P, B, max_items, sms, st, between, parts);
+    case 9: return launch_bsw16_shape<4, 9, 256, 2>(P, B, max_items, sms, st, between, parts);
+    case 10: return launch_bsw16_shape<8, 5, 256, 2>(P, B, max_items, sms, st, between, parts);
+    case 11: return launch_bsw16_shape<8, 9, 256, 2>(P, B, max_items, sms, st, between, parts);
+    case 12: return launch_bsw16_shape<16, 9, 256, 2>(P, B, max_items, sms, st, between, parts);
+    case 13: return launch_bsw16_shape<32, 9, 256, 2>(P, B, max_items, sms, st, between, parts);
     default: return cudaErrorInvalidValue;
   }
 }

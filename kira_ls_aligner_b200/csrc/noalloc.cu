@@ -89,7 +89,7 @@ extern "C" int kira_gpu_bsw_batch_noalloc(const kira_pairs* pairs, const kira_sw
   const int need = 2 * (int)max_band + 1;
   int shape = -1;
   for (int s = 0; s < kNumBswShapes; ++s)
-    if (kBswShapes[s].g * kBswShapes[s].k >= need) {
+    if (!kBswShapes[s].packed && shape_cap(kBswShapes[s]) >= need) {
       shape = s;
       break;
     }
@@ -99,8 +99,7 @@ extern "C" int kira_gpu_bsw_batch_noalloc(const kira_pairs* pairs, const kira_sw
   if (scratch_address(&sp) != cudaSuccess) return KIRA_ERR_RUNTIME;
   const uint32_t n = P.n;
   const BswShapeInfo sh = kBswShapes[shape];
-  const uint32_t lane_bytes = 4u * (uint32_t)((sh.k + 7) / 8);
-  const uint32_t row_stride = (uint32_t)sh.g * lane_bytes;
+  const uint32_t row_stride = shape_row_stride(sh);
   const uint64_t slot = (((uint64_t)(max_q + 1) * row_stride) + 15) & ~15ull;
   const uint32_t meta_stride = max_q + 1;
   const uint32_t slot_cap = max_q + max_w + 2;
@@ -141,7 +140,7 @@ extern "C" int kira_gpu_bsw_batch_noalloc(const kira_pairs* pairs, const kira_sw
   s.gof = c.gap_open + c.gap_extend;
   B.sp = s;
   B.offset = P.band_offset;
-  B.tg = TraceGeom{trace, meta, slot, row_stride, lane_bytes, (uint32_t)sh.k, meta_stride};
+  B.tg = shape_trace_geom(sh, trace, meta, slot, meta_stride);
   B.ends = ends;
   B.cells = nullptr;
   B.cig_slots = slots;
