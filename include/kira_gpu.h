@@ -195,6 +195,12 @@ int kira_gpu_set_bsw_shape(kira_ctx* ctx, uint32_t band, int shape);
  * Results are identical either way. */
 int kira_gpu_set_plain(kira_ctx* ctx, int plain);
 
+/* Device bytes the banded-SW trace arena (trace slots + row metadata) may hold at
+ * once; 0 (default) = half of the free device memory plus what the arena holds,
+ * clamped to [64 MiB, 24 GiB]. Batches needing more run their DP sweep and
+ * traceback in rounds over the same arena; results are identical. */
+int kira_gpu_set_trace_budget(kira_ctx* ctx, uint64_t bytes);
+
 /* Upload the reference as ASCII bases (Index::ref_bases, src/index/mod.rs:1098);
  * it stays resident until the next upload or kira_gpu_destroy. */
 int kira_gpu_ref_upload(kira_ctx* ctx, const uint8_t* seq, uint64_t len);

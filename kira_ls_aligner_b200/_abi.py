@@ -32,7 +32,7 @@ EXPORTS = (
     "kira_gpu_myers_batch", "kira_gpu_bsw_batch", "kira_gpu_verify_batch",
     "kira_gpu_verify_dev", "kira_gpu_profile", "kira_gpu_stage_times",
     "kira_gpu_bsw_shapes", "kira_gpu_set_bsw_shape", "kira_gpu_bsw_batch_noalloc",
-    "kira_gpu_align_batch_simd", "kira_gpu_set_plain",
+    "kira_gpu_align_batch_simd", "kira_gpu_set_plain", "kira_gpu_set_trace_budget",
 )
 SIMD_SCALAR, SIMD_AVX2, SIMD_AVX_VNNI, SIMD_NEON = 0, 1, 2, 3
 STAGES = ("sieve_certify", "myers", "bsw_dp", "bsw_traceback", "cigar_compact")
@@ -116,6 +116,7 @@ def lib():
     L.kira_gpu_profile.argtypes = [vp, C.c_int]
     L.kira_gpu_bsw_shapes.argtypes = [vp, vp, C.c_int]
     L.kira_gpu_set_plain.argtypes = [vp, C.c_int]
+    L.kira_gpu_set_trace_budget.argtypes = [vp, C.c_uint64]
     L.kira_gpu_align_batch_simd.argtypes = [vp, C.POINTER(Pairs), C.POINTER(SwCfg), C.c_int,
                                             C.c_int, vp, C.POINTER(CigarBuf)]
     L.kira_gpu_bsw_batch_noalloc.argtypes = [C.POINTER(Pairs), C.POINTER(SwCfg), vp, vp,

@@ -42,6 +42,7 @@ struct kira_ctx {
   int device = 0;
   int tuned_shape[kBandClasses] = {-1, -1, -1, -1, -1, -1};
   bool plain = false;  // single-launch banded SW (no bucketing): the comparison baseline
+  uint64_t trace_budget = 0;  // bytes for trace slots + row metadata (0: from free HBM)
   int sms = 148;
   cudaStream_t stream = nullptr;
   std::string last_error;
@@ -258,17 +259,40 @@ int pick_shape(const kira_ctx* ctx, uint32_t max_band, uint32_t max_q, const SwP
   return shape_usable(t, max_band, max_q, sp) ? t : default_shape(max_band, max_q, sp);
 }
 
-// Scratch of the banded SW stage for up to `items` items.
-int prepare_bsw(kira_ctx* ctx, uint32_t n_pairs, uint32_t items, const Maxes& mx, int shape,
-                BswLaunch& B) {
+// Bytes the banded-SW trace arena (trace slots + row metadata) may take: the
+// context's override, else half of the free device memory plus what the arena
+// already holds, between 64 MiB and 24 GiB.
+uint64_t trace_budget(kira_ctx* ctx) {
+  if (ctx->trace_budget) return ctx->trace_budget;
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
+  const uint64_t held = ctx->bufs[B_TRACE].bytes + ctx->bufs[B_META].bytes;
+  return std::min<uint64_t>(std::max<uint64_t>((fr + held) / 2, 64ull << 20), 24ull << 30);
+}
+
+// Trace slot bytes of one item of a shape over reads of up to max_q bases.
+uint64_t trace_slot_bytes(int shape, uint32_t max_q) {
+  return (((uint64_t)(max_q + 1) * shape_row_stride(kBswShapes[shape])) + 15) & ~15ull;
+}
+
+// Items one trace round holds (>= 1, <= items).
+uint32_t round_items(kira_ctx* ctx, uint32_t items, int shape, uint32_t max_q) {
+  const uint64_t per = trace_slot_bytes(shape, max_q) + 4ull * (max_q + 1);
+  const uint64_t fit = trace_budget(ctx) / std::max<uint64_t>(per, 1);
+  return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(items, fit));
+}
+
+// Scratch of the banded SW stage for up to `items` items, trace slots and row
+// metadata for `trace_items` of them (one round).
+int prepare_bsw(kira_ctx* ctx, uint32_t n_pairs, uint32_t items, uint32_t trace_items,
+                const Maxes& mx, int shape, BswLaunch& B) {
   cudaError_t cerr = cudaSuccess;
   const BswShapeInfo sh = kBswShapes[shape];
-  const uint32_t row_stride = shape_row_stride(sh);
-  const uint64_t slot = (((uint64_t)(mx.q + 1) * row_stride) + 15) & ~15ull;
+  const uint64_t slot = trace_slot_bytes(shape, mx.q);
   const uint32_t meta_stride = mx.q + 1;
   const uint32_t slot_cap = mx.q + mx.w + 2;
-  KIRA_DBUF(trace, uint8_t, B_TRACE, slot * std::max<uint32_t>(items, 1));
-  KIRA_DBUF(meta, uint32_t, B_META, (uint64_t)meta_stride * std::max<uint32_t>(items, 1));
+  KIRA_DBUF(trace, uint8_t, B_TRACE, slot * std::max<uint32_t>(trace_items, 1));
+  KIRA_DBUF(meta, uint32_t, B_META, (uint64_t)meta_stride * std::max<uint32_t>(trace_items, 1));
   KIRA_DBUF(ends, DpEnd, B_ENDS, std::max<uint32_t>(items, 1));
   KIRA_DBUF(slots, uint32_t, B_CIG_SLOTS, (uint64_t)slot_cap * std::max<uint32_t>(items, 1));
   KIRA_DBUF(iop, uint32_t, B_ITEM_OF_PAIR, std::max<uint32_t>(n_pairs, 1));
@@ -279,6 +303,23 @@ int prepare_bsw(kira_ctx* ctx, uint32_t n_pairs, uint32_t items, const Maxes& mx
   B.item_of_pair = iop;
   B.max_q = mx.q;
   return KIRA_OK;
+}
+
+// DP + traceback of `items` items in rounds of `per_round` (trace slots reused);
+// `between` (profiling) is recorded after the first round's DP.
+// With `work` (dynamic fetch) round r takes its items through counter work[r].
+cudaError_t launch_bsw_rounds(int shape, const DevPairs& D, BswLaunch B, uint32_t items,
+                              uint32_t per_round, int sms, cudaStream_t st, cudaEvent_t between,
+                              uint32_t* work = nullptr) {
+  const uint32_t rounds = (items + per_round - 1) / std::max<uint32_t>(per_round, 1);
+  for (uint32_t r = 0; r < std::max<uint32_t>(rounds, 1); ++r) {
+    B.item_lo = r * per_round;
+    B.item_hi = rounds > 1 ? B.item_lo + per_round : 0u;
+    B.work = work ? work + r : nullptr;
+    cudaError_t e = launch_bsw(shape, D, B, per_round, sms, st, r == 0 ? between : nullptr);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 // CIGAR scan + compaction over all pairs; writes the total op count to total_dev.
@@ -343,7 +384,8 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
   M.flags = counters + 2;
   KIRA_CUDA(launch_myers(D, M, n, ctx->sms, st));
   BswLaunch B{};
-  rc = prepare_bsw(ctx, n, n, mx, shape, B);
+  const uint32_t per_round = round_items(ctx, n, shape, mx.q);
+  rc = prepare_bsw(ctx, n, n, per_round, mx, shape, B);
   mark(ctx, 2, st);
   if (rc) return rc;
   B.list = slist;
@@ -355,7 +397,8 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
   B.out = out;
   B.ncig = ncig;
   B.flags = counters + 2;
-  KIRA_CUDA(launch_bsw(shape, D, B, n, ctx->sms, st, ctx->profile ? ctx->ev[3] : nullptr));
+  KIRA_CUDA(launch_bsw_rounds(shape, D, B, n, per_round, ctx->sms, st,
+                              ctx->profile ? ctx->ev[3] : nullptr));
   if (ctx->profile) ctx->ev_recorded = 4;
   mark(ctx, 4, st);
   rc = finish_cigars(ctx, n, out, ncig, B, ops, cap, total_dev, st);
@@ -408,27 +451,52 @@ int bsw_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const ki
   }
   const SwParams sp = resolve(cfg);
   int shape[kBandClasses];
-  uint64_t slot[kBandClasses] = {}, tbase[kBandClasses + 1] = {}, mbase[kBandClasses + 1] = {};
+  uint64_t slot[kBandClasses] = {}, per[kBandClasses] = {};
+  uint64_t total = 0;
   for (int c = 0; c < kBandClasses; ++c) {
     shape[c] = cnt[c] ? pick_shape(ctx, bmax[c], qmax[c], sp) : -1;
     if (cnt[c] && shape[c] < 0) return fail(ctx, KIRA_ERR_INVALID, "no shape for band %u", bmax[c]);
-    if (cnt[c]) {
-      const uint64_t rs = shape_row_stride(kBswShapes[shape[c]]);
-      slot[c] = (((uint64_t)(qmax[c] + 1) * rs) + 15) & ~15ull;
-    }
-    tbase[c + 1] = tbase[c] + slot[c] * cnt[c];
-    mbase[c + 1] = mbase[c] + (uint64_t)(qmax[c] + 1) * cnt[c];
+    if (!cnt[c]) continue;
+    slot[c] = trace_slot_bytes(shape[c], qmax[c]);
+    per[c] = slot[c] + 4ull * (qmax[c] + 1);
+    total += per[c] * cnt[c];
   }
+  // One round: every class's traces live at once (all DP sweeps, then all
+  // tracebacks). Otherwise each class runs in rounds over a shared arena.
+  const uint64_t budget = trace_budget(ctx);
+  const bool one_round = total <= budget;
+  uint32_t per_round[kBandClasses] = {}, rounds_before[kBandClasses + 1] = {};
+  uint64_t tbase[kBandClasses + 1] = {}, mbase[kBandClasses + 1] = {};
+  uint64_t tbytes = 16, mwords = 1;
+  for (int c = 0; c < kBandClasses; ++c) {
+    uint32_t r = 0;
+    if (cnt[c]) {
+      per_round[c] = one_round ? cnt[c]
+                               : (uint32_t)std::max<uint64_t>(
+                                     1, std::min<uint64_t>(cnt[c], budget / per[c]));
+      r = (cnt[c] + per_round[c] - 1) / per_round[c];
+      tbytes = one_round ? tbytes : std::max(tbytes, slot[c] * per_round[c]);
+      mwords = one_round ? mwords : std::max(mwords, (uint64_t)(qmax[c] + 1) * per_round[c]);
+    }
+    rounds_before[c + 1] = rounds_before[c] + r;
+    tbase[c + 1] = tbase[c] + (one_round ? slot[c] * cnt[c] : 0);
+    mbase[c + 1] = mbase[c] + (one_round ? (uint64_t)(qmax[c] + 1) * cnt[c] : 0);
+  }
+  if (one_round) {
+    tbytes = std::max<uint64_t>(tbase[kBandClasses], 16);
+    mwords = std::max<uint64_t>(mbase[kBandClasses], 1);
+  }
+  const uint32_t nwork = std::max<uint32_t>(rounds_before[kBandClasses], 1);
   const uint32_t cap = qall + wall + 2;
   KIRA_DBUF(dlist, uint32_t, B_SW_LIST, n);
-  KIRA_DBUF(trace, uint8_t, B_TRACE, std::max<uint64_t>(tbase[kBandClasses], 16));
-  KIRA_DBUF(meta, uint32_t, B_META, std::max<uint64_t>(mbase[kBandClasses], 1));
+  KIRA_DBUF(trace, uint8_t, B_TRACE, tbytes);
+  KIRA_DBUF(meta, uint32_t, B_META, mwords);
   KIRA_DBUF(ends, DpEnd, B_ENDS, n);
   KIRA_DBUF(slots, uint32_t, B_CIG_SLOTS, (uint64_t)cap * n);
   KIRA_DBUF(iop, uint32_t, B_ITEM_OF_PAIR, n);
-  KIRA_DBUF(work, uint32_t, B_WORK, kBandClasses);
+  KIRA_DBUF(work, uint32_t, B_WORK, nwork);
   KIRA_CUDA(cudaMemcpyAsync(dlist, list.data(), 4ull * n, cudaMemcpyHostToDevice, st));
-  KIRA_CUDA(cudaMemsetAsync(work, 0, 4 * kBandClasses, st));
+  KIRA_CUDA(cudaMemsetAsync(work, 0, 4ull * nwork, st));
   BswLaunch L[kBandClasses];
   for (int c = 0; c < kBandClasses; ++c) {
     if (!cnt[c]) continue;
@@ -450,16 +518,26 @@ int bsw_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const ki
     B.item_of_pair = iop;
     B.flags = flags_dev;
     B.max_q = qmax[c];
-    B.work = work + c;
+    B.work = work + rounds_before[c];
     B.item_base = base[c];
   }
   mark(ctx, 2, st);
-  // Widest class first (longest rows), then the narrower ones fill in behind it.
-  for (int c = kBandClasses - 1; c >= 0; --c)
-    if (cnt[c]) KIRA_CUDA(launch_bsw(shape[c], D, L[c], cnt[c], ctx->sms, st, nullptr, kBswPartDp));
-  mark(ctx, 3, st);
-  for (int c = kBandClasses - 1; c >= 0; --c)
-    if (cnt[c]) KIRA_CUDA(launch_bsw(shape[c], D, L[c], cnt[c], ctx->sms, st, nullptr, kBswPartTb));
+  if (one_round) {
+    // Widest class first (longest rows), then the narrower ones fill in behind it.
+    for (int c = kBandClasses - 1; c >= 0; --c)
+      if (cnt[c])
+        KIRA_CUDA(launch_bsw(shape[c], D, L[c], cnt[c], ctx->sms, st, nullptr, kBswPartDp));
+    mark(ctx, 3, st);
+    for (int c = kBandClasses - 1; c >= 0; --c)
+      if (cnt[c])
+        KIRA_CUDA(launch_bsw(shape[c], D, L[c], cnt[c], ctx->sms, st, nullptr, kBswPartTb));
+  } else {
+    for (int c = kBandClasses - 1; c >= 0; --c)
+      if (cnt[c])
+        KIRA_CUDA(launch_bsw_rounds(shape[c], D, L[c], cnt[c], per_round[c], ctx->sms, st,
+                                    nullptr, work + rounds_before[c]));
+    mark(ctx, 3, st);
+  }
   mark(ctx, 4, st);
   G = BswLaunch{};
   G.item_of_pair = iop;
@@ -606,6 +684,12 @@ int kira_gpu_set_plain(kira_ctx* ctx, int plain) {
   return KIRA_OK;
 }
 
+int kira_gpu_set_trace_budget(kira_ctx* ctx, uint64_t bytes) {
+  if (!ctx) return KIRA_ERR_INVALID;
+  ctx->trace_budget = bytes;
+  return KIRA_OK;
+}
+
 int kira_gpu_bsw_shapes(int* lanes, int* cells, int max_shapes) {
   const int n = std::min(max_shapes, kNumBswShapes);
   for (int i = 0; i < n; ++i) {
@@ -723,7 +807,8 @@ int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg
     const int shape = plain_shape(mx.band);
     if (shape < 0)
       return fail(ctx, KIRA_ERR_INVALID, "band %u above the int32 one-launch maximum", mx.band);
-    rc = prepare_bsw(ctx, n, n, mx, shape, B);
+    const uint32_t per_round = round_items(ctx, n, shape, mx.q);
+    rc = prepare_bsw(ctx, n, n, per_round, mx, shape, B);
     if (rc) return rc;
     B.count = n;
     B.sp = resolve(*cfg);
@@ -733,7 +818,8 @@ int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg
     B.ncig = ncig;
     B.flags = counters + 2;
     mark(ctx, 2, st);
-    KIRA_CUDA(launch_bsw(shape, D, B, n, ctx->sms, st, ctx->profile ? ctx->ev[3] : nullptr));
+    KIRA_CUDA(launch_bsw_rounds(shape, D, B, n, per_round, ctx->sms, st,
+                                ctx->profile ? ctx->ev[3] : nullptr));
     if (ctx->profile) ctx->ev_recorded = 4;
     mark(ctx, 4, st);
   } else {
@@ -834,7 +920,7 @@ int kira_gpu_align_batch_simd(kira_ctx* ctx, const kira_pairs* pairs, const kira
   KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
   KIRA_CUDA(cudaMemsetAsync(counters, 0, 16, st));
   BswLaunch B{};
-  rc = prepare_bsw(ctx, n, n, mx, shape, B);
+  rc = prepare_bsw(ctx, n, n, n, mx, shape, B);
   if (rc) return rc;
   bool any_abort = false;
   if (P.abort_score)

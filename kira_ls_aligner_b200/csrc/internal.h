@@ -79,6 +79,10 @@ struct BswLaunch {
   uint32_t* work;             // dynamic work counter (null: static grid-stride order)
   uint32_t item_base;         // global index of this launch's first item (CIGAR slots)
   int32_t bias;               // packed int16 shapes: value bias (packed_bias)
+  // Trace round: this launch handles items [item_lo, item_hi) (item_hi 0: no
+  // bound); trace slots and row metadata are indexed by item - item_lo, every
+  // other per-item array by the item itself.
+  uint32_t item_lo, item_hi;
 };
 
 struct CompactLaunch {

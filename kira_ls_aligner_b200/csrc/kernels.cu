@@ -347,6 +347,12 @@ __global__ void __launch_bounds__(128) myers_kernel(DevPairs P, MyersLaunch M) {
 // ---------------------------------------------------------------------------
 // Banded SW: DP sweep (group of G lanes per item) and traceback (thread per item)
 // ---------------------------------------------------------------------------
+// One past the last item of a launch's trace round.
+__device__ __forceinline__ uint32_t bsw_round_end(const BswLaunch& B) {
+  const uint32_t count = B.count_dev ? *B.count_dev : B.count;
+  return B.item_hi ? min(count, B.item_hi) : count;
+}
+
 template <int G, int K, int T, int MINB, bool FULL>
 __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B) {
   extern __shared__ int32_t bsw_smem[];
@@ -358,16 +364,17 @@ __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B
   const uint32_t groups_per_block = blockDim.x / G;
   const uint32_t group_in_block = threadIdx.x / G;
   int32_t* rowbuf = bsw_smem + (size_t)(threadIdx.x >> 5) * 2u * K * 32u;  // per warp
-  const uint32_t count = B.count_dev ? *B.count_dev : B.count;
+  const uint32_t count = bsw_round_end(B);
   const uint32_t ngroups = gridDim.x * groups_per_block;
-  uint32_t item = blockIdx.x * groups_per_block + group_in_block;
+  uint32_t item = B.item_lo + blockIdx.x * groups_per_block + group_in_block;
   for (;;) {
     if (B.work) {  // dynamic fetch: the group leader takes the next item
       uint32_t t = 0;
-      if (g == 0) t = atomicAdd(B.work, 1u);
+      if (g == 0) t = B.item_lo + atomicAdd(B.work, 1u);
       item = __shfl_sync(gmask, t, gw * G);
     }
     if (item >= count) break;
+    const uint32_t slot_item = item - B.item_lo;
     const uint32_t pair = B.list ? B.list[item] : item;
     const uint32_t q = P.read_len[pair], w = P.win_len[pair];
     const int32_t band = max(P.bandwidth ? P.bandwidth[pair] : B.sp.band, 1);
@@ -385,8 +392,8 @@ __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B
     }
     bsw_group_sweep<G, K, FULL>(
         P.read_seq + P.read_off[pair], q, P.win_seq + P.win_off[pair], w, band, offset,
-        abort_score, B.sp, rowbuf, gw * G, B.tg.trace + (size_t)item * B.tg.slot_bytes,
-        B.tg.meta + (size_t)item * B.tg.meta_stride, g, gmask, end, cells,
+        abort_score, B.sp, rowbuf, gw * G, B.tg.trace + (size_t)slot_item * B.tg.slot_bytes,
+        B.tg.meta + (size_t)slot_item * B.tg.meta_stride, g, gmask, end, cells,
         B.rowkeys ? B.rowkeys + (size_t)item * B.tg.meta_stride : nullptr);
     if (g == 0) {
       B.ends[item] = end;
@@ -408,16 +415,17 @@ __global__ void __launch_bounds__(T, MINB) bsw16_dp_kernel(DevPairs P, BswLaunch
   const uint32_t groups_per_block = blockDim.x / G;
   const uint32_t group_in_block = threadIdx.x / G;
   uint16_t* rowbuf = bsw16_smem + (size_t)group_in_block * 4u * G * K;  // per group
-  const uint32_t count = B.count_dev ? *B.count_dev : B.count;
+  const uint32_t count = bsw_round_end(B);
   const uint32_t ngroups = gridDim.x * groups_per_block;
-  uint32_t item = blockIdx.x * groups_per_block + group_in_block;
+  uint32_t item = B.item_lo + blockIdx.x * groups_per_block + group_in_block;
   for (;;) {
     if (B.work) {
       uint32_t t = 0;
-      if (g == 0) t = atomicAdd(B.work, 1u);
+      if (g == 0) t = B.item_lo + atomicAdd(B.work, 1u);
       item = __shfl_sync(gmask, t, gw * G);
     }
     if (item >= count) break;
+    const uint32_t slot_item = item - B.item_lo;
     const uint32_t pair = B.list ? B.list[item] : item;
     const uint32_t q = P.read_len[pair], w = P.win_len[pair];
     const int32_t band = max(P.bandwidth ? P.bandwidth[pair] : B.sp.band, 1);
@@ -435,8 +443,8 @@ __global__ void __launch_bounds__(T, MINB) bsw16_dp_kernel(DevPairs P, BswLaunch
     }
     bsw16_group_sweep<G, K>(P.read_seq + P.read_off[pair], q, P.win_seq + P.win_off[pair], w,
                             band, offset, abort_score, B.sp, B.bias, rowbuf,
-                            B.tg.trace + (size_t)item * B.tg.slot_bytes,
-                            B.tg.meta + (size_t)item * B.tg.meta_stride, g, gmask, end, cells);
+                            B.tg.trace + (size_t)slot_item * B.tg.slot_bytes,
+                            B.tg.meta + (size_t)slot_item * B.tg.meta_stride, g, gmask, end, cells);
     if (g == 0) {
       B.ends[item] = end;
       if (B.cells) atomicAdd(B.cells, (unsigned long long)cells);
@@ -446,15 +454,17 @@ __global__ void __launch_bounds__(T, MINB) bsw16_dp_kernel(DevPairs P, BswLaunch
 }
 
 __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
-  const uint32_t count = B.count_dev ? *B.count_dev : B.count;
+  const uint32_t count = bsw_round_end(B);
   const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t item = blockIdx.x * blockDim.x + threadIdx.x; item < count; item += stride) {
+  for (uint32_t item = B.item_lo + blockIdx.x * blockDim.x + threadIdx.x; item < count;
+       item += stride) {
     const uint32_t pair = B.list ? B.list[item] : item;
     const DpEnd e = B.ends[item];
     int32_t i = e.end_i, j = e.end_j;
     uint32_t overflow = 0;
-    const uint8_t* tr = B.tg.trace + (size_t)item * B.tg.slot_bytes;
-    const uint32_t* mt = B.tg.meta + (size_t)item * B.tg.meta_stride;
+    const uint32_t slot_item = item - B.item_lo;
+    const uint8_t* tr = B.tg.trace + (size_t)slot_item * B.tg.slot_bytes;
+    const uint32_t* mt = B.tg.meta + (size_t)slot_item * B.tg.meta_stride;
     uint32_t* ops = B.cig_slots + (size_t)item * B.slot_cap;
     const uint32_t n =
         B.tg.half ? bsw16_walk(tr, mt, B.tg.k_cells, B.tg.half, B.tg.lane_bytes, B.tg.row_stride,
