@@ -251,8 +251,13 @@ typedef struct kira_verify_params {
   int32_t sieve_threshold; /* certificate mismatch bound; < 0 -> spectral_max_mismatches */
   int32_t myers_k;         /* < 0 -> myers_reject_bound(read_len) */
   int32_t cert_strict;     /* KIRA_CERT_STRICT */
-  int32_t reserved;
+  int32_t flags;           /* KIRA_VERIFY_* bits */
 } kira_verify_params;
+
+/* kira_verify_params.flags: turn off the exact 4-gram prefilter in front of the
+ * Myers stage. The filter only removes pairs whose edit distance provably
+ * exceeds k (q-gram lemma), so results are identical either way. */
+#define KIRA_VERIFY_NO_QGRAM 1
 
 /* Optional per-stage detail. */
 typedef struct kira_verify_detail {

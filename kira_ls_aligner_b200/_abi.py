@@ -35,6 +35,7 @@ EXPORTS = (
     "kira_gpu_align_batch_simd", "kira_gpu_set_plain", "kira_gpu_set_trace_budget",
 )
 SIMD_SCALAR, SIMD_AVX2, SIMD_AVX_VNNI, SIMD_NEON = 0, 1, 2, 3
+VERIFY_NO_QGRAM = 1
 STAGES = ("sieve_certify", "myers", "bsw_dp", "bsw_traceback", "cigar_compact")
 
 
@@ -68,7 +69,7 @@ class SwCfg(C.Structure):
 
 class VerifyParams(C.Structure):
     _fields_ = [("sw", SwCfg), ("sieve_threshold", C.c_int32), ("myers_k", C.c_int32),
-                ("cert_strict", C.c_int32), ("reserved", C.c_int32)]
+                ("cert_strict", C.c_int32), ("flags", C.c_int32)]
 
 
 class CigarBuf(C.Structure):

@@ -275,9 +275,18 @@ uint64_t trace_slot_bytes(int shape, uint32_t max_q) {
   return (((uint64_t)(max_q + 1) * shape_row_stride(kBswShapes[shape])) + 15) & ~15ull;
 }
 
+// True when the trace arena already holds `slot_bytes` of slots and `meta_words`
+// of row metadata (no free-memory query is needed then).
+bool trace_arena_holds(const kira_ctx* ctx, uint64_t slot_bytes, uint64_t meta_words) {
+  return !ctx->trace_budget && ctx->bufs[B_TRACE].bytes >= slot_bytes + 16 &&
+         ctx->bufs[B_META].bytes >= 4 * meta_words + 16;
+}
+
 // Items one trace round holds (>= 1, <= items).
 uint32_t round_items(kira_ctx* ctx, uint32_t items, int shape, uint32_t max_q) {
-  const uint64_t per = trace_slot_bytes(shape, max_q) + 4ull * (max_q + 1);
+  const uint64_t slot = trace_slot_bytes(shape, max_q);
+  if (trace_arena_holds(ctx, slot * items, (uint64_t)(max_q + 1) * items)) return items;
+  const uint64_t per = slot + 4ull * (max_q + 1);
   const uint64_t fit = trace_budget(ctx) / std::max<uint64_t>(per, 1);
   return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(items, fit));
 }
@@ -361,7 +370,8 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
   KIRA_DBUF(slist, uint32_t, B_SW_LIST, n);
   KIRA_DBUF(counters, uint32_t, B_COUNTERS, 4);
   KIRA_CUDA(cudaMemsetAsync(counters, 0, 16, st));
-  VerifyDev V{p.sieve_threshold, p.cert_strict, sp, out, detail, ncig, swoff, mlist, counters};
+  VerifyDev V{p.sieve_threshold, p.cert_strict, sp,       out,       detail, ncig,
+              swoff,             mlist,         counters, p.myers_k, (p.flags & KIRA_VERIFY_NO_QGRAM) ? 0 : 1};
   ctx->ev_recorded = 0;
   mark(ctx, 0, st);
   rc = build_planes(ctx, D, read_bytes, win_bytes, resident, st);
@@ -463,7 +473,13 @@ int bsw_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const ki
   }
   // One round: every class's traces live at once (all DP sweeps, then all
   // tracebacks). Otherwise each class runs in rounds over a shared arena.
-  const uint64_t budget = trace_budget(ctx);
+  uint64_t tneed = 0, mneed = 0;
+  for (int c = 0; c < kBandClasses; ++c) {
+    tneed += slot[c] * cnt[c];
+    mneed += (uint64_t)(qmax[c] + 1) * cnt[c];
+  }
+  const bool held = trace_arena_holds(ctx, tneed, mneed);
+  const uint64_t budget = held ? total : trace_budget(ctx);
   const bool one_round = total <= budget;
   uint32_t per_round[kBandClasses] = {}, rounds_before[kBandClasses + 1] = {};
   uint64_t tbase[kBandClasses + 1] = {}, mbase[kBandClasses + 1] = {};

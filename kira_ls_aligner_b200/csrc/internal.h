@@ -31,6 +31,8 @@ struct VerifyDev {
   int32_t* sw_offset;
   uint32_t* myers_list;
   uint32_t* counters;          // [0] myers items, [1] sw items
+  int32_t myers_k;             // < 0: router bound per read (myers_k_for)
+  int32_t qgram;               // exact 4-gram prefilter before Myers (qgram.cuh)
 };
 
 struct MyersLaunch {

@@ -6,6 +6,7 @@
 #include "internal.h"
 #include "myers.cuh"
 #include "planes.cuh"
+#include "qgram.cuh"
 #include "sieve.cuh"
 
 namespace kira {
@@ -184,7 +185,9 @@ __device__ __forceinline__ uint32_t myers_k_for(int32_t k, uint32_t q) {
 // Stage 1 of the composed path: sieve + certificate, one lane per pair.
 template <int RWMAX>
 __global__ void __launch_bounds__(256) verify_sieve_kernel(DevPairs P, VerifyDev V) {
+  __shared__ uint32_t qset[8][8 * 32];  // per warp: 4-gram bitmap [word][lane]
   const uint32_t lane = threadIdx.x & 31u;
+  uint32_t* myset = &qset[threadIdx.x >> 5][lane];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x; base < P.n; base += stride) {
     const uint32_t p = base + threadIdx.x;
@@ -227,12 +230,26 @@ __global__ void __launch_bounds__(256) verify_sieve_kernel(DevPairs P, VerifyDev
         V.sw_offset[p] = so.hit ? (int32_t)so.shift : 0;
       }
     }
-    // Warp-aggregated append of the uncertified pairs to the Myers list.
-    const uint32_t need = __ballot_sync(0xFFFFFFFFu, valid && !cert);
+    // Exact 4-gram prefilter: a pair it rejects is a Myers None (same result).
+    bool gone = false;
+    if (valid && !cert && V.qgram) {
+      const uint32_t k = myers_k_for(V.myers_k, q);
+      gone = qgram4_reject(P.read_planes, P.read_off[p], q, P.win_planes, P.win_off[p],
+                           P.win_len[p], k, myset);
+      if (gone) {
+        kira_sw_result r{};
+        r.status = KIRA_PAIR_MYERS_REJECT;
+        V.out[p] = r;
+        V.ncig[p] = 0;
+      }
+    }
+    // Warp-aggregated append of the remaining pairs to the Myers list.
+    const bool to_myers = valid && !cert && !gone;
+    const uint32_t need = __ballot_sync(0xFFFFFFFFu, to_myers);
     uint32_t slot0 = 0;
     if (lane == 0 && need) slot0 = atomicAdd(V.counters + 0, (uint32_t)__popc(need));
     slot0 = __shfl_sync(0xFFFFFFFFu, slot0, 0);
-    if (valid && !cert) V.myers_list[slot0 + __popc(need & ((1u << lane) - 1u))] = p;
+    if (to_myers) V.myers_list[slot0 + __popc(need & ((1u << lane) - 1u))] = p;
   }
 }
 

@@ -105,10 +105,12 @@ class VerifyParams:
     sieve_threshold: int = 12
     myers_k: int = 8
     cert_strict: bool = False
+    qgram_filter: bool = True  # exact 4-gram prefilter before Myers (same results)
 
     def to_c(self) -> A.VerifyParams:
         return A.VerifyParams(self.cfg.to_c(), self.sieve_threshold, self.myers_k,
-                              int(self.cert_strict), 0)
+                              int(self.cert_strict),
+                              0 if self.qgram_filter else A.VERIFY_NO_QGRAM)
 
 
 # --- pair batches --------------------------------------------------------------

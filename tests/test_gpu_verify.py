@@ -86,3 +86,24 @@ def test_resident_reference_equals_host_windows(ctx):
     sel = np.arange(0, w.n_pairs, 3)
     out, cig = _oracle(w, a[4], a[5], params, sel)
     _compare(a[0], a[1], a[2], out, cig, sel)
+
+
+@pytest.mark.parametrize("myers_k,sub_hi,indel", [(8, 0.05, 0.002), (-1, 0.08, 0.004),
+                                                  (2, 0.02, 0.001), (30, 0.10, 0.005)])
+def test_qgram_prefilter_changes_nothing(ctx, myers_k, sub_hi, indel):
+    # The 4-gram filter only removes pairs Myers rejects: on/off give identical
+    # statuses, details, scores and CIGARs (and match the oracle on a sample).
+    from kira_ls_aligner_b200 import PairBatch, VerifyParams, synth
+    w = synth.make_workload("q", 2500, 400_000, cands=8, sub_lo=0.0, sub_hi=sub_hi,
+                            indel_rate=indel, repeat_frac=0.2, seed=1000 + max(myers_k, 0))
+    arena, woffs = w.windows_arena()
+    b = PairBatch(w.reads, w.read_off, w.read_len, arena, woffs, w.win_len)
+    on = ctx.verify_batch(b, VerifyParams(sieve_threshold=12, myers_k=myers_k), detail=True)
+    off = ctx.verify_batch(b, VerifyParams(sieve_threshold=12, myers_k=myers_k,
+                                           qgram_filter=False), detail=True)
+    assert np.array_equal(on[0], off[0]) and np.array_equal(on[1], off[1])
+    assert np.array_equal(on[2], off[2]) and on[3] == off[3]
+    assert (on[0]["status"] == 2).sum() > 0
+    sel = np.arange(0, w.n_pairs, 11)
+    out, cig = _oracle(w, arena, woffs, VerifyParams(sieve_threshold=12, myers_k=myers_k), sel)
+    _compare(on[0], on[1], on[2], out, cig, sel)
