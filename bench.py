@@ -413,19 +413,35 @@ def run_ours(args, rank, local, world, dist):
     n_sw = statuses[3]
     n_my = statuses[2] + statuses[3]
     q, wl = 150, 250
-    alg_bytes = {  # algorithmic bytes per launch of each stage (ASCII sequences in HBM)
+    cells_step = cells // max(args.steps, 1)
+    packed = autotune.packed()[tuning["best"]]
+    trace_b = 1.0 if packed else 0.5  # trace bytes per DP cell (byte codes / nibbles)
+    alg_bytes = {  # algorithmic bytes per launch of each stage (sequences in, results out)
         0: n * (q + wl + 24 + 32),
         1: n_my * (q + wl + 8) + n_sw * 4,
-        2: n_sw * (q + wl + 16) + cells // max(args.steps, 1) // 2,
-        3: n_sw * (32 + 16) + cells // max(args.steps, 1) // 2 // 50,
+        2: int(n_sw * (q + wl + 16 + 4 * (q + 1)) + cells_step * trace_b),
+        3: int(n_sw * (32 + 16) + cells_step * trace_b / 50),
         4: n * (32 + 8) + 4 * n,
     }[dom]
+    # DRAM bytes per unit from the ncu captures of the same kernels (800k-pair case,
+    # scaled by units processed): profiles/bsw16_dp_batched_800k.md (1.285 B per DP
+    # cell) and profiles/verify_sieve_batched_800k.md (168.8 B per pair).
+    traffic = {0: 168.8 * n, 2: 1.285 * cells_step if packed else None}.get(dom)
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    dp_ms = stage_ms[2] / args.steps
     roofline = {"bound": "hbm", "kernel": _abi.STAGES[dom], "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None if traffic is None else int(traffic),
                 "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs",
                 "stage_ms_per_step": {s: round(float(t) / args.steps, 4)
-                                      for s, t in zip(_abi.STAGES, stage_ms)}}
+                                      for s, t in zip(_abi.STAGES, stage_ms)},
+                # The sieve, Myers and DP kernels are integer-pipe bound (ncu: ALU pipe
+                # 77-85 % of peak, DRAM < 10 %); their binding roofline is the ALU pipe.
+                "int_pipe": {"kernel": "bsw_dp", "gcups": cells_step / (dp_ms / 1e3) / 1e9
+                             if dp_ms > 0 else None,
+                             "alu_pipe_frac_ncu": 0.845 if packed else 0.757,
+                             "thread_inst_per_cell_ncu": 33.1 if packed else 90.8,
+                             "source": "profiles/bsw16_dp_batched_800k.md"}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -450,7 +466,8 @@ def run_ours(args, rank, local, world, dist):
             "status_counts": {"certified": statuses[1], "myers_reject": statuses[2],
                               "sw": statuses[3]},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            "gpu_launches": 8 * args.steps,
+            # per step: planes pack, sieve, Myers, SW DP, traceback, 3 scan, compaction
+            "gpu_launches": 9 * args.steps,
         }
         print(json.dumps(out))
     ctx.close()

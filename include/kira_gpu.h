@@ -180,12 +180,14 @@ typedef struct kira_cigar_buf {
 int kira_gpu_profile(kira_ctx* ctx, int enable);
 int kira_gpu_stage_times(kira_ctx* ctx, float* ms, int max_stages);
 
-/* Launch shapes of the banded-SW stage (lanes per pair x cells per lane).
- * kira_gpu_bsw_shapes lists them (returns the count); kira_gpu_set_bsw_shape
- * installs a shape for every band in band's class (<=16, 33, 64, 128, 256, 511;
- * -1 restores the default pick). The autotuner (Python runtime) times the shapes
- * that cover a band on a sample and installs the fastest. */
-int kira_gpu_bsw_shapes(int* lanes, int* cells, int max_shapes);
+/* Launch shapes of the banded-SW stage (lanes per pair x cells per lane; packed =
+ * int16 score lanes, two cells per 32-bit register, used only when the batch's
+ * scores provably fit). kira_gpu_bsw_shapes lists them (returns the count; any
+ * output array may be null); kira_gpu_set_bsw_shape installs a shape for every
+ * band in band's class (<=16, 33, 64, 128, 256, 511; -1 restores the default
+ * pick). The autotuner (Python runtime) times the shapes that cover a band on a
+ * sample and installs the fastest. */
+int kira_gpu_bsw_shapes(int* lanes, int* cells, int* packed, int max_shapes);
 int kira_gpu_set_bsw_shape(kira_ctx* ctx, uint32_t band, int shape);
 
 /* kira_gpu_bsw_batch buckets pairs by band class (one tuned launch shape and trace

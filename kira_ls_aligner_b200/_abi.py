@@ -115,7 +115,7 @@ def lib():
     L.kira_gpu_verify_dev.argtypes = [vp, C.POINTER(Pairs), C.POINTER(VerifyParams), vp, vp,
                                       C.c_uint64, vp, vp, vp, vp]
     L.kira_gpu_profile.argtypes = [vp, C.c_int]
-    L.kira_gpu_bsw_shapes.argtypes = [vp, vp, C.c_int]
+    L.kira_gpu_bsw_shapes.argtypes = [vp, vp, vp, C.c_int]
     L.kira_gpu_set_plain.argtypes = [vp, C.c_int]
     L.kira_gpu_set_trace_budget.argtypes = [vp, C.c_uint64]
     L.kira_gpu_align_batch_simd.argtypes = [vp, C.POINTER(Pairs), C.POINTER(SwCfg), C.c_int,

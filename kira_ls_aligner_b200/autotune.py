@@ -16,12 +16,22 @@ _CACHE: dict = {}
 
 
 def shapes() -> list:
+    """(lanes per pair, cells per lane) of every launch shape, by index."""
     L = A.lib()
-    n = L.kira_gpu_bsw_shapes(None, None, 0)
+    n = L.kira_gpu_bsw_shapes(None, None, None, 0)
     g = (C.c_int * n)()
     k = (C.c_int * n)()
-    L.kira_gpu_bsw_shapes(g, k, n)
+    L.kira_gpu_bsw_shapes(g, k, None, n)
     return [(int(g[i]), int(k[i])) for i in range(n)]
+
+
+def packed() -> list:
+    """Per shape: True for the packed int16 score lanes."""
+    L = A.lib()
+    n = L.kira_gpu_bsw_shapes(None, None, None, 0)
+    p = (C.c_int * n)()
+    L.kira_gpu_bsw_shapes(None, None, p, n)
+    return [bool(p[i]) for i in range(n)]
 
 
 def covering(band: int) -> list:

@@ -706,11 +706,12 @@ int kira_gpu_set_trace_budget(kira_ctx* ctx, uint64_t bytes) {
   return KIRA_OK;
 }
 
-int kira_gpu_bsw_shapes(int* lanes, int* cells, int max_shapes) {
+int kira_gpu_bsw_shapes(int* lanes, int* cells, int* packed, int max_shapes) {
   const int n = std::min(max_shapes, kNumBswShapes);
   for (int i = 0; i < n; ++i) {
     if (lanes) lanes[i] = kBswShapes[i].g;
     if (cells) cells[i] = shape_cap(kBswShapes[i]) / kBswShapes[i].g;
+    if (packed) packed[i] = kBswShapes[i].packed;
   }
   return kNumBswShapes;
 }
