@@ -46,9 +46,16 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--shape", type=int, default=-1,
                     help="install this banded-SW launch shape instead of autotuning")
-    ap.add_argument("--workload", choices=["batched", "uneven"], default="batched",
+    ap.add_argument("--workload", choices=["batched", "uneven", "serving", "gapfill"],
+                    default="batched",
                     help="batched: the headline 2M-pair verification; uneven: 500k banded-SW "
-                         "pairs of mixed length and band (bucketed vs one-launch path)")
+                         "pairs of mixed length and band (bucketed vs one-launch path); "
+                         "serving: Poisson request stream through the server vs one request "
+                         "per call; gapfill: long-read gap-fill segments at band 256")
+    ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
+    ap.add_argument("--duration", type=float, default=5.0, help="serving: seconds of arrivals")
+    ap.add_argument("--slots", type=int, default=4, help="serving: concurrent batches")
+    ap.add_argument("--segments", type=int, default=20_000, help="gapfill: segments per call")
     return ap.parse_args()
 
 
@@ -226,6 +233,190 @@ def run_uneven(args, rank, local, world):
     ctx.close()
 
 
+def _slice_short(w, r0, nreads, cands=4):
+    """PairBatch of reads [r0, r0 + nreads) of a short-read pool (compact read arena;
+    windows stay reference coordinates)."""
+    from kira_ls_aligner_b200 import PairBatch
+    a, b = r0 * cands, (r0 + nreads) * cands
+    base = int(w.read_off[a])
+    end = int(w.read_off[b - 1]) + int(w.read_len[b - 1])
+    return PairBatch(np.concatenate([w.reads[base:end], np.zeros(16, np.uint8)]),
+                     w.read_off[a:b] - np.uint64(base), w.read_len[a:b].copy(), None,
+                     w.win_off[a:b].copy(), w.win_len[a:b].copy())
+
+
+def _slice_long(g, s0, n):
+    from kira_ls_aligner_b200 import PairBatch
+    base = int(g.read_off[s0])
+    end = int(g.read_off[s0 + n - 1]) + int(g.read_len[s0 + n - 1])
+    return PairBatch(np.concatenate([g.reads[base:end], np.zeros(16, np.uint8)]),
+                     g.read_off[s0:s0 + n] - np.uint64(base), g.read_len[s0:s0 + n].copy(), None,
+                     g.win_off[s0:s0 + n].copy(), g.win_len[s0:s0 + n].copy(),
+                     g.band_offset[s0:s0 + n].copy(), None, g.bandwidth[s0:s0 + n].copy())
+
+
+def run_serving(args, rank, local, world):
+    """Serving loop: seeded Poisson arrivals (70 % short requests of 1k-64k reads x 4
+    windows, 30 % long requests of 50-2000 gap-fill segments at band 256) over a
+    1 Gbp device-resident reference. The server (continuous batching over `slots`
+    streams) against the plain path (one request per call, in arrival order)."""
+    import torch
+
+    from kira_ls_aligner_b200 import (AlignmentConfig, GpuContext, Server, VerifyParams, _abi,
+                                      synth)
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    pool = synth.serving_pool()
+    sched = synth.arrivals(0xA11, args.rate, args.duration)
+    vp = VerifyParams(sieve_threshold=12, myers_k=8)
+    cfg = AlignmentConfig(1, 4, 6, 1, 256, 100, 5, True, 16)
+    nshort = len(pool.short.read_off) // 4
+    nlong = len(pool.long.read_off)
+    reqs, rs, ls = [], 0, 0
+    for t, kind, n in sched:
+        if kind == "short":
+            rs = 0 if rs + n > nshort else rs
+            reqs.append((t, kind, _slice_short(pool.short, rs, n)))
+            rs += n
+        else:
+            ls = 0 if ls + n > nlong else ls
+            reqs.append((t, kind, _slice_long(pool.long, ls, n)))
+            ls += n
+    total_pairs = sum(b.n for _, _, b in reqs)
+
+    def pct(x, p):
+        return float(np.percentile(np.asarray(x), p)) * 1e3
+
+    def serve(open_loop: bool):
+        srv = Server(local, slots=args.slots, max_batch_pairs=1 << 20)
+        srv.ref_upload(pool.reference)
+        for _ in range(2):  # warm-up: every slot grows its arenas on full batches
+            warm = [srv.submit_verify(b, vp) if kind == "short" else srv.submit_bsw(b, cfg)
+                    for _, kind, b in reqs[:12 * args.slots]]
+            for t in warm:
+                t.wait(600)
+        b0 = srv.stats()["batches"]
+        tickets = []
+        t0 = time.perf_counter()
+        for t, kind, b in reqs:
+            d = t0 + t - time.perf_counter() if open_loop else 0.0
+            if d > 0:
+                time.sleep(d)
+            tickets.append((kind, srv.submit_verify(b, vp) if kind == "short"
+                            else srv.submit_bsw(b, cfg)))
+        t_sub = time.perf_counter() - t0
+        infos = []
+        for kind, tk in tickets:
+            tk.wait(600)
+            infos.append((kind, tk.info()))
+        first = min(i.t_submit_ns for _, i in infos)
+        last = max(i.t_done_ns for _, i in infos)
+        lat = [i.latency_s for _, i in infos]
+        out = {"pairs_per_s": total_pairs / ((last - first) / 1e9),
+               "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+               "p50_short_ms": pct([i.latency_s for k, i in infos if k == "short"], 50),
+               "p99_short_ms": pct([i.latency_s for k, i in infos if k == "short"], 99),
+               "p50_long_ms": pct([i.latency_s for k, i in infos if k == "long"], 50),
+               "p99_long_ms": pct([i.latency_s for k, i in infos if k == "long"], 99),
+               "batches": srv.stats()["batches"] - b0,
+               "host_ms": srv.stats()["host_ms"], "submit_s": t_sub,
+               "mean_requests_per_batch": float(np.mean([i.batch_requests for _, i in infos]))}
+        srv.close()
+        return out
+
+    def plain_run(open_loop: bool):
+        ctx = GpuContext(local)
+        ctx.ref_upload(pool.reference)
+        ctx.check(_abi.lib().kira_gpu_set_plain(ctx.handle, 1))
+        for _, kind, b in reqs[:8]:
+            ctx.verify_batch(b, vp) if kind == "short" else ctx.bsw_batch(b, cfg)
+        plat, pk = [], []
+        t0 = time.perf_counter()
+        for t, kind, b in reqs:
+            arr = t0 + t if open_loop else t0
+            d = arr - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ctx.verify_batch(b, vp) if kind == "short" else ctx.bsw_batch(b, cfg)
+            plat.append(time.perf_counter() - arr)
+            pk.append(kind)
+        span = time.perf_counter() - (t0 + (reqs[0][0] if open_loop else 0.0))
+        ctx.close()
+        return {"pairs_per_s": total_pairs / span, "p50_ms": pct(plat, 50),
+                "p99_ms": pct(plat, 99),
+                "p50_short_ms": pct([x for x, k in zip(plat, pk) if k == "short"], 50),
+                "p99_short_ms": pct([x for x, k in zip(plat, pk) if k == "short"], 99),
+                "p50_long_ms": pct([x for x, k in zip(plat, pk) if k == "long"], 50),
+                "p99_long_ms": pct([x for x, k in zip(plat, pk) if k == "long"], 99)}
+
+    # Open loop: each request submitted at its Poisson arrival time (latency);
+    # saturated: every request submitted at once (capacity in pairs/s).
+    srv_out, srv_sat = serve(True), serve(False)
+    plain, plain_sat = plain_run(True), plain_run(False)
+    print(json.dumps({
+        "metric": "serving pairs/s with p50/p99 request latency (bit-exact)",
+        "value": srv_out["pairs_per_s"], "unit": UNIT, "n_gpus": 1, "steps": len(reqs),
+        "warmup": 4, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic (seeded Poisson arrivals)",
+        "config": {"workload": "serving", "rate_req_s": args.rate, "duration_s": args.duration,
+                   "requests": len(reqs), "pairs": total_pairs, "slots": args.slots,
+                   "short": "1k-64k reads U[100,250] bp x 4 windows (verification)",
+                   "long": "50-2000 gap-fill segments U[200,2000] bp, band 256 (banded SW)",
+                   "reference_bp": int(len(pool.reference))},
+        "server": srv_out, "plain": plain,
+        "saturated": {"server_pairs_per_s": srv_sat["pairs_per_s"],
+                      "plain_pairs_per_s": plain_sat["pairs_per_s"],
+                      "speedup": srv_sat["pairs_per_s"] / plain_sat["pairs_per_s"],
+                      "server_batches": srv_sat["batches"],
+                      "server_mean_requests_per_batch": srv_sat["mean_requests_per_batch"],
+                      "server_host_ms": srv_sat["host_ms"], "server_submit_s": srv_sat["submit_s"]},
+        "p99_ratio_plain_over_server": plain["p99_ms"] / srv_out["p99_ms"],
+        "p50_ratio_plain_over_server": plain["p50_ms"] / srv_out["p50_ms"]}))
+
+
+def run_gapfill(args, rank, local, world):
+    """Long-read gap-fill: segments U[200, 2000] bp at 5-12 % error, band 256, over a
+    resident reference; int32 lanes (scores exceed the packed range), traces in
+    rounds bounded by free device memory. Host API, H2D + D2H per call."""
+    import torch
+
+    from kira_ls_aligner_b200 import AlignmentConfig, GpuContext, PairBatch, _abi, synth
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    g = synth.gapfill(args.segments)
+    b = PairBatch(g.reads, g.read_off, g.read_len, None, g.win_off, g.win_len, g.band_offset,
+                  None, g.bandwidth)
+    cfg = AlignmentConfig(1, 4, 6, 1, 256, 100, 5, True, 16)
+    ctx = GpuContext(local)
+    ctx.ref_upload(g.reference)
+    L = _abi.lib()
+    for _ in range(args.warmup):
+        res, ops, cells = ctx.bsw_batch(b, cfg)
+    ts = [_timed(lambda: ctx.bsw_batch(b, cfg)) for _ in range(args.steps)]
+    res, ops, cells = ctx.bsw_batch(b, cfg)
+    ctx.check(L.kira_gpu_profile(ctx.handle, 1))
+    ctx.bsw_batch(b, cfg)
+    buf = (C.c_float * 8)()
+    k = L.kira_gpu_stage_times(ctx.handle, buf, 8)
+    ctx.check(L.kira_gpu_profile(ctx.handle, 0))
+    ms = sum(ts) / len(ts)
+    print(json.dumps({
+        "metric": "pairs/s and GCUPS (gap-fill banded SW with CIGAR, bit-exact)",
+        "value": g.n_pairs / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+        "config": {"workload": g.name, "segments": g.n_pairs, "band": 256,
+                   "errors": "U[5%,12%] 2:1:1", "reference_bp": int(len(g.reference)),
+                   "path": "host API, pinned-free inputs, H2D + D2H per call"},
+        "gcups": cells / (ms / 1e3) / 1e9, "cells": int(cells),
+        "stage_ms": dict(zip(("upload", "bucketing", "bsw_dp", "bsw_traceback",
+                              "cigar_compact"), [round(float(x), 3) for x in buf[:k]])),
+        "checksum": int(res["score"].astype(np.int64).sum())}))
+    ctx.close()
+
+
 def _subset(w, idx):
     """A compact PairBatch of the pairs `idx` of an SwWorkload (own arenas)."""
     from kira_ls_aligner_b200 import PairBatch
@@ -262,6 +453,10 @@ def main():
     try:
         if args.workload == "uneven":
             run_uneven(args, rank, local, world)
+        elif args.workload == "serving":
+            run_serving(args, rank, local, world)
+        elif args.workload == "gapfill":
+            run_gapfill(args, rank, local, world)
         elif args.impl == "reference":
             run_reference(args, rank, world)
         else:

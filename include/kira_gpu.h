@@ -46,7 +46,8 @@ enum kira_status {
   KIRA_ERR_INVALID = 7,       /* argument outside the supported domain */
   KIRA_ERR_OOM = 8,           /* device memory exhausted / admission refused */
   KIRA_ERR_CAPACITY = 9,      /* caller's output buffer too small (see *_used) */
-  KIRA_ERR_SCRATCH_LIMIT = 10 /* batch needs more than the fixed no-alloc scratch */
+  KIRA_ERR_SCRATCH_LIMIT = 10, /* batch needs more than the fixed no-alloc scratch */
+  KIRA_PENDING = 11            /* server request still queued or running (not an error) */
 };
 
 /* Per-pair status of the composed verification. */
@@ -325,6 +326,72 @@ int kira_gpu_verify_dev(kira_ctx* ctx, const kira_pairs* pairs, const kira_verif
 int kira_gpu_bsw_batch_noalloc(const kira_pairs* pairs, const kira_sw_cfg* cfg,
                                kira_sw_result* out, uint32_t* cigar_ops, uint64_t cigar_cap,
                                uint64_t* cigar_used, void* stream);
+
+/* ------------------------------------------------ serving (continuous batching)
+ *
+ * No counterpart in the reference, whose dispatcher thread runs one blocking
+ * CudaBackend::run_batch at a time (src/cuda/dispatcher.rs:21-78); this is the
+ * asynchronous serving mode of the same path. A server owns `slots` worker
+ * threads, each with its own context (stream + device arena); all share one
+ * device-resident reference. A free slot takes the oldest queued request plus
+ * every later queued request of the same kind and parameters (up to
+ * max_batch_pairs pairs), runs them as one batch and writes each request's
+ * results into that request's buffers. A batch starts only when its device-memory
+ * estimate fits in mem_fraction of the free device memory (plus what the slot
+ * already holds). Results are identical to the direct calls (kira_gpu_verify_batch
+ * / kira_gpu_bsw_batch) on the request alone.
+ *
+ * The caller's input arrays and output buffers are borrowed from submit until the
+ * request leaves KIRA_PENDING. out[i].cigar_off indexes the request's own
+ * cigar_ops; a request whose CIGAR ops exceed cigar_cap ends with
+ * KIRA_ERR_CAPACITY (cigar_used in kira_request_info gives the need). */
+typedef struct kira_server kira_server;
+
+typedef struct kira_server_cfg {
+  int device;
+  int slots;                /* concurrent batches (worker threads / streams), 1..64 */
+  uint32_t max_batch_pairs; /* batch cap in pair-equivalents (a banded-SW pair counts its
+                               band cells / 10050, a 150 bp read at band 33); 0 -> 2^20 */
+  double mem_fraction;      /* admission: share of free device memory; 0 -> 0.5 */
+} kira_server_cfg;
+
+typedef struct kira_request_info {
+  int32_t status;           /* KIRA_PENDING, KIRA_OK or the batch's error */
+  uint32_t n_pairs;
+  uint64_t cigar_used;
+  int64_t t_submit_ns;      /* steady clock */
+  int64_t t_start_ns;       /* batch start (0 while queued) */
+  int64_t t_done_ns;
+  uint64_t batch_id;        /* batch that ran the request */
+  uint32_t batch_requests;  /* requests in that batch */
+  uint32_t reserved;
+} kira_request_info;
+
+int kira_server_create(const kira_server_cfg* cfg, kira_server** out);
+/* Waits for running batches, cancels queued requests (KIRA_ERR_RUNTIME). */
+void kira_server_destroy(kira_server* srv);
+/* Replaces the resident reference (between batches; bounded wait). */
+int kira_server_ref_upload(kira_server* srv, const uint8_t* seq, uint64_t len);
+/* Short-read requests: the composed verification (kira_gpu_verify_batch). */
+int kira_server_submit_verify(kira_server* srv, const kira_pairs* pairs,
+                              const kira_verify_params* params, kira_sw_result* out,
+                              uint32_t* cigar_ops, uint64_t cigar_cap, uint64_t* ticket);
+/* Long gap-fill requests: banded SW per pair (kira_gpu_bsw_batch). */
+int kira_server_submit_bsw(kira_server* srv, const kira_pairs* pairs, const kira_sw_cfg* cfg,
+                           kira_sw_result* out, uint32_t* cigar_ops, uint64_t cigar_cap,
+                           uint64_t* ticket);
+/* KIRA_PENDING while queued or running, else the request's final status. */
+int kira_server_poll(kira_server* srv, uint64_t ticket);
+/* Bounded wait: the final status, or KIRA_ERR_TIMEOUT after timeout_ms. */
+int kira_server_wait(kira_server* srv, uint64_t ticket, int64_t timeout_ms);
+int kira_server_info(kira_server* srv, uint64_t ticket, kira_request_info* info);
+/* Forgets a finished ticket (KIRA_ERR_INVALID while pending). */
+int kira_server_release(kira_server* srv, uint64_t ticket);
+int kira_server_stats(kira_server* srv, uint64_t* batches, uint64_t* pairs, uint32_t* queued);
+int kira_server_last_error(kira_server* srv, char* buf, size_t len);
+/* Host milliseconds summed over batches: [0] staging inputs, [1] the pipeline call
+ * (upload, kernels, result copies), [2] scattering results, [3] admission checks. */
+int kira_server_profile(kira_server* srv, double* ms4);
 
 #ifdef __cplusplus
 }

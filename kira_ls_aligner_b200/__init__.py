@@ -6,9 +6,9 @@ of that boundary; there is no CPU compute path in this package.
 """
 from . import _abi
 from .runtime import (AlignmentConfig, CapacityError, CudaError, GpuContext, InvalidArgument,
-                      PairBatch, SwPublicResult, VerifyParams, cigar_string, decode_cigar,
-                      is_available, results_to_list)
+                      PairBatch, Server, SwPublicResult, Ticket, Timeout, VerifyParams,
+                      cigar_string, decode_cigar, is_available, results_to_list)
 
 __all__ = ["AlignmentConfig", "CapacityError", "CudaError", "GpuContext", "InvalidArgument",
-           "PairBatch", "SwPublicResult", "VerifyParams", "cigar_string", "decode_cigar",
-           "is_available", "results_to_list", "_abi"]
+           "PairBatch", "Server", "SwPublicResult", "Ticket", "Timeout", "VerifyParams",
+           "cigar_string", "decode_cigar", "is_available", "results_to_list", "_abi"]

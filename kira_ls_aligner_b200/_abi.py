@@ -17,8 +17,11 @@ KIRA_OK = 0
 STATUS_NAMES = {
     0: "OK", 1: "NotBuilt", 2: "Driver", 3: "Runtime", 4: "NoDevice", 5: "ReadTooLong",
     6: "Timeout", 7: "Invalid", 8: "OutOfMemory", 9: "Capacity", 10: "ScratchLimit",
+    11: "Pending",
 }
+KIRA_ERR_TIMEOUT = 6
 KIRA_ERR_SCRATCH_LIMIT = 10
+KIRA_PENDING = 11
 NOALLOC_SCRATCH_BYTES = 32 << 20
 PAIR_PENDING, PAIR_CERTIFIED, PAIR_MYERS_REJECT, PAIR_SW = 0, 1, 2, 3
 READ_BYTES_MAX = 64
@@ -33,6 +36,10 @@ EXPORTS = (
     "kira_gpu_verify_dev", "kira_gpu_profile", "kira_gpu_stage_times",
     "kira_gpu_bsw_shapes", "kira_gpu_set_bsw_shape", "kira_gpu_bsw_batch_noalloc",
     "kira_gpu_align_batch_simd", "kira_gpu_set_plain", "kira_gpu_set_trace_budget",
+    "kira_server_create", "kira_server_destroy", "kira_server_ref_upload",
+    "kira_server_submit_verify", "kira_server_submit_bsw", "kira_server_poll",
+    "kira_server_wait", "kira_server_info", "kira_server_release", "kira_server_stats",
+    "kira_server_last_error", "kira_server_profile",
 )
 SIMD_SCALAR, SIMD_AVX2, SIMD_AVX_VNNI, SIMD_NEON = 0, 1, 2, 3
 VERIFY_NO_QGRAM = 1
@@ -70,6 +77,18 @@ class SwCfg(C.Structure):
 class VerifyParams(C.Structure):
     _fields_ = [("sw", SwCfg), ("sieve_threshold", C.c_int32), ("myers_k", C.c_int32),
                 ("cert_strict", C.c_int32), ("flags", C.c_int32)]
+
+
+class ServerCfg(C.Structure):
+    _fields_ = [("device", C.c_int), ("slots", C.c_int), ("max_batch_pairs", C.c_uint32),
+                ("mem_fraction", C.c_double)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("n_pairs", C.c_uint32), ("cigar_used", C.c_uint64),
+                ("t_submit_ns", C.c_int64), ("t_start_ns", C.c_int64), ("t_done_ns", C.c_int64),
+                ("batch_id", C.c_uint64), ("batch_requests", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class CigarBuf(C.Structure):
@@ -124,9 +143,25 @@ def lib():
                                              C.c_uint64, vp, vp]
     L.kira_gpu_set_bsw_shape.argtypes = [vp, C.c_uint32, C.c_int]
     L.kira_gpu_stage_times.argtypes = [vp, C.POINTER(C.c_float), C.c_int]
+    L.kira_server_create.argtypes = [C.POINTER(ServerCfg), C.POINTER(vp)]
+    L.kira_server_destroy.argtypes = [vp]
+    L.kira_server_destroy.restype = None
+    L.kira_server_ref_upload.argtypes = [vp, vp, C.c_uint64]
+    L.kira_server_submit_verify.argtypes = [vp, C.POINTER(Pairs), C.POINTER(VerifyParams), vp,
+                                            vp, C.c_uint64, C.POINTER(C.c_uint64)]
+    L.kira_server_submit_bsw.argtypes = [vp, C.POINTER(Pairs), C.POINTER(SwCfg), vp, vp,
+                                         C.c_uint64, C.POINTER(C.c_uint64)]
+    L.kira_server_poll.argtypes = [vp, C.c_uint64]
+    L.kira_server_wait.argtypes = [vp, C.c_uint64, C.c_int64]
+    L.kira_server_info.argtypes = [vp, C.c_uint64, C.POINTER(RequestInfo)]
+    L.kira_server_release.argtypes = [vp, C.c_uint64]
+    L.kira_server_stats.argtypes = [vp, vp, vp, vp]
+    L.kira_server_last_error.argtypes = [vp, C.c_char_p, C.c_size_t]
+    L.kira_server_profile.argtypes = [vp, C.POINTER(C.c_double)]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype or C.c_int
     L.kira_gpu_destroy.restype = None
+    L.kira_server_destroy.restype = None
     L.kira_gpu_arena_bytes.restype = C.c_uint64
     _lib = L
     return L

@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -52,6 +53,7 @@ struct kira_ctx {
   uint8_t* ref_dev = nullptr;
   uint4* ref_planes = nullptr;  // 2-bit + valid planes of the resident reference
   uint64_t ref_len = 0;
+  std::shared_ptr<void> ref_owner;  // frees ref_dev / ref_planes with the last holder
   DevBuf bufs[B_COUNT];
 };
 
@@ -75,16 +77,19 @@ int cuda_fail(kira_ctx* ctx, cudaError_t e, const char* what) {
 }
 
 // Grow-only device buffer (ensure_capacity_*, src/cuda/backend.rs:271-308);
-// 16 bytes of slack so vector loads may read to the next 16-byte boundary.
+// 16 bytes of slack so vector loads may read to the next 16-byte boundary. Growth
+// is stream-ordered on the context's stream (cudaMallocAsync / cudaFreeAsync from
+// the device's pool), so it never synchronises other contexts' streams; a buffer
+// grows by at least a quarter to keep regrowth rare.
 void* dbuf(kira_ctx* ctx, BufId id, size_t bytes, cudaError_t* err) {
   DevBuf& b = ctx->bufs[id];
   const size_t need = bytes + 16;
   if (b.bytes >= need) return b.p;
-  if (b.p) cudaFree(b.p);
+  const size_t cap = std::max(need, b.bytes + b.bytes / 4);
+  if (b.p) cudaFreeAsync(b.p, ctx->stream);
   b.p = nullptr;
   b.bytes = 0;
-  const size_t cap = std::max(need, b.bytes * 2);
-  cudaError_t e = cudaMalloc(&b.p, cap);
+  cudaError_t e = cudaMallocAsync(&b.p, cap, ctx->stream);
   if (e != cudaSuccess) {
     *err = e;
     b.p = nullptr;
@@ -583,6 +588,13 @@ int kira_gpu_init(int device, kira_ctx** out) {
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return KIRA_ERR_DRIVER;
   if (prop.major < 10) return KIRA_ERR_NO_DEVICE;  // sm_100a binary only
+  // Freed arena blocks stay in the device's default pool for reuse instead of
+  // going back to the driver at every synchronisation.
+  cudaMemPool_t pool = nullptr;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   kira_ctx* ctx = new kira_ctx();
   ctx->device = device;
   ctx->sms = prop.multiProcessorCount;
@@ -599,11 +611,11 @@ void kira_gpu_destroy(kira_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   for (auto& b : ctx->bufs)
-    if (b.p) cudaFree(b.p);
+    if (b.p) cudaFreeAsync(b.p, ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);
-  if (ctx->ref_dev) cudaFree(ctx->ref_dev);
-  if (ctx->ref_planes) cudaFree(ctx->ref_planes);
+  ctx->ref_owner.reset();
   cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -740,16 +752,32 @@ int kira_gpu_stage_times(kira_ctx* ctx, float* ms, int max_stages) {
 int kira_gpu_ref_upload(kira_ctx* ctx, const uint8_t* seq, uint64_t len) {
   if (!ctx) return KIRA_ERR_INVALID;
   cudaSetDevice(ctx->device);
-  if (ctx->ref_dev) cudaFree(ctx->ref_dev);
-  if (ctx->ref_planes) cudaFree(ctx->ref_planes);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->ref_owner.reset();
   ctx->ref_dev = nullptr;
   ctx->ref_planes = nullptr;
   ctx->ref_len = 0;
   if (len == 0) return KIRA_OK;
-  KIRA_CUDA(cudaMalloc(&ctx->ref_dev, len + 16));
-  KIRA_CUDA(cudaMemcpy(ctx->ref_dev, seq, len, cudaMemcpyHostToDevice));
+  uint8_t* dev = nullptr;
+  uint4* planes = nullptr;
+  const int device = ctx->device;
+  KIRA_CUDA(cudaMalloc(&dev, len + 16));
   const uint64_t nb = plane_blocks(len);
-  KIRA_CUDA(cudaMalloc(&ctx->ref_planes, nb * sizeof(uint4)));
+  cudaError_t e = cudaMalloc(&planes, nb * sizeof(uint4));
+  if (e != cudaSuccess) {
+    cudaFree(dev);
+    return cuda_fail(ctx, e, "cudaMalloc(reference planes)");
+  }
+  // One holder frees both arrays when the last context sharing them lets go.
+  ctx->ref_owner = std::shared_ptr<void>(dev, [device, planes](void* p) {
+    cudaSetDevice(device);
+    cudaFree(p);
+    cudaFree(planes);
+  });
+  ctx->ref_dev = dev;
+  ctx->ref_planes = planes;
+  KIRA_CUDA(cudaMemcpy(ctx->ref_dev, seq, len, cudaMemcpyHostToDevice));
+  KIRA_CUDA(cudaMemsetAsync(ctx->ref_dev + len, 0, 16, ctx->stream));
   KIRA_CUDA(launch_pack_planes(ctx->ref_dev, len, ctx->ref_planes, nb, ctx->sms, ctx->stream));
   KIRA_CUDA(cudaStreamSynchronize(ctx->stream));
   ctx->ref_len = len;
@@ -1054,3 +1082,15 @@ int kira_gpu_verify_dev(kira_ctx* ctx, const kira_pairs* pairs, const kira_verif
 }
 
 }  // extern "C"
+
+namespace kira {
+// Makes `dst` use `src`'s resident reference (shared, freed with the last holder).
+int ctx_share_reference(kira_ctx* dst, const kira_ctx* src) {
+  if (!dst || !src || dst->device != src->device) return KIRA_ERR_INVALID;
+  dst->ref_owner = src->ref_owner;
+  dst->ref_dev = src->ref_dev;
+  dst->ref_planes = src->ref_planes;
+  dst->ref_len = src->ref_len;
+  return KIRA_OK;
+}
+}  // namespace kira

@@ -156,4 +156,6 @@ cudaError_t launch_cigar_scan(const uint32_t* ncig, uint32_t n, uint32_t* off,
                               uint32_t* chunk_sums, uint64_t* total_dev, cudaStream_t st);
 cudaError_t launch_cigar_compact(const CompactLaunch& C, int sms, cudaStream_t st);
 
+int ctx_share_reference(kira_ctx* dst, const kira_ctx* src);
+
 }  // namespace kira

@@ -179,6 +179,14 @@ class PairBatch:
         return p
 
 
+def default_sw_cigar_cap(batch: "PairBatch") -> int:
+    """CIGAR capacity that covers gapped alignments without a retry: 8 ops per pair
+    or one op per 4 read bases, whichever is larger (a retry with the exact need
+    follows only past that)."""
+    bases = int(np.asarray(batch.read_len, np.uint64).sum()) if batch.n else 0
+    return max(16, 8 * batch.n, bases // 4)
+
+
 def decode_cigar(ops) -> list:
     return [(int(w) >> 4, OP_CHARS[int(w) & 0xF]) for w in ops]
 
@@ -294,7 +302,7 @@ class GpuContext:
     def bsw_batch(self, batch: PairBatch, cfg: AlignmentConfig, cigar_cap: int | None = None):
         n = batch.n
         res = np.zeros(n, A.SW_RESULT_DTYPE)
-        cap = cigar_cap if cigar_cap is not None else max(16, 8 * n)
+        cap = cigar_cap if cigar_cap is not None else default_sw_cigar_cap(batch)
         ops = np.zeros(cap, np.uint32)
         cb = A.CigarBuf(A.ptr(ops), cap, 0)
         cells = C.c_uint64()
@@ -342,3 +350,126 @@ class GpuContext:
             return self.verify_batch(batch, params, detail, int(cb.used) + 16)
         self.check(rc)
         return res, ops[: cb.used], det, int(cells.value)
+
+
+# --- serving (continuous batching) ----------------------------------------------
+@dataclass
+class RequestInfo:
+    status: int
+    n_pairs: int
+    cigar_used: int
+    t_submit_ns: int
+    t_start_ns: int
+    t_done_ns: int
+    batch_id: int
+    batch_requests: int
+
+    @property
+    def latency_s(self) -> float:
+        return (self.t_done_ns - self.t_submit_ns) / 1e9
+
+
+class Ticket:
+    """One submitted request: owns its result buffers and keeps its inputs alive
+    until the server has finished with them."""
+
+    def __init__(self, server: "Server", tid: int, batch: PairBatch, res, ops, keep):
+        self.server, self.id, self.batch = server, tid, batch
+        self.res, self.ops, self._keep = res, ops, keep
+
+    def poll(self) -> int:
+        return int(self.server._lib.kira_server_poll(self.server._h, self.id))
+
+    def done(self) -> bool:
+        return self.poll() != A.KIRA_PENDING
+
+    def wait(self, timeout_s: float = 60.0):
+        """Results (per-pair structured array, this request's CIGAR ops); raises
+        Timeout when the bounded wait expires, or the request's error."""
+        rc = int(self.server._lib.kira_server_wait(self.server._h, self.id,
+                                                   int(timeout_s * 1000)))
+        if rc != A.KIRA_OK:
+            raise_for(rc, f"request {self.id}: {self.server.last_error()}")
+        return self.res, self.ops[: self.info().cigar_used]
+
+    def info(self) -> RequestInfo:
+        i = A.RequestInfo()
+        raise_for(self.server._lib.kira_server_info(self.server._h, self.id, C.byref(i)),
+                  f"no ticket {self.id}")
+        return RequestInfo(i.status, i.n_pairs, i.cigar_used, i.t_submit_ns, i.t_start_ns,
+                           i.t_done_ns, i.batch_id, i.batch_requests)
+
+    def release(self) -> None:
+        self.server._lib.kira_server_release(self.server._h, self.id)
+
+
+class Server:
+    """kira_server: `slots` concurrent batches over one device-resident reference;
+    requests of the same kind and parameters that queue up are run as one batch."""
+
+    def __init__(self, device: int = 0, slots: int = 2, max_batch_pairs: int = 1 << 20,
+                 mem_fraction: float = 0.5):
+        self._lib = A.lib()
+        h = C.c_void_p()
+        cfg = A.ServerCfg(device, slots, max_batch_pairs, mem_fraction)
+        raise_for(self._lib.kira_server_create(C.byref(cfg), C.byref(h)),
+                  f"kira_server_create(device={device}, slots={slots}) failed")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.kira_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def last_error(self) -> str:
+        buf = C.create_string_buffer(1024)
+        self._lib.kira_server_last_error(self._h, buf, 1024)
+        return buf.value.decode(errors="replace")
+
+    def ref_upload(self, seq) -> None:
+        a = np.frombuffer(bytes(seq), np.uint8) if not isinstance(seq, np.ndarray) else seq
+        raise_for(self._lib.kira_server_ref_upload(self._h, A.ptr(a), int(a.nbytes)),
+                  self.last_error())
+
+    def _submit(self, fn, batch: PairBatch, params, cigar_cap):
+        n = batch.n
+        res = np.zeros(max(n, 1), A.SW_RESULT_DTYPE)
+        cap = cigar_cap if cigar_cap is not None else max(16, 4 * n)
+        ops = np.zeros(cap, np.uint32)
+        pc = batch.to_c()
+        cp = params.to_c()
+        t = C.c_uint64()
+        raise_for(fn(self._h, C.byref(pc), C.byref(cp), A.ptr(res), A.ptr(ops), cap, C.byref(t)),
+                  "submit refused")
+        return Ticket(self, int(t.value), batch, res[:n], ops, (pc, cp))
+
+    def submit_verify(self, batch: PairBatch, params: VerifyParams,
+                      cigar_cap: int | None = None) -> Ticket:
+        return self._submit(self._lib.kira_server_submit_verify, batch, params, cigar_cap)
+
+    def submit_bsw(self, batch: PairBatch, cfg: AlignmentConfig,
+                   cigar_cap: int | None = None) -> Ticket:
+        if cigar_cap is None:
+            cigar_cap = default_sw_cigar_cap(batch)
+        return self._submit(self._lib.kira_server_submit_bsw, batch, cfg, cigar_cap)
+
+    def stats(self) -> dict:
+        b, p, q = C.c_uint64(), C.c_uint64(), C.c_uint32()
+        self._lib.kira_server_stats(self._h, C.byref(b), C.byref(p), C.byref(q))
+        ms = (C.c_double * 4)()
+        self._lib.kira_server_profile(self._h, ms)
+        return {"batches": b.value, "pairs": p.value, "queued": q.value,
+                "host_ms": {"staging": ms[0], "pipeline": ms[1], "scatter": ms[2],
+                            "admission": ms[3]}}

@@ -170,6 +170,7 @@ class SwWorkload:
     win_len: np.ndarray
     band_offset: np.ndarray
     bandwidth: np.ndarray
+    reference: np.ndarray | None = None  # set when win_off are reference coordinates
 
     @property
     def n_pairs(self) -> int:
@@ -201,3 +202,101 @@ def uneven(n_pairs: int = 500_000, seed: int = 0x3E3E, q_lo: int = 50, q_hi: int
     return SwWorkload("uneven_500k_q50-300_band16-128", np.concatenate([read_arena, np.zeros(16, np.uint8)]),
                       read_off, q.astype(np.uint32), np.concatenate([wins, np.zeros(16, np.uint8)]),
                       win_off, w.astype(np.uint32), b.astype(np.int32), b.astype(np.int32))
+
+
+def random_genome(rng, ref_len: int, repeat_frac: float = 0.10) -> np.ndarray:
+    """Uniform ACGT with `repeat_frac` of the bases in 300 bp repeat families
+    (copies at 2-10 % divergence) -- the long-read reference of the gap-fill runs."""
+    return random_reference(rng, ref_len, repeat_frac)
+
+
+def gapfill(n_segments: int = 20_000, seed: int = 0x6A9F, seg_lo: int = 200, seg_hi: int = 2000,
+            band: int = 256, err_lo: float = 0.05, err_hi: float = 0.12,
+            reference: np.ndarray | None = None, ref_len: int = 50_000_000) -> SwWorkload:
+    """Long-read gap-fill segments: U[200, 2000] bp of a long read between two exact
+    anchors, error U[5 %, 12 %] at 2:1:1 (subs:ins:del), aligned with band 256 in a
+    window of segment + 2 x band taken straight from the (device-resident) reference:
+    win_off are reference coordinates and the segment starts at window offset band."""
+    rng = np.random.default_rng(seed)
+    ref = reference if reference is not None else random_genome(rng, ref_len)
+    q = rng.integers(seg_lo, seg_hi + 1, n_segments).astype(np.int64)
+    w = q + 2 * band
+    start = rng.integers(0, len(ref) - int(w.max()) - seg_hi - 512, n_segments)
+    L = seg_hi + 400  # room for deletions
+    reads = np.empty((n_segments, seg_hi), np.uint8)
+    for a in range(0, n_segments, 4096):  # bounded temporaries
+        b = min(a + 4096, n_segments)
+        frag = ref[(start[a:b] + band)[:, None] + np.arange(L)[None, :]]
+        m = _mutate_matrix(rng, frag, q[a:b], rng.uniform(err_lo, err_hi, b - a),
+                           split=(2, 1, 1))
+        reads[a:b, :m.shape[1]] = m
+    mask = np.arange(seg_hi)[None, :] < q[:, None]
+    read_off = np.zeros(n_segments, np.uint64)
+    read_off[1:] = np.cumsum(q[:-1])
+    return SwWorkload(f"gapfill_{n_segments}_{seg_lo}-{seg_hi}_band{band}",
+                      np.concatenate([reads[mask], np.zeros(16, np.uint8)]), read_off,
+                      q.astype(np.uint32), None, start.astype(np.uint64), w.astype(np.uint32),
+                      np.full(n_segments, band, np.int32), np.full(n_segments, band, np.int32),
+                      ref)
+
+
+@dataclass
+class ServingPool:
+    """Pools the serving requests are cut from, over one shared reference."""
+    reference: np.ndarray
+    short: Workload     # reads U[100, 250] bp x 4 candidate windows (1 true)
+    long: SwWorkload    # gap-fill segments, band 256
+
+
+def short_reads(rng, ref: np.ndarray, n_reads: int, cands: int = 4, q_lo: int = 100,
+                q_hi: int = 250, pad: int = 100, sub: float = 0.01,
+                indel: float = 0.001) -> Workload:
+    """Variable-length short reads (U[q_lo, q_hi]) with `cands` windows of read + pad
+    each, one of them the read's origin; win_off are reference coordinates."""
+    q = rng.integers(q_lo, q_hi + 1, n_reads).astype(np.int64)
+    L = q_hi + 32
+    origins = rng.integers(pad, len(ref) - q_hi - pad - 64, n_reads)
+    frag = ref[origins[:, None] + np.arange(L)[None, :]]
+    rate = np.full(n_reads, sub + 2 * indel)
+    reads = _mutate_matrix(rng, frag, q, rate, split=(int(sub * 1000), int(indel * 1000),
+                                                      int(indel * 1000)))[:, :q_hi]
+    mask = np.arange(q_hi)[None, :] < q[:, None]
+    roff = np.zeros(n_reads, np.uint64)
+    roff[1:] = np.cumsum(q[:-1])
+    n_pairs = n_reads * cands
+    wl = np.repeat(q + pad, cands)
+    win_off = rng.integers(0, len(ref) - q_hi - pad - 1, n_pairs).astype(np.uint64)
+    true_slot = rng.integers(0, cands, n_reads)
+    true_idx = np.arange(n_reads) * cands + true_slot
+    win_off[true_idx] = (origins - rng.integers(0, pad + 1, n_reads)).astype(np.uint64)
+    is_true = np.zeros(n_pairs, bool)
+    is_true[true_idx] = True
+    return Workload("short_reads", ref, np.concatenate([reads[mask], np.zeros(16, np.uint8)]),
+                    np.repeat(roff, cands), np.repeat(q, cands).astype(np.uint32), win_off,
+                    wl.astype(np.uint32), is_true)
+
+
+def serving_pool(seed: int = 0x5E7E, ref_len: int = 1_000_000_000, short_reads_n: int = 400_000,
+                 long_segments: int = 40_000) -> ServingPool:
+    """1 Gbp reference (10 % repeats), a pool of short reads (x 4 windows) and a pool of
+    gap-fill segments; requests are contiguous slices of the pools."""
+    rng = np.random.default_rng(seed)
+    ref = random_genome(rng, ref_len)
+    sr = short_reads(rng, ref, short_reads_n)
+    lg = gapfill(long_segments, seed=seed + 1, reference=ref)
+    return ServingPool(ref, sr, lg)
+
+
+def arrivals(seed: int, rate: float, duration_s: float, long_frac: float = 0.3,
+             short_reads=(1_000, 64_000), long_reads=(50, 2_000)):
+    """Seeded Poisson arrivals: (time_s, kind 'short'|'long', reads) per request."""
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration_s:
+            return out
+        if rng.random() < long_frac:
+            out.append((t, "long", int(rng.integers(long_reads[0], long_reads[1] + 1))))
+        else:
+            out.append((t, "short", int(rng.integers(short_reads[0], short_reads[1] + 1))))

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     src = open(os.path.join(ROOT, "include", "kira_gpu.h")).read()
-    return sorted(set(re.findall(r"\b(kira_gpu_\w+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(kira_(?:gpu|server)_\w+)\s*\(", src)))
 
 
 def test_library_exports_every_declared_symbol():
