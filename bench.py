@@ -203,6 +203,8 @@ def run_uneven(args, rank, local, world):
     out = {}
     for mode in ("plain", "bucketed"):
         ctx.check(L.kira_gpu_set_plain(ctx.handle, 1 if mode == "plain" else 0))
+        # The bucketed form replays its per-class launches from a CUDA graph.
+        ctx.check(L.kira_gpu_set_graphs(ctx.handle, 0 if mode == "plain" else 1, None, None))
         for _ in range(args.warmup):
             res, ops, cells = ctx.bsw_batch(batch, cfg)
         ts = [_timed(lambda: ctx.bsw_batch(batch, cfg)) for _ in range(args.steps)]
@@ -229,6 +231,7 @@ def run_uneven(args, rank, local, world):
                    "path": "host API, pinned inputs, H2D + D2H per call"},
         "bucketed": out["bucketed"], "plain": out["plain"],
         "speedup_vs_plain": out["bucketed"]["pairs_per_s"] / out["plain"]["pairs_per_s"],
+        "cuda_graphs": graph_counts(ctx),
         "autotune": tuned}))
     ctx.close()
 
@@ -429,6 +432,13 @@ def _subset(w, idx):
     wo = np.concatenate([[0], np.cumsum(wl[:-1], dtype=np.uint64)]).astype(np.uint64)
     return PairBatch(reads, ro, rl.copy(), wins, wo, wl.copy(), w.band_offset[idx].copy(), None,
                      w.bandwidth[idx].copy())
+
+
+def graph_counts(ctx) -> dict:
+    from kira_ls_aligner_b200 import _abi
+    c, r = C.c_uint64(), C.c_uint64()
+    _abi.lib().kira_gpu_set_graphs(ctx.handle, -1, C.byref(c), C.byref(r))
+    return {"captures": c.value, "replays": r.value}
 
 
 def _timed(fn) -> float:

@@ -200,9 +200,17 @@ int kira_gpu_set_plain(kira_ctx* ctx, int plain);
 
 /* Device bytes the banded-SW trace arena (trace slots + row metadata) may hold at
  * once; 0 (default) = half of the free device memory plus what the arena holds,
- * clamped to [64 MiB, 24 GiB]. Batches needing more run their DP sweep and
+ * clamped to [64 MiB, 64 GiB]. Batches needing more run their DP sweep and
  * traceback in rounds over the same arena; results are identical. */
 int kira_gpu_set_trace_budget(kira_ctx* ctx, uint64_t bytes);
+
+/* CUDA-graph replay of the bucketed banded-SW launches (per-class DP sweeps,
+ * tracebacks, CIGAR scan and compaction) of kira_gpu_bsw_batch: a call whose
+ * launch parameters (device buffers, per-class counts, shapes, rounds) equal the
+ * previous graph's replays it, any other call captures a new one. enable: 1 on,
+ * 0 off, -1 unchanged; captures / replays (optional) receive the counts so far.
+ * Results are identical with and without graphs. */
+int kira_gpu_set_graphs(kira_ctx* ctx, int enable, uint64_t* captures, uint64_t* replays);
 
 /* Upload the reference as ASCII bases (Index::ref_bases, src/index/mod.rs:1098);
  * it stays resident until the next upload or kira_gpu_destroy. */

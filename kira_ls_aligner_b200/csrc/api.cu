@@ -44,6 +44,10 @@ struct kira_ctx {
   int tuned_shape[kBandClasses] = {-1, -1, -1, -1, -1, -1};
   bool plain = false;  // single-launch banded SW (no bucketing): the comparison baseline
   uint64_t trace_budget = 0;  // bytes for trace slots + row metadata (0: from free HBM)
+  bool graphs = false;        // replay the bucketed banded-SW launches from a CUDA graph
+  cudaGraphExec_t graph_exec = nullptr;
+  std::vector<uint8_t> graph_key;  // launch parameters the cached graph was captured with
+  uint64_t graph_replays = 0, graph_captures = 0;
   int sms = 148;
   cudaStream_t stream = nullptr;
   std::string last_error;
@@ -266,13 +270,13 @@ int pick_shape(const kira_ctx* ctx, uint32_t max_band, uint32_t max_q, const SwP
 
 // Bytes the banded-SW trace arena (trace slots + row metadata) may take: the
 // context's override, else half of the free device memory plus what the arena
-// already holds, between 64 MiB and 24 GiB.
+// already holds, between 64 MiB and 64 GiB.
 uint64_t trace_budget(kira_ctx* ctx) {
   if (ctx->trace_budget) return ctx->trace_budget;
   size_t fr = 0, tot = 0;
   if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
   const uint64_t held = ctx->bufs[B_TRACE].bytes + ctx->bufs[B_META].bytes;
-  return std::min<uint64_t>(std::max<uint64_t>((fr + held) / 2, 64ull << 20), 24ull << 30);
+  return std::min<uint64_t>(std::max<uint64_t>((fr + held) / 2, 64ull << 20), 64ull << 30);
 }
 
 // Trace slot bytes of one item of a shape over reads of up to max_q bases.
@@ -425,9 +429,49 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
 // class (each class gets the launch shape tuned for it and a trace geometry sized
 // for its longest read), sorted longest-first inside a class, and fetched
 // dynamically by the DP kernel's groups. One DP + one traceback launch per class.
-int bsw_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const kira_sw_cfg& cfg,
-                 kira_sw_result* dout, uint32_t* ncig, uint32_t* flags_dev,
-                 unsigned long long* cells_dev, BswLaunch& G, cudaStream_t st) {
+// Device launches of one bucketed banded-SW call (everything after the host-side
+// ordering and the work-list upload): value-initialised so its bytes are a key.
+struct BucketRun {
+  int shape[kBandClasses];
+  uint32_t cnt[kBandClasses], per_round[kBandClasses];
+  uint32_t one_round, nwork;
+  uint32_t* work;
+  BswLaunch L[kBandClasses];
+};
+
+// Enqueues the launches of a planned bucketed call on `st` (capturable).
+cudaError_t enqueue_bucketed(kira_ctx* ctx, const DevPairs& D, const BucketRun& R,
+                             cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(R.work, 0, 4ull * R.nwork, st);
+  if (e != cudaSuccess) return e;
+  mark(ctx, 2, st);
+  if (R.one_round) {
+    // Widest class first (longest rows), then the narrower ones fill in behind it.
+    for (int c = kBandClasses - 1; c >= 0; --c)
+      if (R.cnt[c] && (e = launch_bsw(R.shape[c], D, R.L[c], R.cnt[c], ctx->sms, st, nullptr,
+                                      kBswPartDp)) != cudaSuccess)
+        return e;
+    mark(ctx, 3, st);
+    for (int c = kBandClasses - 1; c >= 0; --c)
+      if (R.cnt[c] && (e = launch_bsw(R.shape[c], D, R.L[c], R.cnt[c], ctx->sms, st, nullptr,
+                                      kBswPartTb)) != cudaSuccess)
+        return e;
+  } else {
+    for (int c = kBandClasses - 1; c >= 0; --c)
+      if (R.cnt[c] && (e = launch_bsw_rounds(R.shape[c], D, R.L[c], R.cnt[c], R.per_round[c],
+                                             ctx->sms, st, nullptr, R.L[c].work)) != cudaSuccess)
+        return e;
+    mark(ctx, 3, st);
+  }
+  mark(ctx, 4, st);
+  return cudaSuccess;
+}
+
+// Host side of the bucketed call: band classes, ordering, shapes, trace rounds,
+// scratch and the work-list upload. Fills R (launched by enqueue_bucketed).
+int plan_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const kira_sw_cfg& cfg,
+                  kira_sw_result* dout, uint32_t* ncig, uint32_t* flags_dev,
+                  unsigned long long* cells_dev, BswLaunch& G, BucketRun& R, cudaStream_t st) {
   cudaError_t cerr = cudaSuccess;
   const uint32_t n = P.n;
   std::vector<uint8_t> cls(n);
@@ -517,13 +561,17 @@ int bsw_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const ki
   KIRA_DBUF(iop, uint32_t, B_ITEM_OF_PAIR, n);
   KIRA_DBUF(work, uint32_t, B_WORK, nwork);
   KIRA_CUDA(cudaMemcpyAsync(dlist, list.data(), 4ull * n, cudaMemcpyHostToDevice, st));
-  KIRA_CUDA(cudaMemsetAsync(work, 0, 4ull * nwork, st));
-  BswLaunch L[kBandClasses];
+  R = BucketRun{};
+  R.one_round = one_round ? 1u : 0u;
+  R.nwork = nwork;
+  R.work = work;
   for (int c = 0; c < kBandClasses; ++c) {
+    R.shape[c] = shape[c];
+    R.cnt[c] = cnt[c];
+    R.per_round[c] = per_round[c];
     if (!cnt[c]) continue;
     const BswShapeInfo sh = kBswShapes[shape[c]];
-    BswLaunch& B = L[c];
-    B = BswLaunch{};
+    BswLaunch& B = R.L[c];
     B.list = dlist + base[c];
     B.count = cnt[c];
     B.sp = sp;
@@ -542,29 +590,76 @@ int bsw_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const ki
     B.work = work + rounds_before[c];
     B.item_base = base[c];
   }
-  mark(ctx, 2, st);
-  if (one_round) {
-    // Widest class first (longest rows), then the narrower ones fill in behind it.
-    for (int c = kBandClasses - 1; c >= 0; --c)
-      if (cnt[c])
-        KIRA_CUDA(launch_bsw(shape[c], D, L[c], cnt[c], ctx->sms, st, nullptr, kBswPartDp));
-    mark(ctx, 3, st);
-    for (int c = kBandClasses - 1; c >= 0; --c)
-      if (cnt[c])
-        KIRA_CUDA(launch_bsw(shape[c], D, L[c], cnt[c], ctx->sms, st, nullptr, kBswPartTb));
-  } else {
-    for (int c = kBandClasses - 1; c >= 0; --c)
-      if (cnt[c])
-        KIRA_CUDA(launch_bsw_rounds(shape[c], D, L[c], cnt[c], per_round[c], ctx->sms, st,
-                                    nullptr, work + rounds_before[c]));
-    mark(ctx, 3, st);
-  }
-  mark(ctx, 4, st);
   G = BswLaunch{};
   G.item_of_pair = iop;
   G.cig_slots = slots;
   G.slot_cap = cap;
   return KIRA_OK;
+}
+
+// Runs `enqueue` on `st` through a CUDA graph: replays the cached executable
+// graph when every launch parameter matches the one it was captured with,
+// otherwise captures anew (updating the executable in place when the topology
+// allows). Any capture failure falls back to plain launches.
+template <class F>
+cudaError_t run_as_graph(kira_ctx* ctx, const DevPairs& D, const BucketRun& R,
+                         const CompactLaunch& CL, const uint64_t* total_dev, cudaStream_t st,
+                         F&& enqueue) {
+  // Key: every value the launches read, field by field (struct padding excluded).
+  std::vector<uint8_t> key;
+  auto put = [&key](const auto& v) {
+    const uint8_t* b = reinterpret_cast<const uint8_t*>(&v);
+    key.insert(key.end(), b, b + sizeof(v));
+  };
+  put(D.n), put(D.read_seq), put(D.read_off), put(D.read_len), put(D.win_seq);
+  put(D.win_off), put(D.win_len), put(D.band_offset), put(D.abort_score), put(D.bandwidth);
+  put(R.one_round), put(R.nwork), put(R.work), put(ctx->sms);
+  for (int c = 0; c < kBandClasses; ++c) {
+    put(R.shape[c]), put(R.cnt[c]), put(R.per_round[c]);
+    if (!R.cnt[c]) continue;
+    const BswLaunch& B = R.L[c];
+    put(B.list), put(B.count), put(B.sp), put(B.offset), put(B.bias), put(B.max_q);
+    put(B.tg.trace), put(B.tg.meta), put(B.tg.slot_bytes), put(B.tg.row_stride);
+    put(B.tg.lane_bytes), put(B.tg.k_cells), put(B.tg.meta_stride), put(B.tg.half);
+    put(B.ends), put(B.cells), put(B.cig_slots), put(B.slot_cap), put(B.out), put(B.ncig);
+    put(B.item_of_pair), put(B.flags), put(B.work), put(B.item_base);
+  }
+  put(CL.n), put(CL.out), put(CL.ncig), put(CL.off), put(CL.item_of_pair), put(CL.slots);
+  put(CL.slot_cap), put(CL.ops), put(CL.cap), put(total_dev);
+  if (ctx->graph_exec && key == ctx->graph_key) {
+    ++ctx->graph_replays;
+    return cudaGraphLaunch(ctx->graph_exec, st);
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return enqueue();
+  cudaError_t ee = enqueue();
+  e = cudaStreamEndCapture(st, &g);
+  if (ee != cudaSuccess || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    ctx->graph_key.clear();
+    return enqueue();
+  }
+  if (ctx->graph_exec) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(ctx->graph_exec, g, &info) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(ctx->graph_exec);
+      ctx->graph_exec = nullptr;
+    }
+  }
+  if (!ctx->graph_exec && cudaGraphInstantiate(&ctx->graph_exec, g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->graph_exec = nullptr;
+    cudaGraphDestroy(g);
+    ctx->graph_key.clear();
+    return enqueue();
+  }
+  cudaGraphDestroy(g);
+  ctx->graph_key = std::move(key);
+  ++ctx->graph_captures;
+  return cudaGraphLaunch(ctx->graph_exec, st);
 }
 
 }  // namespace
@@ -616,6 +711,7 @@ void kira_gpu_destroy(kira_ctx* ctx) {
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);
   ctx->ref_owner.reset();
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -709,6 +805,14 @@ int kira_gpu_set_bsw_shape(kira_ctx* ctx, uint32_t band, int shape) {
 int kira_gpu_set_plain(kira_ctx* ctx, int plain) {
   if (!ctx) return KIRA_ERR_INVALID;
   ctx->plain = plain != 0;
+  return KIRA_OK;
+}
+
+int kira_gpu_set_graphs(kira_ctx* ctx, int enable, uint64_t* captures, uint64_t* replays) {
+  if (!ctx) return KIRA_ERR_INVALID;
+  if (enable >= 0) ctx->graphs = enable != 0;
+  if (captures) *captures = ctx->graph_captures;
+  if (replays) *replays = ctx->graph_replays;
   return KIRA_OK;
 }
 
@@ -867,12 +971,27 @@ int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg
                                 ctx->profile ? ctx->ev[3] : nullptr));
     if (ctx->profile) ctx->ev_recorded = 4;
     mark(ctx, 4, st);
-  } else {
-    rc = bsw_bucketed(ctx, P, D, *cfg, dout, ncig, counters + 2, cells_dev, B, st);
+    rc = finish_cigars(ctx, n, dout, ncig, B, ops, cigar->cap, total_dev, st);
     if (rc) return rc;
+  } else {
+    BucketRun R;
+    rc = plan_bucketed(ctx, P, D, *cfg, dout, ncig, counters + 2, cells_dev, B, R, st);
+    if (rc) return rc;
+    KIRA_DBUF(off, uint32_t, B_CIG_OFF, std::max<uint32_t>(n, 1));
+    KIRA_DBUF(sums, uint32_t, B_CHUNK_SUMS, n / 4096 + 2);
+    CompactLaunch CL{n, dout, ncig, off, B.item_of_pair, B.cig_slots, B.slot_cap, ops, cigar->cap};
+    auto enqueue_all = [&]() -> cudaError_t {
+      cudaError_t e = enqueue_bucketed(ctx, D, R, st);
+      if (e == cudaSuccess) e = launch_cigar_scan(ncig, n, off, sums, total_dev, st);
+      if (e == cudaSuccess) e = launch_cigar_compact(CL, ctx->sms, st);
+      return e;
+    };
+    if (ctx->graphs && !ctx->profile) {
+      KIRA_CUDA(run_as_graph(ctx, D, R, CL, total_dev, st, enqueue_all));
+    } else {
+      KIRA_CUDA(enqueue_all());
+    }
   }
-  rc = finish_cigars(ctx, n, dout, ncig, B, ops, cigar->cap, total_dev, st);
-  if (rc) return rc;
   mark(ctx, 5, st);
   uint64_t total = 0;
   unsigned long long hcells = 0;
