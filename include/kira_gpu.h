@@ -212,6 +212,14 @@ int kira_gpu_set_trace_budget(kira_ctx* ctx, uint64_t bytes);
  * Results are identical with and without graphs. */
 int kira_gpu_set_graphs(kira_ctx* ctx, int enable, uint64_t* captures, uint64_t* replays);
 
+/* kira_gpu_verify_batch on batches of at least 2 chunks runs chunk by chunk
+ * through separate copy-in, compute and copy-out streams, so uploads, kernels and
+ * downloads of consecutive chunks overlap (pinned host buffers make the copies
+ * asynchronous). pairs < 0: automatic (a quarter of the batch, at least 2^18
+ * pairs; the default), 0: off, else the chunk size. Results are identical either
+ * way. */
+int kira_gpu_set_chunk_pairs(kira_ctx* ctx, int64_t pairs);
+
 /* Upload the reference as ASCII bases (Index::ref_bases, src/index/mod.rs:1098);
  * it stays resident until the next upload or kira_gpu_destroy. */
 int kira_gpu_ref_upload(kira_ctx* ctx, const uint8_t* seq, uint64_t len);

@@ -5,8 +5,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <future>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
@@ -48,6 +50,9 @@ struct kira_ctx {
   cudaGraphExec_t graph_exec = nullptr;
   std::vector<uint8_t> graph_key;  // launch parameters the cached graph was captured with
   uint64_t graph_replays = 0, graph_captures = 0;
+  cudaStream_t h2d = nullptr, d2h = nullptr;   // copy streams of the chunked host path
+  int64_t chunk_pairs = -1;                    // chunked host path: -1 auto, 0 off, else pairs
+  std::vector<cudaEvent_t> ev_up, ev_comp;     // per chunk: inputs landed / results ready
   int sms = 148;
   cudaStream_t stream = nullptr;
   std::string last_error;
@@ -343,11 +348,11 @@ cudaError_t launch_bsw_rounds(int shape, const DevPairs& D, BswLaunch B, uint32_
 // CIGAR scan + compaction over all pairs; writes the total op count to total_dev.
 int finish_cigars(kira_ctx* ctx, uint32_t n, kira_sw_result* out, const uint32_t* ncig,
                   const BswLaunch& B, uint32_t* ops, uint64_t cap, uint64_t* total_dev,
-                  cudaStream_t st) {
+                  cudaStream_t st, bool accumulate = false) {
   cudaError_t cerr = cudaSuccess;
   KIRA_DBUF(off, uint32_t, B_CIG_OFF, std::max<uint32_t>(n, 1));
   KIRA_DBUF(sums, uint32_t, B_CHUNK_SUMS, n / 4096 + 2);
-  KIRA_CUDA(launch_cigar_scan(ncig, n, off, sums, total_dev, st));
+  KIRA_CUDA(launch_cigar_scan(ncig, n, off, sums, total_dev, st, accumulate));
   CompactLaunch C{n, out, ncig, off, B.item_of_pair, B.cig_slots, B.slot_cap, ops, cap};
   KIRA_CUDA(launch_cigar_compact(C, ctx->sms, st));
   return KIRA_OK;
@@ -359,11 +364,20 @@ void mark(kira_ctx* ctx, int i, cudaStream_t st) {
   ctx->ev_recorded = i + 1;
 }
 
+// How one call of the composed path fits into a chunked batch: planes already
+// built by the caller, whether the flag word is reset, and whether CIGAR offsets
+// continue from the running total in total_dev.
+struct ChunkMode {
+  bool planes_ready = false;
+  bool first = true;
+  bool accumulate = false;
+};
+
 // The composed path on device buffers, enqueued on `st`.
 int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verify_params& p,
                     uint64_t read_bytes, uint64_t win_bytes, bool resident, kira_sw_result* out,
                     uint32_t* ops, uint64_t cap, uint64_t* total_dev, kira_verify_detail* detail,
-                    unsigned long long* cells_dev, cudaStream_t st) {
+                    unsigned long long* cells_dev, cudaStream_t st, ChunkMode cm = ChunkMode()) {
   cudaError_t cerr = cudaSuccess;
   const uint32_t n = D.n;
   if (n == 0) return KIRA_OK;
@@ -378,13 +392,15 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
   KIRA_DBUF(mlist, uint32_t, B_MYERS_LIST, n);
   KIRA_DBUF(slist, uint32_t, B_SW_LIST, n);
   KIRA_DBUF(counters, uint32_t, B_COUNTERS, 4);
-  KIRA_CUDA(cudaMemsetAsync(counters, 0, 16, st));
+  KIRA_CUDA(cudaMemsetAsync(counters, 0, cm.first ? 16 : 8, st));
   VerifyDev V{p.sieve_threshold, p.cert_strict, sp,       out,       detail, ncig,
               swoff,             mlist,         counters, p.myers_k, (p.flags & KIRA_VERIFY_NO_QGRAM) ? 0 : 1};
   ctx->ev_recorded = 0;
   mark(ctx, 0, st);
-  rc = build_planes(ctx, D, read_bytes, win_bytes, resident, st);
-  if (rc) return rc;
+  if (!cm.planes_ready) {
+    rc = build_planes(ctx, D, read_bytes, win_bytes, resident, st);
+    if (rc) return rc;
+  }
   KIRA_CUDA(launch_verify_sieve(D, V, mx.q, ctx->sms, st));
   mark(ctx, 1, st);
   MyersLaunch M{};
@@ -420,7 +436,7 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
                               ctx->profile ? ctx->ev[3] : nullptr));
   if (ctx->profile) ctx->ev_recorded = 4;
   mark(ctx, 4, st);
-  rc = finish_cigars(ctx, n, out, ncig, B, ops, cap, total_dev, st);
+  rc = finish_cigars(ctx, n, out, ncig, B, ops, cap, total_dev, st, cm.accumulate);
   mark(ctx, 5, st);
   return rc;
 }
@@ -597,6 +613,190 @@ int plan_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const k
   return KIRA_OK;
 }
 
+// kira_gpu_verify_batch for large host batches: chunks of `chunk` pairs flow
+// through three streams -- copies in (h2d), the composed path (the context's
+// stream), results out (d2h) -- so the upload of chunk c+1, the kernels of chunk
+// c and the download of chunk c-1 overlap. The host checks of all chunks run
+// first, on parallel host threads. The read (and host window) arena is uploaded
+// as far as each chunk needs it and its planes are packed for the new range
+// only; CIGAR offsets stay global through the running total in total_dev.
+// Results are identical to the one-shot path.
+int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_params& p,
+                         kira_sw_result* out, kira_cigar_buf* cigar, kira_verify_detail* detail,
+                         uint64_t* cells, uint32_t chunk) {
+  cudaError_t cerr = cudaSuccess;
+  const uint32_t n = P.n;
+  const uint32_t nch = (n + chunk - 1) / chunk;
+  cudaStream_t st = ctx->stream;
+  const bool host_w = P.win_seq != nullptr;
+  if (!host_w && !ctx->ref_dev) return fail(ctx, KIRA_ERR_INVALID, "no resident reference uploaded");
+  const uint64_t wlim = host_w ? P.win_seq_bytes : ctx->ref_len;
+  // Host checks (bounds as upload_pairs, maxes as host_maxes) of every chunk.
+  struct Scan {
+    Maxes mx;
+    uint64_t rend = 0, wend = 0;
+    int64_t bad = -1;  // first offending pair
+    int kind = 0;      // 1: read outside read_seq, 2: window outside
+  };
+  std::vector<Scan> scans(nch);
+  auto scan_chunk = [&](uint32_t c) {
+    Scan& sc = scans[c];
+    const uint32_t lo = c * chunk, hi = std::min(n, lo + chunk);
+    for (uint32_t i = lo; i < hi; ++i) {
+      const uint64_t re = P.read_off[i] + P.read_len[i], we = P.win_off[i] + P.win_len[i];
+      if (sc.bad < 0 && (re > P.read_seq_bytes || we > wlim)) {
+        sc.bad = i;
+        sc.kind = re > P.read_seq_bytes ? 1 : 2;
+      }
+      sc.rend = std::max(sc.rend, re);
+      sc.wend = std::max(sc.wend, we);
+      sc.mx.q = std::max(sc.mx.q, P.read_len[i]);
+      sc.mx.w = std::max(sc.mx.w, P.win_len[i]);
+      const int32_t b = P.bandwidth ? P.bandwidth[i] : p.sw.bandwidth;
+      sc.mx.band = std::max(sc.mx.band, (uint32_t)std::max(b, 1));
+    }
+  };
+  // Chunk 0 is checked here and enqueued at once; host threads check the others
+  // meanwhile, each chunk's enqueue waiting for its own check.
+  std::vector<std::future<void>> pending(nch);
+  for (uint32_t c = 1; c < nch; ++c) pending[c] = std::async(std::launch::async, scan_chunk, c);
+  scan_chunk(0);
+  auto checked = [&](uint32_t c) -> int {
+    if (c && pending[c].valid()) pending[c].get();
+    if (scans[c].bad < 0) return KIRA_OK;
+    return fail(ctx, KIRA_ERR_INVALID, "pair %lld: %s outside %s", (long long)scans[c].bad,
+                scans[c].kind == 1 ? "read" : "window",
+                scans[c].kind == 1 ? "read_seq" : (host_w ? "win_seq" : "the resident reference"));
+  };
+  // Every check finishes before this call returns (the futures join on destruction).
+  if (!ctx->h2d) KIRA_CUDA(cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
+  if (!ctx->d2h) KIRA_CUDA(cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
+  while (ctx->ev_up.size() < nch + 1) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    KIRA_CUDA(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+    KIRA_CUDA(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    ctx->ev_up.push_back(a);
+    ctx->ev_comp.push_back(b);
+  }
+  // Full-size buffers first, on the compute stream; the copy stream starts after.
+  KIRA_DBUF(rs, uint8_t, B_READ_SEQ, P.read_seq_bytes);
+  KIRA_DBUF(rp, uint4, B_READ_PLANES, plane_blocks(P.read_seq_bytes));
+  uint8_t* ws = ctx->ref_dev;
+  uint4* wp = ctx->ref_planes;
+  if (host_w) {
+    KIRA_DBUF(w, uint8_t, B_WIN_SEQ, P.win_seq_bytes);
+    KIRA_DBUF(wpl, uint4, B_WIN_PLANES, plane_blocks(P.win_seq_bytes));
+    ws = w;
+    wp = wpl;
+  }
+  KIRA_DBUF(ro, uint64_t, B_READ_OFF, n);
+  KIRA_DBUF(rl, uint32_t, B_READ_LEN, n);
+  KIRA_DBUF(wo, uint64_t, B_WIN_OFF, n);
+  KIRA_DBUF(wl, uint32_t, B_WIN_LEN, n);
+  int32_t *bo = nullptr, *ab = nullptr, *bw = nullptr;
+  if (P.band_offset) {
+    KIRA_DBUF(b, int32_t, B_BAND_OFF, n);
+    bo = b;
+  }
+  if (P.abort_score) {
+    KIRA_DBUF(b, int32_t, B_ABORT, n);
+    ab = b;
+  }
+  if (P.bandwidth) {
+    KIRA_DBUF(b, int32_t, B_BANDW, n);
+    bw = b;
+  }
+  KIRA_DBUF(dout, kira_sw_result, B_OUT, n);
+  kira_verify_detail* ddet = nullptr;
+  if (detail) {
+    KIRA_DBUF(dd, kira_verify_detail, B_DETAIL, n);
+    ddet = dd;
+  }
+  KIRA_DBUF(cells_dev, unsigned long long, B_CELLS, 1);
+  KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
+  KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
+  KIRA_CUDA(cudaMemsetAsync(cells_dev, 0, 8, st));
+  KIRA_CUDA(cudaMemsetAsync(total_dev, 0, 8, st));
+  KIRA_CUDA(cudaEventRecord(ctx->ev_up[nch], st));
+  KIRA_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->ev_up[nch], 0));
+  uint64_t rdone = 0, wdone = 0;
+  for (uint32_t c = 0; c < nch; ++c) {
+    if (int rc = checked(c)) {
+      // Nothing of chunk c or later is enqueued; let the queued chunks finish first.
+      cudaStreamSynchronize(st);
+      cudaStreamSynchronize(ctx->d2h);
+      return rc;
+    }
+    const uint32_t lo = c * chunk, hi = std::min(n, lo + chunk), m = hi - lo;
+    const Maxes mx = scans[c].mx;
+    const uint64_t rneed = std::max(rdone, scans[c].rend), wneed = std::max(wdone, scans[c].wend);
+    cudaStream_t up = ctx->h2d;
+    KIRA_CUDA(cudaMemcpyAsync(ro + lo, P.read_off + lo, 8ull * m, cudaMemcpyHostToDevice, up));
+    KIRA_CUDA(cudaMemcpyAsync(rl + lo, P.read_len + lo, 4ull * m, cudaMemcpyHostToDevice, up));
+    KIRA_CUDA(cudaMemcpyAsync(wo + lo, P.win_off + lo, 8ull * m, cudaMemcpyHostToDevice, up));
+    KIRA_CUDA(cudaMemcpyAsync(wl + lo, P.win_len + lo, 4ull * m, cudaMemcpyHostToDevice, up));
+    if (bo) KIRA_CUDA(cudaMemcpyAsync(bo + lo, P.band_offset + lo, 4ull * m, cudaMemcpyHostToDevice, up));
+    if (ab) KIRA_CUDA(cudaMemcpyAsync(ab + lo, P.abort_score + lo, 4ull * m, cudaMemcpyHostToDevice, up));
+    if (bw) KIRA_CUDA(cudaMemcpyAsync(bw + lo, P.bandwidth + lo, 4ull * m, cudaMemcpyHostToDevice, up));
+    if (rneed > rdone)
+      KIRA_CUDA(cudaMemcpyAsync(rs + rdone, P.read_seq + rdone, rneed - rdone,
+                                cudaMemcpyHostToDevice, up));
+    if (host_w && wneed > wdone)
+      KIRA_CUDA(cudaMemcpyAsync(ws + wdone, P.win_seq + wdone, wneed - wdone,
+                                cudaMemcpyHostToDevice, up));
+    KIRA_CUDA(cudaEventRecord(ctx->ev_up[c], up));
+    KIRA_CUDA(cudaStreamWaitEvent(st, ctx->ev_up[c], 0));
+    // Planes of the newly arrived range, from its first (possibly partial) block.
+    if (rneed > rdone) {
+      const uint64_t b0 = rdone / 32, nb = plane_blocks(rneed);
+      KIRA_CUDA(launch_pack_planes(rs + b0 * 32, rneed - b0 * 32, rp + b0, nb - b0, ctx->sms, st));
+      rdone = rneed;
+    }
+    if (host_w && wneed > wdone) {
+      const uint64_t b0 = wdone / 32, nb = plane_blocks(wneed);
+      KIRA_CUDA(launch_pack_planes(ws + b0 * 32, wneed - b0 * 32, wp + b0, nb - b0, ctx->sms, st));
+      wdone = wneed;
+    }
+    DevPairs D{m,       rs,      ro + lo, rl + lo, ws,
+               wo + lo, wl + lo, bo ? bo + lo : nullptr, ab ? ab + lo : nullptr,
+               bw ? bw + lo : nullptr, rp, wp};
+    ChunkMode cm;
+    cm.planes_ready = true;
+    cm.first = c == 0;
+    cm.accumulate = true;
+    int rc = verify_pipeline(ctx, D, mx, p, P.read_seq_bytes, P.win_seq_bytes, !host_w, dout + lo,
+                             ops, cigar->cap, total_dev, ddet ? ddet + lo : nullptr, cells_dev, st,
+                             cm);
+    if (rc) return rc;
+    KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], st));
+    KIRA_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->ev_comp[c], 0));
+    KIRA_CUDA(cudaMemcpyAsync(out + lo, dout + lo, sizeof(kira_sw_result) * m,
+                              cudaMemcpyDeviceToHost, ctx->d2h));
+    if (detail)
+      KIRA_CUDA(cudaMemcpyAsync(detail + lo, ddet + lo, sizeof(kira_verify_detail) * m,
+                                cudaMemcpyDeviceToHost, ctx->d2h));
+  }
+  uint64_t total = 0;
+  unsigned long long hcells = 0;
+  uint32_t flags[4];
+  KIRA_CUDA(cudaMemcpyAsync(&total, total_dev, 8, cudaMemcpyDeviceToHost, ctx->d2h));
+  KIRA_CUDA(cudaMemcpyAsync(&hcells, cells_dev, 8, cudaMemcpyDeviceToHost, ctx->d2h));
+  KIRA_CUDA(cudaMemcpyAsync(flags, ctx->bufs[B_COUNTERS].p, 16, cudaMemcpyDeviceToHost, ctx->d2h));
+  KIRA_CUDA(cudaStreamSynchronize(ctx->d2h));
+  cigar->used = total;
+  if (cells) *cells = hcells;
+  if (flags[2] & 1u) return fail(ctx, KIRA_ERR_RUNTIME, "CIGAR slot overflow");
+  if (flags[2] & 6u) return fail(ctx, KIRA_ERR_INVALID, "a pair exceeded the launch's length bounds");
+  if (total > cigar->cap)
+    return fail(ctx, KIRA_ERR_CAPACITY, "CIGAR buffer holds %llu ops, %llu needed",
+                (unsigned long long)cigar->cap, (unsigned long long)total);
+  if (total) {
+    KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * total, cudaMemcpyDeviceToHost, ctx->d2h));
+    KIRA_CUDA(cudaStreamSynchronize(ctx->d2h));
+  }
+  return KIRA_OK;
+}
+
 // Runs `enqueue` on `st` through a CUDA graph: replays the cached executable
 // graph when every launch parameter matches the one it was captured with,
 // otherwise captures anew (updating the executable in place when the topology
@@ -712,6 +912,10 @@ void kira_gpu_destroy(kira_ctx* ctx) {
     if (e) cudaEventDestroy(e);
   ctx->ref_owner.reset();
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  for (auto e : ctx->ev_up) cudaEventDestroy(e);
+  for (auto e : ctx->ev_comp) cudaEventDestroy(e);
+  if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
+  if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -813,6 +1017,12 @@ int kira_gpu_set_graphs(kira_ctx* ctx, int enable, uint64_t* captures, uint64_t*
   if (enable >= 0) ctx->graphs = enable != 0;
   if (captures) *captures = ctx->graph_captures;
   if (replays) *replays = ctx->graph_replays;
+  return KIRA_OK;
+}
+
+int kira_gpu_set_chunk_pairs(kira_ctx* ctx, int64_t pairs) {
+  if (!ctx || pairs > UINT32_MAX) return KIRA_ERR_INVALID;
+  ctx->chunk_pairs = pairs < 0 ? -1 : pairs;
   return KIRA_OK;
 }
 
@@ -1132,6 +1342,14 @@ int kira_gpu_verify_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_ver
   if (cells) *cells = 0;
   if (P.n == 0) return KIRA_OK;
   cudaSetDevice(ctx->device);
+  // Chunks run one after another on the compute stream and each pays the DP and
+  // traceback latency of its longest pair, so a few large chunks overlap the
+  // copies best: by default a quarter of the batch, at least 2^18 pairs.
+  const uint64_t chunk = ctx->chunk_pairs < 0
+                             ? std::max<uint64_t>(1u << 18, (P.n + 3ull) / 4)
+                             : (uint64_t)ctx->chunk_pairs;
+  if (!ctx->profile && chunk && P.n >= 2 * chunk)
+    return verify_batch_chunked(ctx, P, *p, out, cigar, detail, cells, (uint32_t)chunk);
   const Maxes mx = host_maxes(P, p->sw.bandwidth);
   DevPairs D;
   int rc = upload_pairs(ctx, P, D);

@@ -153,7 +153,8 @@ cudaError_t launch_bsw(int shape, const DevPairs& P, const BswLaunch& B, uint32_
                        int sms, cudaStream_t st, cudaEvent_t between = nullptr,
                        int parts = kBswPartDp | kBswPartTb);
 cudaError_t launch_cigar_scan(const uint32_t* ncig, uint32_t n, uint32_t* off,
-                              uint32_t* chunk_sums, uint64_t* total_dev, cudaStream_t st);
+                              uint32_t* chunk_sums, uint64_t* total_dev, cudaStream_t st,
+                              bool accumulate = false);
 cudaError_t launch_cigar_compact(const CompactLaunch& C, int sms, cudaStream_t st);
 
 int ctx_share_reference(kira_ctx* dst, const kira_ctx* src);

@@ -612,11 +612,15 @@ __global__ void __launch_bounds__(kScanThreads) scan_chunk_sums(const uint32_t* 
   if (threadIdx.x == 0) sums[blockIdx.x] = total;
 }
 
+// With `accumulate` the scan continues from *total_out (ops already placed by
+// earlier chunks of the same batch) and leaves the running total there.
 __global__ void __launch_bounds__(kScanThreads) scan_sums(uint32_t* __restrict__ sums,
                                                           uint32_t nchunks,
-                                                          uint64_t* __restrict__ total_out) {
+                                                          uint64_t* __restrict__ total_out,
+                                                          int accumulate) {
   __shared__ uint32_t sh[32];
-  uint32_t carry = 0;
+  uint32_t carry = accumulate && total_out ? (uint32_t)*total_out : 0u;
+  __syncthreads();
   for (uint32_t base = 0; base < nchunks; base += kScanThreads) {
     const uint32_t i = base + threadIdx.x;
     const uint32_t v = i < nchunks ? sums[i] : 0u;
@@ -805,11 +809,11 @@ cudaError_t launch_bsw(int shape, const DevPairs& P, const BswLaunch& B, uint32_
 }
 
 cudaError_t launch_cigar_scan(const uint32_t* ncig, uint32_t n, uint32_t* off, uint32_t* chunk_sums,
-                              uint64_t* total_dev, cudaStream_t st) {
+                              uint64_t* total_dev, cudaStream_t st, bool accumulate) {
   const uint32_t chunks = (n + kScanChunk - 1) / kScanChunk;
   if (chunks == 0) return cudaSuccess;
   scan_chunk_sums<<<chunks, kScanThreads, 0, st>>>(ncig, n, chunk_sums);
-  scan_sums<<<1, kScanThreads, 0, st>>>(chunk_sums, chunks, total_dev);
+  scan_sums<<<1, kScanThreads, 0, st>>>(chunk_sums, chunks, total_dev, accumulate ? 1 : 0);
   scan_apply<<<chunks, kScanThreads, 0, st>>>(ncig, n, chunk_sums, off);
   return cudaGetLastError();
 }

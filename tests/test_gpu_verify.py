@@ -107,3 +107,60 @@ def test_qgram_prefilter_changes_nothing(ctx, myers_k, sub_hi, indel):
     sel = np.arange(0, w.n_pairs, 11)
     out, cig = _oracle(w, arena, woffs, VerifyParams(sieve_threshold=12, myers_k=myers_k), sel)
     _compare(on[0], on[1], on[2], out, cig, sel)
+
+
+@pytest.mark.parametrize("resident,shuffle", [(False, False), (True, False), (True, True)])
+def test_chunked_host_path_equals_one_shot(ctx, resident, shuffle):
+    # kira_gpu_verify_batch in chunks (copy-in / compute / copy-out streams, read
+    # arena and planes uploaded as far as each chunk needs) == the one-shot path.
+    from kira_ls_aligner_b200 import PairBatch, VerifyParams, _abi, synth
+    w = synth.make_workload("c", 9000, 500_000, cands=4, sub_lo=0.0, sub_hi=0.04, seed=77)
+    arena, woffs = w.windows_arena()
+    idx = np.arange(w.n_pairs)
+    if shuffle:
+        idx = np.random.default_rng(5).permutation(w.n_pairs)
+    if resident:
+        ctx.ref_upload(w.reference)
+        b = PairBatch(w.reads, w.read_off[idx].copy(), w.read_len[idx].copy(), None,
+                      w.win_off[idx].copy(), w.win_len[idx].copy())
+    else:
+        b = PairBatch(w.reads, w.read_off[idx].copy(), w.read_len[idx].copy(), arena,
+                      woffs[idx].copy(), w.win_len[idx].copy())
+    params = VerifyParams(sieve_threshold=12, myers_k=8)
+    L = _abi.lib()
+    try:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, 0))
+        one = ctx.verify_batch(b, params, detail=True)
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, 3000))
+        chunked = ctx.verify_batch(b, params, detail=True)
+    finally:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, -1))
+    assert np.array_equal(one[0], chunked[0]) and np.array_equal(one[1], chunked[1])
+    assert np.array_equal(one[2], chunked[2]) and one[3] == chunked[3]
+    sel = np.arange(0, w.n_pairs, 13)
+    out, cig = _oracle(w, arena, woffs, params, np.asarray(idx)[sel])
+    _compare(chunked[0], chunked[1], chunked[2], out, cig, sel)
+
+
+def test_chunked_host_path_rejects_out_of_range_pair(ctx):
+    # A pair in a later chunk whose read lies outside the arena fails the whole
+    # call with InvalidArgument (after the earlier chunks drain), and the context
+    # keeps working.
+    from kira_ls_aligner_b200 import InvalidArgument, PairBatch, VerifyParams, _abi, synth
+    w = synth.make_workload("e", 2000, 200_000, cands=4, seed=78)
+    arena, woffs = w.windows_arena()
+    roff = w.read_off.copy()
+    roff[6500] = len(w.reads) + 10
+    bad = PairBatch(w.reads, roff, w.read_len, arena, woffs, w.win_len)
+    good = PairBatch(w.reads, w.read_off, w.read_len, arena, woffs, w.win_len)
+    params = VerifyParams(sieve_threshold=12, myers_k=8)
+    L = _abi.lib()
+    try:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, 1000))
+        with pytest.raises(InvalidArgument):
+            ctx.verify_batch(bad, params)
+        res, ops, _, _ = ctx.verify_batch(good, params)
+    finally:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, -1))
+    ref = ctx.verify_batch(good, params)
+    assert np.array_equal(res, ref[0]) and np.array_equal(ops, ref[1])
