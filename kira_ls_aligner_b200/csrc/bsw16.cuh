@@ -37,8 +37,9 @@ template <int G, int K>
 struct Bsw16Shape {
   static constexpr int kHalf = G * K;                  // cells per half row
   static constexpr int kCap = 2 * kHalf;               // cells per row
-  static constexpr int kWords = (K + 1) / 2;           // trace words per lane per row
-  static constexpr int kLaneBytes = 4 * kWords;        // one code byte per cell
+  static constexpr int kWords = (K + 1) / 2;           // code words per lane per row
+  static constexpr int kSlabs = (kWords + 1) / 2;      // 8-byte stores per lane per row
+  static constexpr int kLaneBytes = 8 * kSlabs;        // one code byte per cell
   static constexpr int kRowStride = G * kLaneBytes;
 };
 
@@ -110,7 +111,7 @@ __device__ __forceinline__ void bsw16_group_sweep(
     uint32_t gmask, DpEnd& out, uint64_t& cells_out) {
   constexpr int H = G * K;
   constexpr int NW = Bsw16Shape<G, K>::kWords;
-  constexpr int LB = Bsw16Shape<G, K>::kLaneBytes;
+  constexpr int NS = Bsw16Shape<G, K>::kSlabs;
   constexpr int S = Bsw16Shape<G, K>::kRowStride;
   const int32_t gi = (int32_t)g;
   const int32_t c0 = gi * K;
@@ -138,6 +139,11 @@ __device__ __forceinline__ void bsw16_group_sweep(
     pe[k] = 0u;
     act[k] = 0u;
   }
+  // Window bytes of this lane's cells, four per word: word j holds cells 2j (low
+  // half, high half) and 2j+1 (low, high) as bytes 0..3.
+  uint32_t wb[NW];
+#pragma unroll
+  for (int j = 0; j < NW; ++j) wb[j] = 0u;
 
   for (uint32_t iu = 1; iu <= q; ++iu) {
     const int32_t i = (int32_t)iu;
@@ -159,7 +165,6 @@ __device__ __forceinline__ void bsw16_group_sweep(
     const int32_t row_len = je - js + 1;
     cells += (uint64_t)row_len;
     const uint32_t qb = ldb(rd, (uint64_t)(i - 1));
-    const uint32_t qb2 = qb * 0x10001u;
     const int32_t sft = js - prev_start - 1;
     if (sft != 0 && prev_len > 0) bsw16_realign<G, K>(ph, pe, sft, prev_len, rowbuf, c0, B2, gmask);
     if (row_len != act_len) {
@@ -176,7 +181,37 @@ __device__ __forceinline__ void bsw16_group_sweep(
       ne = prmt(ne, 0u, 0x5432u);
     }
     const uint8_t* wrow = wn + (js - 1);
-    const int32_t rl1 = row_len - 1;
+    // Window bytes: cells past the window end repeat its last byte (never active
+    // in this or a later row); cells past the row end hold real window bytes, so
+    // a row whose band moved one column takes the previous row's bytes shifted by
+    // one cell (the group's last lane fetches the one new byte).
+    const int32_t wlast = wl - js;
+    if ((K & 1) && sft == 0 && prev_len > 0) {
+      const uint32_t n0 = __shfl_sync(gmask, wb[0], (gi + 1) & (G - 1), G);
+#pragma unroll
+      for (int j = 0; j + 1 < NW; ++j) wb[j] = prmt(wb[j], wb[j + 1], 0x5432u);
+      wb[NW - 1] = gi == G - 1
+                       ? prmt(n0, (uint32_t)__ldg(wrow + min(2 * H - 1, wlast)), 0x0041u)
+                       : n0;
+    } else {
+#pragma unroll
+      for (int j = 0; j < NW; ++j) {
+        const int ka = 2 * j, kb = 2 * j + 1 < K ? 2 * j + 1 : K - 1;
+        const uint32_t b0 = __ldg(wrow + min(c0 + ka, wlast));
+        const uint32_t b1 = __ldg(wrow + min(H + c0 + ka, wlast));
+        const uint32_t b2 = __ldg(wrow + min(c0 + kb, wlast));
+        const uint32_t b3 = __ldg(wrow + min(H + c0 + kb, wlast));
+        wb[j] = prmt(prmt(b0, b1, 0x0040u), prmt(b2, b3, 0x0040u), 0x5410u);
+      }
+    }
+    // Bit 7 of each byte of z: that cell's window base differs from the read base.
+    const uint32_t qb4 = qb * 0x01010101u;
+    uint32_t z[NW];
+#pragma unroll
+    for (int j = 0; j < NW; ++j) {
+      const uint32_t x = wb[j] ^ qb4;
+      z[j] = x | ((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu);
+    }
 
     // Pass 1: E (+ extend flag), H_diag + s, the diag-vs-E flag, max(Hdiag+s, E)
     // and the F-scan operand G = max(Hdiag+s, E, 0) - gof + idx*ge.
@@ -190,10 +225,8 @@ __device__ __forceinline__ void bsw16_group_sweep(
       const uint32_t t = uh - GOFS;                      // H_up - gof
       const uint32_t e = __viaddmax_s16x2(ue, NGE2, t);  // max(E_up - ge, H_up - gof)
       const uint32_t yee = e + 0x0FFF0FFFu - t;          // bit 12: e > t (E extended)
-      const uint32_t bl = __ldg(wrow + min(c0 + k, rl1));
-      const uint32_t bh = __ldg(wrow + min(H + c0 + k, rl1));
-      const uint32_t x = prmt(bl, bh, 0x5410u) ^ qb2;    // per half: 0 iff bases equal
-      const uint32_t ms = prmt(x + 0x7FFF7FFFu, 0u, 0xBB99u);  // 0xFFFF per mismatching half
+      // 0xFFFF per mismatching half (sign of the cell's byte replicated).
+      const uint32_t ms = prmt(z[k >> 1], 0u, (k & 1) ? 0xBBAAu : 0x9988u);
       const uint32_t s2 = bsel(MAT2, MIS2, ms);
       const uint32_t hm = __viaddmax_s16x2(ph[k], s2, B2);     // max(Hdiag + s, 0)
       const uint32_t y1 = hm + 0x40004000u - e;          // bit 14: hm >= e
@@ -240,10 +273,18 @@ __device__ __forceinline__ void bsw16_group_sweep(
       pe[k] = ev[k] & act[k];
       ck += GE2S;
     }
-    uint32_t* trow = reinterpret_cast<uint32_t*>(trace + (size_t)i * S + (size_t)g * LB);
+    // Row layout [slab][lane] of 8-byte words: a group's lanes fill one contiguous
+    // G x 8-byte run per slab, so each store instruction writes whole sectors.
+    uint2* trow = reinterpret_cast<uint2*>(trace + (size_t)i * S) + g;
 #pragma unroll
-    for (int x = 0; x < NW; ++x)
-      trow[x] = prmt(code[2 * x], code[2 * x + 1 < K ? 2 * x + 1 : 2 * x], 0x7531u);
+    for (int x2 = 0; x2 < NS; ++x2) {
+      constexpr int kLast = K - 1;
+      const int a = 4 * x2, b = a + 1 <= kLast ? a + 1 : kLast, c = a + 2 <= kLast ? a + 2 : kLast,
+                d = a + 3 <= kLast ? a + 3 : kLast;
+      const uint32_t w0 = prmt(code[a], code[b], 0x7531u);
+      const uint32_t w1 = 2 * x2 + 1 < NW ? prmt(code[c], code[d], 0x7531u) : 0u;
+      trow[x2 * G] = make_uint2(w0, w1);
+    }
     if (g == 0) meta[i] = ((uint32_t)js << 11) | (uint32_t)row_len;
 
     // Row max and its first cell: per half the first k with the max (descending
@@ -336,8 +377,10 @@ __device__ __forceinline__ uint32_t bsw16_walk(const uint8_t* __restrict__ trace
     const uint32_t hi = (uint32_t)idx >= half ? 1u : 0u;
     const uint32_t c = (uint32_t)idx - hi * half;
     const uint32_t gi = c / k_words, kk = c - gi * k_words;
-    const uint32_t b = trace[(size_t)i * row_stride + gi * lane_bytes + (kk >> 1) * 4u +
-                             (kk & 1u) * 2u + hi];
+    // [slab][lane] rows of 8-byte words: word kk/2 of lane gi sits in slab kk/4.
+    const uint32_t lanes = half / k_words;
+    const uint32_t b = trace[(size_t)i * row_stride + (kk >> 2) * lanes * 8u + gi * 8u +
+                             ((kk >> 1) & 1u) * 4u + (kk & 1u) * 2u + hi];
     if (state == 0) {
       if (!(b & 0x80u)) break;  // H == 0
       if ((b & 0x60u) == 0x60u) {

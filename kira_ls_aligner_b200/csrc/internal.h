@@ -109,7 +109,8 @@ extern const int kNumBswShapes;
 
 inline int shape_cap(const BswShapeInfo& s) { return (s.packed ? 2 : 1) * s.g * s.k; }
 inline uint32_t shape_lane_bytes(const BswShapeInfo& s) {
-  return s.packed ? 4u * (uint32_t)((s.k + 1) / 2) : 4u * (uint32_t)((s.k + 7) / 8);
+  // packed: one code byte per cell, in 8-byte words (two cells per 32-bit half).
+  return s.packed ? 8u * (uint32_t)(((s.k + 1) / 2 + 1) / 2) : 4u * (uint32_t)((s.k + 7) / 8);
 }
 inline uint32_t shape_row_stride(const BswShapeInfo& s) {
   return (uint32_t)s.g * shape_lane_bytes(s);
