@@ -343,6 +343,22 @@ int kira_gpu_bsw_batch_noalloc(const kira_pairs* pairs, const kira_sw_cfg* cfg,
                                kira_sw_result* out, uint32_t* cigar_ops, uint64_t cigar_cap,
                                uint64_t* cigar_used, void* stream);
 
+/* ------------------------------------------------------------- NM and MD:Z
+ *
+ * compute_nm_md / nm_md_from_cigar (src/alignment/mod.rs:1774-1782,
+ * src/alignment/md.rs:162-205) for every pair of a batch, on the device, from the
+ * results and CIGAR ops that kira_gpu_verify_batch / kira_gpu_bsw_batch /
+ * kira_gpu_align_batch_simd returned for the same `pairs` (window coordinates:
+ * read_start / ref_start into the pair's read and window). nm[i] is the SAM NM
+ * (0xFFFFFFFF for a pair without an alignment, n_cigar == 0); pair i's MD:Z text
+ * is md[md_off[i] .. md_off[i + 1]) (no NUL; md_off has n + 1 entries).
+ * KIRA_ERR_CAPACITY when the text exceeds md_cap (*md_used gives the need; nm and
+ * md_off are filled). Stage times (kira_gpu_stage_times): [0] inputs uploaded,
+ * [1] NM + MD lengths + offsets, [2] host check, [3] MD text. */
+int kira_gpu_nm_md(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_result* results,
+                   const uint32_t* cigar_ops, uint64_t n_ops, uint32_t* nm, uint32_t* md_off,
+                   char* md, uint64_t md_cap, uint64_t* md_used);
+
 /* ------------------------------------------------ serving (continuous batching)
  *
  * No counterpart in the reference, whose dispatcher thread runs one blocking

@@ -17,7 +17,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIB_DIR, "libkira_gpu.so")
 SOURCES = ["kernels.cu", "api.cu", "noalloc.cu", "server.cpp"]
-HEADERS = ["common.cuh", "sieve.cuh", "myers.cuh", "bsw.cuh", "bsw16.cuh", "qgram.cuh",
+HEADERS = ["common.cuh", "sieve.cuh", "myers.cuh", "bsw.cuh", "bsw16.cuh", "qgram.cuh", "nmmd.cuh",
            "planes.cuh", "addchain.cuh", "internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -19,6 +19,7 @@ using namespace kira;
 namespace {
 
 enum BufId {
+  B_NMMD_RES, B_NMMD_OPS, B_NMMD_NM, B_NMMD_LEN, B_NMMD_OFF, B_NMMD_OUT, B_NMMD_FLAGS,
   B_READ_SEQ, B_WIN_SEQ, B_READ_OFF, B_READ_LEN, B_WIN_OFF, B_WIN_LEN, B_BAND_OFF, B_ABORT,
   B_BANDW, B_OUT, B_DETAIL, B_CIGAR_OUT, B_NCIG, B_CIG_OFF, B_CHUNK_SUMS, B_SW_OFFSET,
   B_MYERS_LIST, B_SW_LIST, B_COUNTERS, B_ENDS, B_TRACE, B_META, B_CIG_SLOTS, B_ITEM_OF_PAIR,
@@ -1017,6 +1018,65 @@ int kira_gpu_set_graphs(kira_ctx* ctx, int enable, uint64_t* captures, uint64_t*
   if (enable >= 0) ctx->graphs = enable != 0;
   if (captures) *captures = ctx->graph_captures;
   if (replays) *replays = ctx->graph_replays;
+  return KIRA_OK;
+}
+
+int kira_gpu_nm_md(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_result* results,
+                   const uint32_t* cigar_ops, uint64_t n_ops, uint32_t* nm, uint32_t* md_off,
+                   char* md, uint64_t md_cap, uint64_t* md_used) {
+  if (!ctx || !pairs || !results || !nm || !md_off || !md_used) return KIRA_ERR_INVALID;
+  const kira_pairs& P = *pairs;
+  *md_used = 0;
+  md_off[0] = 0;
+  if (P.n == 0) return KIRA_OK;
+  if (n_ops && !cigar_ops) return KIRA_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  ctx->ev_recorded = 0;
+  mark(ctx, 0, st);
+  DevPairs D;
+  int rc = upload_pairs(ctx, P, D);
+  if (rc) return rc;
+  cudaError_t cerr = cudaSuccess;
+  const uint32_t n = P.n;
+  KIRA_DBUF(dres, kira_sw_result, B_NMMD_RES, n);
+  KIRA_DBUF(dops, uint32_t, B_NMMD_OPS, std::max<uint64_t>(n_ops, 1));
+  KIRA_DBUF(dnm, uint32_t, B_NMMD_NM, n);
+  KIRA_DBUF(dlen, uint32_t, B_NMMD_LEN, n);
+  KIRA_DBUF(doff, uint32_t, B_NMMD_OFF, n);
+  KIRA_DBUF(sums, uint32_t, B_CHUNK_SUMS, n / 4096 + 2);
+  KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
+  KIRA_DBUF(flags, uint32_t, B_NMMD_FLAGS, 1);
+  KIRA_CUDA(cudaMemcpyAsync(dres, results, sizeof(kira_sw_result) * n, cudaMemcpyHostToDevice, st));
+  if (n_ops)
+    KIRA_CUDA(cudaMemcpyAsync(dops, cigar_ops, 4ull * n_ops, cudaMemcpyHostToDevice, st));
+  KIRA_CUDA(cudaMemsetAsync(flags, 0, 4, st));
+  mark(ctx, 1, st);
+  NmMdLaunch L{n, dres, dops, n_ops, dnm, dlen, doff, nullptr, flags};
+  KIRA_CUDA(launch_nm_md(D, L, false, ctx->sms, st));
+  KIRA_CUDA(launch_cigar_scan(dlen, n, doff, sums, total_dev, st));
+  mark(ctx, 2, st);
+  uint64_t total = 0;
+  uint32_t hflags = 0;
+  KIRA_CUDA(cudaMemcpyAsync(&total, total_dev, 8, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(&hflags, flags, 4, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(nm, dnm, 4ull * n, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(md_off, doff, 4ull * n, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaStreamSynchronize(st));
+  if (hflags & 1u) return fail(ctx, KIRA_ERR_INVALID, "a result's CIGAR lies outside cigar_ops");
+  if (total > UINT32_MAX) return fail(ctx, KIRA_ERR_INVALID, "MD text above 4 GiB: split the batch");
+  md_off[n] = (uint32_t)total;
+  *md_used = total;
+  if (total > md_cap)
+    return fail(ctx, KIRA_ERR_CAPACITY, "MD buffer holds %llu bytes, %llu needed",
+                (unsigned long long)md_cap, (unsigned long long)total);
+  KIRA_DBUF(dmd, char, B_NMMD_OUT, std::max<uint64_t>(total, 1));
+  L.md = dmd;
+  mark(ctx, 3, st);
+  KIRA_CUDA(launch_nm_md(D, L, true, ctx->sms, st));
+  mark(ctx, 4, st);
+  if (total) KIRA_CUDA(cudaMemcpyAsync(md, dmd, total, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaStreamSynchronize(st));
   return KIRA_OK;
 }
 

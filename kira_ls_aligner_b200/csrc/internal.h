@@ -99,6 +99,19 @@ struct CompactLaunch {
   uint64_t cap;
 };
 
+// NM / MD:Z pass over a batch's results (nmmd.cuh).
+struct NmMdLaunch {
+  uint32_t n;
+  const kira_sw_result* res;  // per pair, from the alignment call
+  const uint32_t* ops;        // that call's CIGAR ops
+  uint64_t n_ops;
+  uint32_t* nm;               // pass 1 out: NM (0xFFFFFFFF: no alignment)
+  uint32_t* len;              // pass 1 out: MD length
+  const uint32_t* off;        // pass 2 in: MD offset of each pair
+  char* md;                   // pass 2 out
+  uint32_t* flags;            // bit 0: a result's CIGAR range lies outside the ops
+};
+
 // Banded-SW launch shape: G lanes per pair, K cells (int32) or K packed words of
 // two int16 cells (packed) per lane.
 struct BswShapeInfo {
@@ -157,6 +170,8 @@ cudaError_t launch_cigar_scan(const uint32_t* ncig, uint32_t n, uint32_t* off,
                               uint32_t* chunk_sums, uint64_t* total_dev, cudaStream_t st,
                               bool accumulate = false);
 cudaError_t launch_cigar_compact(const CompactLaunch& C, int sms, cudaStream_t st);
+cudaError_t launch_nm_md(const DevPairs& P, const NmMdLaunch& L, bool write, int sms,
+                         cudaStream_t st);
 
 int ctx_share_reference(kira_ctx* dst, const kira_ctx* src);
 

@@ -5,6 +5,7 @@
 #include "bsw16.cuh"
 #include "internal.h"
 #include "myers.cuh"
+#include "nmmd.cuh"
 #include "planes.cuh"
 #include "qgram.cuh"
 #include "sieve.cuh"
@@ -672,6 +673,29 @@ __global__ void __launch_bounds__(256) cigar_compact_kernel(CompactLaunch C) {
   }
 }
 
+// NM / MD:Z of every pair's alignment, one thread per pair (nmmd.cuh). Pass 1
+// (write = 0) stores NM and the MD length, pass 2 the MD bytes at their offsets.
+__global__ void __launch_bounds__(128) nmmd_kernel(DevPairs P, NmMdLaunch L, int write) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < L.n; p += stride) {
+    const kira_sw_result r = L.res[p];
+    uint32_t nm = 0xFFFFFFFFu, len = 0;
+    if (r.n_cigar) {
+      if ((uint64_t)r.cigar_off + r.n_cigar > L.n_ops || r.read_start < 0) {
+        if (!write) atomicOr(L.flags, 1u);
+      } else {
+        len = nmmd_walk(P.read_seq + P.read_off[p], P.read_len[p], P.win_seq + P.win_off[p],
+                        P.win_len[p], (uint32_t)r.read_start, r.ref_start, L.ops + r.cigar_off,
+                        r.n_cigar, nm, write ? L.md + L.off[p] : nullptr);
+      }
+    }
+    if (!write) {
+      L.nm[p] = nm;
+      L.len[p] = len;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
@@ -815,6 +839,13 @@ cudaError_t launch_cigar_scan(const uint32_t* ncig, uint32_t n, uint32_t* off, u
   scan_chunk_sums<<<chunks, kScanThreads, 0, st>>>(ncig, n, chunk_sums);
   scan_sums<<<1, kScanThreads, 0, st>>>(chunk_sums, chunks, total_dev, accumulate ? 1 : 0);
   scan_apply<<<chunks, kScanThreads, 0, st>>>(ncig, n, chunk_sums, off);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_nm_md(const DevPairs& P, const NmMdLaunch& L, bool write, int sms,
+                         cudaStream_t st) {
+  const int blocks = grid_for(L.n, 128, sms * 16);
+  nmmd_kernel<<<blocks, 128, 0, st>>>(P, L, write ? 1 : 0);
   return cudaGetLastError();
 }
 

@@ -332,6 +332,28 @@ class GpuContext:
         self.check(rc)
         return res[:n], ops[: cb.used]
 
+    # -- NM / MD:Z of a batch's alignments
+    def nm_md(self, batch: PairBatch, res: np.ndarray, ops: np.ndarray,
+              md_cap: int | None = None):
+        """(nm per pair, list of MD strings) for the results `res` / CIGAR `ops`
+        an alignment call returned on `batch` (nm 0xFFFFFFFF without alignment)."""
+        n = batch.n
+        res = np.ascontiguousarray(res)
+        ops = np.ascontiguousarray(ops, np.uint32)
+        nm = np.zeros(max(n, 1), np.uint32)
+        off = np.zeros(n + 1, np.uint32)
+        cap = md_cap if md_cap is not None else max(64, 8 * n)
+        md = np.zeros(cap, np.uint8)
+        used = C.c_uint64()
+        pc = batch.to_c()
+        rc = self._lib.kira_gpu_nm_md(self._h, C.byref(pc), A.ptr(res), A.ptr(ops) if len(ops) else None,
+                                      len(ops), A.ptr(nm), A.ptr(off), A.ptr(md), cap, C.byref(used))
+        if rc == 9 and md_cap is None:
+            return self.nm_md(batch, res, ops, int(used.value) + 16)
+        self.check(rc)
+        text = md.tobytes()
+        return nm[:n], [text[off[i]:off[i + 1]].decode() for i in range(n)]
+
     # -- composed verification
     def verify_batch(self, batch: PairBatch, params: VerifyParams, detail: bool = False,
                      cigar_cap: int | None = None):

@@ -17,6 +17,7 @@
 #include <atomic>
 #include <climits>
 #include <cstring>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -1435,3 +1436,146 @@ int orc_sieve_batch(uint32_t n, const uint8_t* reads, const uint64_t* read_off,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// NM / MD:Z (src/alignment/md.rs). MdBuilder (md.rs:24-133): a match extends
+// the run; a mismatch writes the run count and the reference letter; a deletion
+// writes the count, '^' and the deleted reference letters; an insertion only
+// adds to NM; a skip is invisible; the string always ends with a count.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Md {
+  std::string text;
+  uint32_t run = 0, nm = 0;
+  void flush() {
+    text += std::to_string(run);
+    run = 0;
+  }
+  // reference_letter (md.rs:52-58): ASCII letters upper-cased, anything else 'N'.
+  static char letter(uint8_t b) {
+    const bool alpha = (b >= 'A' && b <= 'Z') || (b >= 'a' && b <= 'z');
+    return alpha ? (char)(b & 0xDF) : 'N';
+  }
+  void matched() { ++run; }
+  void mismatch(uint8_t rb) {
+    flush();
+    text += letter(rb);
+    ++nm;
+  }
+  // identical_base_is_edit (md.rs:135-138)
+  static bool ident_edit(uint8_t b) {
+    const uint8_t u = (b >= 'a' && b <= 'z') ? (uint8_t)(b - 32) : b;
+    return !(u == 'A' || u == 'C' || u == 'G' || u == 'T' || u == '=');
+  }
+  // column (md.rs:77-86): '=' or case-insensitive equality extends the run.
+  void column(uint8_t qb, uint8_t rb) {
+    const auto low = [](uint8_t c) { return (c >= 'A' && c <= 'Z') ? (uint8_t)(c + 32) : c; };
+    if (qb == '=' || low(qb) == low(rb)) {
+      matched();
+      nm += ident_edit(qb) ? 1u : 0u;
+    } else {
+      mismatch(rb);
+    }
+  }
+  void insertion(uint32_t len) { nm += len; }
+  void deletion(const uint8_t* bases, size_t len) {
+    if (!len) return;
+    flush();
+    text += '^';
+    for (size_t i = 0; i < len; ++i) text += letter(bases[i]);
+    nm += (uint32_t)len;
+  }
+  uint32_t finish(uint32_t* nm_out, char* md, uint32_t cap) {
+    flush();
+    *nm_out = nm;
+    std::memcpy(md, text.data(), std::min<size_t>(cap, text.size()));
+    return (uint32_t)text.size();
+  }
+};
+
+}  // namespace
+
+extern "C" uint32_t orc_nm_md(const uint8_t* read, size_t read_len, const uint8_t* ref,
+                              size_t ref_len, size_t read_start, size_t ref_start,
+                              const uint32_t* cigar, uint32_t n_cigar, uint32_t* nm, char* md,
+                              uint32_t md_cap) {
+  Md b;
+  size_t q = read_start, r = ref_start;
+  for (uint32_t k = 0; k < n_cigar; ++k) {
+    const size_t len = cigar[k] >> 4;
+    switch (cigar[k] & 15u) {
+      case 0:  // M: positions past either end read as 'N' (md.rs:176-181)
+        for (size_t t = 0; t < len; ++t, ++q, ++r)
+          b.column(q < read_len ? read[q] : 'N', r < ref_len ? ref[r] : 'N');
+        break;
+      case 1:
+        b.insertion((uint32_t)len);
+        q += len;
+        break;
+      case 2: {  // D: bases past the reference end still count toward NM (md.rs:188-194)
+        const size_t end = std::min(r + len, ref_len), start = std::min(r, end);
+        b.deletion(ref + start, end - start);
+        b.nm += (uint32_t)(len - (end - start));
+        r += len;
+        break;
+      }
+      case 3:
+        r += len;
+        break;
+      default:  // S
+        q += len;
+        break;
+    }
+  }
+  return b.finish(nm, md, md_cap);
+}
+
+extern "C" uint32_t orc_md_builder(const char* script, const uint8_t* read, const uint8_t* ref,
+                                   const uint32_t* lens, uint32_t n, uint32_t* nm, char* md,
+                                   uint32_t md_cap) {
+  Md b;
+  size_t at = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    switch (script[i]) {
+      case 'M': b.matched(); break;
+      case 'X': b.mismatch(ref[at++]); break;
+      case 'C': b.column(read[at], ref[at]); ++at; break;
+      case 'I': b.insertion(lens[i]); break;
+      case 'D': b.deletion(ref + at, lens[i]); at += lens[i]; break;
+      default: break;
+    }
+  }
+  return b.finish(nm, md, md_cap);
+}
+
+extern "C" int orc_nm_md_batch(uint32_t n, const uint8_t* reads, const uint64_t* read_off,
+                               const uint32_t* read_len, const uint8_t* wins,
+                               const uint64_t* win_off, const uint32_t* win_len,
+                               const int32_t* read_start, const uint32_t* ref_start,
+                               const uint32_t* cig_off, const uint32_t* n_cig,
+                               const uint32_t* ops, int nthreads, uint32_t* nm,
+                               uint32_t* md_len, char* md, uint32_t md_stride) {
+  std::atomic<uint32_t> next{0};
+  auto work = [&]() {
+    for (;;) {
+      const uint32_t i = next.fetch_add(64);
+      if (i >= n) return;
+      for (uint32_t p = i; p < std::min(n, i + 64); ++p) {
+        if (!n_cig[p]) {
+          nm[p] = 0xFFFFFFFFu;
+          md_len[p] = 0;
+          continue;
+        }
+        md_len[p] = orc_nm_md(reads + read_off[p], read_len[p], wins + win_off[p], win_len[p],
+                              (size_t)read_start[p], ref_start[p], ops + cig_off[p], n_cig[p],
+                              nm + p, md + (size_t)p * md_stride, md_stride);
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < std::max(nthreads, 1); ++t) th.emplace_back(work);
+  work();
+  for (auto& t : th) t.join();
+  return 0;
+}

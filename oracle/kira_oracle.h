@@ -161,6 +161,25 @@ int orc_sieve_batch(uint32_t n, const uint8_t* reads, const uint64_t* read_off,
                     const uint32_t* win_len, int nthreads, int32_t* shift, int32_t* mism,
                     int32_t* second);
 
+/* NM and MD:Z of one alignment: nm_md_from_cigar (src/alignment/md.rs:162-205)
+ * with the MdBuilder rules (md.rs:24-146). cigar words are len << 4 | op with
+ * op 0 M, 1 I, 2 D, 3 N, 4 S. Writes at most md_cap bytes of MD (no NUL) and
+ * returns the full MD length. */
+uint32_t orc_nm_md(const uint8_t* read, size_t read_len, const uint8_t* ref, size_t ref_len,
+                   size_t read_start, size_t ref_start, const uint32_t* cigar, uint32_t n_cigar,
+                   uint32_t* nm, char* md, uint32_t md_cap);
+/* MdBuilder driven directly (the md_format.rs cases): ops 'M' matched, 'X'
+ * mismatch(ref[i]), 'C' column(read[i], ref[i]), 'I' insertion(len), 'D'
+ * deletion(ref bytes of length len). */
+uint32_t orc_md_builder(const char* script, const uint8_t* read, const uint8_t* ref,
+                        const uint32_t* lens, uint32_t n, uint32_t* nm, char* md, uint32_t md_cap);
+/* Threaded batch: NM/MD of each pair's alignment (window coordinates). */
+int orc_nm_md_batch(uint32_t n, const uint8_t* reads, const uint64_t* read_off,
+                    const uint32_t* read_len, const uint8_t* wins, const uint64_t* win_off,
+                    const uint32_t* win_len, const int32_t* read_start, const uint32_t* ref_start,
+                    const uint32_t* cig_off, const uint32_t* n_cig, const uint32_t* ops,
+                    int nthreads, uint32_t* nm, uint32_t* md_len, char* md, uint32_t md_stride);
+
 #ifdef __cplusplus
 }
 #endif

@@ -81,6 +81,13 @@ def lib():
                                               C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.orc_byte_scan.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.c_size_t,
                                     C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.orc_nm_md.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.c_size_t,
+                                C.c_size_t, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32),
+                                C.c_char_p, C.c_uint32]
+        L.orc_nm_md.restype = C.c_uint32
+        L.orc_md_builder.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_void_p, C.c_uint32,
+                                     C.POINTER(C.c_uint32), C.c_char_p, C.c_uint32]
+        L.orc_md_builder.restype = C.c_uint32
         L.orc_myers.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.c_size_t, C.c_int,
                                 C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         L.orc_banded_sw.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.c_int32,
@@ -406,3 +413,41 @@ def sieve_batch(reads, read_off, read_len, wins, win_off, win_len, nthreads):
     lib().orc_sieve_batch(n, _p(reads), _p(read_off), _p(read_len), _p(wins), _p(win_off),
                           _p(win_len), nthreads, _p(s), _p(m), _p(sec))
     return s, m, sec
+
+
+CIGAR_CODES = {"M": 0, "I": 1, "D": 2, "N": 3, "S": 4}
+
+
+def nm_md(read: bytes, ref: bytes, read_start: int, ref_start: int, cigar) -> tuple:
+    """nm_md_from_cigar (md.rs:162-205); cigar as [(len, 'M'|'I'|'D'|'N'|'S')] or
+    packed words. Returns (NM, MD)."""
+    words = [w if isinstance(w, int) else (w[0] << 4) | CIGAR_CODES[w[1]] for w in cigar]
+    arr = np.asarray(words or [0], np.uint32)
+    nm = C.c_uint32()
+    cap = 4 * (len(read) + len(ref)) + 64
+    buf = C.create_string_buffer(cap)
+    n = lib().orc_nm_md(read, len(read), ref, len(ref), read_start, ref_start,
+                        arr.ctypes.data, len(words), C.byref(nm), buf, cap)
+    return nm.value, buf.raw[:n].decode()
+
+
+def md_builder(script: str, read: bytes = b"", ref: bytes = b"", lens=None) -> tuple:
+    """MdBuilder driven op by op (see orc_md_builder)."""
+    lens = np.asarray(lens if lens is not None else [0] * len(script), np.uint32)
+    nm = C.c_uint32()
+    buf = C.create_string_buffer(4096)
+    n = lib().orc_md_builder(script.encode(), read or b"\0", ref or b"\0", lens.ctypes.data,
+                             len(script), C.byref(nm), buf, 4096)
+    return nm.value, buf.raw[:n].decode()
+
+
+def nm_md_batch(reads, read_off, read_len, wins, win_off, win_len, read_start, ref_start,
+                cig_off, n_cig, ops, nthreads: int, md_stride: int = 2048):
+    n = len(read_off)
+    nm = np.zeros(n, np.uint32)
+    md_len = np.zeros(n, np.uint32)
+    md = np.zeros(n * md_stride, np.uint8)
+    lib().orc_nm_md_batch(n, _p(reads), _p(read_off), _p(read_len), _p(wins), _p(win_off),
+                          _p(win_len), _p(read_start), _p(ref_start), _p(cig_off), _p(n_cig),
+                          _p(ops), nthreads, _p(nm), _p(md_len), _p(md), md_stride)
+    return nm, md_len, md.reshape(n, md_stride)
