@@ -701,9 +701,9 @@ def run_ours(args, rank, local, world, dist):
         4: n * (32 + 8) + 4 * n,
     }[dom]
     # DRAM bytes per unit from the ncu captures of the same kernels (800k-pair case,
-    # scaled by units processed): profiles/bsw16_dp_batched_800k.md (1.285 B per DP
-    # cell) and profiles/verify_sieve_batched_800k.md (168.8 B per pair).
-    traffic = {0: 168.8 * n, 2: 1.285 * cells_step if packed else None}.get(dom)
+    # scaled by units processed): profiles/bsw16_dp_batched_800k.md (1.496 B per DP
+    # cell) and profiles/verify_sieve_batched_800k.md (169.8 B per pair).
+    traffic = {0: 169.8 * n, 2: 1.496 * cells_step if packed else None}.get(dom)
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     dp_ms = stage_ms[2] / args.steps
     roofline = {"bound": "hbm", "kernel": _abi.STAGES[dom], "achieved": achieved, "peak": peak,
@@ -716,8 +716,8 @@ def run_ours(args, rank, local, world, dist):
                 # 77-85 % of peak, DRAM < 10 %); their binding roofline is the ALU pipe.
                 "int_pipe": {"kernel": "bsw_dp", "gcups": cells_step / (dp_ms / 1e3) / 1e9
                              if dp_ms > 0 else None,
-                             "alu_pipe_frac_ncu": 0.845 if packed else 0.757,
-                             "thread_inst_per_cell_ncu": 33.1 if packed else 90.8,
+                             "alu_pipe_frac_ncu": 0.770 if packed else 0.757,
+                             "thread_inst_per_cell_ncu": 28.3 if packed else 90.8,
                              "source": "profiles/bsw16_dp_batched_800k.md"}}
 
     cpu = None
