@@ -359,6 +359,57 @@ int kira_gpu_nm_md(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_result*
                    const uint32_t* cigar_ops, uint64_t n_ops, uint32_t* nm, uint32_t* md_off,
                    char* md, uint64_t md_cap, uint64_t* md_used);
 
+/* ------------------------------------------------------------------- WFA
+ *
+ * Wavefront alignment (src/alignment/wfa.rs), the cascade step between Myers and
+ * banded SW: try_fast_dp_alignment's wfa_align_scored call (src/alignment/
+ * mod.rs:344-439) and the score probes ungapped_beaten_by_gap /
+ * locus_alignment_score (mod.rs:162-240). The whole read (pattern) is aligned to
+ * a prefix of the window (text) with affine gaps; trailing text is free and up to
+ * text_begin_free leading text bases are free. */
+
+/* WfaPenalties / AlignmentConfig plus WfaOptions (wfa.rs:9-17, 81-111). */
+typedef struct kira_wfa_params {
+  int32_t mismatch;        /* WfaPenalties.mismatch, or AlignmentConfig.mismatch when scored */
+  int32_t gap_open;
+  int32_t gap_extend;
+  int32_t match_score;     /* scored only */
+  int32_t scored;          /* 1: WfaCosts::scored (wfa.rs:41-52): mismatch + match per
+                              mismatch, gap_extend + match per inserted base */
+  int32_t max_score;       /* WfaOptions.max_score; < 0: router::wfa_score_budget of each
+                              read (router.rs:160-165) */
+  int32_t budget_pct;      /* KIRA_WFA_BUDGET_PCT of that budget; < 0: 25 */
+  int32_t adaptive_drop;   /* WfaOptions.adaptive_drop: >= 0 Some(drop), < 0 None */
+  int32_t text_begin_free; /* WfaOptions.text_begin_free */
+  int32_t traceback;       /* 1: wfa_align / wfa_align_scored (CIGAR + text_start);
+                              0: wfa_score_only / wfa_score_only_scored */
+} kira_wfa_params;
+
+/* WfaAlignment (wfa.rs:113-124) of one pair. found = 0 for None (no alignment of
+ * cost <= max_score, or scored costs that WfaCosts::scored refuses). */
+typedef struct kira_wfa_result {
+  int32_t cost;        /* WfaAlignment.score: the WFA cost (the loss when scored); -1 for None */
+  int32_t score;       /* scored: read_len * match_score - cost (wfa_score_only_scored); else cost */
+  uint32_t text_start; /* traceback only (0 otherwise) */
+  uint32_t text_end;
+  uint32_t cigar_off;  /* ops[cigar_off .. + n_cigar) of the call's CIGAR buffer (M, I, D) */
+  uint32_t n_cigar;
+  uint32_t found;
+  uint32_t reserved;
+} kira_wfa_result;
+
+/* wfa_align / wfa_score_only (and the scored forms) for every pair of the batch.
+ * Per-pair max_score and text_begin_free arrays override the params when given
+ * (the per-read budgets of ungapped_beaten_by_gap, the ends-free retry of
+ * mod.rs:393-419). Reads and windows up to 30000 bases. Plain penalties need
+ * mismatch >= 1, gap_open >= 0 and gap_extend >= 1 (KIRA_ERR_INVALID otherwise);
+ * cigar may be NULL when traceback = 0. Stage times: [0] inputs uploaded,
+ * [1] wavefronts and traceback, [2] CIGAR scan and compaction, [3] results
+ * downloaded. */
+int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_params* p,
+                       const int32_t* max_score, const int32_t* text_begin_free,
+                       kira_wfa_result* out, kira_cigar_buf* cigar);
+
 /* ------------------------------------------------ serving (continuous batching)
  *
  * No counterpart in the reference, whose dispatcher thread runs one blocking

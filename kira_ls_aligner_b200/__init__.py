@@ -7,8 +7,8 @@ of that boundary; there is no CPU compute path in this package.
 from . import _abi
 from .runtime import (AlignmentConfig, CapacityError, CudaError, GpuContext, InvalidArgument,
                       PairBatch, Server, SwPublicResult, Ticket, Timeout, VerifyParams,
-                      cigar_string, decode_cigar, is_available, results_to_list)
+                      WfaParams, cigar_string, decode_cigar, is_available, results_to_list)
 
 __all__ = ["AlignmentConfig", "CapacityError", "CudaError", "GpuContext", "InvalidArgument",
            "PairBatch", "Server", "SwPublicResult", "Ticket", "Timeout", "VerifyParams",
-           "cigar_string", "decode_cigar", "is_available", "results_to_list", "_abi"]
+           "WfaParams", "cigar_string", "decode_cigar", "is_available", "results_to_list", "_abi"]

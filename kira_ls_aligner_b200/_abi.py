@@ -36,7 +36,7 @@ EXPORTS = (
     "kira_gpu_verify_dev", "kira_gpu_profile", "kira_gpu_stage_times",
     "kira_gpu_bsw_shapes", "kira_gpu_set_bsw_shape", "kira_gpu_bsw_batch_noalloc",
     "kira_gpu_align_batch_simd", "kira_gpu_set_plain", "kira_gpu_set_trace_budget",
-    "kira_gpu_set_graphs", "kira_gpu_set_chunk_pairs", "kira_gpu_nm_md",
+    "kira_gpu_set_graphs", "kira_gpu_set_chunk_pairs", "kira_gpu_nm_md", "kira_gpu_wfa_batch",
     "kira_server_create", "kira_server_destroy", "kira_server_ref_upload",
     "kira_server_submit_verify", "kira_server_submit_bsw", "kira_server_poll",
     "kira_server_wait", "kira_server_info", "kira_server_release", "kira_server_stats",
@@ -80,6 +80,12 @@ class VerifyParams(C.Structure):
                 ("cert_strict", C.c_int32), ("flags", C.c_int32)]
 
 
+class WfaParams(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in
+                ("mismatch", "gap_open", "gap_extend", "match_score", "scored", "max_score",
+                 "budget_pct", "adaptive_drop", "text_begin_free", "traceback")]
+
+
 class ServerCfg(C.Structure):
     _fields_ = [("device", C.c_int), ("slots", C.c_int), ("max_batch_pairs", C.c_uint32),
                 ("mem_fraction", C.c_double)]
@@ -102,7 +108,11 @@ SW_RESULT_DTYPE = np.dtype([("score", "<i4"), ("ref_start", "<u4"), ("ref_end", 
                             ("reserved", "<u2")])
 DETAIL_DTYPE = np.dtype([("sieve_shift", "<i4"), ("sieve_mism", "<i4"),
                          ("sieve_second", "<i4"), ("myers_dist", "<i4"), ("myers_end", "<i4")])
+WFA_RESULT_DTYPE = np.dtype([("cost", "<i4"), ("score", "<i4"), ("text_start", "<u4"),
+                             ("text_end", "<u4"), ("cigar_off", "<u4"), ("n_cigar", "<u4"),
+                             ("found", "<u4"), ("reserved", "<u4")])
 assert SW_RESULT_DTYPE.itemsize == 32 and DETAIL_DTYPE.itemsize == 20
+assert WFA_RESULT_DTYPE.itemsize == 32
 
 _lib = None
 
@@ -142,6 +152,8 @@ def lib():
     L.kira_gpu_set_chunk_pairs.argtypes = [vp, C.c_int64]
     L.kira_gpu_nm_md.argtypes = [vp, C.POINTER(Pairs), vp, vp, C.c_uint64, vp, vp, vp,
                                  C.c_uint64, C.POINTER(C.c_uint64)]
+    L.kira_gpu_wfa_batch.argtypes = [vp, C.POINTER(Pairs), C.POINTER(WfaParams), vp, vp, vp,
+                                     C.POINTER(CigarBuf)]
     L.kira_gpu_align_batch_simd.argtypes = [vp, C.POINTER(Pairs), C.POINTER(SwCfg), C.c_int,
                                             C.c_int, vp, C.POINTER(CigarBuf)]
     L.kira_gpu_bsw_batch_noalloc.argtypes = [C.POINTER(Pairs), C.POINTER(SwCfg), vp, vp,

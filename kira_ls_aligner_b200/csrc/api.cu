@@ -24,7 +24,8 @@ enum BufId {
   B_BANDW, B_OUT, B_DETAIL, B_CIGAR_OUT, B_NCIG, B_CIG_OFF, B_CHUNK_SUMS, B_SW_OFFSET,
   B_MYERS_LIST, B_SW_LIST, B_COUNTERS, B_ENDS, B_TRACE, B_META, B_CIG_SLOTS, B_ITEM_OF_PAIR,
   B_DIST, B_END, B_SIEVE_OUT, B_SIEVE_JOBS, B_CELLS, B_TOTAL, B_READ_PLANES, B_WIN_PLANES,
-  B_ROWKEYS, B_DONE_ROW, B_WORK, B_COUNT
+  B_ROWKEYS, B_DONE_ROW, B_WORK, B_WFA_MAXS, B_WFA_TBF, B_WFA_OUT, B_WFA_NCIG, B_WFA_SLOTS,
+  B_WFA_SCRATCH, B_WFA_FLAGS, B_COUNT
 };
 
 struct DevBuf {
@@ -1076,6 +1077,194 @@ int kira_gpu_nm_md(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_result*
   KIRA_CUDA(launch_nm_md(D, L, true, ctx->sms, st));
   mark(ctx, 4, st);
   if (total) KIRA_CUDA(cudaMemcpyAsync(md, dmd, total, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaStreamSynchronize(st));
+  return KIRA_OK;
+}
+
+namespace {
+
+// router::wfa_score_budget (src/alignment/router.rs:160-165) on the host.
+int64_t wfa_budget_host(int64_t read_len, int64_t pct, int64_t x, int64_t o, int64_t e) {
+  return std::max(read_len * pct / 100 * x, (o + e * 4) * 3);
+}
+
+constexpr uint64_t kWfaScratchBudget = 4ull << 30;  // per-call warp history, bytes
+
+}  // namespace
+
+int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_params* prm,
+                       const int32_t* max_score, const int32_t* text_begin_free,
+                       kira_wfa_result* out, kira_cigar_buf* cigar) {
+  if (!ctx || !pairs || !prm || !out) return KIRA_ERR_INVALID;
+  const bool tb = prm->traceback != 0;
+  if (tb && !cigar) return fail(ctx, KIRA_ERR_INVALID, "traceback needs a CIGAR buffer");
+  if (cigar) cigar->used = 0;
+  const kira_pairs& P = *pairs;
+  const uint32_t n = P.n;
+  if (n == 0) return KIRA_OK;
+  if (tb && cigar->cap && !cigar->ops) return KIRA_ERR_INVALID;
+  WfaLaunch L{};
+  L.n = n;
+  L.valid = 1;
+  const int64_t kCostMax = 1 << 20;
+  if (prm->scored) {
+    // WfaCosts::scored (wfa.rs:41-52): refused costs give None for every pair.
+    const int64_t a = prm->match_score, b = prm->mismatch, o = prm->gap_open, e = prm->gap_extend;
+    if (a <= 0 || b <= 0 || o < 0 || e <= 0) {
+      L.valid = 0;
+    } else {
+      if (a + b > kCostMax || o > kCostMax || a + e > kCostMax)
+        return fail(ctx, KIRA_ERR_INVALID, "WFA costs above 2^20");
+      L.x = (int32_t)(a + b), L.o = (int32_t)o, L.ei = (int32_t)(a + e), L.ed = (int32_t)e;
+    }
+  } else {
+    if (prm->mismatch < 1 || prm->gap_open < 0 || prm->gap_extend < 1)
+      return fail(ctx, KIRA_ERR_INVALID, "WFA penalties need mismatch >= 1, gap_open >= 0, "
+                  "gap_extend >= 1");
+    if (prm->mismatch > kCostMax || prm->gap_open > kCostMax || prm->gap_extend > kCostMax)
+      return fail(ctx, KIRA_ERR_INVALID, "WFA costs above 2^20");
+    L.x = prm->mismatch, L.o = prm->gap_open, L.ei = prm->gap_extend, L.ed = prm->gap_extend;
+  }
+  if (!L.valid) {
+    for (uint32_t i = 0; i < n; ++i) {
+      out[i] = kira_wfa_result{};
+      out[i].cost = -1;
+    }
+    return KIRA_OK;
+  }
+  L.lookback = std::max(L.x, std::max(L.o + L.ei, L.o + L.ed));
+  L.scored = prm->scored ? 1 : 0;
+  L.match = prm->match_score;
+  L.max_score = prm->max_score;
+  L.budget_pct = prm->budget_pct < 0 ? 25 : prm->budget_pct;
+  L.budget_x = L.x, L.budget_o = L.o, L.budget_e = L.ei;
+  L.tbf = prm->text_begin_free;
+  L.drop = prm->adaptive_drop < 0 ? -1 : prm->adaptive_drop;
+
+  // Batch bounds that size the per-warp history.
+  uint32_t m_max = 0, n_max = 0;
+  int64_t s_max = INT64_MIN, tbf_max = INT64_MIN;
+  for (uint32_t i = 0; i < n; ++i) {
+    m_max = std::max(m_max, P.read_len[i]);
+    n_max = std::max(n_max, P.win_len[i]);
+    if (max_score) s_max = std::max<int64_t>(s_max, max_score[i]);
+    if (text_begin_free) tbf_max = std::max<int64_t>(tbf_max, text_begin_free[i]);
+  }
+  if (m_max > (uint32_t)kWfaMaxLen || n_max > (uint32_t)kWfaMaxLen)
+    return fail(ctx, KIRA_ERR_READ_TOO_LONG, "WFA reads and windows up to %d bases", kWfaMaxLen);
+  if (!max_score)
+    s_max = prm->max_score >= 0 ? prm->max_score
+                                : wfa_budget_host(m_max, L.budget_pct, L.x, L.o, L.ei);
+  if (!text_begin_free) tbf_max = prm->text_begin_free;
+  tbf_max = std::min<int64_t>(std::max<int64_t>(tbf_max, 0), std::max<int64_t>(n_max - 1, 0));
+  const int64_t cost_cap = L.drop < 0 ? (int64_t)L.o + (int64_t)L.ei * m_max
+                                      : (int64_t)std::max(L.x, L.o + L.ei) * (2 * m_max + n_max + 2);
+  const int64_t S = std::max<int64_t>(0, std::min(s_max, cost_cap));
+  auto width = [&](int64_t s) {
+    return std::min<int64_t>(tbf_max + 1 + s / L.ei + s / L.ed, (int64_t)m_max + n_max + 3);
+  };
+  uint64_t hist = 0, meta_slots = 0, ring_width = 0;
+  if (tb) {
+    for (int64_t s = 0; s <= S; ++s) hist += 3ull * (uint64_t)width(s);
+    meta_slots = (uint64_t)S + 1;
+  } else {
+    meta_slots = (uint64_t)L.lookback + 1;
+    ring_width = (uint64_t)width(S);
+    hist = meta_slots * 3ull * ring_width;
+  }
+  if (hist >= (1ull << 31) || meta_slots >= (1ull << 26))
+    return fail(ctx, KIRA_ERR_OOM, "WFA history of %llu entries per pair: lower max_score",
+                (unsigned long long)hist);
+  const uint64_t meta_bytes = (meta_slots * 3ull * sizeof(int2) + 255) & ~255ull;
+  const uint64_t warp_bytes = meta_bytes + ((hist * 2ull + 255) & ~255ull);
+  L.meta_bytes = (uint32_t)meta_bytes;
+  L.meta_slots = (uint32_t)meta_slots;
+  L.hist_cap = (uint32_t)hist;
+  L.ring_width = (uint32_t)ring_width;
+  L.warp_bytes = warp_bytes;
+  L.pat_region = 32u + ((m_max + 15u) & ~15u);
+  L.smem_warp = L.pat_region + 32u + ((n_max + 15u) & ~15u);
+  const uint32_t min_cost = (uint32_t)(L.o + std::min(L.ei, L.ed));
+  L.slot_cap = (uint32_t)(2 * (S / min_cost) + 2);
+  L.max_score_pp = nullptr;
+  L.tbf_pp = nullptr;
+
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  ctx->ev_recorded = 0;
+  mark(ctx, 0, st);
+  DevPairs D;
+  int rc = upload_pairs(ctx, P, D);
+  if (rc) return rc;
+  cudaError_t cerr = cudaSuccess;
+  if (max_score) {
+    KIRA_DBUF(b, int32_t, B_WFA_MAXS, n);
+    KIRA_CUDA(cudaMemcpyAsync(b, max_score, 4ull * n, cudaMemcpyHostToDevice, st));
+    L.max_score_pp = b;
+  }
+  if (text_begin_free) {
+    KIRA_DBUF(b, int32_t, B_WFA_TBF, n);
+    KIRA_CUDA(cudaMemcpyAsync(b, text_begin_free, 4ull * n, cudaMemcpyHostToDevice, st));
+    L.tbf_pp = b;
+  }
+  // Launch shape: four warps per block while their staged bytes fit comfortably.
+  uint32_t wpb = 4;
+  while (wpb > 1 && (uint64_t)wpb * L.smem_warp > (160u << 10)) wpb >>= 1;
+  const size_t smem = (size_t)wpb * L.smem_warp;
+  int per_sm = 0;
+  KIRA_CUDA(wfa_blocks_per_sm(tb, smem, (int)(32 * wpb), &per_sm));
+  if (per_sm < 1) return fail(ctx, KIRA_ERR_INVALID, "WFA: %zu shared bytes per block", smem);
+  uint64_t blocks = std::min<uint64_t>((n + wpb - 1) / wpb, (uint64_t)ctx->sms * per_sm);
+  blocks = std::min<uint64_t>(blocks, std::max<uint64_t>(1, kWfaScratchBudget / (wpb * warp_bytes)));
+  KIRA_DBUF(scratch, uint8_t, B_WFA_SCRATCH, blocks * wpb * warp_bytes);
+  KIRA_DBUF(dout, kira_wfa_result, B_WFA_OUT, n);
+  KIRA_DBUF(work, uint32_t, B_WORK, 2);
+  L.scratch = scratch;
+  L.out = dout;
+  L.work = work;
+  L.flags = work + 1;
+  uint32_t* ncig = nullptr;
+  if (tb) {
+    KIRA_DBUF(nc, uint32_t, B_WFA_NCIG, n);
+    KIRA_DBUF(sl, uint32_t, B_WFA_SLOTS, (uint64_t)n * L.slot_cap);
+    ncig = nc;
+    L.ncig = nc;
+    L.slots = sl;
+  }
+  KIRA_CUDA(cudaMemsetAsync(work, 0, 8, st));
+  mark(ctx, 1, st);
+  KIRA_CUDA(launch_wfa(D, L, (uint32_t)blocks, wpb, tb, st));
+  mark(ctx, 2, st);
+  uint64_t total = 0;
+  uint32_t* ops = nullptr;
+  if (tb) {
+    KIRA_DBUF(off, uint32_t, B_CIG_OFF, n);
+    KIRA_DBUF(sums, uint32_t, B_CHUNK_SUMS, n / 4096 + 2);
+    KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
+    KIRA_DBUF(dops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
+    ops = dops;
+    KIRA_CUDA(launch_cigar_scan(ncig, n, off, sums, total_dev, st));
+    WfaCompact C{n, dout, ncig, off, L.slots, L.slot_cap, dops, cigar->cap};
+    KIRA_CUDA(launch_wfa_compact(C, ctx->sms, st));
+    KIRA_CUDA(cudaMemcpyAsync(&total, total_dev, 8, cudaMemcpyDeviceToHost, st));
+  }
+  mark(ctx, 3, st);
+  uint32_t flags = 0;
+  KIRA_CUDA(cudaMemcpyAsync(&flags, work + 1, 4, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_wfa_result) * n, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaStreamSynchronize(st));
+  if (flags & 2u) return fail(ctx, KIRA_ERR_RUNTIME, "WFA history above its computed bound");
+  if (flags & 1u) return fail(ctx, KIRA_ERR_RUNTIME, "WFA CIGAR above its computed bound");
+  if (!tb) {
+    mark(ctx, 4, st);
+    return KIRA_OK;
+  }
+  cigar->used = total;
+  if (total > cigar->cap)
+    return fail(ctx, KIRA_ERR_CAPACITY, "CIGAR buffer holds %llu ops, %llu needed",
+                (unsigned long long)cigar->cap, (unsigned long long)total);
+  if (total) KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * total, cudaMemcpyDeviceToHost, st));
+  mark(ctx, 4, st);
   KIRA_CUDA(cudaStreamSynchronize(st));
   return KIRA_OK;
 }

@@ -13,6 +13,7 @@ constexpr int32_t kAbortOff = INT32_MIN / 8;  // i32::MIN / 8: abort bound disab
 constexpr int kKeyIdxBits = 10;               // row argmax key: (h << 10) | (1023 - idx)
 constexpr int kMaxBand = 1023;                // 2*band+1 cells must fit the 10-bit index
 constexpr int kMaxRowLen = 2 * kMaxBand + 1;
+constexpr int kWfaMaxLen = 30000;             // WFA offsets and diagonals fit int16
 
 // Per-pair inputs in device memory (mirrors kira_pairs with device pointers).
 struct DevPairs {

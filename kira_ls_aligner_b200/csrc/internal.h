@@ -112,6 +112,46 @@ struct NmMdLaunch {
   uint32_t* flags;            // bit 0: a result's CIGAR range lies outside the ops
 };
 
+// WFA batch (wfa.cuh / wfa.cu): warp per pair over a per-warp history.
+struct WfaLaunch {
+  uint32_t n;
+  int32_t valid;               // 0: the scored costs were refused (every pair None)
+  int32_t x, o, ei, ed;        // WfaCosts (wfa.rs:22-52)
+  int32_t lookback;            // max(x, o + ei, o + ed)
+  int32_t scored, match;       // scored: score = read_len * match - cost
+  int32_t max_score;           // < 0 (and no per-pair array): router budget per read
+  int32_t budget_pct, budget_x, budget_o, budget_e;  // router::wfa_score_budget arguments
+  const int32_t* max_score_pp; // per pair (may be null)
+  int32_t tbf;                 // text_begin_free
+  const int32_t* tbf_pp;       // per pair (may be null)
+  int32_t drop;                // adaptive drop; < 0: exact
+  uint8_t* scratch;            // per warp: meta (int2 x 3 per score slot), then history
+  uint64_t warp_bytes;
+  uint32_t meta_bytes;
+  uint32_t meta_slots;         // scores held: every score (traceback) or the ring length
+  uint32_t hist_cap;           // traceback: int16 history entries per warp
+  uint32_t ring_width;         // score-only: entries per layer per ring slot; 0: traceback
+  uint32_t pat_region;         // shared bytes per warp before the text (pattern + guards)
+  uint32_t smem_warp;          // shared bytes per warp
+  uint32_t* work;              // dynamic pair counter
+  kira_wfa_result* out;
+  uint32_t* ncig;              // traceback: ops per pair
+  uint32_t* slots;             // traceback: slot_cap ops per pair, newest first
+  uint32_t slot_cap;
+  uint32_t* flags;             // bit 0: CIGAR slot overflow, bit 1: history overflow
+};
+
+struct WfaCompact {
+  uint32_t n;
+  kira_wfa_result* out;
+  const uint32_t* ncig;
+  const uint32_t* off;
+  const uint32_t* slots;
+  uint32_t slot_cap;
+  uint32_t* ops;
+  uint64_t cap;
+};
+
 // Banded-SW launch shape: G lanes per pair, K cells (int32) or K packed words of
 // two int16 cells (packed) per lane.
 struct BswShapeInfo {
@@ -172,6 +212,11 @@ cudaError_t launch_cigar_scan(const uint32_t* ncig, uint32_t n, uint32_t* off,
 cudaError_t launch_cigar_compact(const CompactLaunch& C, int sms, cudaStream_t st);
 cudaError_t launch_nm_md(const DevPairs& P, const NmMdLaunch& L, bool write, int sms,
                          cudaStream_t st);
+
+cudaError_t wfa_blocks_per_sm(bool traceback, size_t smem, int threads, int* per_sm);
+cudaError_t launch_wfa(const DevPairs& P, const WfaLaunch& L, uint32_t blocks,
+                       uint32_t warps_per_block, bool traceback, cudaStream_t st);
+cudaError_t launch_wfa_compact(const WfaCompact& C, int sms, cudaStream_t st);
 
 int ctx_share_reference(kira_ctx* dst, const kira_ctx* src);
 

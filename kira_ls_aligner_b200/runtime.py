@@ -113,6 +113,36 @@ class VerifyParams:
                               0 if self.qgram_filter else A.VERIFY_NO_QGRAM)
 
 
+@dataclass
+class WfaParams:
+    """WfaPenalties / AlignmentConfig and WfaOptions (src/alignment/wfa.rs:9-111).
+
+    scored=True selects WfaCosts::scored (wfa_align_scored / wfa_score_only_scored)
+    with match_score > 0; max_score < 0 uses router::wfa_score_budget per read
+    (budget_pct < 0: 25); adaptive_drop None is the exact search."""
+    mismatch: int = 4
+    gap_open: int = 6
+    gap_extend: int = 1
+    max_score: int = -1
+    adaptive_drop: int | None = None
+    text_begin_free: int = 0
+    traceback: bool = True
+    scored: bool = False
+    match_score: int = 0
+    budget_pct: int = -1
+
+    @classmethod
+    def scored_from(cls, cfg: "AlignmentConfig", **kw) -> "WfaParams":
+        return cls(cfg.mismatch, cfg.gap_open, cfg.gap_extend, scored=True,
+                   match_score=cfg.match_score, **kw)
+
+    def to_c(self) -> A.WfaParams:
+        return A.WfaParams(self.mismatch, self.gap_open, self.gap_extend, self.match_score,
+                           int(self.scored), self.max_score, self.budget_pct,
+                           -1 if self.adaptive_drop is None else self.adaptive_drop,
+                           self.text_begin_free, int(self.traceback))
+
+
 # --- pair batches --------------------------------------------------------------
 @dataclass
 class PairBatch:
@@ -353,6 +383,27 @@ class GpuContext:
         self.check(rc)
         text = md.tobytes()
         return nm[:n], [text[off[i]:off[i + 1]].decode() for i in range(n)]
+
+    # -- WFA
+    def wfa_batch(self, batch: PairBatch, params: WfaParams, max_score=None,
+                  text_begin_free=None, cigar_cap: int | None = None):
+        """kira_gpu_wfa_batch -> (results [WFA_RESULT_DTYPE], CIGAR ops). Optional
+        per-pair int32 arrays override params.max_score / params.text_begin_free."""
+        n = batch.n
+        res = np.zeros(max(n, 1), A.WFA_RESULT_DTYPE)
+        cap = cigar_cap if cigar_cap is not None else max(16, 4 * n)
+        ops = np.zeros(max(cap, 1), np.uint32)
+        cb = A.CigarBuf(A.ptr(ops), cap, 0)
+        ms = None if max_score is None else np.ascontiguousarray(max_score, np.int32)
+        tf = None if text_begin_free is None else np.ascontiguousarray(text_begin_free, np.int32)
+        pc = batch.to_c()
+        wp = params.to_c()
+        rc = self._lib.kira_gpu_wfa_batch(self._h, C.byref(pc), C.byref(wp), A.ptr(ms),
+                                          A.ptr(tf), A.ptr(res), C.byref(cb))
+        if rc == 9 and cigar_cap is None:
+            return self.wfa_batch(batch, params, max_score, text_begin_free, int(cb.used) + 16)
+        self.check(rc)
+        return res[:n], ops[: cb.used]
 
     # -- composed verification
     def verify_batch(self, batch: PairBatch, params: VerifyParams, detail: bool = False,

@@ -240,6 +240,34 @@ def gapfill(n_segments: int = 20_000, seed: int = 0x6A9F, seg_lo: int = 200, seg
                       ref)
 
 
+def wfa_cascade(n_pairs: int = 2_000_000, seed: int = 0x3FA0, read_len: int = 150,
+                band: int = 33, err_hi: float = 0.04, split=(4, 1, 1),
+                reference: np.ndarray | None = None, ref_len: int = 50_000_000) -> SwWorkload:
+    """Pairs of the WFA step of the cascade (try_fast_dp_alignment): a read of
+    read_len bases against the text at its seed-implied start, read_len + band bases
+    long (mod.rs:344-371: the window begins at the read's origin and carries band
+    bases of trailing slack). Errors U[0, err_hi] per read at subs:ins:del = 4:1:1,
+    the indel-bearing reads that reach WFA after the ungapped paths decline.
+    win_off are reference coordinates (a device-resident reference)."""
+    rng = np.random.default_rng(seed)
+    ref = reference if reference is not None else random_genome(rng, ref_len)
+    q = np.full(n_pairs, read_len, np.int64)
+    w = q + band
+    start = rng.integers(0, len(ref) - int(w.max()) - read_len - 64, n_pairs)
+    L = read_len + 48
+    reads = np.empty((n_pairs, read_len), np.uint8)
+    for a in range(0, n_pairs, 1 << 18):  # bounded temporaries
+        b = min(a + (1 << 18), n_pairs)
+        frag = ref[start[a:b, None] + np.arange(L)[None, :]]
+        reads[a:b] = _mutate_matrix(rng, frag, q[a:b], rng.uniform(0.0, err_hi, b - a),
+                                    split=split)[:, :read_len]
+    read_off = np.arange(n_pairs, dtype=np.uint64) * np.uint64(read_len)
+    return SwWorkload(f"wfa_{n_pairs}_{read_len}_pad{band}",
+                      np.concatenate([reads.reshape(-1), np.zeros(16, np.uint8)]), read_off,
+                      q.astype(np.uint32), None, start.astype(np.uint64), w.astype(np.uint32),
+                      np.zeros(n_pairs, np.int32), np.full(n_pairs, band, np.int32), ref)
+
+
 @dataclass
 class ServingPool:
     """Pools the serving requests are cut from, over one shared reference."""

@@ -1579,3 +1579,326 @@ extern "C" int orc_nm_md_batch(uint32_t n, const uint8_t* reads, const uint64_t*
   for (auto& t : th) t.join();
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// WFA (src/alignment/wfa.rs): wfa_align_with_costs (:549-648), step (:374-526),
+// extend_wavefront (:277-291), prune_wavefront (:293-346), check_done
+// (:348-358), build_cigar (:762-952). Same recurrence, same edge order.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int32_t kWfaNone = INT32_MIN / 4;
+
+struct Wf {
+  int32_t lo = 0, hi = -1;
+  std::vector<int32_t> off;
+  bool empty() const { return hi < lo; }
+  int32_t get(int32_t k) const { return (k < lo || k > hi) ? kWfaNone : off[(size_t)(k - lo)]; }
+};
+
+struct WfaCostsO {
+  int32_t x, o, ei, ed;
+};
+
+int32_t wfa_extend_diag(const uint8_t* p, int32_t m, const uint8_t* t, int32_t n, int32_t k,
+                        int32_t off) {
+  for (;;) {
+    const int32_t i = off, j = off + k;
+    if (i >= m || j < 0 || j >= n) break;
+    if (p[i] != t[j]) break;
+    ++off;
+  }
+  return off;
+}
+
+void wfa_extend(const uint8_t* p, int32_t m, const uint8_t* t, int32_t n, Wf& w) {
+  for (int32_t k = w.lo; k <= w.hi; ++k) {
+    int32_t& o = w.off[(size_t)(k - w.lo)];
+    if (o != kWfaNone) o = wfa_extend_diag(p, m, t, n, k, o);
+  }
+}
+
+void wfa_prune(Wf& w, int32_t drop) {
+  if (w.empty()) return;
+  int32_t max_ad = INT32_MIN;
+  for (int32_t k = w.lo; k <= w.hi; ++k) {
+    const int32_t o = w.off[(size_t)(k - w.lo)];
+    if (o != kWfaNone) max_ad = std::max(max_ad, 2 * o + k);
+  }
+  if (max_ad == INT32_MIN) return;
+  const int32_t th = max_ad - drop;
+  int32_t lo = w.lo;
+  while (lo <= w.hi) {
+    const int32_t o = w.off[(size_t)(lo - w.lo)];
+    if (o != kWfaNone && 2 * o + lo >= th) break;
+    ++lo;
+  }
+  int32_t hi = w.hi;
+  while (hi >= lo) {
+    const int32_t o = w.off[(size_t)(hi - w.lo)];
+    if (o != kWfaNone && 2 * o + hi >= th) break;
+    --hi;
+  }
+  if (lo > hi) {
+    w = Wf();
+    return;
+  }
+  std::vector<int32_t> nv((size_t)(hi - lo + 1));
+  for (int32_t k = lo; k <= hi; ++k) {
+    int32_t o = w.off[(size_t)(k - w.lo)];
+    if (o != kWfaNone && 2 * o + k < th) o = kWfaNone;
+    nv[(size_t)(k - lo)] = o;
+  }
+  w.lo = lo;
+  w.hi = hi;
+  w.off.swap(nv);
+}
+
+bool wfa_done(const Wf& w, int32_t m, int32_t* k_end) {
+  for (int32_t k = w.lo; k <= w.hi; ++k)
+    if (w.off[(size_t)(k - w.lo)] >= m) {
+      *k_end = k;
+      return true;
+    }
+  return false;
+}
+
+const Wf* wfa_src(const std::vector<Wf>& h, int32_t s) {
+  if (s < 0 || (size_t)s >= h.size() || h[(size_t)s].empty()) return nullptr;
+  return &h[(size_t)s];
+}
+
+void wfa_step(int32_t s, const WfaCostsO& c, const std::vector<Wf>& M, const std::vector<Wf>& I,
+              const std::vector<Wf>& D, int32_t m, int32_t n, Wf& nm, Wf& ni, Wf& nd) {
+  const Wf* mx = wfa_src(M, s - c.x);
+  const Wf* moi = wfa_src(M, s - c.o - c.ei);
+  const Wf* mod = wfa_src(M, s - c.o - c.ed);
+  const Wf* ie = wfa_src(I, s - c.ei);
+  const Wf* de = wfa_src(D, s - c.ed);
+  int32_t ilo = INT32_MAX, ihi = INT32_MIN, dlo = INT32_MAX, dhi = INT32_MIN;
+  if (moi) ilo = std::min(ilo, moi->lo - 1), ihi = std::max(ihi, moi->hi - 1);
+  if (ie) ilo = std::min(ilo, ie->lo - 1), ihi = std::max(ihi, ie->hi - 1);
+  if (mod) dlo = std::min(dlo, mod->lo + 1), dhi = std::max(dhi, mod->hi + 1);
+  if (de) dlo = std::min(dlo, de->lo + 1), dhi = std::max(dhi, de->hi + 1);
+  int32_t mlo = INT32_MAX, mhi = INT32_MIN;
+  if (mx) mlo = std::min(mlo, mx->lo), mhi = std::max(mhi, mx->hi);
+  if (ilo <= ihi) mlo = std::min(mlo, ilo), mhi = std::max(mhi, ihi);
+  if (dlo <= dhi) mlo = std::min(mlo, dlo), mhi = std::max(mhi, dhi);
+  ni = Wf();
+  if (ilo <= ihi) {
+    ni.lo = ilo, ni.hi = ihi, ni.off.assign((size_t)(ihi - ilo + 1), kWfaNone);
+    for (int32_t k = ilo; k <= ihi; ++k) {
+      int32_t b = kWfaNone;
+      if (moi) {
+        const int32_t v = moi->get(k + 1);
+        if (v != kWfaNone && v < m) b = std::max(b, v + 1);
+      }
+      if (ie) {
+        const int32_t v = ie->get(k + 1);
+        if (v != kWfaNone && v < m) b = std::max(b, v + 1);
+      }
+      ni.off[(size_t)(k - ilo)] = b;
+    }
+  }
+  nd = Wf();
+  if (dlo <= dhi) {
+    nd.lo = dlo, nd.hi = dhi, nd.off.assign((size_t)(dhi - dlo + 1), kWfaNone);
+    for (int32_t k = dlo; k <= dhi; ++k) {
+      int32_t b = kWfaNone;
+      if (mod) {
+        const int32_t v = mod->get(k - 1);
+        if (v != kWfaNone && v + k <= n) b = std::max(b, v);
+      }
+      if (de) {
+        const int32_t v = de->get(k - 1);
+        if (v != kWfaNone && v + k <= n) b = std::max(b, v);
+      }
+      nd.off[(size_t)(k - dlo)] = b;
+    }
+  }
+  nm = Wf();
+  if (mlo <= mhi) {
+    nm.lo = mlo, nm.hi = mhi, nm.off.assign((size_t)(mhi - mlo + 1), kWfaNone);
+    for (int32_t k = mlo; k <= mhi; ++k) {
+      int32_t b = kWfaNone;
+      if (mx) {
+        const int32_t v = mx->get(k);
+        if (v != kWfaNone && v < m && v + k < n) b = std::max(b, v + 1);
+      }
+      const int32_t vi = ni.get(k);
+      if (vi != kWfaNone) b = std::max(b, vi);
+      const int32_t vd = nd.get(k);
+      if (vd != kWfaNone) b = std::max(b, vd);
+      nm.off[(size_t)(k - mlo)] = b;
+    }
+  }
+}
+
+struct CigarRev {  // push_cigar (wfa.rs:954-962) on the reversed op list
+  std::vector<uint32_t> ops;
+  void push(uint32_t op, uint32_t len) {
+    if (!ops.empty() && (ops.back() & 15u) == op) {
+      ops.back() += len << 4;
+      return;
+    }
+    ops.push_back((len << 4) | op);
+  }
+};
+
+int32_t wfa_traceback(const uint8_t* p, int32_t m, const uint8_t* t, int32_t n,
+                      const std::vector<Wf>& M, const std::vector<Wf>& I,
+                      const std::vector<Wf>& D, int32_t s, int32_t k, const WfaCostsO& c,
+                      CigarRev& cr) {
+  int32_t off = m;
+  int layer = 0;  // 0 M, 1 I, 2 D
+  auto get = [&](int L, int32_t sc, int32_t kk) -> int32_t {
+    const std::vector<Wf>& h = L == 0 ? M : (L == 1 ? I : D);
+    if (sc < 0 || (size_t)sc >= h.size()) return kWfaNone;
+    const Wf& w = h[(size_t)sc];
+    return w.empty() ? kWfaNone : w.get(kk);
+  };
+  while (!(s == 0 && layer == 0 && off == 0)) {
+    if (layer == 0) {
+      int32_t walk = off;
+      while (walk != 0) {
+        if (get(1, s, k) == walk) break;
+        if (get(2, s, k) == walk) break;
+        if (s >= c.x) {
+          const int32_t prev = get(0, s - c.x, k);
+          if (prev != kWfaNone && prev + 1 == walk) break;
+        }
+        const int32_t i = walk - 1, j = walk - 1 + k;
+        if (i < 0 || j < 0 || i >= m || j >= n) break;
+        if (p[i] != t[j]) break;
+        --walk;
+      }
+      if (off - walk > 0) cr.push(0, (uint32_t)(off - walk));
+      off = walk;
+      if (s == 0 && off == 0) break;
+      bool took = false;
+      if (s >= c.x) {
+        const int32_t prev = get(0, s - c.x, k);
+        if (prev != kWfaNone && prev + 1 == off) {
+          cr.push(0, 1);
+          off -= 1;
+          s -= c.x;
+          took = true;
+        }
+      }
+      if (!took && get(1, s, k) == off) layer = 1, took = true;
+      if (!took && get(2, s, k) == off) layer = 2, took = true;
+      if (!took) break;
+    } else if (layer == 1) {
+      bool took = false;
+      if (s >= c.o + c.ei) {
+        const int32_t prev = get(0, s - c.o - c.ei, k + 1);
+        if (prev != kWfaNone && prev + 1 == off) {
+          cr.push(1, 1);
+          off -= 1, k += 1, s -= c.o + c.ei, layer = 0, took = true;
+        }
+      }
+      if (!took && s >= c.ei) {
+        const int32_t prev = get(1, s - c.ei, k + 1);
+        if (prev != kWfaNone && prev + 1 == off) {
+          cr.push(1, 1);
+          off -= 1, k += 1, s -= c.ei, took = true;
+        }
+      }
+      if (!took) break;
+    } else {
+      bool took = false;
+      if (s >= c.o + c.ed) {
+        const int32_t prev = get(0, s - c.o - c.ed, k - 1);
+        if (prev != kWfaNone && prev == off) {
+          cr.push(2, 1);
+          k -= 1, s -= c.o + c.ed, layer = 0, took = true;
+        }
+      }
+      if (!took && s >= c.ed) {
+        const int32_t prev = get(2, s - c.ed, k - 1);
+        if (prev != kWfaNone && prev == off) {
+          cr.push(2, 1);
+          k -= 1, s -= c.ed, took = true;
+        }
+      }
+      if (!took) break;
+    }
+  }
+  return k;
+}
+
+}  // namespace
+
+extern "C" int orc_wfa(const uint8_t* pattern, size_t m_, const uint8_t* text, size_t n_,
+                       const orc_wfa_cfg* cfg, int32_t* score, uint32_t* text_start,
+                       uint32_t* text_end, uint32_t* cigar, uint32_t cap, uint32_t* n_cigar) {
+  const int32_t m = (int32_t)m_, n = (int32_t)n_;
+  *n_cigar = 0;
+  WfaCostsO c;
+  if (cfg->scored) {  // WfaCosts::scored (wfa.rs:41-52)
+    if (cfg->match_score <= 0 || cfg->mismatch <= 0 || cfg->gap_open < 0 || cfg->gap_extend <= 0)
+      return -1;
+    c = {cfg->match_score + cfg->mismatch, cfg->gap_open, cfg->match_score + cfg->gap_extend,
+         cfg->gap_extend};
+  } else {
+    c = {cfg->mismatch, cfg->gap_open, cfg->gap_extend, cfg->gap_extend};
+  }
+  if (m == 0) {
+    *score = 0, *text_start = 0, *text_end = 0;
+    return 1;
+  }
+  const int32_t tbf = std::min(std::max(cfg->text_begin_free, 0), std::max(n - 1, 0));
+  std::vector<Wf> M, I, D;
+  Wf m0;
+  m0.lo = 0, m0.hi = tbf, m0.off.assign((size_t)(tbf + 1), 0);
+  wfa_extend(pattern, m, text, n, m0);
+  if (cfg->adaptive_drop >= 0) wfa_prune(m0, cfg->adaptive_drop);
+  int32_t k_end = 0, s_end = -1;
+  M.push_back(m0), I.push_back(Wf()), D.push_back(Wf());
+  if (wfa_done(M[0], m, &k_end)) s_end = 0;
+  for (int32_t s = 1; s_end < 0 && s <= cfg->max_score; ++s) {
+    Wf nm, ni, nd;
+    wfa_step(s, c, M, I, D, m, n, nm, ni, nd);
+    wfa_extend(pattern, m, text, n, nm);
+    if (cfg->adaptive_drop >= 0) wfa_prune(nm, cfg->adaptive_drop);
+    M.push_back(nm), I.push_back(ni), D.push_back(nd);
+    if (wfa_done(M[(size_t)s], m, &k_end)) s_end = s;
+  }
+  if (s_end < 0) return 0;
+  *score = s_end;
+  *text_end = (uint32_t)(m + k_end);
+  *text_start = 0;
+  if (cfg->traceback) {
+    CigarRev cr;
+    const int32_t k0 = wfa_traceback(pattern, m, text, n, M, I, D, s_end, k_end, c, cr);
+    *text_start = (uint32_t)std::max(k0, 0);
+    const uint32_t nc = (uint32_t)cr.ops.size();
+    for (uint32_t t = 0; t < nc && t < cap; ++t) cigar[t] = cr.ops[nc - 1 - t];
+    *n_cigar = nc;
+  }
+  return 1;
+}
+
+extern "C" int orc_wfa_batch(uint32_t n, const uint8_t* reads, const uint64_t* read_off,
+                             const uint32_t* read_len, const uint8_t* wins,
+                             const uint64_t* win_off, const uint32_t* win_len,
+                             const orc_wfa_cfg* c, int nthreads, int32_t* found, int32_t* score,
+                             uint32_t* text_start, uint32_t* text_end, uint32_t* n_cigar,
+                             uint32_t* cigar, uint32_t cap_per_pair) {
+  std::atomic<uint32_t> next{0};
+  auto work = [&]() {
+    for (;;) {
+      const uint32_t i = next.fetch_add(16);
+      if (i >= n) return;
+      for (uint32_t p = i; p < std::min(n, i + 16); ++p)
+        found[p] = orc_wfa(reads + read_off[p], read_len[p], wins + win_off[p], win_len[p], c,
+                           score + p, text_start + p, text_end + p,
+                           cigar + (size_t)p * cap_per_pair, cap_per_pair, n_cigar + p);
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < std::max(nthreads, 1); ++t) th.emplace_back(work);
+  work();
+  for (auto& t : th) t.join();
+  return 0;
+}

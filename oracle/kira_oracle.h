@@ -180,6 +180,26 @@ int orc_nm_md_batch(uint32_t n, const uint8_t* reads, const uint64_t* read_off,
                     const uint32_t* cig_off, const uint32_t* n_cig, const uint32_t* ops,
                     int nthreads, uint32_t* nm, uint32_t* md_len, char* md, uint32_t md_stride);
 
+/* Wavefront alignment (src/alignment/wfa.rs): affine-gap, the whole pattern
+ * against a text prefix (ends-free leading text up to text_begin_free, free
+ * trailing text). Costs: plain (WfaPenalties: ins = del = gap_extend) or scored
+ * (WfaCosts::scored, wfa.rs:41-52: mismatch = a + b, ins_extend = a + e,
+ * del_extend = e). adaptive_drop < 0: exact. Returns 1 with the cost (score),
+ * text span and CIGAR (len << 4 | op, 5'->3') when an alignment of cost <=
+ * max_score exists, else 0. traceback = 0 leaves the CIGAR empty (wfa_score_only). */
+typedef struct orc_wfa_cfg {
+  int32_t mismatch, gap_open, gap_extend, match_score, scored;
+  int32_t max_score, adaptive_drop, text_begin_free, traceback;
+} orc_wfa_cfg;
+int orc_wfa(const uint8_t* pattern, size_t m, const uint8_t* text, size_t n, const orc_wfa_cfg* c,
+            int32_t* score, uint32_t* text_start, uint32_t* text_end, uint32_t* cigar,
+            uint32_t cap, uint32_t* n_cigar);
+int orc_wfa_batch(uint32_t n, const uint8_t* reads, const uint64_t* read_off,
+                  const uint32_t* read_len, const uint8_t* wins, const uint64_t* win_off,
+                  const uint32_t* win_len, const orc_wfa_cfg* c, int nthreads, int32_t* found,
+                  int32_t* score, uint32_t* text_start, uint32_t* text_end, uint32_t* n_cigar,
+                  uint32_t* cigar, uint32_t cap_per_pair);
+
 #ifdef __cplusplus
 }
 #endif

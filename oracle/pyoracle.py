@@ -50,6 +50,12 @@ class OrcVerifyResult(C.Structure):
                 ("sw", OrcSwResult)]
 
 
+class OrcWfaCfg(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in
+                ("mismatch", "gap_open", "gap_extend", "match_score", "scored", "max_score",
+                 "adaptive_drop", "text_begin_free", "traceback")]
+
+
 def build() -> None:
     subprocess.check_call(["make", "-s", "-C", _HERE, "all"])
 
@@ -130,6 +136,10 @@ def lib():
         L.orc_myers_batch.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, vp, C.c_uint32, C.c_int,
                                       vp, vp]
         L.orc_sieve_batch.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, vp, C.c_int, vp, vp, vp]
+        L.orc_wfa.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t,
+                              C.POINTER(OrcWfaCfg), vp, vp, vp, vp, C.c_uint32, vp]
+        L.orc_wfa_batch.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, vp, C.POINTER(OrcWfaCfg),
+                                    C.c_int, vp, vp, vp, vp, vp, vp, C.c_uint32]
         _lib = L
     return _lib
 
@@ -451,3 +461,73 @@ def nm_md_batch(reads, read_off, read_len, wins, win_off, win_len, read_start, r
                           _p(win_len), _p(read_start), _p(ref_start), _p(cig_off), _p(n_cig),
                           _p(ops), nthreads, _p(nm), _p(md_len), _p(md), md_stride)
     return nm, md_len, md.reshape(n, md_stride)
+
+
+# ---------------------------------------------------------------------------
+# WFA (src/alignment/wfa.rs)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class WfaRes:
+    score: int        # WFA cost (the loss for the scored cost model)
+    cigar: list       # [(len, op_char)]; empty for score-only
+    text_start: int
+    text_end: int
+
+    def cigar_str(self) -> str:
+        return "".join(f"{n}{c}" for n, c in self.cigar)
+
+
+def wfa_cfg(mismatch=4, gap_open=6, gap_extend=1, max_score=100, adaptive_drop=None,
+            text_begin_free=0, match_score=0, scored=False, traceback=True) -> OrcWfaCfg:
+    return OrcWfaCfg(mismatch, gap_open, gap_extend, match_score, int(scored), max_score,
+                     -1 if adaptive_drop is None else adaptive_drop, text_begin_free,
+                     int(traceback))
+
+
+def wfa(pattern: bytes, text: bytes, c: OrcWfaCfg):
+    """wfa_align / wfa_score_only and their scored forms (wfa.rs:549-745) -> None | WfaRes."""
+    cap = 2 * len(pattern) + len(text) + 8
+    cig = (C.c_uint32 * cap)()
+    sc, ts, te, nc = C.c_int32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+    rc = lib().orc_wfa(pattern, len(pattern), text, len(text), C.byref(c), C.byref(sc),
+                       C.byref(ts), C.byref(te), cig, cap, C.byref(nc))
+    if rc < 0:
+        raise ValueError("invalid WFA costs")
+    if rc == 0:
+        return None
+    return WfaRes(sc.value, decode_cigar(cig[: nc.value]), ts.value, te.value)
+
+
+def wfa_scored(pattern: bytes, text: bytes, a: int, b: int, o: int, e: int, max_score: int,
+               adaptive_drop=None, text_begin_free=0, traceback=True):
+    """wfa_align_scored (wfa.rs:57-65); with traceback=False the value of
+    wfa_score_only_scored (wfa.rs:69-79): the affine score m*a - loss."""
+    r = wfa(pattern, text, wfa_cfg(b, o, e, max_score, adaptive_drop, text_begin_free, a, True,
+                                   traceback))
+    if r is None or traceback:
+        return r
+    return len(pattern) * a - r.score
+
+
+def wfa_batch(reads: np.ndarray, read_off, read_len, wins: np.ndarray, win_off, win_len,
+              c: OrcWfaCfg, threads: int = 0, cap_per_pair: int = 64):
+    """Per-pair orc_wfa on host threads -> (found, score, text_start, text_end, n_cigar, cigar)."""
+    n = len(read_len)
+    ro = np.ascontiguousarray(read_off, np.uint64)
+    rl = np.ascontiguousarray(read_len, np.uint32)
+    wo = np.ascontiguousarray(win_off, np.uint64)
+    wl = np.ascontiguousarray(win_len, np.uint32)
+    rs = np.ascontiguousarray(reads, np.uint8)
+    ws = np.ascontiguousarray(wins, np.uint8)
+    found = np.zeros(n, np.int32)
+    score = np.zeros(n, np.int32)
+    ts = np.zeros(n, np.uint32)
+    te = np.zeros(n, np.uint32)
+    nc = np.zeros(n, np.uint32)
+    cig = np.zeros((n, cap_per_pair), np.uint32)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    lib().orc_wfa_batch(n, p(rs), p(ro), p(rl), p(ws), p(wo), p(wl), C.byref(c),
+                        threads or os.cpu_count() or 1, p(found), p(score), p(ts), p(te),
+                        p(nc), p(cig), cap_per_pair)
+    return found, score, ts, te, nc, cig
