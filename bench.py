@@ -46,16 +46,23 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--shape", type=int, default=-1,
                     help="install this banded-SW launch shape instead of autotuning")
-    ap.add_argument("--workload", choices=["batched", "uneven", "serving", "gapfill", "nmmd"],
+    ap.add_argument("--workload", choices=["batched", "uneven", "serving", "gapfill", "nmmd",
+                                           "wfa"],
                     default="batched",
                     help="batched: the headline 2M-pair verification; uneven: 500k banded-SW "
                          "pairs of mixed length and band (bucketed vs one-launch path); "
                          "serving: Poisson request stream through the server vs one request "
-                         "per call; gapfill: long-read gap-fill segments at band 256")
+                         "per call; gapfill: long-read gap-fill segments at band 256; nmmd: "
+                         "NM + MD:Z of the batched alignments; wfa: the cascade's WFA step "
+                         "(scored costs, router budget) with and without traceback")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=5.0, help="serving: seconds of arrivals")
     ap.add_argument("--slots", type=int, default=4, help="serving: concurrent batches")
     ap.add_argument("--segments", type=int, default=20_000, help="gapfill: segments per call")
+    ap.add_argument("--wfa-pairs", type=int, default=1_000_000, help="wfa: pairs per call")
+    ap.add_argument("--wfa-drop", type=int, default=-1, help="wfa: adaptive drop (< 0 exact)")
+    ap.add_argument("--wfa-lanes", type=int, default=0,
+                    help="wfa: lanes per pair (8, 16, 32; 0 = library default)")
     return ap.parse_args()
 
 
@@ -306,6 +313,96 @@ def run_nmmd(args, rank, local, world):
     ctx.close()
 
 
+def run_wfa(args, rank, local, world):
+    """The cascade's WFA step (try_fast_dp_alignment, mod.rs:344-439): 150 bp reads
+    against read + 33 bp of text at the seed-implied start over a resident
+    reference, scored costs +1/-4/-6/-1, router budget (25 % of the read x 5),
+    exact search. Both wfa_align_scored (traceback + CIGAR) and
+    wfa_score_only_scored (locus_alignment_score) through the host API with
+    pinned inputs (H2D + D2H inside the timed region); `value` is the traceback
+    form, the kernel time from the library's stage events."""
+    import torch
+
+    from kira_ls_aligner_b200 import AlignmentConfig, GpuContext, PairBatch, WfaParams, _abi, synth
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    w = synth.wfa_cascade(args.wfa_pairs)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    b = PairBatch(pin(w.reads), pin(w.read_off), pin(w.read_len), None, pin(w.win_off),
+                  pin(w.win_len))
+    ctx = GpuContext(local)
+    ctx.ref_upload(w.reference)
+    L = _abi.lib()
+    ctx.check(L.kira_gpu_set_wfa_lanes(ctx.handle, args.wfa_lanes))
+    n = w.n_pairs
+    drop = None if args.wfa_drop < 0 else args.wfa_drop
+    out = {}
+    for mode, tb in (("traceback", True), ("score_only", False)):
+        p = WfaParams.scored_from(AlignmentConfig(), adaptive_drop=drop, traceback=tb)
+        res = np.zeros(n, _abi.WFA_RESULT_DTYPE)
+        ops = pin(np.zeros(8 * n, np.uint32))
+        cb = _abi.CigarBuf(_abi.ptr(ops), len(ops), 0)
+        pc, wp = b.to_c(), p.to_c()
+
+        def call():  # the C entry point on preallocated host buffers
+            ctx.check(L.kira_gpu_wfa_batch(ctx.handle, C.byref(pc), C.byref(wp), None, None,
+                                           _abi.ptr(res), C.byref(cb)))
+        for _ in range(args.warmup):
+            call()
+        ts = [_timed(call) for _ in range(args.steps)]
+        ctx.check(L.kira_gpu_profile(ctx.handle, 1))
+        kern = []
+        for _ in range(3):
+            call()
+            buf = (C.c_float * 8)()
+            k = L.kira_gpu_stage_times(ctx.handle, buf, 8)
+            kern.append([float(x) for x in buf[:k]])
+        ctx.check(L.kira_gpu_profile(ctx.handle, 0))
+        ms = sum(ts) / len(ts)
+        kms = statistics.median(s[1] for s in kern)
+        cost = res["cost"][res["found"] == 1].astype(np.float64)
+        out[mode] = {"e2e_pairs_per_s": n / (ms / 1e3), "ms_per_call": ms,
+                     "kernel_ms": kms, "kernel_pairs_per_s": n / (kms / 1e3),
+                     "stage_ms": dict(zip(("upload", "wavefronts", "cigar_compact", "download"),
+                                          [round(x, 3) for x in kern[-1]])),
+                     "found": int(res["found"].sum()), "mean_cost": float(cost.mean()),
+                     "cigar_ops": int(cb.used),
+                     "checksum": int(res["cost"].astype(np.int64).sum())}
+    assert out["traceback"]["checksum"] == out["score_only"]["checksum"]
+    cpu = None
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as O
+        nthreads = os.cpu_count() or 1
+        m = min(n, 200_000)
+        c = O.wfa_cfg(4, 6, 1, 185, drop, 0, 1, True, True)
+        wins = w.reference
+        t = time.perf_counter()
+        O.wfa_batch(w.reads, w.read_off[:m], w.read_len[:m], wins, w.win_off[:m], w.win_len[:m],
+                    c, nthreads, 64)
+        el = time.perf_counter() - t
+        cpu = {"value": m / el, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": f"first {m} pairs of the workload, traceback form"}
+    tb = out["traceback"]
+    h2d = int(w.read_len.sum()) + n * (8 + 4 + 8 + 4)
+    print(json.dumps({
+        "metric": "pairs/s (WFA step of the cascade: scored wfa_align with CIGAR, bit-exact)",
+        "value": tb["kernel_pairs_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tb["kernel_ms"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int16/int32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": w.name, "pairs": n, "read_len": 150, "text_len": 183,
+                   "costs": "scored 1/4/6/1", "max_score": "router budget (185)",
+                   "adaptive_drop": drop, "errors": "U[0,4%] 4:1:1",
+                   "lanes_per_pair": args.wfa_lanes or "default",
+                   "path": "resident reference, host API, pinned inputs"},
+        "e2e": {"value": tb["e2e_pairs_per_s"], "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 32 * n + 4 * tb["cigar_ops"]},
+        "modes": out, "cpu_baseline": cpu}))
+    ctx.close()
+
+
 def _slice_short(w, r0, nreads, cands=4):
     """PairBatch of reads [r0, r0 + nreads) of a short-read pool (compact read arena;
     windows stay reference coordinates)."""
@@ -539,6 +636,8 @@ def main():
             run_gapfill(args, rank, local, world)
         elif args.workload == "nmmd":
             run_nmmd(args, rank, local, world)
+        elif args.workload == "wfa":
+            run_wfa(args, rank, local, world)
         elif args.impl == "reference":
             run_reference(args, rank, world)
         else:

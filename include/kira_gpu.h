@@ -410,6 +410,11 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
                        const int32_t* max_score, const int32_t* text_begin_free,
                        kira_wfa_result* out, kira_cigar_buf* cigar);
 
+/* Lanes that align one WFA pair: 8, 16 or 32 (32 / lanes pairs share a warp and
+ * step in lockstep); 0 (default) picks 8 for reads up to 512 bases, else 32.
+ * Results are identical for every choice. */
+int kira_gpu_set_wfa_lanes(kira_ctx* ctx, int lanes);
+
 /* ------------------------------------------------ serving (continuous batching)
  *
  * No counterpart in the reference, whose dispatcher thread runs one blocking

@@ -37,6 +37,7 @@ EXPORTS = (
     "kira_gpu_bsw_shapes", "kira_gpu_set_bsw_shape", "kira_gpu_bsw_batch_noalloc",
     "kira_gpu_align_batch_simd", "kira_gpu_set_plain", "kira_gpu_set_trace_budget",
     "kira_gpu_set_graphs", "kira_gpu_set_chunk_pairs", "kira_gpu_nm_md", "kira_gpu_wfa_batch",
+    "kira_gpu_set_wfa_lanes",
     "kira_server_create", "kira_server_destroy", "kira_server_ref_upload",
     "kira_server_submit_verify", "kira_server_submit_bsw", "kira_server_poll",
     "kira_server_wait", "kira_server_info", "kira_server_release", "kira_server_stats",
@@ -154,6 +155,7 @@ def lib():
                                  C.c_uint64, C.POINTER(C.c_uint64)]
     L.kira_gpu_wfa_batch.argtypes = [vp, C.POINTER(Pairs), C.POINTER(WfaParams), vp, vp, vp,
                                      C.POINTER(CigarBuf)]
+    L.kira_gpu_set_wfa_lanes.argtypes = [vp, C.c_int]
     L.kira_gpu_align_batch_simd.argtypes = [vp, C.POINTER(Pairs), C.POINTER(SwCfg), C.c_int,
                                             C.c_int, vp, C.POINTER(CigarBuf)]
     L.kira_gpu_bsw_batch_noalloc.argtypes = [C.POINTER(Pairs), C.POINTER(SwCfg), vp, vp,

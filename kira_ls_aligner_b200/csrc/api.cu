@@ -54,6 +54,7 @@ struct kira_ctx {
   uint64_t graph_replays = 0, graph_captures = 0;
   cudaStream_t h2d = nullptr, d2h = nullptr;   // copy streams of the chunked host path
   int64_t chunk_pairs = -1;                    // chunked host path: -1 auto, 0 off, else pairs
+  int wfa_lanes = 0;                           // WFA lanes per pair: 0 auto, else 8 / 16 / 32
   std::vector<cudaEvent_t> ev_up, ev_comp;     // per chunk: inputs landed / results ready
   int sms = 148;
   cudaStream_t stream = nullptr;
@@ -1163,27 +1164,37 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
   auto width = [&](int64_t s) {
     return std::min<int64_t>(tbf_max + 1 + s / L.ei + s / L.ed, (int64_t)m_max + n_max + 3);
   };
+  // Lanes per pair: short reads keep their fronts narrow, so several pairs share a
+  // warp; long reads take a warp each.
+  L.group = ctx->wfa_lanes ? ctx->wfa_lanes : (m_max <= 512 ? 8 : 32);
+  const uint64_t R = (uint64_t)L.lookback + 1;
   uint64_t hist = 0, meta_slots = 0, ring_width = 0;
   if (tb) {
     for (int64_t s = 0; s <= S; ++s) hist += 3ull * (uint64_t)width(s);
     meta_slots = (uint64_t)S + 1;
   } else {
-    meta_slots = (uint64_t)L.lookback + 1;
     ring_width = (uint64_t)width(S);
-    hist = meta_slots * 3ull * ring_width;
+    hist = R * 3ull * ring_width;
   }
-  if (hist >= (1ull << 31) || meta_slots >= (1ull << 26))
+  if (hist >= (1ull << 31) || meta_slots >= (1ull << 26) || R > (1u << 20))
     return fail(ctx, KIRA_ERR_OOM, "WFA history of %llu entries per pair: lower max_score",
                 (unsigned long long)hist);
+  const uint64_t ring_sz = (R * 3ull * sizeof(int2) + 15) & ~15ull;
+  const bool ring_shared = ring_sz <= 512;
   const uint64_t meta_bytes = (meta_slots * 3ull * sizeof(int2) + 255) & ~255ull;
-  const uint64_t warp_bytes = meta_bytes + ((hist * 2ull + 255) & ~255ull);
-  L.meta_bytes = (uint32_t)meta_bytes;
+  const uint64_t ring_goff = meta_bytes;
+  const uint64_t hist_off = ring_goff + (ring_shared ? 0 : ((ring_sz + 255) & ~255ull));
+  const uint64_t group_bytes = hist_off + ((hist * 2ull + 255) & ~255ull);
   L.meta_slots = (uint32_t)meta_slots;
   L.hist_cap = (uint32_t)hist;
+  L.ring_len = (uint32_t)R;
   L.ring_width = (uint32_t)ring_width;
-  L.warp_bytes = warp_bytes;
+  L.ring_bytes = ring_shared ? (uint32_t)ring_sz : 0u;
+  L.ring_goff = (uint32_t)ring_goff;
+  L.hist_off = (uint32_t)hist_off;
+  L.group_bytes = group_bytes;
   L.pat_region = 32u + ((m_max + 15u) & ~15u);
-  L.smem_warp = L.pat_region + 32u + ((n_max + 15u) & ~15u);
+  L.smem_group = L.ring_bytes + L.pat_region + 32u + ((n_max + 15u) & ~15u);
   const uint32_t min_cost = (uint32_t)(L.o + std::min(L.ei, L.ed));
   L.slot_cap = (uint32_t)(2 * (S / min_cost) + 2);
   L.max_score_pp = nullptr;
@@ -1208,15 +1219,18 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
     L.tbf_pp = b;
   }
   // Launch shape: four warps per block while their staged bytes fit comfortably.
+  const uint32_t groups_per_warp = 32u / (uint32_t)L.group;
   uint32_t wpb = 4;
-  while (wpb > 1 && (uint64_t)wpb * L.smem_warp > (160u << 10)) wpb >>= 1;
-  const size_t smem = (size_t)wpb * L.smem_warp;
+  while (wpb > 1 && (uint64_t)wpb * groups_per_warp * L.smem_group > (160u << 10)) wpb >>= 1;
+  const uint32_t gpb = wpb * groups_per_warp;
+  const size_t smem = (size_t)gpb * L.smem_group;
   int per_sm = 0;
-  KIRA_CUDA(wfa_blocks_per_sm(tb, smem, (int)(32 * wpb), &per_sm));
+  KIRA_CUDA(wfa_blocks_per_sm(L.group, tb, smem, (int)(32 * wpb), &per_sm));
   if (per_sm < 1) return fail(ctx, KIRA_ERR_INVALID, "WFA: %zu shared bytes per block", smem);
-  uint64_t blocks = std::min<uint64_t>((n + wpb - 1) / wpb, (uint64_t)ctx->sms * per_sm);
-  blocks = std::min<uint64_t>(blocks, std::max<uint64_t>(1, kWfaScratchBudget / (wpb * warp_bytes)));
-  KIRA_DBUF(scratch, uint8_t, B_WFA_SCRATCH, blocks * wpb * warp_bytes);
+  uint64_t blocks = std::min<uint64_t>((n + gpb - 1) / gpb, (uint64_t)ctx->sms * per_sm);
+  blocks = std::min<uint64_t>(blocks,
+                              std::max<uint64_t>(1, kWfaScratchBudget / (gpb * group_bytes)));
+  KIRA_DBUF(scratch, uint8_t, B_WFA_SCRATCH, blocks * gpb * group_bytes);
   KIRA_DBUF(dout, kira_wfa_result, B_WFA_OUT, n);
   KIRA_DBUF(work, uint32_t, B_WORK, 2);
   L.scratch = scratch;
@@ -1266,6 +1280,12 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
   if (total) KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * total, cudaMemcpyDeviceToHost, st));
   mark(ctx, 4, st);
   KIRA_CUDA(cudaStreamSynchronize(st));
+  return KIRA_OK;
+}
+
+int kira_gpu_set_wfa_lanes(kira_ctx* ctx, int lanes) {
+  if (!ctx || (lanes != 0 && lanes != 8 && lanes != 16 && lanes != 32)) return KIRA_ERR_INVALID;
+  ctx->wfa_lanes = lanes;
   return KIRA_OK;
 }
 

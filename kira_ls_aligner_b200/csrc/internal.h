@@ -125,14 +125,18 @@ struct WfaLaunch {
   int32_t tbf;                 // text_begin_free
   const int32_t* tbf_pp;       // per pair (may be null)
   int32_t drop;                // adaptive drop; < 0: exact
-  uint8_t* scratch;            // per warp: meta (int2 x 3 per score slot), then history
-  uint64_t warp_bytes;
-  uint32_t meta_bytes;
-  uint32_t meta_slots;         // scores held: every score (traceback) or the ring length
-  uint32_t hist_cap;           // traceback: int16 history entries per warp
+  int32_t group;               // lanes per pair: 8, 16 or 32
+  uint8_t* scratch;            // per group: meta (traceback), global meta ring, history
+  uint64_t group_bytes;
+  uint32_t hist_off;           // byte offset of the history in a group's scratch
+  uint32_t meta_slots;         // traceback: scores held in the global meta (S + 1)
+  uint32_t hist_cap;           // traceback: int16 history entries per group
+  uint32_t ring_len;           // scores in the meta ring (and the score-only history ring)
   uint32_t ring_width;         // score-only: entries per layer per ring slot; 0: traceback
-  uint32_t pat_region;         // shared bytes per warp before the text (pattern + guards)
-  uint32_t smem_warp;          // shared bytes per warp
+  uint32_t ring_bytes;         // shared bytes of the meta ring per group; 0: ring in scratch
+  uint32_t ring_goff;          // byte offset of the meta ring in scratch when not shared
+  uint32_t pat_region;         // shared bytes per group before the text (pattern + guards)
+  uint32_t smem_group;         // shared bytes per group
   uint32_t* work;              // dynamic pair counter
   kira_wfa_result* out;
   uint32_t* ncig;              // traceback: ops per pair
@@ -213,7 +217,7 @@ cudaError_t launch_cigar_compact(const CompactLaunch& C, int sms, cudaStream_t s
 cudaError_t launch_nm_md(const DevPairs& P, const NmMdLaunch& L, bool write, int sms,
                          cudaStream_t st);
 
-cudaError_t wfa_blocks_per_sm(bool traceback, size_t smem, int threads, int* per_sm);
+cudaError_t wfa_blocks_per_sm(int group, bool traceback, size_t smem, int threads, int* per_sm);
 cudaError_t launch_wfa(const DevPairs& P, const WfaLaunch& L, uint32_t blocks,
                        uint32_t warps_per_block, bool traceback, cudaStream_t st);
 cudaError_t launch_wfa_compact(const WfaCompact& C, int sms, cudaStream_t st);

@@ -110,86 +110,106 @@ __device__ int wfa_traceback(const WfaLaunch& L, const int2* __restrict__ meta,
   return k;
 }
 
-template <bool TB>
+// G lanes align one pair; the 32 / G groups of a warp step in lockstep through
+// an outer loop of three phases so that their warp instructions are shared:
+//   fetch   -- groups without a pair take the next one and stage its bytes;
+//   step    -- every group in the forward search computes its next score;
+//   finish  -- groups whose search ended write the result (traceback in the
+//              group's first lane).
+// Sync primitives run on the full warp outside divergent code; each group reads
+// its own bits of the ballots and shuffles from its own lanes.
+template <int G, bool TB>
 __global__ void __launch_bounds__(128) wfa_kernel(DevPairs P, WfaLaunch L) {
+  constexpr int NG = 32 / G;
+  constexpr unsigned kGroupBits = G == 32 ? kFull : ((1u << G) - 1u);
   extern __shared__ __align__(16) uint8_t wfa_smem[];
   const int lane = threadIdx.x & 31;
+  const int g = lane / G, gl = lane % G, gbase = g * G;
+  const unsigned gmask = kGroupBits << gbase;
   const uint32_t wib = threadIdx.x >> 5;
-  const uint32_t warp = blockIdx.x * (blockDim.x >> 5) + wib;
-  uint8_t* my = wfa_smem + (size_t)wib * L.smem_warp;
-  uint32_t* pw = (uint32_t*)(my + 16);
-  uint32_t* tw = (uint32_t*)(my + L.pat_region + 16);
+  const uint32_t grp = (blockIdx.x * (blockDim.x >> 5) + wib) * NG + (uint32_t)g;
+  uint8_t* my = wfa_smem + (size_t)(wib * NG + (uint32_t)g) * L.smem_group;
+  uint8_t* scr = L.scratch + (size_t)grp * L.group_bytes;
+  int2* ring = L.ring_bytes ? (int2*)my : (int2*)(scr + L.ring_goff);
+  uint32_t* pw = (uint32_t*)(my + L.ring_bytes + 16);
+  uint32_t* tw = (uint32_t*)(my + L.ring_bytes + L.pat_region + 16);
   uint8_t* pb = (uint8_t*)pw;
   uint8_t* tb = (uint8_t*)tw;
-  uint8_t* scr = L.scratch + (size_t)warp * L.warp_bytes;
-  int2* meta = (int2*)scr;
-  int16_t* H = (int16_t*)(scr + L.meta_bytes);
+  int2* meta = (int2*)scr;  // traceback: every score
+  int16_t* H = (int16_t*)(scr + L.hist_off);
   const int x = L.x, oi = L.o + L.ei, od = L.o + L.ed;
+  const uint32_t R = L.ring_len;
 
+  int phase = 0;  // 0: needs a pair, 1: forward search, 2: no pairs left
+  uint32_t p = 0, top = 0;
+  int m = 0, n = 0, S_loop = 0, tbf = 0, s = 0, last_live = 0;
   for (;;) {
-    uint32_t p = 0;
-    if (lane == 0) p = atomicAdd(L.work, 1u);
-    p = __shfl_sync(kFull, p, 0);
-    if (p >= L.n) break;
-    const int m = (int)P.read_len[p], n = (int)P.win_len[p];
-    kira_wfa_result res{};
-    res.cost = -1;
-    res.score = 0;
-    if (!L.valid) {  // WfaCosts::scored refused the configuration: None
-      if (lane == 0) {
-        L.out[p] = res;
-        if (TB) L.ncig[p] = 0;
+    // ---- fetch
+    if (phase == 0) {
+      uint32_t q = 0;
+      if (gl == 0) q = atomicAdd(L.work, 1u);
+      q = __shfl_sync(gmask, q, gbase);
+      if (q >= L.n) {
+        phase = 2;
+      } else {
+        p = q;
+        m = (int)P.read_len[p];
+        n = (int)P.win_len[p];
+        if (!L.valid || m == 0) {  // WfaCosts::scored refused: None; empty read: wfa.rs:555-563
+          if (gl == 0) {
+            kira_wfa_result res{};
+            res.cost = L.valid ? 0 : -1;
+            res.found = L.valid ? 1u : 0u;
+            L.out[p] = res;
+            if (TB) L.ncig[p] = 0;
+          }
+        } else {
+          const uint8_t* rs = P.read_seq + P.read_off[p];
+          const uint8_t* ws = P.win_seq + P.win_off[p];
+          for (int i = gl; i < m; i += G) pb[i] = __ldg(rs + i);
+          for (int i = gl; i < n; i += G) tb[i] = __ldg(ws + i);
+          int S = L.max_score_pp ? L.max_score_pp[p] : L.max_score;
+          if (!L.max_score_pp && S < 0) S = wfa_budget(m, L);
+          // The all-insertion path reaches the pattern end by cost o + ei*m, so
+          // the exact search ends by then; a pruned search advances its furthest
+          // point by an antidiagonal at least every max(x, o + ei).
+          const int64_t cap = L.drop < 0 ? (int64_t)L.o + (int64_t)L.ei * m
+                                         : (int64_t)max(x, oi) * (2 * m + n + 2);
+          S_loop = (int)max((int64_t)0, min((int64_t)S, cap));  // score 0 always runs
+          tbf = L.tbf_pp ? L.tbf_pp[p] : L.tbf;
+          tbf = min(max(tbf, 0), max(n - 1, 0));
+          s = 0;
+          top = 0;
+          last_live = 0;
+          phase = 1;
+        }
       }
-      continue;
     }
-    if (m == 0) {  // wfa.rs:555-563
-      if (lane == 0) {
-        res.found = 1;
-        res.cost = 0;
-        L.out[p] = res;
-        if (TB) L.ncig[p] = 0;
-      }
-      continue;
-    }
-    const uint8_t* rs = P.read_seq + P.read_off[p];
-    const uint8_t* ws = P.win_seq + P.win_off[p];
-    for (int i = lane; i < m; i += 32) pb[i] = __ldg(rs + i);
-    for (int i = lane; i < n; i += 32) tb[i] = __ldg(ws + i);
-    int S = L.max_score_pp ? L.max_score_pp[p] : L.max_score;
-    if (!L.max_score_pp && S < 0) S = wfa_budget(m, L);
-    // The all-insertion path reaches the pattern end by cost o + ei*m, so the
-    // exact search ends by then; a pruned search advances its furthest point
-    // by an antidiagonal at least every max(x, o + ei).
-    const int64_t cap = L.drop < 0 ? (int64_t)L.o + (int64_t)L.ei * m
-                                   : (int64_t)max(x, oi) * (2 * m + n + 2);
-    const int S_loop = (int)max((int64_t)0, min((int64_t)S, cap));  // score 0 always runs
-    int tbf = L.tbf_pp ? L.tbf_pp[p] : L.tbf;
-    tbf = min(max(tbf, 0), max(n - 1, 0));
     __syncwarp();
+    if (__all_sync(kFull, phase == 2)) break;
 
-    uint32_t top = 0;  // traceback mode: next free history entry
-    int done_s = -1, k_end = 0, last_live = 0;
-    bool overflow = false;
-    for (int s = 0; s <= S_loop; ++s) {
-      // Sources: lanes 0..4 fetch M[s-x], M[s-o-ei], M[s-o-ed], I[s-ei], D[s-ed].
-      int2 mv = wfa_empty();
-      if (s > 0 && lane < 5) {
-        const int sc = lane == 0 ? s - x : lane == 1 ? s - oi : lane == 2 ? s - od
-                       : lane == 3 ? s - L.ei : s - L.ed;
-        const int layer = lane < 3 ? 0 : lane - 2;
-        if (sc >= 0 && sc < s) mv = meta[wfa_slot(L, sc) * 3u + layer];
-      }
-      WfaWave src[5];
+    // ---- one score step of every searching group
+    const bool fwd = phase == 1;
+    int2 mv = wfa_empty();
+    if (fwd && s > 0 && gl < 5) {  // M[s-x], M[s-o-ei], M[s-o-ed], I[s-ei], D[s-ed]
+      const int sc = gl == 0 ? s - x : gl == 1 ? s - oi : gl == 2 ? s - od
+                     : gl == 3 ? s - L.ei : s - L.ed;
+      const int layer = gl < 3 ? 0 : gl - 2;
+      if (sc >= 0 && sc < s) mv = ring[((uint32_t)sc % R) * 3u + layer];
+    }
+    WfaWave src[5];
 #pragma unroll
-      for (int t = 0; t < 5; ++t)
-        src[t] = wfa_unpack(make_int2(__shfl_sync(kFull, mv.x, t), __shfl_sync(kFull, mv.y, t)));
-      const WfaWave& mx = src[0];
-      const WfaWave& moi = src[1];
-      const WfaWave& mod = src[2];
-      const WfaWave& ie = src[3];
-      const WfaWave& de = src[4];
-      int ilo = INT32_MAX, ihi = INT32_MIN, dlo = INT32_MAX, dhi = INT32_MIN;
-      int mlo = INT32_MAX, mhi = INT32_MIN;
+    for (int t = 0; t < 5; ++t)
+      src[t] = wfa_unpack(make_int2(__shfl_sync(kFull, mv.x, gbase + t),
+                                    __shfl_sync(kFull, mv.y, gbase + t)));
+    const WfaWave& mx = src[0];
+    const WfaWave& moi = src[1];
+    const WfaWave& mod = src[2];
+    const WfaWave& ie = src[3];
+    const WfaWave& de = src[4];
+    int ilo = INT32_MAX, ihi = INT32_MIN, dlo = INT32_MAX, dhi = INT32_MIN;
+    int mlo = INT32_MAX, mhi = INT32_MIN;
+    if (fwd) {
       if (s == 0) {
         mlo = 0;
         mhi = tbf;
@@ -202,129 +222,156 @@ __global__ void __launch_bounds__(128) wfa_kernel(DevPairs P, WfaLaunch L) {
         if (ilo <= ihi) mlo = min(mlo, ilo), mhi = max(mhi, ihi);
         if (dlo <= dhi) mlo = min(mlo, dlo), mhi = max(mhi, dhi);
       }
-      const int iw = ilo <= ihi ? ihi - ilo + 1 : 0;
-      const int dw = dlo <= dhi ? dhi - dlo + 1 : 0;
-      const int mw = mlo <= mhi ? mhi - mlo + 1 : 0;
-      uint32_t ib, db, mb;
-      if (L.ring_width) {
-        const uint32_t sl = wfa_slot(L, s) * 3u * L.ring_width;
-        mb = sl;
-        ib = sl + L.ring_width;
-        db = sl + 2u * L.ring_width;
-        if ((uint32_t)max(mw, max(iw, dw)) > L.ring_width) overflow = true;
-      } else {
+    }
+    const int iw = ilo <= ihi ? ihi - ilo + 1 : 0;
+    const int dw = dlo <= dhi ? dhi - dlo + 1 : 0;
+    const int mw = mlo <= mhi ? mhi - mlo + 1 : 0;
+    uint32_t ib = 0, db = 0, mb = 0;
+    int fin = 0;  // 1: found, 2: no alignment, 3: history bound exceeded
+    if (fwd) {
+      if (TB) {
         ib = top;
         db = ib + (uint32_t)iw;
         mb = db + (uint32_t)dw;
         top = mb + (uint32_t)mw;
-        if (top > L.hist_cap || (uint32_t)s >= L.meta_slots) overflow = true;
+        if (top > L.hist_cap || (uint32_t)s >= L.meta_slots) fin = 3;
+      } else {
+        const uint32_t sl = ((uint32_t)s % R) * 3u * L.ring_width;
+        mb = sl;
+        ib = sl + L.ring_width;
+        db = sl + 2u * L.ring_width;
+        if ((uint32_t)max(mw, max(iw, dw)) > L.ring_width) fin = 3;
       }
-      if (overflow) break;
+    }
+    const int nch = fwd && !fin ? (mw + G - 1) / G : 0;
+    const int maxch = __reduce_max_sync(kFull, nch);
 
-      // Pass 1: I, D, M per diagonal; extension; trimming and done ballots.
-      int ifirst = INT32_MAX, ilast = INT32_MIN, dfirst = INT32_MAX, dlast = INT32_MIN;
-      int mfirst = INT32_MAX, mlast = INT32_MIN, kdone = INT32_MAX, mad = INT32_MIN;
-      for (int c0 = mlo; c0 <= mhi; c0 += 32) {
-        const int k = c0 + lane;
-        const bool act = k <= mhi;
-        int vi = kWfaNone, vd = kWfaNone, vm = kWfaNone;
-        if (act) {
-          if (s == 0) {
-            vm = 0;
-          } else {
-            if (k >= ilo && k <= ihi) {
-              const int a = wfa_get(H, moi, k + 1), b = wfa_get(H, ie, k + 1);
-              if (a != kWfaNone && a < m) vi = max(vi, a + 1);
-              if (b != kWfaNone && b < m) vi = max(vi, b + 1);
-              H[ib + (uint32_t)(k - ilo)] = wfa_enc(vi);
-            }
-            if (k >= dlo && k <= dhi) {
-              const int a = wfa_get(H, mod, k - 1), b = wfa_get(H, de, k - 1);
-              if (a != kWfaNone && a + k <= n) vd = max(vd, a);
-              if (b != kWfaNone && b + k <= n) vd = max(vd, b);
-              H[db + (uint32_t)(k - dlo)] = wfa_enc(vd);
-            }
-            const int a = wfa_get(H, mx, k);
-            if (a != kWfaNone && a < m && a + k < n) vm = a + 1;
-            vm = max(vm, max(vi, vd));
+    // Pass 1: I, D, M per diagonal; extension; trimming and done ballots.
+    int ifirst = INT32_MAX, ilast = INT32_MIN, dfirst = INT32_MAX, dlast = INT32_MIN;
+    int mfirst = INT32_MAX, mlast = INT32_MIN, kdone = INT32_MAX, mad = INT32_MIN;
+    for (int c = 0; c < maxch; ++c) {
+      const int c0 = mlo + c * G;
+      const int k = c0 + gl;
+      const bool act = c < nch && k <= mhi;
+      int vi = kWfaNone, vd = kWfaNone, vm = kWfaNone;
+      if (act) {
+        if (s == 0) {
+          vm = 0;
+        } else {
+          if (k >= ilo && k <= ihi) {
+            const int a = wfa_get(H, moi, k + 1), b = wfa_get(H, ie, k + 1);
+            if (a != kWfaNone && a < m) vi = max(vi, a + 1);
+            if (b != kWfaNone && b < m) vi = max(vi, b + 1);
+            H[ib + (uint32_t)(k - ilo)] = wfa_enc(vi);
           }
-          if (vm != kWfaNone) {
-            vm = wfa_extend(pw, tw, m, n, k, vm);
-            mad = max(mad, 2 * vm + k);
+          if (k >= dlo && k <= dhi) {
+            const int a = wfa_get(H, mod, k - 1), b = wfa_get(H, de, k - 1);
+            if (a != kWfaNone && a + k <= n) vd = max(vd, a);
+            if (b != kWfaNone && b + k <= n) vd = max(vd, b);
+            H[db + (uint32_t)(k - dlo)] = wfa_enc(vd);
           }
-          H[mb + (uint32_t)(k - mlo)] = wfa_enc(vm);
+          const int a = wfa_get(H, mx, k);
+          if (a != kWfaNone && a < m && a + k < n) vm = a + 1;
+          vm = max(vm, max(vi, vd));
         }
-        const unsigned bi = __ballot_sync(kFull, vi != kWfaNone);
-        const unsigned bd = __ballot_sync(kFull, vd != kWfaNone);
-        const unsigned bm = __ballot_sync(kFull, vm != kWfaNone);
-        const unsigned bx = __ballot_sync(kFull, act && vm >= m);
-        if (bi) ifirst = min(ifirst, c0 + wfa_low_bit(bi)), ilast = c0 + wfa_high_bit(bi);
-        if (bd) dfirst = min(dfirst, c0 + wfa_low_bit(bd)), dlast = c0 + wfa_high_bit(bd);
-        if (bm) mfirst = min(mfirst, c0 + wfa_low_bit(bm)), mlast = c0 + wfa_high_bit(bm);
-        if (bx && kdone == INT32_MAX) kdone = c0 + wfa_low_bit(bx);
+        if (vm != kWfaNone) {
+          vm = wfa_extend(pw, tw, m, n, k, vm);
+          mad = max(mad, 2 * vm + k);
+        }
+        H[mb + (uint32_t)(k - mlo)] = wfa_enc(vm);
       }
-      // Pass 2 (adaptive): prune_wavefront on the extended M, then the done test.
-      if (L.drop >= 0 && mfirst <= mlast) {
-        const int th = __reduce_max_sync(kFull, mad) - L.drop;
-        mfirst = INT32_MAX, mlast = INT32_MIN, kdone = INT32_MAX;
-        for (int c0 = mlo; c0 <= mhi; c0 += 32) {
-          const int k = c0 + lane;
-          int v = kWfaNone;
-          if (k <= mhi) {
-            const uint32_t at = mb + (uint32_t)(k - mlo);
-            v = wfa_dec(H[at]);
-            if (v != kWfaNone && 2 * v + k < th) {
-              v = kWfaNone;
-              H[at] = wfa_enc(v);
-            }
+      const unsigned bi = (__ballot_sync(kFull, vi != kWfaNone) >> gbase) & kGroupBits;
+      const unsigned bd = (__ballot_sync(kFull, vd != kWfaNone) >> gbase) & kGroupBits;
+      const unsigned bm = (__ballot_sync(kFull, vm != kWfaNone) >> gbase) & kGroupBits;
+      const unsigned bx = (__ballot_sync(kFull, act && vm >= m) >> gbase) & kGroupBits;
+      if (bi) ifirst = min(ifirst, c0 + wfa_low_bit(bi)), ilast = c0 + wfa_high_bit(bi);
+      if (bd) dfirst = min(dfirst, c0 + wfa_low_bit(bd)), dlast = c0 + wfa_high_bit(bd);
+      if (bm) mfirst = min(mfirst, c0 + wfa_low_bit(bm)), mlast = c0 + wfa_high_bit(bm);
+      if (bx && kdone == INT32_MAX) kdone = c0 + wfa_low_bit(bx);
+    }
+    // Pass 2 (adaptive): prune_wavefront on the extended M, then the done test.
+    if (L.drop >= 0) {
+#pragma unroll
+      for (int o = G / 2; o > 0; o >>= 1) mad = max(mad, __shfl_xor_sync(kFull, mad, o));
+      const bool prune = nch > 0 && mfirst <= mlast;
+      const int th = prune ? mad - L.drop : 0;
+      if (prune) mfirst = INT32_MAX, mlast = INT32_MIN, kdone = INT32_MAX;
+      for (int c = 0; c < maxch; ++c) {
+        const int c0 = mlo + c * G;
+        const int k = c0 + gl;
+        int v = kWfaNone;
+        if (prune && c < nch && k <= mhi) {
+          const uint32_t at = mb + (uint32_t)(k - mlo);
+          v = wfa_dec(H[at]);
+          if (v != kWfaNone && 2 * v + k < th) {
+            v = kWfaNone;
+            H[at] = wfa_enc(v);
           }
-          const unsigned bm = __ballot_sync(kFull, v != kWfaNone);
-          const unsigned bx = __ballot_sync(kFull, v != kWfaNone && v >= m);
+        }
+        const unsigned bm = (__ballot_sync(kFull, v != kWfaNone) >> gbase) & kGroupBits;
+        const unsigned bx = (__ballot_sync(kFull, v != kWfaNone && v >= m) >> gbase) & kGroupBits;
+        if (prune) {
           if (bm) mfirst = min(mfirst, c0 + wfa_low_bit(bm)), mlast = c0 + wfa_high_bit(bm);
           if (bx && kdone == INT32_MAX) kdone = c0 + wfa_low_bit(bx);
         }
       }
-      if (lane == 0) {
-        const uint32_t sl = wfa_slot(L, s) * 3u;
-        meta[sl + 0] = mfirst <= mlast ? wfa_pack(mfirst, mlast, mb + (uint32_t)(mfirst - mlo))
-                                       : wfa_empty();
-        meta[sl + 1] = ifirst <= ilast ? wfa_pack(ifirst, ilast, ib + (uint32_t)(ifirst - ilo))
-                                       : wfa_empty();
-        meta[sl + 2] = dfirst <= dlast ? wfa_pack(dfirst, dlast, db + (uint32_t)(dfirst - dlo))
-                                       : wfa_empty();
-      }
-      __syncwarp();
-      if (kdone != INT32_MAX) {
-        done_s = s;
-        k_end = kdone;
-        break;
-      }
-      // Nothing reached within the look-back window: no later score can reach anything.
-      if (mfirst <= mlast || ifirst <= ilast || dfirst <= dlast) last_live = s;
-      else if (s - last_live > L.lookback) break;
     }
-
-    if (overflow) {
-      if (lane == 0) atomicOr(L.flags, 2u);
-    } else if (done_s >= 0) {
-      res.found = 1;
-      res.cost = done_s;
-      res.score = L.scored ? m * L.match - done_s : done_s;
-      res.text_end = (uint32_t)(m + k_end);
-    }
-    if (lane == 0) {
-      if (TB) {
-        uint32_t nops = 0;
-        if (res.found) {
-          bool ovf = false;
-          uint32_t* slot = L.slots + (size_t)p * L.slot_cap;
-          const int k0 = wfa_traceback(L, meta, H, pw, tw, m, n, done_s, k_end, slot, nops, ovf);
-          res.text_start = (uint32_t)max(k0, 0);
-          if (ovf) atomicOr(L.flags, 1u);
+    if (fwd && !fin) {
+      if (gl == 0) {
+        const int2 wm = mfirst <= mlast ? wfa_pack(mfirst, mlast, mb + (uint32_t)(mfirst - mlo))
+                                        : wfa_empty();
+        const int2 wi = ifirst <= ilast ? wfa_pack(ifirst, ilast, ib + (uint32_t)(ifirst - ilo))
+                                        : wfa_empty();
+        const int2 wd = dfirst <= dlast ? wfa_pack(dfirst, dlast, db + (uint32_t)(dfirst - dlo))
+                                        : wfa_empty();
+        const uint32_t rs = ((uint32_t)s % R) * 3u;
+        ring[rs + 0] = wm;
+        ring[rs + 1] = wi;
+        ring[rs + 2] = wd;
+        if (TB) {
+          meta[(uint32_t)s * 3u + 0] = wm;
+          meta[(uint32_t)s * 3u + 1] = wi;
+          meta[(uint32_t)s * 3u + 2] = wd;
         }
-        L.ncig[p] = nops;
       }
-      L.out[p] = res;
+      if (kdone != INT32_MAX) {
+        fin = 1;
+      } else if (s >= S_loop) {
+        fin = 2;
+      } else {
+        // Nothing reached within the look-back window: no later score reaches anything.
+        if (mfirst <= mlast || ifirst <= ilast || dfirst <= dlast) last_live = s;
+        if (s - last_live > L.lookback) fin = 2;
+        else ++s;
+      }
+    }
+    __syncwarp();
+
+    // ---- finish
+    if (fwd && fin) {
+      if (gl == 0) {
+        kira_wfa_result res{};
+        res.cost = -1;
+        uint32_t nops = 0;
+        if (fin == 3) {
+          atomicOr(L.flags, 2u);
+        } else if (fin == 1) {
+          res.found = 1;
+          res.cost = s;
+          res.score = L.scored ? m * L.match - s : s;
+          res.text_end = (uint32_t)(m + kdone);
+          if (TB) {
+            bool ovf = false;
+            uint32_t* slot = L.slots + (size_t)p * L.slot_cap;
+            const int k0 = wfa_traceback(L, meta, H, pw, tw, m, n, s, kdone, slot, nops, ovf);
+            res.text_start = (uint32_t)max(k0, 0);
+            if (ovf) atomicOr(L.flags, 1u);
+          }
+        }
+        if (TB) L.ncig[p] = nops;
+        L.out[p] = res;
+      }
+      phase = 0;
     }
     __syncwarp();
   }
@@ -346,19 +393,41 @@ __global__ void __launch_bounds__(256) wfa_compact_kernel(WfaCompact C) {
 
 }  // namespace
 
-cudaError_t wfa_blocks_per_sm(bool traceback, size_t smem, int threads, int* per_sm) {
-  auto kern = traceback ? wfa_kernel<true> : wfa_kernel<false>;
+template <int G>
+static cudaError_t wfa_occupancy(bool traceback, size_t smem, int threads, int* per_sm) {
+  auto kern = traceback ? wfa_kernel<G, true> : wfa_kernel<G, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, threads, smem);
 }
 
+cudaError_t wfa_blocks_per_sm(int group, bool traceback, size_t smem, int threads, int* per_sm) {
+  switch (group) {
+    case 8: return wfa_occupancy<8>(traceback, smem, threads, per_sm);
+    case 16: return wfa_occupancy<16>(traceback, smem, threads, per_sm);
+    case 32: return wfa_occupancy<32>(traceback, smem, threads, per_sm);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int G>
+static void wfa_launch_g(const DevPairs& P, const WfaLaunch& L, uint32_t blocks, uint32_t threads,
+                         size_t smem, bool traceback, cudaStream_t st) {
+  if (traceback) wfa_kernel<G, true><<<blocks, threads, smem, st>>>(P, L);
+  else wfa_kernel<G, false><<<blocks, threads, smem, st>>>(P, L);
+}
+
 cudaError_t launch_wfa(const DevPairs& P, const WfaLaunch& L, uint32_t blocks,
                        uint32_t warps_per_block, bool traceback, cudaStream_t st) {
-  const size_t smem = (size_t)L.smem_warp * warps_per_block;
+  const uint32_t groups = warps_per_block * (32u / (uint32_t)L.group);
+  const size_t smem = (size_t)L.smem_group * groups;
   const uint32_t threads = 32u * warps_per_block;
-  if (traceback) wfa_kernel<true><<<blocks, threads, smem, st>>>(P, L);
-  else wfa_kernel<false><<<blocks, threads, smem, st>>>(P, L);
+  switch (L.group) {
+    case 8: wfa_launch_g<8>(P, L, blocks, threads, smem, traceback, st); break;
+    case 16: wfa_launch_g<16>(P, L, blocks, threads, smem, traceback, st); break;
+    case 32: wfa_launch_g<32>(P, L, blocks, threads, smem, traceback, st); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 

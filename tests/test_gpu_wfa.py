@@ -175,10 +175,13 @@ def test_scored_corpus(ctx):
 
 # --- the cascade workload -----------------------------------------------------------
 
-@pytest.mark.parametrize("drop,tbf,traceback", [(None, 0, True), (None, 0, False),
-                                                (50, 0, True), (None, 5, True), (8, 3, False)])
-def test_cascade_workload(ctx, drop, tbf, traceback):
-    from kira_ls_aligner_b200 import AlignmentConfig, PairBatch, WfaParams, synth
+@pytest.mark.parametrize("drop,tbf,traceback,lanes", [
+    (None, 0, True, 0), (None, 0, False, 0), (50, 0, True, 0), (None, 5, True, 0),
+    (8, 3, False, 0), (None, 0, True, 16), (None, 0, True, 32), (50, 2, False, 32),
+    (3, 0, True, 16)])
+def test_cascade_workload(ctx, drop, tbf, traceback, lanes):
+    from kira_ls_aligner_b200 import AlignmentConfig, PairBatch, WfaParams, _abi, synth
+    ctx.check(_abi.lib().kira_gpu_set_wfa_lanes(ctx.handle, lanes))
     w = synth.wfa_cascade(3000, seed=0x51 + tbf, err_hi=0.08, ref_len=400_000)
     ref = w.reference
     pairs = [(w.reads[int(w.read_off[i]):int(w.read_off[i]) + int(w.read_len[i])].tobytes(),
@@ -195,6 +198,7 @@ def test_cascade_workload(ctx, drop, tbf, traceback):
     b = PairBatch(w.reads, w.read_off, w.read_len, None, w.win_off, w.win_len)
     res, ops = ctx.wfa_batch(b, p)
     res2, ops2 = ctx.wfa_batch(_batch(pairs), p)
+    ctx.check(_abi.lib().kira_gpu_set_wfa_lanes(ctx.handle, 0))
     assert np.array_equal(res, res2) and np.array_equal(ops, ops2)
 
 
@@ -221,8 +225,10 @@ def test_edge_cases(ctx):
     assert got[2] == (10, 10, 0, 0, [(4, "I")])
 
 
-def test_long_reads(ctx):
-    from kira_ls_aligner_b200 import synth
+@pytest.mark.parametrize("lanes", [0, 8])
+def test_long_reads(ctx, lanes):
+    from kira_ls_aligner_b200 import _abi, synth
+    ctx.check(_abi.lib().kira_gpu_set_wfa_lanes(ctx.handle, lanes))
     w = synth.gapfill(n_segments=60, seed=0x77, seg_lo=400, seg_hi=1500, err_lo=0.01,
                       err_hi=0.03, ref_len=2_000_000)
     pairs = []
@@ -230,9 +236,12 @@ def test_long_reads(ctx):
         q = w.reads[int(w.read_off[i]):int(w.read_off[i]) + int(w.read_len[i])].tobytes()
         s = int(w.win_off[i]) + int(w.band_offset[i])
         pairs.append((q, w.reference[s:s + len(q) + 64].tobytes()))
-    for tb in (True, False):
-        got = _check(ctx, pairs, _pen(max_score=400, traceback=tb))
-        assert sum(x is not None for x in got) > 10
+    try:
+        for tb in (True, False):
+            got = _check(ctx, pairs, _pen(max_score=400, traceback=tb))
+            assert sum(x is not None for x in got) > 10
+    finally:
+        ctx.check(_abi.lib().kira_gpu_set_wfa_lanes(ctx.handle, 0))
 
 
 def test_refused_costs_and_capacity(ctx):
