@@ -47,14 +47,15 @@ def parse():
     ap.add_argument("--shape", type=int, default=-1,
                     help="install this banded-SW launch shape instead of autotuning")
     ap.add_argument("--workload", choices=["batched", "uneven", "serving", "gapfill", "nmmd",
-                                           "wfa"],
+                                           "wfa", "prefilter"],
                     default="batched",
                     help="batched: the headline 2M-pair verification; uneven: 500k banded-SW "
                          "pairs of mixed length and band (bucketed vs one-launch path); "
                          "serving: Poisson request stream through the server vs one request "
                          "per call; gapfill: long-read gap-fill segments at band 256; nmmd: "
                          "NM + MD:Z of the batched alignments; wfa: the cascade's WFA step "
-                         "(scored costs, router budget) with and without traceback")
+                         "(scored costs, router budget) with and without traceback; "
+                         "prefilter: stage-4 exact match + ungapped prefilter per chain")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=5.0, help="serving: seconds of arrivals")
     ap.add_argument("--slots", type=int, default=4, help="serving: concurrent batches")
@@ -340,7 +341,8 @@ def run_wfa(args, rank, local, world):
     out = {}
     for mode, tb in (("traceback", True), ("score_only", False)):
         p = WfaParams.scored_from(AlignmentConfig(), adaptive_drop=drop, traceback=tb)
-        res = np.zeros(n, _abi.WFA_RESULT_DTYPE)
+        res = pin(np.zeros(n * _abi.WFA_RESULT_DTYPE.itemsize, np.uint8)).view(
+            _abi.WFA_RESULT_DTYPE)
         ops = pin(np.zeros(8 * n, np.uint32))
         cb = _abi.CigarBuf(_abi.ptr(ops), len(ops), 0)
         pc, wp = b.to_c(), p.to_c()
@@ -400,6 +402,91 @@ def run_wfa(args, rank, local, world):
         "e2e": {"value": tb["e2e_pairs_per_s"], "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": 32 * n + 4 * tb["cigar_ops"]},
         "modes": out, "cpu_baseline": cpu}))
+    ctx.close()
+
+
+def run_prefilter(args, rank, local, world):
+    """Stage 4's step before the cascade (stage4_alignment.rs:728-776): per chain
+    exact_match_alignment, else prefilter_chain (ungapped x-drop extension, span
+    Hamming count, accept cascade, [S]M[S] CIGAR + NM + MD:Z for accepts), with
+    the `mem` defaults. 2M chains of 150 bp reads over a resident 50 Mbp contig;
+    host API with pinned inputs (H2D + D2H inside the timed region); the kernel
+    time is passes 1 + 2 from the library's stage events."""
+    import torch
+
+    from kira_ls_aligner_b200 import GpuContext, PairBatch, PrefilterConfig, _abi, synth
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    w = synth.prefilter_chains()
+    n = w.n_pairs
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    b = PairBatch(pin(w.reads), pin(w.read_off), pin(w.read_len), None,
+                  pin(np.zeros(n, np.uint64)), pin(np.full(n, len(w.reference), np.uint32)))
+    chains = pin(w.chains)  # (n, 4) uint32 = kira_chain
+    top1, margin = pin(w.is_top1), pin(w.score_margin)
+    ctx = GpuContext(local)
+    ctx.ref_upload(w.reference)
+    L = _abi.lib()
+    cfg = PrefilterConfig()
+    res = pin(np.zeros(n * _abi.PREFILTER_RESULT_DTYPE.itemsize, np.uint8)).view(
+        _abi.PREFILTER_RESULT_DTYPE)
+    ops = pin(np.zeros(3 * n, np.uint32))
+    md = pin(np.zeros(16 * n, np.uint8))
+    cb = _abi.CigarBuf(_abi.ptr(ops), len(ops), 0)
+    used = C.c_uint64()
+    pc, pf = b.to_c(), cfg.to_c()
+
+    def call():  # the C entry point on preallocated pinned host buffers
+        ctx.check(L.kira_gpu_prefilter_batch(ctx.handle, C.byref(pc), _abi.ptr(chains),
+                                             _abi.ptr(top1), _abi.ptr(margin), C.byref(pf),
+                                             _abi.ptr(res), C.byref(cb), _abi.ptr(md), md.nbytes,
+                                             C.byref(used)))
+    for _ in range(args.warmup):
+        call()
+    ts = [_timed(call) for _ in range(args.steps)]
+    ctx.check(L.kira_gpu_profile(ctx.handle, 1))
+    stages = []
+    for _ in range(3):
+        call()
+        buf = (C.c_float * 8)()
+        k = L.kira_gpu_stage_times(ctx.handle, buf, 8)
+        stages.append([float(x) for x in buf[:k]])
+    ctx.check(L.kira_gpu_profile(ctx.handle, 0))
+    ms = sum(ts) / len(ts)
+    st = [statistics.median(s[i] for s in stages) for i in range(len(stages[0]))]
+    kms = st[1] + st[3]
+    kinds = np.bincount(res["result"], minlength=4)
+    cpu = None
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as O
+        nthreads = os.cpu_count() or 1
+        m = min(n, 1_000_000)
+        oc = O.prefilter_cfg(1, 4, 100, True, True, 15, 98.5, 5, 0, 500)
+        t = time.perf_counter()
+        O.prefilter_batch(w.reads, w.read_off[:m], w.read_len[:m], w.reference,
+                          np.zeros(m, np.uint64), np.full(m, len(w.reference), np.uint32),
+                          w.chains[:m], w.is_top1[:m], w.score_margin[:m], oc, True, nthreads, 32)
+        el = time.perf_counter() - t
+        cpu = {"value": m / el, "unit": "chains/s", "cores": nthreads, "kind": "port",
+               "sample": f"first {m} chains of the workload"}
+    h2d = int(w.read_len.sum()) + n * (8 + 4 + 8 + 4 + 16 + 1 + 4)
+    print(json.dumps({
+        "metric": "chains/s (stage-4 exact match + ungapped prefilter with CIGAR/NM/MD, bit-exact)",
+        "value": n / (kms / 1e3), "unit": "chains/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": kms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
+        "config": {"workload": w.name, "chains": n, "read_len": 150,
+                   "reference_bp": int(len(w.reference)), "cfg": "mem defaults",
+                   "path": "resident contig, host API, pinned inputs"},
+        "e2e": {"value": n / (ms / 1e3), "unit": "chains/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 48 * n + 4 * int(cb.used) + int(used.value)},
+        "stage_ms": dict(zip(("upload", "extend_decide", "offsets", "cigar_md", "download"),
+                             [round(x, 3) for x in st])),
+        "outcomes": {"accept": int(kinds[0]), "reject": int(kinds[1]),
+                     "fallback": int(kinds[2]), "exact": int(kinds[3])},
+        "cpu_baseline": cpu}))
     ctx.close()
 
 
@@ -638,6 +725,8 @@ def main():
             run_nmmd(args, rank, local, world)
         elif args.workload == "wfa":
             run_wfa(args, rank, local, world)
+        elif args.workload == "prefilter":
+            run_prefilter(args, rank, local, world)
         elif args.impl == "reference":
             run_reference(args, rank, world)
         else:

@@ -415,6 +415,97 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
  * Results are identical for every choice. */
 int kira_gpu_set_wfa_lanes(kira_ctx* ctx, int lanes);
 
+/* ------------------------------------- ungapped prefilter and exact matches
+ *
+ * The step before the cascade in stage-4 alignment (src/pipeline/
+ * stage4_alignment.rs:728-776): exact_match_alignment (src/alignment/
+ * mod.rs:779-832) and prefilter_chain (src/alignment/prefilter.rs:93-517). A
+ * pair's window is the chain's reference sequence (index.ref_bases(ref_id), or
+ * the slice of it the caller ships; a resident reference with win_off = the
+ * contig start); the chain's coordinates are relative to it. */
+
+/* AnchorSpan (src/alignment/mod.rs) without ref_id / strand: the read is already
+ * oriented for the strand. */
+typedef struct kira_chain {
+  uint32_t ref_start;
+  uint32_t ref_end;
+  uint32_t read_start;
+  uint32_t read_end;
+} kira_chain;
+
+/* prefilter_chain's arguments (prefilter.rs:93-108) and the knobs it reads from
+ * the environment. */
+typedef struct kira_prefilter_cfg {
+  int32_t match_score;            /* AlignmentConfig.match_score */
+  int32_t mismatch;               /* AlignmentConfig.mismatch */
+  int32_t xdrop;                  /* AlignmentConfig.xdrop */
+  int32_t accept_enable;
+  int32_t accept_only_top1;
+  uint32_t accept_span_slack;
+  float accept_min_identity;      /* percent; floor = (x * 100).round() as u16 */
+  uint32_t accept_max_mismatches;
+  int32_t accept_require_score_margin;
+  uint32_t long_read_threshold;
+  int32_t multi_alignments_enabled;
+  int32_t tail;                   /* KIRA_UNGAP_TAIL (default 1) */
+  int32_t min_identity_x10000;    /* KIRA_UNGAP_MINID; < 0: unset */
+  int32_t exact_first;            /* 1: exact_match_alignment first, as stage 4 does */
+} kira_prefilter_cfg;
+
+enum kira_prefilter_kind {
+  KIRA_PREFILTER_ACCEPT = 0,      /* PrefilterResult::Accept */
+  KIRA_PREFILTER_REJECT = 1,      /* PrefilterResult::Reject */
+  KIRA_PREFILTER_FALLBACK = 2,    /* PrefilterResult::Fallback */
+  KIRA_PREFILTER_EXACT = 3        /* exact_match_alignment returned Some (exact_first) */
+};
+
+/* PrefilterOutcome (prefilter.rs:76-82) of one chain. reason = PrefilterReason::idx();
+ * reason 9 (Other) carries other = 1 read_len0, 2 non_monotonic, 3 anchor0,
+ * 4 span0, 5 neg_start, 6 span_oob, 7 margin_fail. len .. ref_start are the
+ * UngappedStats when has_metrics; for ACCEPT and EXACT they also give the
+ * alignment's span (read_start, ref_start, len M columns) and score, with nm,
+ * the CIGAR ([S] M [S]; EXACT: read_len M) and the MD:Z text md[md_off, +md_len). */
+typedef struct kira_prefilter_result {
+  uint8_t result;
+  uint8_t reason;
+  uint8_t other;
+  uint8_t has_metrics;
+  uint16_t len;
+  uint16_t mism;
+  uint16_t matches;
+  uint16_t identity_x10000;
+  int32_t score;
+  uint32_t read_start;
+  uint32_t ref_start;
+  uint32_t nm;
+  uint32_t cigar_off;
+  uint32_t n_cigar;
+  uint32_t md_off;
+  uint32_t md_len;
+  uint32_t reserved;
+} kira_prefilter_result;
+
+/* prefilter_chain per chain (with exact_match_alignment first when cfg.exact_first).
+ * is_top1 (NULL: all 1) and score_margin (NULL: INT32_MAX) are per chain. Reads up
+ * to 65535 bases; a chain that reaches the extension must end inside its read and
+ * window (the reference panics otherwise): KIRA_ERR_INVALID. KIRA_ERR_CAPACITY when
+ * the CIGAR or MD output is too small (cigar->used / *md_used give the need).
+ * Stage times: [0] inputs uploaded, [1] extension + decisions, [2] offsets,
+ * [3] CIGAR + MD text, [4] downloaded. The opt-in WFA gap check
+ * (KIRA_UNGAP_GAP_CHECK) is the score-only kira_gpu_wfa_batch with per-pair
+ * max_score = mism * (match_score + mismatch) - 1 (ungapped_beaten_by_gap,
+ * mod.rs:162-204), run by the caller on the accepted chains. */
+int kira_gpu_prefilter_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_chain* chains,
+                             const uint8_t* is_top1, const int32_t* score_margin,
+                             const kira_prefilter_cfg* cfg, kira_prefilter_result* out,
+                             kira_cigar_buf* cigar, char* md, uint64_t md_cap,
+                             uint64_t* md_used);
+
+/* exact_match_exists (mod.rs:819-832) per chain: out[i] = 1 when the whole read
+ * equals the window bytes at the chain's co-linear span. */
+int kira_gpu_exact_match_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_chain* chains,
+                               uint8_t* out);
+
 /* ------------------------------------------------ serving (continuous batching)
  *
  * No counterpart in the reference, whose dispatcher thread runs one blocking

@@ -6,9 +6,9 @@ of that boundary; there is no CPU compute path in this package.
 """
 from . import _abi
 from .runtime import (AlignmentConfig, CapacityError, CudaError, GpuContext, InvalidArgument,
-                      PairBatch, Server, SwPublicResult, Ticket, Timeout, VerifyParams,
+                      PairBatch, PrefilterConfig, Server, SwPublicResult, Ticket, Timeout, VerifyParams,
                       WfaParams, cigar_string, decode_cigar, is_available, results_to_list)
 
 __all__ = ["AlignmentConfig", "CapacityError", "CudaError", "GpuContext", "InvalidArgument",
-           "PairBatch", "Server", "SwPublicResult", "Ticket", "Timeout", "VerifyParams",
+           "PairBatch", "PrefilterConfig", "Server", "SwPublicResult", "Ticket", "Timeout", "VerifyParams",
            "WfaParams", "cigar_string", "decode_cigar", "is_available", "results_to_list", "_abi"]

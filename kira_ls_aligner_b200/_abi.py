@@ -37,7 +37,7 @@ EXPORTS = (
     "kira_gpu_bsw_shapes", "kira_gpu_set_bsw_shape", "kira_gpu_bsw_batch_noalloc",
     "kira_gpu_align_batch_simd", "kira_gpu_set_plain", "kira_gpu_set_trace_budget",
     "kira_gpu_set_graphs", "kira_gpu_set_chunk_pairs", "kira_gpu_nm_md", "kira_gpu_wfa_batch",
-    "kira_gpu_set_wfa_lanes",
+    "kira_gpu_set_wfa_lanes", "kira_gpu_prefilter_batch", "kira_gpu_exact_match_batch",
     "kira_server_create", "kira_server_destroy", "kira_server_ref_upload",
     "kira_server_submit_verify", "kira_server_submit_bsw", "kira_server_poll",
     "kira_server_wait", "kira_server_info", "kira_server_release", "kira_server_stats",
@@ -87,6 +87,21 @@ class WfaParams(C.Structure):
                  "budget_pct", "adaptive_drop", "text_begin_free", "traceback")]
 
 
+class Chain(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("ref_start", "ref_end", "read_start", "read_end")]
+
+
+class PrefilterCfg(C.Structure):
+    _fields_ = [("match_score", C.c_int32), ("mismatch", C.c_int32), ("xdrop", C.c_int32),
+                ("accept_enable", C.c_int32), ("accept_only_top1", C.c_int32),
+                ("accept_span_slack", C.c_uint32), ("accept_min_identity", C.c_float),
+                ("accept_max_mismatches", C.c_uint32),
+                ("accept_require_score_margin", C.c_int32),
+                ("long_read_threshold", C.c_uint32), ("multi_alignments_enabled", C.c_int32),
+                ("tail", C.c_int32), ("min_identity_x10000", C.c_int32),
+                ("exact_first", C.c_int32)]
+
+
 class ServerCfg(C.Structure):
     _fields_ = [("device", C.c_int), ("slots", C.c_int), ("max_batch_pairs", C.c_uint32),
                 ("mem_fraction", C.c_double)]
@@ -114,6 +129,16 @@ WFA_RESULT_DTYPE = np.dtype([("cost", "<i4"), ("score", "<i4"), ("text_start", "
                              ("found", "<u4"), ("reserved", "<u4")])
 assert SW_RESULT_DTYPE.itemsize == 32 and DETAIL_DTYPE.itemsize == 20
 assert WFA_RESULT_DTYPE.itemsize == 32
+PREFILTER_RESULT_DTYPE = np.dtype([("result", "u1"), ("reason", "u1"), ("other", "u1"),
+                                   ("has_metrics", "u1"), ("len", "<u2"), ("mism", "<u2"),
+                                   ("matches", "<u2"), ("identity_x10000", "<u2"),
+                                   ("score", "<i4"), ("read_start", "<u4"), ("ref_start", "<u4"),
+                                   ("nm", "<u4"), ("cigar_off", "<u4"), ("n_cigar", "<u4"),
+                                   ("md_off", "<u4"), ("md_len", "<u4"), ("reserved", "<u4")])
+CHAIN_DTYPE = np.dtype([("ref_start", "<u4"), ("ref_end", "<u4"), ("read_start", "<u4"),
+                        ("read_end", "<u4")])
+assert PREFILTER_RESULT_DTYPE.itemsize == 48 and CHAIN_DTYPE.itemsize == 16
+PREFILTER_ACCEPT, PREFILTER_REJECT, PREFILTER_FALLBACK, PREFILTER_EXACT = 0, 1, 2, 3
 
 _lib = None
 
@@ -156,6 +181,10 @@ def lib():
     L.kira_gpu_wfa_batch.argtypes = [vp, C.POINTER(Pairs), C.POINTER(WfaParams), vp, vp, vp,
                                      C.POINTER(CigarBuf)]
     L.kira_gpu_set_wfa_lanes.argtypes = [vp, C.c_int]
+    L.kira_gpu_prefilter_batch.argtypes = [vp, C.POINTER(Pairs), vp, vp, vp,
+                                           C.POINTER(PrefilterCfg), vp, C.POINTER(CigarBuf), vp,
+                                           C.c_uint64, C.POINTER(C.c_uint64)]
+    L.kira_gpu_exact_match_batch.argtypes = [vp, C.POINTER(Pairs), vp, vp]
     L.kira_gpu_align_batch_simd.argtypes = [vp, C.POINTER(Pairs), C.POINTER(SwCfg), C.c_int,
                                             C.c_int, vp, C.POINTER(CigarBuf)]
     L.kira_gpu_bsw_batch_noalloc.argtypes = [C.POINTER(Pairs), C.POINTER(SwCfg), vp, vp,

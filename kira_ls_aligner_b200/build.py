@@ -16,7 +16,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIB_DIR, "libkira_gpu.so")
-SOURCES = ["kernels.cu", "wfa.cu", "api.cu", "noalloc.cu", "server.cpp"]
+SOURCES = ["kernels.cu", "wfa.cu", "prefilter.cu", "api.cu", "noalloc.cu", "server.cpp"]
 HEADERS = ["common.cuh", "sieve.cuh", "myers.cuh", "bsw.cuh", "bsw16.cuh", "qgram.cuh", "nmmd.cuh",
            "planes.cuh", "addchain.cuh", "wfa.cuh", "internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -25,7 +26,8 @@ enum BufId {
   B_MYERS_LIST, B_SW_LIST, B_COUNTERS, B_ENDS, B_TRACE, B_META, B_CIG_SLOTS, B_ITEM_OF_PAIR,
   B_DIST, B_END, B_SIEVE_OUT, B_SIEVE_JOBS, B_CELLS, B_TOTAL, B_READ_PLANES, B_WIN_PLANES,
   B_ROWKEYS, B_DONE_ROW, B_WORK, B_WFA_MAXS, B_WFA_TBF, B_WFA_OUT, B_WFA_NCIG, B_WFA_SLOTS,
-  B_WFA_SCRATCH, B_WFA_FLAGS, B_COUNT
+  B_WFA_SCRATCH, B_WFA_FLAGS, B_PF_CHAINS, B_PF_TOP1, B_PF_MARGIN, B_PF_OUT, B_PF_NCIG,
+  B_PF_MDLEN, B_PF_MDOFF, B_PF_MD, B_PF_EXACT, B_COUNT
 };
 
 struct DevBuf {
@@ -1279,6 +1281,157 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
                 (unsigned long long)cigar->cap, (unsigned long long)total);
   if (total) KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * total, cudaMemcpyDeviceToHost, st));
   mark(ctx, 4, st);
+  KIRA_CUDA(cudaStreamSynchronize(st));
+  return KIRA_OK;
+}
+
+namespace {
+
+// Chains that reach ungapped_extend must lie inside their read and window: the
+// reference's u32 subtractions and slices panic otherwise (prefilter.rs:362-364).
+int check_chains(kira_ctx* ctx, const kira_pairs& P, const kira_chain* chains) {
+  for (uint32_t i = 0; i < P.n; ++i) {
+    const kira_chain& c = chains[i];
+    if (P.read_len[i] > 65535u)
+      return fail(ctx, KIRA_ERR_READ_TOO_LONG, "pair %u: reads up to 65535 bases", i);
+    const bool extends = P.read_len[i] > 0 && c.read_start <= c.read_end &&
+                         c.ref_start <= c.ref_end && c.read_end > c.read_start;
+    if (extends && (c.read_end > P.read_len[i] || c.ref_end > P.win_len[i]))
+      return fail(ctx, KIRA_ERR_INVALID, "chain %u ends outside its read or window", i);
+  }
+  return KIRA_OK;
+}
+
+// (accept_min_identity * 100.0).round() as u16 (prefilter.rs:266): f32 product,
+// rounding half away from zero, saturating cast (NaN -> 0).
+int32_t identity_floor(float pct) {
+  const float v = pct * 100.0f;
+  if (!(v == v)) return 0;
+  const float r = std::round(v);
+  return r <= 0.0f ? 0 : (r >= 65535.0f ? 65535 : (int32_t)r);
+}
+
+}  // namespace
+
+int kira_gpu_prefilter_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_chain* chains,
+                             const uint8_t* is_top1, const int32_t* score_margin,
+                             const kira_prefilter_cfg* cfg, kira_prefilter_result* out,
+                             kira_cigar_buf* cigar, char* md, uint64_t md_cap,
+                             uint64_t* md_used) {
+  if (!ctx || !pairs || !chains || !cfg || !out || !cigar || !md_used) return KIRA_ERR_INVALID;
+  const kira_pairs& P = *pairs;
+  const uint32_t n = P.n;
+  cigar->used = 0;
+  *md_used = 0;
+  if (n == 0) return KIRA_OK;
+  if ((cigar->cap && !cigar->ops) || (md_cap && !md)) return KIRA_ERR_INVALID;
+  int rc = check_chains(ctx, P, chains);
+  if (rc) return rc;
+  PrefilterLaunch L{};
+  L.match = cfg->match_score;
+  L.mismatch = cfg->mismatch;
+  L.xdrop = cfg->xdrop;
+  L.accept_enable = cfg->accept_enable != 0;
+  L.only_top1 = cfg->accept_only_top1 != 0;
+  L.multi = cfg->multi_alignments_enabled != 0;
+  L.tail = cfg->tail != 0;
+  L.exact_first = cfg->exact_first != 0;
+  L.span_slack = cfg->accept_span_slack;
+  L.max_mismatches = cfg->accept_max_mismatches;
+  L.long_read_threshold = cfg->long_read_threshold;
+  L.require_margin = cfg->accept_require_score_margin;
+  L.identity_floor = cfg->min_identity_x10000 >= 0 ? cfg->min_identity_x10000
+                                                   : identity_floor(cfg->accept_min_identity);
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  ctx->ev_recorded = 0;
+  mark(ctx, 0, st);
+  DevPairs D;
+  rc = upload_pairs(ctx, P, D);
+  if (rc) return rc;
+  cudaError_t cerr = cudaSuccess;
+  KIRA_DBUF(dch, kira_chain, B_PF_CHAINS, n);
+  KIRA_CUDA(cudaMemcpyAsync(dch, chains, sizeof(kira_chain) * n, cudaMemcpyHostToDevice, st));
+  L.chains = dch;
+  if (is_top1) {
+    KIRA_DBUF(b, uint8_t, B_PF_TOP1, n);
+    KIRA_CUDA(cudaMemcpyAsync(b, is_top1, n, cudaMemcpyHostToDevice, st));
+    L.is_top1 = b;
+  }
+  if (score_margin) {
+    KIRA_DBUF(b, int32_t, B_PF_MARGIN, n);
+    KIRA_CUDA(cudaMemcpyAsync(b, score_margin, 4ull * n, cudaMemcpyHostToDevice, st));
+    L.score_margin = b;
+  }
+  KIRA_DBUF(dout, kira_prefilter_result, B_PF_OUT, n);
+  KIRA_DBUF(ncig, uint32_t, B_PF_NCIG, n);
+  KIRA_DBUF(mdlen, uint32_t, B_PF_MDLEN, n);
+  KIRA_DBUF(cig_off, uint32_t, B_CIG_OFF, n);
+  KIRA_DBUF(md_off, uint32_t, B_PF_MDOFF, n);
+  KIRA_DBUF(sums, uint32_t, B_CHUNK_SUMS, n / 4096 + 2);
+  KIRA_DBUF(totals, uint64_t, B_TOTAL, 2);
+  KIRA_DBUF(flags, uint32_t, B_WORK, 1);
+  L.out = dout;
+  L.ncig = ncig;
+  L.mdlen = mdlen;
+  L.flags = flags;
+  KIRA_CUDA(cudaMemsetAsync(flags, 0, 4, st));
+  mark(ctx, 1, st);
+  KIRA_CUDA(launch_prefilter(D, L, false, ctx->sms, st));
+  mark(ctx, 2, st);
+  KIRA_CUDA(launch_cigar_scan(ncig, n, cig_off, sums, totals, st));
+  KIRA_CUDA(launch_cigar_scan(mdlen, n, md_off, sums, totals + 1, st));
+  KIRA_CUDA(launch_prefilter_offsets(n, dout, cig_off, md_off, ctx->sms, st));
+  uint64_t tot[2] = {0, 0};
+  uint32_t hflags = 0;
+  KIRA_CUDA(cudaMemcpyAsync(tot, totals, 16, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(&hflags, flags, 4, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaStreamSynchronize(st));
+  if (hflags & 1u) return fail(ctx, KIRA_ERR_RUNTIME, "a chain ended outside its read or window");
+  cigar->used = tot[0];
+  *md_used = tot[1];
+  if (tot[0] > cigar->cap || tot[1] > md_cap) {
+    KIRA_CUDA(cudaMemcpy(out, dout, sizeof(kira_prefilter_result) * n, cudaMemcpyDeviceToHost));
+    return fail(ctx, KIRA_ERR_CAPACITY, "CIGAR / MD buffers hold %llu ops / %llu bytes; "
+                "%llu / %llu needed", (unsigned long long)cigar->cap,
+                (unsigned long long)md_cap, (unsigned long long)tot[0],
+                (unsigned long long)tot[1]);
+  }
+  KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(tot[0], 1));
+  KIRA_DBUF(dmd, char, B_PF_MD, std::max<uint64_t>(tot[1], 1));
+  L.ops = ops;
+  L.cigar_cap = tot[0];
+  L.md = dmd;
+  mark(ctx, 3, st);
+  KIRA_CUDA(launch_prefilter(D, L, true, ctx->sms, st));
+  mark(ctx, 4, st);
+  KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_prefilter_result) * n, cudaMemcpyDeviceToHost,
+                            st));
+  if (tot[0])
+    KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * tot[0], cudaMemcpyDeviceToHost, st));
+  if (tot[1]) KIRA_CUDA(cudaMemcpyAsync(md, dmd, tot[1], cudaMemcpyDeviceToHost, st));
+  mark(ctx, 5, st);
+  KIRA_CUDA(cudaStreamSynchronize(st));
+  return KIRA_OK;
+}
+
+int kira_gpu_exact_match_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_chain* chains,
+                               uint8_t* out) {
+  if (!ctx || !pairs || !chains || !out) return KIRA_ERR_INVALID;
+  const kira_pairs& P = *pairs;
+  const uint32_t n = P.n;
+  if (n == 0) return KIRA_OK;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  DevPairs D;
+  int rc = upload_pairs(ctx, P, D);
+  if (rc) return rc;
+  cudaError_t cerr = cudaSuccess;
+  KIRA_DBUF(dch, kira_chain, B_PF_CHAINS, n);
+  KIRA_DBUF(dout, uint8_t, B_PF_EXACT, n);
+  KIRA_CUDA(cudaMemcpyAsync(dch, chains, sizeof(kira_chain) * n, cudaMemcpyHostToDevice, st));
+  KIRA_CUDA(launch_exact_match(D, dch, dout, ctx->sms, st));
+  KIRA_CUDA(cudaMemcpyAsync(out, dout, n, cudaMemcpyDeviceToHost, st));
   KIRA_CUDA(cudaStreamSynchronize(st));
   return KIRA_OK;
 }

@@ -156,6 +156,24 @@ struct WfaCompact {
   uint64_t cap;
 };
 
+// Ungapped prefilter (prefilter.cu): warp per chain.
+struct PrefilterLaunch {
+  const kira_chain* chains;
+  const uint8_t* is_top1;       // may be null: every chain is the top one
+  const int32_t* score_margin;  // may be null: INT32_MAX
+  int32_t match, mismatch, xdrop;
+  int32_t accept_enable, only_top1, multi, tail, exact_first;
+  uint32_t span_slack, max_mismatches, long_read_threshold;
+  int32_t require_margin, identity_floor;
+  kira_prefilter_result* out;
+  uint32_t* ncig;               // pass 1: CIGAR ops per chain
+  uint32_t* mdlen;              // pass 1: MD bytes per chain
+  uint32_t* ops;                // pass 2: CIGAR output
+  uint64_t cigar_cap;
+  char* md;                     // pass 2: MD output
+  uint32_t* flags;              // bit 0: a chain outside its read / window
+};
+
 // Banded-SW launch shape: G lanes per pair, K cells (int32) or K packed words of
 // two int16 cells (packed) per lane.
 struct BswShapeInfo {
@@ -221,6 +239,14 @@ cudaError_t wfa_blocks_per_sm(int group, bool traceback, size_t smem, int thread
 cudaError_t launch_wfa(const DevPairs& P, const WfaLaunch& L, uint32_t blocks,
                        uint32_t warps_per_block, bool traceback, cudaStream_t st);
 cudaError_t launch_wfa_compact(const WfaCompact& C, int sms, cudaStream_t st);
+
+cudaError_t launch_prefilter(const DevPairs& P, const PrefilterLaunch& L, bool write, int sms,
+                             cudaStream_t st);
+cudaError_t launch_prefilter_offsets(uint32_t n, kira_prefilter_result* out,
+                                     const uint32_t* cig_off, const uint32_t* md_off, int sms,
+                                     cudaStream_t st);
+cudaError_t launch_exact_match(const DevPairs& P, const kira_chain* chains, uint8_t* out, int sms,
+                               cudaStream_t st);
 
 int ctx_share_reference(kira_ctx* dst, const kira_ctx* src);
 

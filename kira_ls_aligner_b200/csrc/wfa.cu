@@ -21,12 +21,6 @@ __device__ __forceinline__ int32_t wfa_budget(int read_len, const WfaLaunch& L) 
 __device__ __forceinline__ int wfa_low_bit(unsigned b) { return __ffs(b) - 1; }
 __device__ __forceinline__ int wfa_high_bit(unsigned b) { return 31 - __clz(b); }
 
-// Where wavefront (score s, layer) lives: traceback keeps every score, score-only
-// a ring of meta_slots scores with ring_width entries per layer.
-__device__ __forceinline__ uint32_t wfa_slot(const WfaLaunch& L, int s) {
-  return L.ring_width ? (uint32_t)s % L.meta_slots : (uint32_t)s;
-}
-
 // Traceback in one lane (build_cigar, wfa.rs:762-952). Ops are pushed in reverse
 // order into the pair's slot with push_cigar's merging (wfa.rs:954-962); returns
 // the diagonal at termination (the alignment's text start).

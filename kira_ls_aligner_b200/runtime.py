@@ -143,6 +143,45 @@ class WfaParams:
                            self.text_begin_free, int(self.traceback))
 
 
+@dataclass
+class PrefilterConfig:
+    """prefilter_chain's arguments (src/alignment/prefilter.rs:93-108), defaults of the
+    `mem` command (src/cli/args/mem.rs:460-477), and the KIRA_UNGAP_TAIL /
+    KIRA_UNGAP_MINID knobs; exact_first runs exact_match_alignment first as stage 4
+    does (stage4_alignment.rs:728-735)."""
+    match_score: int = 1
+    mismatch: int = 4
+    xdrop: int = 100
+    accept_enable: bool = True
+    accept_only_top1: bool = True
+    accept_span_slack: int = 15
+    accept_min_identity: float = 98.5
+    accept_max_mismatches: int = 5
+    accept_require_score_margin: int = 0
+    long_read_threshold: int = 500
+    multi_alignments_enabled: bool = False
+    tail: bool = True
+    min_identity_x10000: int = -1
+    exact_first: bool = True
+
+    def to_c(self) -> A.PrefilterCfg:
+        return A.PrefilterCfg(self.match_score, self.mismatch, self.xdrop, int(self.accept_enable),
+                              int(self.accept_only_top1), self.accept_span_slack,
+                              self.accept_min_identity, self.accept_max_mismatches,
+                              self.accept_require_score_margin, self.long_read_threshold,
+                              int(self.multi_alignments_enabled), int(self.tail),
+                              self.min_identity_x10000, int(self.exact_first))
+
+
+def _chains(chains) -> np.ndarray:
+    """kira_chain records from a CHAIN_DTYPE array or an (n, 4) integer array of
+    (ref_start, ref_end, read_start, read_end)."""
+    a = np.asarray(chains)
+    if a.dtype == A.CHAIN_DTYPE:
+        return np.ascontiguousarray(a)
+    return np.ascontiguousarray(a, np.uint32).reshape(-1, 4).view(A.CHAIN_DTYPE).reshape(-1)
+
+
 # --- pair batches --------------------------------------------------------------
 @dataclass
 class PairBatch:
@@ -404,6 +443,43 @@ class GpuContext:
             return self.wfa_batch(batch, params, max_score, text_begin_free, int(cb.used) + 16)
         self.check(rc)
         return res[:n], ops[: cb.used]
+
+    # -- ungapped prefilter and exact matches
+    def prefilter_batch(self, batch: PairBatch, chains: np.ndarray, cfg: PrefilterConfig,
+                        is_top1=None, score_margin=None, cigar_cap: int | None = None,
+                        md_cap: int | None = None):
+        """kira_gpu_prefilter_batch -> (results [PREFILTER_RESULT_DTYPE], CIGAR ops,
+        MD bytes). chains is a CHAIN_DTYPE array (window coordinates)."""
+        n = batch.n
+        ch = _chains(chains)
+        res = np.zeros(max(n, 1), A.PREFILTER_RESULT_DTYPE)
+        ccap = cigar_cap if cigar_cap is not None else max(16, 3 * n)
+        mcap = md_cap if md_cap is not None else max(64, 8 * n)
+        ops = np.zeros(max(ccap, 1), np.uint32)
+        md = np.zeros(max(mcap, 1), np.uint8)
+        cb = A.CigarBuf(A.ptr(ops), ccap, 0)
+        used = C.c_uint64()
+        top = None if is_top1 is None else np.ascontiguousarray(is_top1, np.uint8)
+        mar = None if score_margin is None else np.ascontiguousarray(score_margin, np.int32)
+        pc, pf = batch.to_c(), cfg.to_c()
+        rc = self._lib.kira_gpu_prefilter_batch(self._h, C.byref(pc), A.ptr(ch), A.ptr(top),
+                                                A.ptr(mar), C.byref(pf), A.ptr(res),
+                                                C.byref(cb), A.ptr(md), mcap, C.byref(used))
+        if rc == 9 and cigar_cap is None and md_cap is None:
+            return self.prefilter_batch(batch, chains, cfg, is_top1, score_margin,
+                                        int(cb.used) + 16, int(used.value) + 64)
+        self.check(rc)
+        return res[:n], ops[: cb.used], md[: used.value]
+
+    def exact_match_batch(self, batch: PairBatch, chains: np.ndarray) -> np.ndarray:
+        """kira_gpu_exact_match_batch -> uint8 per chain (exact_match_exists)."""
+        n = batch.n
+        ch = _chains(chains)
+        out = np.zeros(max(n, 1), np.uint8)
+        pc = batch.to_c()
+        self.check(self._lib.kira_gpu_exact_match_batch(self._h, C.byref(pc), A.ptr(ch),
+                                                        A.ptr(out)))
+        return out[:n]
 
     # -- composed verification
     def verify_batch(self, batch: PairBatch, params: VerifyParams, detail: bool = False,

@@ -269,6 +269,57 @@ def wfa_cascade(n_pairs: int = 2_000_000, seed: int = 0x3FA0, read_len: int = 15
 
 
 @dataclass
+class ChainWorkload:
+    """Reads with one chain each over one contig (window = the whole contig)."""
+    name: str
+    reads: np.ndarray
+    read_off: np.ndarray
+    read_len: np.ndarray
+    reference: np.ndarray
+    chains: np.ndarray        # (ref_start, ref_end, read_start, read_end) per read, uint32
+    is_top1: np.ndarray       # uint8
+    score_margin: np.ndarray  # int32
+
+    @property
+    def n_pairs(self) -> int:
+        return int(len(self.read_off))
+
+
+def prefilter_chains(n_chains: int = 2_000_000, seed: int = 0x9F17, read_len: int = 150,
+                     err_hi: float = 0.02, exact_frac: float = 0.3, indel_frac: float = 0.1,
+                     ref_len: int = 50_000_000, reference: np.ndarray | None = None) -> ChainWorkload:
+    """Stage-4 prefilter input: a read_len read per chain, errors U[0, err_hi] per
+    read (8:1:1) except an exact_frac of error-free reads, and one chain per read
+    over the contig. The chain is the read's co-linear anchor: read [s, e) with s
+    in [0, 40) and e in (read_len - 40, read_len] (the whole read for error-free
+    reads), ref_start = origin + s, and a ref span 1-3 bases off the read span for
+    an indel_frac of chains (the indel-suspect case)."""
+    rng = np.random.default_rng(seed)
+    ref = reference if reference is not None else random_genome(rng, ref_len)
+    n = n_chains
+    origin = rng.integers(64, len(ref) - read_len - 128, n)
+    L = read_len + 48
+    rate = np.where(rng.random(n) < exact_frac, 0.0, rng.uniform(0.0, err_hi, n))
+    reads = np.empty((n, read_len), np.uint8)
+    for a in range(0, n, 1 << 18):
+        b = min(a + (1 << 18), n)
+        frag = ref[origin[a:b, None] + np.arange(L)[None, :]]
+        reads[a:b] = _mutate_matrix(rng, frag, np.full(b - a, read_len), rate[a:b])[:, :read_len]
+    exact = rate == 0.0
+    s = np.where(exact, 0, rng.integers(0, 40, n))
+    e = np.where(exact, read_len, read_len - rng.integers(0, 40, n))
+    delta = np.where(rng.random(n) < indel_frac, rng.integers(1, 4, n) * rng.choice([-1, 1], n), 0)
+    rs = origin + s
+    chains = np.stack([rs, rs + (e - s) + delta, s, e], axis=1).astype(np.uint32)
+    return ChainWorkload(f"prefilter_{n}_{read_len}",
+                         np.concatenate([reads.reshape(-1), np.zeros(16, np.uint8)]),
+                         np.arange(n, dtype=np.uint64) * np.uint64(read_len),
+                         np.full(n, read_len, np.uint32), ref, chains,
+                         (rng.random(n) < 0.9).astype(np.uint8),
+                         rng.integers(-5, 40, n).astype(np.int32))
+
+
+@dataclass
 class ServingPool:
     """Pools the serving requests are cut from, over one shared reference."""
     reference: np.ndarray

@@ -1902,3 +1902,236 @@ extern "C" int orc_wfa_batch(uint32_t n, const uint8_t* reads, const uint64_t* r
   for (auto& t : th) t.join();
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Ungapped extension prefilter (src/alignment/prefilter.rs) and exact matches
+// (src/alignment/mod.rs:779-832). count_mismatches (kira-simd 0.1.0,
+// compare::count_mismatches) is the number of unequal bytes of two equal-length
+// slices; every call site passes equal lengths.
+// ---------------------------------------------------------------------------
+namespace {
+
+size_t pf_count_mismatches(const uint8_t* a, const uint8_t* b, size_t n) {
+  size_t c = 0;
+  for (size_t i = 0; i < n; ++i) c += a[i] != b[i];
+  return c;
+}
+
+// identity_x10000 (prefilter.rs:84-91)
+uint16_t pf_identity_x10000(size_t len, size_t mism) {
+  if (len == 0) return 0;
+  const uint64_t matches = len > mism ? len - mism : 0;
+  uint64_t prod = matches * 10000ull;
+  if (prod > UINT32_MAX) prod = UINT32_MAX;  // u32 saturating_mul
+  const uint64_t id = prod / (uint32_t)len;
+  return (uint16_t)std::min<uint64_t>(id, 65535);
+}
+
+// min_len_required (prefilter.rs:297-315)
+size_t pf_min_len_required(size_t read_len, uint16_t id, size_t mism, size_t span_slack) {
+  size_t slack = 0;
+  if (id >= 9933) slack = 15;
+  else if (id >= 9900 && mism <= 2) slack = 10;
+  else if (id >= 9870 && mism <= 3) slack = 5;
+  if (span_slack > 0) slack = std::min(slack, span_slack);
+  const size_t min_len = read_len > slack ? read_len - slack : 0;
+  const size_t floor = read_len * 85 / 100;
+  return std::max(floor, min_len);
+}
+
+// ungapped_extend (prefilter.rs:356-453): x-drop over 32-byte blocks on each
+// side of the anchor, then the sub-block remainder when the walk did not drop.
+void pf_ungapped_extend(const uint8_t* read, size_t read_len, const uint8_t* ref, size_t ref_len,
+                        const orc_chain& c, const orc_prefilter_cfg& cfg, size_t* left_out,
+                        size_t* right_out) {
+  const size_t block = 32;
+  size_t left = 0, right = 0;
+  const size_t max_left = std::min(c.read_start, c.ref_start);
+  const size_t max_right = std::min<size_t>(read_len - c.read_end, ref_len - c.ref_end);
+  for (int side = 0; side < 2; ++side) {
+    const size_t maxe = side ? max_right : max_left;
+    size_t& ext = side ? right : left;
+    int32_t score = 0, best = 0;
+    size_t i = 0;
+    bool broke = false;
+    auto offs = [&](size_t at, size_t len, size_t* ro, size_t* fo) {
+      if (side == 0) {
+        *ro = c.read_start - at - len;
+        *fo = c.ref_start - at - len;
+      } else {
+        *ro = c.read_end + at;
+        *fo = c.ref_end + at;
+      }
+    };
+    while (i + block <= maxe) {
+      size_t ro, fo;
+      offs(i, block, &ro, &fo);
+      const int32_t mism = (int32_t)pf_count_mismatches(read + ro, ref + fo, block);
+      score += ((int32_t)block - mism) * cfg.match_score - mism * cfg.mismatch;
+      if (score > best) {
+        best = score;
+        ext = i + block;
+      } else if (best - score > cfg.xdrop) {
+        broke = true;
+        break;
+      }
+      i += block;
+    }
+    if (cfg.tail && !broke && i < maxe) {
+      const size_t rem = maxe - i;
+      size_t ro, fo;
+      offs(i, rem, &ro, &fo);
+      const int32_t mism = (int32_t)pf_count_mismatches(read + ro, ref + fo, rem);
+      score += ((int32_t)rem - mism) * cfg.match_score - mism * cfg.mismatch;
+      if (score > best) ext = i + rem;
+    }
+  }
+  *left_out = left;
+  *right_out = right;
+}
+
+}  // namespace
+
+extern "C" uint32_t orc_identical_nm(const uint8_t* bases, size_t len) {
+  uint32_t nm = 0;  // md::identical_nm (md.rs:134-145)
+  for (size_t i = 0; i < len; ++i) {
+    const uint8_t u = (bases[i] >= 'a' && bases[i] <= 'z') ? bases[i] - 32 : bases[i];
+    nm += !(u == 'A' || u == 'C' || u == 'G' || u == 'T' || u == '=');
+  }
+  return nm;
+}
+
+extern "C" int orc_exact_match_exists(const uint8_t* read, size_t read_len, const uint8_t* ref,
+                                      size_t ref_len, const orc_chain* c) {
+  // exact_match_exists (mod.rs:819-832)
+  if (c->read_start != 0 || c->read_end != read_len || c->ref_end < c->ref_start ||
+      c->ref_end - c->ref_start != read_len)
+    return 0;
+  const size_t start = c->ref_start;
+  if (start + read_len > ref_len) return 0;
+  return pf_count_mismatches(read, ref + start, read_len) == 0;
+}
+
+extern "C" int orc_prefilter(const uint8_t* read, size_t read_len, const uint8_t* ref,
+                             size_t ref_len, const orc_chain* cp, int is_top1,
+                             int32_t score_margin, const orc_prefilter_cfg* cfgp,
+                             orc_prefilter_out* out, char* md, size_t md_cap) {
+  // prefilter_chain (prefilter.rs:93-294)
+  const orc_chain& c = *cp;
+  const orc_prefilter_cfg& cfg = *cfgp;
+  *out = orc_prefilter_out{};
+  auto other = [&](int code) {
+    out->result = 2;
+    out->reason = 9;
+    out->other = code;
+    return 0;
+  };
+  if (read_len == 0) return other(1);
+  if (c.read_start > c.read_end || c.ref_start > c.ref_end) return other(2);
+  const size_t anchor = c.read_end - c.read_start;
+  if (anchor == 0) return other(3);
+  if (c.read_end > read_len || c.ref_end > ref_len) return -1;
+  size_t left = 0, right = 0;
+  pf_ungapped_extend(read, read_len, ref, ref_len, c, cfg, &left, &right);
+  const size_t total = anchor + left + right;
+  if (total == 0) return other(4);
+  const int64_t urs = (int64_t)c.read_start - (int64_t)left;
+  const int64_t ufs = (int64_t)c.ref_start - (int64_t)left;
+  if (urs < 0 || ufs < 0) return other(5);
+  if ((size_t)urs + total > read_len || (size_t)ufs + total > ref_len) return other(6);
+  const size_t ham = pf_count_mismatches(read + urs, ref + ufs, total);
+  const int32_t score = (int32_t)(total > ham ? total - ham : 0) * cfg.match_score -
+                        (int32_t)ham * cfg.mismatch;
+  const uint16_t len16 = (uint16_t)std::min<size_t>(total, 65535);
+  const uint16_t mism16 = (uint16_t)std::min<size_t>(std::min(ham, total), 65535);
+  const uint16_t id = pf_identity_x10000(total, ham);
+  out->has_metrics = 1;
+  out->len = len16;
+  out->mism = mism16;
+  out->matches = len16 > mism16 ? len16 - mism16 : 0;
+  out->identity_x10000 = id;
+  out->score = score;
+  out->read_start = (uint32_t)urs;
+  out->ref_start = (uint32_t)ufs;
+  auto fallback = [&](int reason) {
+    out->result = 2;
+    out->reason = reason;
+    return 0;
+  };
+  if (total < read_len / 2) {
+    out->result = 1;
+    out->reason = 5;
+    return 0;
+  }
+  if (!cfg.accept_enable) return fallback(1);
+  if (cfg.multi_alignments_enabled) return fallback(4);
+  if (cfg.accept_only_top1 && !is_top1) return fallback(3);
+  if (read_len > cfg.long_read_threshold) return fallback(2);
+  if (cfg.accept_require_score_margin > 0 && score_margin < cfg.accept_require_score_margin) {
+    out->result = 2;
+    out->reason = 9;
+    out->other = 7;
+    return 0;
+  }
+  if (c.ref_end - c.ref_start != c.read_end - c.read_start) return fallback(8);
+  const size_t hard_max = (read_len * 5 + 149) / 150;
+  if (ham > std::min<size_t>(cfg.accept_max_mismatches, hard_max)) return fallback(6);
+  const int32_t floor = cfg.min_id_override >= 0 ? cfg.min_id_override : cfg.identity_floor;
+  if ((int32_t)id < floor) return fallback(7);
+  if (total < pf_min_len_required(read_len, id, ham, cfg.accept_span_slack)) return fallback(5);
+  // build_ungapped_alignment (prefilter.rs:455-517): [S] M [S], MdBuilder::columns.
+  out->result = 0;
+  out->reason = 0;
+  const size_t span = len16, rs = (size_t)urs, re = rs + span;
+  if (rs > 0) out->cigar[out->n_cigar++] = ((uint32_t)rs << 4) | 4u;
+  out->cigar[out->n_cigar++] = ((uint32_t)span << 4) | 0u;
+  if (re < read_len) out->cigar[out->n_cigar++] = ((uint32_t)(read_len - re) << 4) | 4u;
+  const uint32_t op = ((uint32_t)span << 4) | 0u;
+  uint32_t nm = 0;
+  const uint32_t mdlen =
+      orc_nm_md(read, read_len, ref, ref_len, rs, (size_t)ufs, &op, 1, &nm, nullptr, 0);
+  if (md && mdlen <= md_cap)
+    orc_nm_md(read, read_len, ref, ref_len, rs, (size_t)ufs, &op, 1, &nm, md, (uint32_t)md_cap);
+  out->nm = nm;
+  return (int)mdlen;
+}
+
+extern "C" int orc_prefilter_batch(uint32_t n, const uint8_t* reads, const uint64_t* read_off,
+                                   const uint32_t* read_len, const uint8_t* wins,
+                                   const uint64_t* win_off, const uint32_t* win_len,
+                                   const orc_chain* chains, const uint8_t* is_top1,
+                                   const int32_t* score_margin, const orc_prefilter_cfg* cfg,
+                                   int exact_first, int nthreads, orc_prefilter_out* out,
+                                   char* md, uint32_t md_stride) {
+  std::atomic<uint32_t> next{0};
+  std::atomic<int> bad{0};
+  auto work = [&]() {
+    for (;;) {
+      const uint32_t i = next.fetch_add(64);
+      if (i >= n) return;
+      for (uint32_t p = i; p < std::min(n, i + 64); ++p) {
+        const uint8_t* rd = reads + read_off[p];
+        const uint8_t* wn = wins + win_off[p];
+        char* m = md ? md + (size_t)p * md_stride : nullptr;
+        if (exact_first && orc_exact_match_exists(rd, read_len[p], wn, win_len[p], chains + p)) {
+          out[p] = orc_prefilter_out{};
+          out[p].result = 3;
+          out[p].nm = orc_identical_nm(rd, read_len[p]);
+          out[p].n_cigar = 1;
+          out[p].cigar[0] = read_len[p] << 4;
+          if (m) snprintf(m, md_stride, "%u", read_len[p]);
+          continue;
+        }
+        if (orc_prefilter(rd, read_len[p], wn, win_len[p], chains + p,
+                          is_top1 ? is_top1[p] : 1, score_margin ? score_margin[p] : INT32_MAX,
+                          cfg, out + p, m, m ? md_stride : 0) < 0)
+          bad = 1;
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < std::max(nthreads, 1); ++t) th.emplace_back(work);
+  work();
+  for (auto& t : th) t.join();
+  return bad ? -1 : 0;
+}

@@ -200,6 +200,50 @@ int orc_wfa_batch(uint32_t n, const uint8_t* reads, const uint64_t* read_off,
                   int32_t* score, uint32_t* text_start, uint32_t* text_end, uint32_t* n_cigar,
                   uint32_t* cigar, uint32_t cap_per_pair);
 
+/* Ungapped extension prefilter (src/alignment/prefilter.rs:93-453) and the
+ * exact-match fast path (src/alignment/mod.rs:779-832) for one chain. */
+typedef struct orc_chain {
+  uint32_t ref_start, ref_end, read_start, read_end;
+} orc_chain;
+typedef struct orc_prefilter_cfg {
+  int32_t match_score, mismatch, xdrop;
+  int32_t accept_enable, accept_only_top1;
+  uint32_t accept_span_slack;
+  int32_t identity_floor;        /* (accept_min_identity * 100).round() as u16 */
+  uint32_t accept_max_mismatches;
+  int32_t accept_require_score_margin;
+  uint32_t long_read_threshold;
+  int32_t multi_alignments_enabled;
+  int32_t tail;                  /* KIRA_UNGAP_TAIL (default 1) */
+  int32_t min_id_override;       /* KIRA_UNGAP_MINID, < 0: unset */
+} orc_prefilter_cfg;
+typedef struct orc_prefilter_out {
+  int32_t result;  /* 0 Accept, 1 Reject, 2 Fallback */
+  int32_t reason;  /* PrefilterReason::idx() */
+  int32_t other;   /* Other(..): 1 read_len0 2 non_monotonic 3 anchor0 4 span0 5 neg_start 6 span_oob 7 margin_fail */
+  int32_t has_metrics;
+  uint32_t len, mism, matches, identity_x10000;
+  int32_t score;
+  uint32_t read_start, ref_start;
+  uint32_t nm, n_cigar, cigar[3];  /* Accept: build_ungapped_alignment */
+} orc_prefilter_out;
+/* Returns the MD length (Accept), written to md when md_cap allows; -1 when the
+ * chain lies outside the read or reference (the reference panics there). */
+int orc_prefilter(const uint8_t* read, size_t read_len, const uint8_t* ref, size_t ref_len,
+                  const orc_chain* chain, int is_top1, int32_t score_margin,
+                  const orc_prefilter_cfg* cfg, orc_prefilter_out* out, char* md, size_t md_cap);
+int orc_exact_match_exists(const uint8_t* read, size_t read_len, const uint8_t* ref,
+                           size_t ref_len, const orc_chain* chain);
+uint32_t orc_identical_nm(const uint8_t* bases, size_t len);
+/* Stage-4 order over a batch on host threads: exact_match_exists first when
+ * exact_first (result 3), else orc_prefilter; md_stride bytes of MD per chain. */
+int orc_prefilter_batch(uint32_t n, const uint8_t* reads, const uint64_t* read_off,
+                        const uint32_t* read_len, const uint8_t* wins, const uint64_t* win_off,
+                        const uint32_t* win_len, const orc_chain* chains, const uint8_t* is_top1,
+                        const int32_t* score_margin, const orc_prefilter_cfg* cfg,
+                        int exact_first, int nthreads, orc_prefilter_out* out, char* md,
+                        uint32_t md_stride);
+
 #ifdef __cplusplus
 }
 #endif

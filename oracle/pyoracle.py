@@ -56,6 +56,28 @@ class OrcWfaCfg(C.Structure):
                  "adaptive_drop", "text_begin_free", "traceback")]
 
 
+class OrcChain(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("ref_start", "ref_end", "read_start", "read_end")]
+
+
+class OrcPrefilterCfg(C.Structure):
+    _fields_ = [("match_score", C.c_int32), ("mismatch", C.c_int32), ("xdrop", C.c_int32),
+                ("accept_enable", C.c_int32), ("accept_only_top1", C.c_int32),
+                ("accept_span_slack", C.c_uint32), ("identity_floor", C.c_int32),
+                ("accept_max_mismatches", C.c_uint32),
+                ("accept_require_score_margin", C.c_int32),
+                ("long_read_threshold", C.c_uint32), ("multi_alignments_enabled", C.c_int32),
+                ("tail", C.c_int32), ("min_id_override", C.c_int32)]
+
+
+class OrcPrefilterOut(C.Structure):
+    _fields_ = [("result", C.c_int32), ("reason", C.c_int32), ("other", C.c_int32),
+                ("has_metrics", C.c_int32), ("len", C.c_uint32), ("mism", C.c_uint32),
+                ("matches", C.c_uint32), ("identity_x10000", C.c_uint32), ("score", C.c_int32),
+                ("read_start", C.c_uint32), ("ref_start", C.c_uint32), ("nm", C.c_uint32),
+                ("n_cigar", C.c_uint32), ("cigar", C.c_uint32 * 3)]
+
+
 def build() -> None:
     subprocess.check_call(["make", "-s", "-C", _HERE, "all"])
 
@@ -136,6 +158,17 @@ def lib():
         L.orc_myers_batch.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, vp, C.c_uint32, C.c_int,
                                       vp, vp]
         L.orc_sieve_batch.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, vp, C.c_int, vp, vp, vp]
+        L.orc_prefilter.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t,
+                                    C.POINTER(OrcChain), C.c_int, C.c_int32,
+                                    C.POINTER(OrcPrefilterCfg), C.POINTER(OrcPrefilterOut),
+                                    C.c_char_p, C.c_size_t]
+        L.orc_prefilter_batch.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                          C.POINTER(OrcPrefilterCfg), C.c_int, C.c_int, vp, vp,
+                                          C.c_uint32]
+        L.orc_exact_match_exists.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t,
+                                             C.POINTER(OrcChain)]
+        L.orc_identical_nm.restype = C.c_uint32
+        L.orc_identical_nm.argtypes = [C.c_char_p, C.c_size_t]
         L.orc_wfa.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t,
                               C.POINTER(OrcWfaCfg), vp, vp, vp, vp, C.c_uint32, vp]
         L.orc_wfa_batch.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, vp, C.POINTER(OrcWfaCfg),
@@ -531,3 +564,99 @@ def wfa_batch(reads: np.ndarray, read_off, read_len, wins: np.ndarray, win_off, 
                         threads or os.cpu_count() or 1, p(found), p(score), p(ts), p(te),
                         p(nc), p(cig), cap_per_pair)
     return found, score, ts, te, nc, cig
+
+
+# ---------------------------------------------------------------------------
+# Ungapped prefilter (src/alignment/prefilter.rs) and exact matches (mod.rs:779-832)
+# ---------------------------------------------------------------------------
+PREFILTER_REASONS = ("accept", "disabled", "not_short_preset", "not_top1",
+                     "max_alignments_not_one", "span_too_small", "mism_too_high", "id_too_low",
+                     "indel_suspect", "other")
+PREFILTER_OTHER = (None, "read_len0", "non_monotonic", "anchor0", "span0", "neg_start",
+                   "span_oob", "margin_fail")
+
+
+def identity_floor(accept_min_identity: float) -> int:
+    """(accept_min_identity * 100.0).round() as u16 (f32 arithmetic, saturating)."""
+    v = float(np.float32(accept_min_identity) * np.float32(100.0))
+    if v != v:
+        return 0
+    r = np.floor(abs(v) + 0.5) * (1 if v >= 0 else -1)
+    return int(min(max(r, 0), 65535))
+
+
+def prefilter_cfg(match_score=1, mismatch=4, xdrop=50, accept_enable=True, accept_only_top1=True,
+                  accept_span_slack=5, accept_min_identity=98.0, accept_max_mismatches=2,
+                  accept_require_score_margin=0, long_read_threshold=300,
+                  multi_alignments_enabled=False, tail=True, min_id_override=None):
+    return OrcPrefilterCfg(match_score, mismatch, xdrop, int(accept_enable),
+                           int(accept_only_top1), accept_span_slack,
+                           identity_floor(accept_min_identity), accept_max_mismatches,
+                           accept_require_score_margin, long_read_threshold,
+                           int(multi_alignments_enabled), int(tail),
+                           -1 if min_id_override is None else min_id_override)
+
+
+@dataclass
+class PrefilterRes:
+    result: str            # accept | reject | fallback
+    reason: str
+    metrics: tuple | None  # (len, mism, matches, identity_x10000, score, read_start, ref_start)
+    nm: int = 0
+    md: str = ""
+    cigar: list = None
+
+
+def prefilter(read: bytes, ref: bytes, chain, c: OrcPrefilterCfg, is_top1=True,
+              score_margin=2**31 - 1) -> PrefilterRes:
+    """prefilter_chain (prefilter.rs:93-294); chain = (ref_start, ref_end, read_start, read_end)."""
+    ch = OrcChain(*chain)
+    out = OrcPrefilterOut()
+    md = C.create_string_buffer(len(read) * 4 + 32)
+    n = lib().orc_prefilter(read, len(read), ref, len(ref), C.byref(ch), int(is_top1),
+                            score_margin, C.byref(c), C.byref(out), md, len(md))
+    if n < 0:
+        raise ValueError("chain outside the read or reference")
+    reason = PREFILTER_REASONS[out.reason]
+    if out.reason == 9:
+        reason = PREFILTER_OTHER[out.other]
+    met = None
+    if out.has_metrics:
+        met = (out.len, out.mism, out.matches, out.identity_x10000, out.score, out.read_start,
+               out.ref_start)
+    res = PrefilterRes(("accept", "reject", "fallback")[out.result], reason, met)
+    if out.result == 0:
+        res.nm = out.nm
+        res.md = md.raw[:n].decode()
+        res.cigar = decode_cigar(list(out.cigar)[: out.n_cigar])
+    return res
+
+
+def exact_match_exists(read: bytes, ref: bytes, chain) -> bool:
+    return bool(lib().orc_exact_match_exists(read, len(read), ref, len(ref),
+                                             C.byref(OrcChain(*chain))))
+
+
+def identical_nm(bases: bytes) -> int:
+    return int(lib().orc_identical_nm(bases, len(bases)))
+
+
+def prefilter_batch(reads, read_off, read_len, wins, win_off, win_len, chains, is_top1,
+                    score_margin, c: OrcPrefilterCfg, exact_first=True, threads=0,
+                    md_stride=0):
+    """orc_prefilter_batch on host threads -> array of OrcPrefilterOut (and MD bytes)."""
+    n = len(read_len)
+    arrs = [np.ascontiguousarray(a, dt) for a, dt in
+            ((reads, np.uint8), (read_off, np.uint64), (read_len, np.uint32), (wins, np.uint8),
+             (win_off, np.uint64), (win_len, np.uint32), (chains, np.uint32))]
+    top = None if is_top1 is None else np.ascontiguousarray(is_top1, np.uint8)
+    mar = None if score_margin is None else np.ascontiguousarray(score_margin, np.int32)
+    out = (OrcPrefilterOut * max(n, 1))()
+    md = np.zeros(max(n * md_stride, 1), np.uint8) if md_stride else None
+    p = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    rc = lib().orc_prefilter_batch(n, *[p(a) for a in arrs], p(top), p(mar), C.byref(c),
+                                   int(exact_first), threads or os.cpu_count() or 1, out,
+                                   p(md), md_stride)
+    if rc < 0:
+        raise ValueError("a chain lies outside its read or window")
+    return out, md
