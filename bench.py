@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--segments", type=int, default=20_000, help="gapfill: segments per call")
     ap.add_argument("--wfa-pairs", type=int, default=1_000_000, help="wfa: pairs per call")
     ap.add_argument("--wfa-drop", type=int, default=-1, help="wfa: adaptive drop (< 0 exact)")
+    ap.add_argument("--chains", type=int, default=2_000_000, help="prefilter: chains per call")
     ap.add_argument("--wfa-lanes", type=int, default=0,
                     help="wfa: lanes per pair (8, 16, 32; 0 = library default)")
     return ap.parse_args()
@@ -418,7 +419,7 @@ def run_prefilter(args, rank, local, world):
     if rank != 0:
         return
     torch.cuda.set_device(local)
-    w = synth.prefilter_chains()
+    w = synth.prefilter_chains(args.chains)
     n = w.n_pairs
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
     b = PairBatch(pin(w.reads), pin(w.read_off), pin(w.read_len), None,

@@ -9,6 +9,11 @@
  *   - banded affine Smith-Waterman + CIGAR   (src/alignment/mod.rs:1331-1771)
  *   - full-window batch SW (align_batch_simd) (src/alignment/mod.rs:1111-1169,1846-2135,
  *                                            src/alignment/sw_int8_vnni.rs)
+ * and the steps on either side of it:
+ *   - wavefront alignment (WFA)              (src/alignment/wfa.rs)
+ *   - exact matches + ungapped prefilter     (src/alignment/mod.rs:779-832,
+ *                                            src/alignment/prefilter.rs)
+ *   - NM / MD:Z from the CIGARs              (src/alignment/md.rs)
  *
  * Conventions
  *   - Every entry point returns an int status (kira_status). 0 is success.
