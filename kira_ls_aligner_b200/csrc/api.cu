@@ -2,7 +2,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -33,6 +37,62 @@ enum BufId {
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+};
+
+// Host threads a context keeps for its per-pair host checks: run() hands every
+// worker the same function once and returns at once; wait() returns when all of
+// them finished it.
+class HostPool {
+ public:
+  explicit HostPool(int n) {
+    for (int i = 0; i < n; ++i) th_.emplace_back([this] { loop(); });
+  }
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  void run(std::function<void()> fn) {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      job_ = std::move(fn);
+      ++gen_;
+      busy_ = (int)th_.size();
+    }
+    cv_.notify_all();
+  }
+  void wait() {
+    std::unique_lock<std::mutex> g(mu_);
+    done_.wait(g, [&] { return busy_ == 0; });
+  }
+
+ private:
+  void loop() {
+    uint64_t seen = 0;
+    for (;;) {
+      std::function<void()> f;
+      {
+        std::unique_lock<std::mutex> g(mu_);
+        cv_.wait(g, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+        f = job_;
+      }
+      f();
+      std::lock_guard<std::mutex> g(mu_);
+      if (--busy_ == 0) done_.notify_all();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_;
+  std::function<void()> job_;
+  uint64_t gen_ = 0;
+  int busy_ = 0;
+  bool stop_ = false;
 };
 
 }  // namespace
@@ -68,6 +128,9 @@ struct kira_ctx {
   uint4* ref_planes = nullptr;  // 2-bit + valid planes of the resident reference
   uint64_t ref_len = 0;
   std::shared_ptr<void> ref_owner;  // frees ref_dev / ref_planes with the last holder
+  std::unique_ptr<HostPool> pool;   // host threads of the chunked path's pair checks
+  kira_ctx* twin = nullptr;          // second compute stream + scratch of the chunked path
+  std::vector<cudaEvent_t> ev_pack, ev_scan;  // per chunk: planes packed / CIGARs placed
   DevBuf bufs[B_COUNT];
 };
 
@@ -376,6 +439,8 @@ struct ChunkMode {
   bool planes_ready = false;
   bool first = true;
   bool accumulate = false;
+  cudaEvent_t before_scan = nullptr;  // the CIGAR scan waits for it (the previous chunk's)
+  cudaEvent_t after_scan = nullptr;   // recorded once this chunk's CIGARs are placed
 };
 
 // The composed path on device buffers, enqueued on `st`.
@@ -441,7 +506,9 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
                               ctx->profile ? ctx->ev[3] : nullptr));
   if (ctx->profile) ctx->ev_recorded = 4;
   mark(ctx, 4, st);
+  if (cm.before_scan) KIRA_CUDA(cudaStreamWaitEvent(st, cm.before_scan, 0));
   rc = finish_cigars(ctx, n, out, ncig, B, ops, cap, total_dev, st, cm.accumulate);
+  if (!rc && cm.after_scan) KIRA_CUDA(cudaEventRecord(cm.after_scan, st));
   mark(ctx, 5, st);
   return rc;
 }
@@ -636,53 +703,131 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
   const bool host_w = P.win_seq != nullptr;
   if (!host_w && !ctx->ref_dev) return fail(ctx, KIRA_ERR_INVALID, "no resident reference uploaded");
   const uint64_t wlim = host_w ? P.win_seq_bytes : ctx->ref_len;
-  // Host checks (bounds as upload_pairs, maxes as host_maxes) of every chunk.
+  // Host checks (bounds as upload_pairs, maxes as host_maxes) of every chunk, in
+  // sub-ranges of 2^14 pairs (about 50 us of reading each) spread over the
+  // context's host threads in chunk order; this thread helps until the chunk it
+  // needs next is checked, so the first chunk's copies start after a fraction of
+  // the batch was read.
   struct Scan {
     Maxes mx;
     uint64_t rend = 0, wend = 0;
     int64_t bad = -1;  // first offending pair
     int kind = 0;      // 1: read outside read_seq, 2: window outside
   };
-  std::vector<Scan> scans(nch);
-  auto scan_chunk = [&](uint32_t c) {
-    Scan& sc = scans[c];
-    const uint32_t lo = c * chunk, hi = std::min(n, lo + chunk);
-    for (uint32_t i = lo; i < hi; ++i) {
+  const int32_t cfg_band = std::max(p.sw.bandwidth, 1);
+  auto scan_range = [&](uint32_t lo, uint32_t hi, Scan& sc) {
+    uint64_t rend = 0, wend = 0;
+    uint32_t q = 0, w = 0, band = 0;
+    for (uint32_t i = lo; i < hi; ++i) {  // branch-free maxima
       const uint64_t re = P.read_off[i] + P.read_len[i], we = P.win_off[i] + P.win_len[i];
-      if (sc.bad < 0 && (re > P.read_seq_bytes || we > wlim)) {
-        sc.bad = i;
-        sc.kind = re > P.read_seq_bytes ? 1 : 2;
+      rend = re > rend ? re : rend;
+      wend = we > wend ? we : wend;
+      q = P.read_len[i] > q ? P.read_len[i] : q;
+      w = P.win_len[i] > w ? P.win_len[i] : w;
+    }
+    if (P.bandwidth) {
+      for (uint32_t i = lo; i < hi; ++i) {
+        const uint32_t b = (uint32_t)std::max(P.bandwidth[i], 1);
+        band = b > band ? b : band;
       }
-      sc.rend = std::max(sc.rend, re);
-      sc.wend = std::max(sc.wend, we);
-      sc.mx.q = std::max(sc.mx.q, P.read_len[i]);
-      sc.mx.w = std::max(sc.mx.w, P.win_len[i]);
-      const int32_t b = P.bandwidth ? P.bandwidth[i] : p.sw.bandwidth;
-      sc.mx.band = std::max(sc.mx.band, (uint32_t)std::max(b, 1));
+    } else {
+      band = (uint32_t)cfg_band;
+    }
+    sc.rend = rend, sc.wend = wend, sc.mx.q = q, sc.mx.w = w, sc.mx.band = band;
+    if (rend > P.read_seq_bytes || wend > wlim) {
+      for (uint32_t i = lo; i < hi; ++i) {
+        const uint64_t re = P.read_off[i] + P.read_len[i], we = P.win_off[i] + P.win_len[i];
+        if (re > P.read_seq_bytes || we > wlim) {
+          sc.bad = i;
+          sc.kind = re > P.read_seq_bytes ? 1 : 2;
+          break;
+        }
+      }
     }
   };
-  // Chunk 0 is checked here and enqueued at once; host threads check the others
-  // meanwhile, each chunk's enqueue waiting for its own check.
-  std::vector<std::future<void>> pending(nch);
-  for (uint32_t c = 1; c < nch; ++c) pending[c] = std::async(std::launch::async, scan_chunk, c);
-  scan_chunk(0);
-  auto checked = [&](uint32_t c) -> int {
-    if (c && pending[c].valid()) pending[c].get();
-    if (scans[c].bad < 0) return KIRA_OK;
-    return fail(ctx, KIRA_ERR_INVALID, "pair %lld: %s outside %s", (long long)scans[c].bad,
-                scans[c].kind == 1 ? "read" : "window",
-                scans[c].kind == 1 ? "read_seq" : (host_w ? "win_seq" : "the resident reference"));
+  constexpr uint32_t kSub = 1u << 14;
+  std::vector<uint32_t> sub_lo, sub_chunk, first_sub(nch + 1);
+  for (uint32_t c = 0; c < nch; ++c) {
+    first_sub[c] = (uint32_t)sub_lo.size();
+    const uint32_t lo = c * chunk, hi = std::min(n, lo + chunk);
+    for (uint32_t x = lo; x < hi; x += kSub) sub_lo.push_back(x), sub_chunk.push_back(c);
+  }
+  first_sub[nch] = (uint32_t)sub_lo.size();
+  const uint32_t nsub = (uint32_t)sub_lo.size();
+  std::vector<Scan> subs(nsub);
+  std::unique_ptr<std::atomic<uint32_t>[]> left(new std::atomic<uint32_t>[nch]);
+  for (uint32_t c = 0; c < nch; ++c) left[c].store(first_sub[c + 1] - first_sub[c]);
+  std::atomic<uint32_t> next{0};
+  auto take_one = [&]() -> bool {
+    const uint32_t sidx = next.fetch_add(1, std::memory_order_relaxed);
+    if (sidx >= nsub) return false;
+    const uint32_t c = sub_chunk[sidx];
+    const uint32_t hi = std::min(std::min(n, c * chunk + chunk), sub_lo[sidx] + kSub);
+    scan_range(sub_lo[sidx], hi, subs[sidx]);
+    left[c].fetch_sub(1, std::memory_order_release);
+    return true;
   };
-  // Every check finishes before this call returns (the futures join on destruction).
+  if (!ctx->pool) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    ctx->pool.reset(new HostPool((int)std::min(15u, std::max(2u, hw) - 1u)));
+  }
+  ctx->pool->run([&] {
+    while (take_one()) {
+    }
+  });
+  // Every host check finishes before this call returns, on every return path.
+  struct JoinChecks {
+    HostPool* pool;
+    std::atomic<uint32_t>* next;
+    uint32_t nsub;
+    ~JoinChecks() {
+      next->store(nsub);
+      pool->wait();
+    }
+  } join_checks{ctx->pool.get(), &next, nsub};
+  std::vector<Scan> scans(nch);
+  auto checked = [&](uint32_t c) -> int {
+    while (left[c].load(std::memory_order_acquire) != 0)
+      if (!take_one()) std::this_thread::yield();
+    Scan& sc = scans[c];
+    for (uint32_t x = first_sub[c]; x < first_sub[c + 1]; ++x) {
+      const Scan& u = subs[x];
+      sc.rend = std::max(sc.rend, u.rend);
+      sc.wend = std::max(sc.wend, u.wend);
+      sc.mx.q = std::max(sc.mx.q, u.mx.q);
+      sc.mx.w = std::max(sc.mx.w, u.mx.w);
+      sc.mx.band = std::max(sc.mx.band, u.mx.band);
+      if (sc.bad < 0 && u.bad >= 0) sc.bad = u.bad, sc.kind = u.kind;
+    }
+    if (sc.bad < 0) return KIRA_OK;
+    return fail(ctx, KIRA_ERR_INVALID, "pair %lld: %s outside %s", (long long)sc.bad,
+                sc.kind == 1 ? "read" : "window",
+                sc.kind == 1 ? "read_seq" : (host_w ? "win_seq" : "the resident reference"));
+  };
   if (!ctx->h2d) KIRA_CUDA(cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
   if (!ctx->d2h) KIRA_CUDA(cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
   while (ctx->ev_up.size() < nch + 1) {
-    cudaEvent_t a = nullptr, b = nullptr;
-    KIRA_CUDA(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
-    KIRA_CUDA(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
-    ctx->ev_up.push_back(a);
-    ctx->ev_comp.push_back(b);
+    cudaEvent_t e[4] = {};
+    for (auto& x : e) KIRA_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    ctx->ev_up.push_back(e[0]);
+    ctx->ev_comp.push_back(e[1]);
+    ctx->ev_pack.push_back(e[2]);
+    ctx->ev_scan.push_back(e[3]);
   }
+  // Consecutive chunks alternate between this context's stream and a twin's (own
+  // stream and scratch, same reference and settings), so one chunk's row-serial
+  // DP / traceback tail overlaps the next chunk's sieve and Myers. Planes are
+  // packed in chunk order (each chunk waits for the previous chunk's packing) and
+  // the CIGAR scans run in chunk order (the running total in total_dev).
+  if (!ctx->twin) {
+    int rc = kira_gpu_init(ctx->device, &ctx->twin);
+    if (rc) return fail(ctx, rc, "second compute stream of the chunked path");
+  }
+  kira_ctx* twin = ctx->twin;
+  std::copy(std::begin(ctx->tuned_shape), std::end(ctx->tuned_shape), twin->tuned_shape);
+  twin->trace_budget = ctx->trace_budget;
+  ctx_share_reference(twin, ctx);
+  kira_ctx* const cxs[2] = {ctx, twin};
   // Full-size buffers first, on the compute stream; the copy stream starts after.
   KIRA_DBUF(rs, uint8_t, B_READ_SEQ, P.read_seq_bytes);
   KIRA_DBUF(rp, uint4, B_READ_PLANES, plane_blocks(P.read_seq_bytes));
@@ -724,11 +869,13 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
   KIRA_CUDA(cudaMemsetAsync(total_dev, 0, 8, st));
   KIRA_CUDA(cudaEventRecord(ctx->ev_up[nch], st));
   KIRA_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->ev_up[nch], 0));
+  KIRA_CUDA(cudaStreamWaitEvent(twin->stream, ctx->ev_up[nch], 0));
   uint64_t rdone = 0, wdone = 0;
   for (uint32_t c = 0; c < nch; ++c) {
     if (int rc = checked(c)) {
       // Nothing of chunk c or later is enqueued; let the queued chunks finish first.
       cudaStreamSynchronize(st);
+      cudaStreamSynchronize(twin->stream);
       cudaStreamSynchronize(ctx->d2h);
       return rc;
     }
@@ -749,31 +896,42 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
     if (host_w && wneed > wdone)
       KIRA_CUDA(cudaMemcpyAsync(ws + wdone, P.win_seq + wdone, wneed - wdone,
                                 cudaMemcpyHostToDevice, up));
+    kira_ctx* const cx = cxs[c & 1];
+    cudaStream_t cs = cx->stream;
     KIRA_CUDA(cudaEventRecord(ctx->ev_up[c], up));
-    KIRA_CUDA(cudaStreamWaitEvent(st, ctx->ev_up[c], 0));
+    KIRA_CUDA(cudaStreamWaitEvent(cs, ctx->ev_up[c], 0));
+    if (c) KIRA_CUDA(cudaStreamWaitEvent(cs, ctx->ev_pack[c - 1], 0));
     // Planes of the newly arrived range, from its first (possibly partial) block.
     if (rneed > rdone) {
       const uint64_t b0 = rdone / 32, nb = plane_blocks(rneed);
-      KIRA_CUDA(launch_pack_planes(rs + b0 * 32, rneed - b0 * 32, rp + b0, nb - b0, ctx->sms, st));
+      KIRA_CUDA(launch_pack_planes(rs + b0 * 32, rneed - b0 * 32, rp + b0, nb - b0, ctx->sms, cs));
       rdone = rneed;
     }
     if (host_w && wneed > wdone) {
       const uint64_t b0 = wdone / 32, nb = plane_blocks(wneed);
-      KIRA_CUDA(launch_pack_planes(ws + b0 * 32, wneed - b0 * 32, wp + b0, nb - b0, ctx->sms, st));
+      KIRA_CUDA(launch_pack_planes(ws + b0 * 32, wneed - b0 * 32, wp + b0, nb - b0, ctx->sms, cs));
       wdone = wneed;
     }
+    KIRA_CUDA(cudaEventRecord(ctx->ev_pack[c], cs));
     DevPairs D{m,       rs,      ro + lo, rl + lo, ws,
                wo + lo, wl + lo, bo ? bo + lo : nullptr, ab ? ab + lo : nullptr,
                bw ? bw + lo : nullptr, rp, wp};
     ChunkMode cm;
     cm.planes_ready = true;
-    cm.first = c == 0;
+    cm.first = c < 2;  // each context's first chunk resets its flag word
     cm.accumulate = true;
-    int rc = verify_pipeline(ctx, D, mx, p, P.read_seq_bytes, P.win_seq_bytes, !host_w, dout + lo,
-                             ops, cigar->cap, total_dev, ddet ? ddet + lo : nullptr, cells_dev, st,
+    cm.before_scan = c ? ctx->ev_scan[c - 1] : nullptr;
+    cm.after_scan = ctx->ev_scan[c];
+    int rc = verify_pipeline(cx, D, mx, p, P.read_seq_bytes, P.win_seq_bytes, !host_w, dout + lo,
+                             ops, cigar->cap, total_dev, ddet ? ddet + lo : nullptr, cells_dev, cs,
                              cm);
-    if (rc) return rc;
-    KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], st));
+    if (rc) {
+      if (cx != ctx) ctx->last_error = cx->last_error;
+      cudaStreamSynchronize(st);
+      cudaStreamSynchronize(twin->stream);
+      return rc;
+    }
+    KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], cs));
     KIRA_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->ev_comp[c], 0));
     KIRA_CUDA(cudaMemcpyAsync(out + lo, dout + lo, sizeof(kira_sw_result) * m,
                               cudaMemcpyDeviceToHost, ctx->d2h));
@@ -783,13 +941,17 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
   }
   uint64_t total = 0;
   unsigned long long hcells = 0;
-  uint32_t flags[4];
+  uint32_t flags[4] = {}, flags2[4] = {};
   KIRA_CUDA(cudaMemcpyAsync(&total, total_dev, 8, cudaMemcpyDeviceToHost, ctx->d2h));
   KIRA_CUDA(cudaMemcpyAsync(&hcells, cells_dev, 8, cudaMemcpyDeviceToHost, ctx->d2h));
   KIRA_CUDA(cudaMemcpyAsync(flags, ctx->bufs[B_COUNTERS].p, 16, cudaMemcpyDeviceToHost, ctx->d2h));
+  if (nch > 1)
+    KIRA_CUDA(cudaMemcpyAsync(flags2, twin->bufs[B_COUNTERS].p, 16, cudaMemcpyDeviceToHost,
+                              ctx->d2h));
   KIRA_CUDA(cudaStreamSynchronize(ctx->d2h));
   cigar->used = total;
   if (cells) *cells = hcells;
+  flags[2] |= flags2[2];
   if (flags[2] & 1u) return fail(ctx, KIRA_ERR_RUNTIME, "CIGAR slot overflow");
   if (flags[2] & 6u) return fail(ctx, KIRA_ERR_INVALID, "a pair exceeded the launch's length bounds");
   if (total > cigar->cap)
@@ -908,6 +1070,7 @@ int kira_gpu_init(int device, kira_ctx** out) {
 
 void kira_gpu_destroy(kira_ctx* ctx) {
   if (!ctx) return;
+  if (ctx->twin) kira_gpu_destroy(ctx->twin);
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   for (auto& b : ctx->bufs)
@@ -919,6 +1082,8 @@ void kira_gpu_destroy(kira_ctx* ctx) {
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   for (auto e : ctx->ev_up) cudaEventDestroy(e);
   for (auto e : ctx->ev_comp) cudaEventDestroy(e);
+  for (auto e : ctx->ev_pack) cudaEventDestroy(e);
+  for (auto e : ctx->ev_scan) cudaEventDestroy(e);
   if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
   if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
   cudaStreamDestroy(ctx->stream);
@@ -1764,9 +1929,10 @@ int kira_gpu_verify_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_ver
   if (cells) *cells = 0;
   if (P.n == 0) return KIRA_OK;
   cudaSetDevice(ctx->device);
-  // Chunks run one after another on the compute stream and each pays the DP and
-  // traceback latency of its longest pair, so a few large chunks overlap the
-  // copies best: by default a quarter of the batch, at least 2^18 pairs.
+  // Chunks alternate between two compute streams so each chunk's row-serial DP and
+  // traceback tail overlaps the next chunk; a few large chunks still do best
+  // (each pays some fixed launch and tail cost): by default a quarter of the
+  // batch, at least 2^18 pairs.
   const uint64_t chunk = ctx->chunk_pairs < 0
                              ? std::max<uint64_t>(1u << 18, (P.n + 3ull) / 4)
                              : (uint64_t)ctx->chunk_pairs;

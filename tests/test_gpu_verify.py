@@ -164,3 +164,30 @@ def test_chunked_host_path_rejects_out_of_range_pair(ctx):
         ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, -1))
     ref = ctx.verify_batch(good, params)
     assert np.array_equal(res, ref[0]) and np.array_equal(ops, ref[1])
+
+
+def test_chunked_host_checks_in_sub_ranges(ctx):
+    # Chunks of 140k pairs are checked in 2^14-pair sub-ranges on the context's host
+    # threads, and alternate between two compute streams: results equal the
+    # one-shot path, and a bad pair in the middle of a later chunk still fails the
+    # call with InvalidArgument.
+    from kira_ls_aligner_b200 import InvalidArgument, PairBatch, VerifyParams, _abi, synth
+    w = synth.make_workload("s", 80_000, 2_000_000, cands=4, sub_lo=0.0, sub_hi=0.03, seed=79)
+    ctx.ref_upload(w.reference)
+    b = PairBatch(w.reads, w.read_off, w.read_len, None, w.win_off, w.win_len)
+    params = VerifyParams(sieve_threshold=12, myers_k=8)
+    L = _abi.lib()
+    try:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, 0))
+        one = ctx.verify_batch(b, params)
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, 140_000))
+        chunked = ctx.verify_batch(b, params)
+        woff = w.win_off.copy()
+        woff[140_000 + 70_000] = len(w.reference)
+        bad = PairBatch(w.reads, w.read_off, w.read_len, None, woff, w.win_len)
+        with pytest.raises(InvalidArgument) as ei:
+            ctx.verify_batch(bad, params)
+        assert "pair 210000" in str(ei.value)
+    finally:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, -1))
+    assert np.array_equal(one[0], chunked[0]) and np.array_equal(one[1], chunked[1])
