@@ -254,14 +254,58 @@ struct Maxes {
   uint32_t q = 0, w = 0, band = 0;
 };
 
-Maxes host_maxes(const kira_pairs& P, int32_t cfg_band) {
-  Maxes m;
-  for (uint32_t i = 0; i < P.n; ++i) {
-    m.q = std::max(m.q, P.read_len[i]);
-    m.w = std::max(m.w, P.win_len[i]);
-    const int32_t b = P.bandwidth ? P.bandwidth[i] : cfg_band;
-    m.band = std::max(m.band, (uint32_t)std::max(b, 1));
+HostPool* host_pool(kira_ctx* ctx) {
+  if (!ctx->pool) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    ctx->pool.reset(new HostPool((int)std::min(15u, std::max(2u, hw) - 1u)));
   }
+  return ctx->pool.get();
+}
+
+// Per-pair host passes (bounds, maxima) read ~24 B per pair, ~3.5 ns per pair on
+// one core: batches of more than one part of 2^15 pairs are split over the
+// context's host threads and the calling thread. fn(lo, hi, part) fills the
+// caller's per-part slot; host_parts(n) slots are needed.
+constexpr uint32_t kHostPart = 1u << 15;
+inline uint32_t host_parts(uint32_t n) { return std::max<uint32_t>(1, (n + kHostPart - 1) / kHostPart); }
+
+template <class F>
+void host_for(kira_ctx* ctx, uint32_t n, F&& fn) {
+  const uint32_t parts = host_parts(n);
+  if (parts == 1) {
+    fn(0u, n, 0u);
+    return;
+  }
+  std::atomic<uint32_t> next{0};
+  auto body = [&] {
+    for (;;) {
+      const uint32_t k = next.fetch_add(1, std::memory_order_relaxed);
+      if (k >= parts) return;
+      fn(k * kHostPart, std::min(n, (k + 1) * kHostPart), k);
+    }
+  };
+  HostPool* pool = host_pool(ctx);
+  pool->run(body);
+  body();
+  pool->wait();
+}
+
+Maxes host_maxes(kira_ctx* ctx, const kira_pairs& P, int32_t cfg_band) {
+  std::vector<Maxes> part(host_parts(P.n));
+  const uint32_t cb = (uint32_t)std::max(cfg_band, 1);
+  host_for(ctx, P.n, [&](uint32_t lo, uint32_t hi, uint32_t k) {
+    uint32_t q = 0, w = 0, band = P.bandwidth ? 0u : cb;
+    for (uint32_t i = lo; i < hi; ++i) {
+      q = P.read_len[i] > q ? P.read_len[i] : q;
+      w = P.win_len[i] > w ? P.win_len[i] : w;
+    }
+    if (P.bandwidth)
+      for (uint32_t i = lo; i < hi; ++i) band = std::max(band, (uint32_t)std::max(P.bandwidth[i], 1));
+    part[k] = Maxes{q, w, band};
+  });
+  Maxes m;
+  for (const Maxes& x : part)
+    m.q = std::max(m.q, x.q), m.w = std::max(m.w, x.w), m.band = std::max(m.band, x.band);
   return m;
 }
 
@@ -270,13 +314,28 @@ int upload_pairs(kira_ctx* ctx, const kira_pairs& P, DevPairs& D) {
   cudaError_t cerr = cudaSuccess;
   cudaStream_t st = ctx->stream;
   const uint32_t n = P.n;
-  for (uint32_t i = 0; i < n; ++i) {
+  const uint64_t wlim = P.win_seq ? P.win_seq_bytes : ctx->ref_len;
+  std::vector<int64_t> bad(host_parts(n), -1);  // first pair outside its arena, per part
+  host_for(ctx, n, [&](uint32_t lo, uint32_t hi, uint32_t k) {
+    uint64_t rend = 0, wend = 0;
+    for (uint32_t i = lo; i < hi; ++i) {
+      const uint64_t re = P.read_off[i] + P.read_len[i], we = P.win_off[i] + P.win_len[i];
+      rend = re > rend ? re : rend;
+      wend = we > wend ? we : wend;
+    }
+    if (rend <= P.read_seq_bytes && wend <= wlim) return;
+    for (uint32_t i = lo; i < hi; ++i)
+      if (P.read_off[i] + P.read_len[i] > P.read_seq_bytes || P.win_off[i] + P.win_len[i] > wlim) {
+        bad[k] = i;
+        return;
+      }
+  });
+  for (const int64_t i : bad) {
+    if (i < 0) continue;
     if (P.read_off[i] + P.read_len[i] > P.read_seq_bytes)
-      return fail(ctx, KIRA_ERR_INVALID, "pair %u: read outside read_seq", i);
-    const uint64_t wlim = P.win_seq ? P.win_seq_bytes : ctx->ref_len;
-    if (P.win_off[i] + P.win_len[i] > wlim)
-      return fail(ctx, KIRA_ERR_INVALID, "pair %u: window outside %s", i,
-                  P.win_seq ? "win_seq" : "the resident reference");
+      return fail(ctx, KIRA_ERR_INVALID, "pair %u: read outside read_seq", (uint32_t)i);
+    return fail(ctx, KIRA_ERR_INVALID, "pair %u: window outside %s", (uint32_t)i,
+                P.win_seq ? "win_seq" : "the resident reference");
   }
   KIRA_DBUF(rs, uint8_t, B_READ_SEQ, P.read_seq_bytes);
   KIRA_CUDA(cudaMemcpyAsync(rs, P.read_seq, P.read_seq_bytes, cudaMemcpyHostToDevice, st));
@@ -767,11 +826,7 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
     left[c].fetch_sub(1, std::memory_order_release);
     return true;
   };
-  if (!ctx->pool) {
-    const unsigned hw = std::thread::hardware_concurrency();
-    ctx->pool.reset(new HostPool((int)std::min(15u, std::max(2u, hw) - 1u)));
-  }
-  ctx->pool->run([&] {
+  host_pool(ctx)->run([&] {
     while (take_one()) {
     }
   });
@@ -1310,13 +1365,30 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
   L.drop = prm->adaptive_drop < 0 ? -1 : prm->adaptive_drop;
 
   // Batch bounds that size the per-warp history.
+  struct WfaMax {
+    uint32_t m = 0, n = 0;
+    int64_t s = INT64_MIN, tbf = INT64_MIN;
+  };
+  std::vector<WfaMax> wm(host_parts(n));
+  host_for(ctx, n, [&](uint32_t lo, uint32_t hi, uint32_t k) {
+    WfaMax x;
+    for (uint32_t i = lo; i < hi; ++i) {
+      x.m = P.read_len[i] > x.m ? P.read_len[i] : x.m;
+      x.n = P.win_len[i] > x.n ? P.win_len[i] : x.n;
+    }
+    if (max_score)
+      for (uint32_t i = lo; i < hi; ++i) x.s = std::max<int64_t>(x.s, max_score[i]);
+    if (text_begin_free)
+      for (uint32_t i = lo; i < hi; ++i) x.tbf = std::max<int64_t>(x.tbf, text_begin_free[i]);
+    wm[k] = x;
+  });
   uint32_t m_max = 0, n_max = 0;
   int64_t s_max = INT64_MIN, tbf_max = INT64_MIN;
-  for (uint32_t i = 0; i < n; ++i) {
-    m_max = std::max(m_max, P.read_len[i]);
-    n_max = std::max(n_max, P.win_len[i]);
-    if (max_score) s_max = std::max<int64_t>(s_max, max_score[i]);
-    if (text_begin_free) tbf_max = std::max<int64_t>(tbf_max, text_begin_free[i]);
+  for (const WfaMax& x : wm) {
+    m_max = std::max(m_max, x.m);
+    n_max = std::max(n_max, x.n);
+    s_max = std::max(s_max, x.s);
+    tbf_max = std::max(tbf_max, x.tbf);
   }
   if (m_max > (uint32_t)kWfaMaxLen || n_max > (uint32_t)kWfaMaxLen)
     return fail(ctx, KIRA_ERR_READ_TOO_LONG, "WFA reads and windows up to %d bases", kWfaMaxLen);
@@ -1455,14 +1527,26 @@ namespace {
 // Chains that reach ungapped_extend must lie inside their read and window: the
 // reference's u32 subtractions and slices panic otherwise (prefilter.rs:362-364).
 int check_chains(kira_ctx* ctx, const kira_pairs& P, const kira_chain* chains) {
-  for (uint32_t i = 0; i < P.n; ++i) {
-    const kira_chain& c = chains[i];
-    if (P.read_len[i] > 65535u)
-      return fail(ctx, KIRA_ERR_READ_TOO_LONG, "pair %u: reads up to 65535 bases", i);
-    const bool extends = P.read_len[i] > 0 && c.read_start <= c.read_end &&
-                         c.ref_start <= c.ref_end && c.read_end > c.read_start;
-    if (extends && (c.read_end > P.read_len[i] || c.ref_end > P.win_len[i]))
-      return fail(ctx, KIRA_ERR_INVALID, "chain %u ends outside its read or window", i);
+  std::vector<int64_t> bad(host_parts(P.n), -1);
+  std::vector<int> kind(host_parts(P.n), 0);
+  host_for(ctx, P.n, [&](uint32_t lo, uint32_t hi, uint32_t k) {
+    for (uint32_t i = lo; i < hi; ++i) {
+      const kira_chain& c = chains[i];
+      const bool extends = P.read_len[i] > 0 && c.read_start <= c.read_end &&
+                           c.ref_start <= c.ref_end && c.read_end > c.read_start;
+      const bool outside = extends && (c.read_end > P.read_len[i] || c.ref_end > P.win_len[i]);
+      if (P.read_len[i] > 65535u || outside) {
+        bad[k] = i;
+        kind[k] = P.read_len[i] > 65535u ? 1 : 2;
+        return;
+      }
+    }
+  });
+  for (size_t k = 0; k < bad.size(); ++k) {
+    if (bad[k] < 0) continue;
+    if (kind[k] == 1)
+      return fail(ctx, KIRA_ERR_READ_TOO_LONG, "pair %u: reads up to 65535 bases", (uint32_t)bad[k]);
+    return fail(ctx, KIRA_ERR_INVALID, "chain %u ends outside its read or window", (uint32_t)bad[k]);
   }
   return KIRA_OK;
 }
@@ -1691,7 +1775,7 @@ int kira_gpu_myers_batch(kira_ctx* ctx, const kira_pairs* pairs, uint32_t max_k,
   const kira_pairs& P = *pairs;
   if (P.n == 0) return KIRA_OK;
   cudaSetDevice(ctx->device);
-  const Maxes mx = host_maxes(P, 1);
+  const Maxes mx = host_maxes(ctx, P, 1);
   if (mx.q > 512) return fail(ctx, KIRA_ERR_INVALID, "pattern of %u bases > 512", mx.q);
   DevPairs D;
   int rc = upload_pairs(ctx, P, D);
@@ -1728,7 +1812,7 @@ int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg
   if (cells) *cells = 0;
   if (P.n == 0) return KIRA_OK;
   cudaSetDevice(ctx->device);
-  const Maxes mx = host_maxes(P, cfg->bandwidth);
+  const Maxes mx = host_maxes(ctx, P, cfg->bandwidth);
   int rc = check_sw_cfg(ctx, *cfg, mx.q, mx.band);
   if (rc) return rc;
   DevPairs D;
@@ -1938,7 +2022,7 @@ int kira_gpu_verify_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_ver
                              : (uint64_t)ctx->chunk_pairs;
   if (!ctx->profile && chunk && P.n >= 2 * chunk)
     return verify_batch_chunked(ctx, P, *p, out, cigar, detail, cells, (uint32_t)chunk);
-  const Maxes mx = host_maxes(P, p->sw.bandwidth);
+  const Maxes mx = host_maxes(ctx, P, p->sw.bandwidth);
   DevPairs D;
   int rc = upload_pairs(ctx, P, D);
   if (rc) return rc;
