@@ -1087,6 +1087,141 @@ cudaError_t run_as_graph(kira_ctx* ctx, const DevPairs& D, const BucketRun& R,
 }  // namespace
 
 // ---------------------------------------------------------------------------
+namespace {
+
+// Chunked host input of the WFA and prefilter entry points: the pair arrays and
+// the read / window arenas go up chunk by chunk on the copy-in stream (the arenas
+// as far as each chunk needs them), and each chunk's kernels wait for its own
+// copies, so uploads, kernels and result downloads of consecutive chunks overlap.
+struct ChunkedInput {
+  uint32_t chunk = 0, nch = 0;
+  std::vector<uint64_t> rend, wend;  // per chunk: arena bytes needed up to it
+  DevPairs D{};                      // full-size device buffers
+  uint64_t rdone = 0, wdone = 0;
+};
+
+// Checks every pair's bounds (as upload_pairs) and plans the arena ranges; chunk is
+// rounded up to a multiple of the host pass's part size.
+int chunked_plan(kira_ctx* ctx, const kira_pairs& P, uint64_t want, ChunkedInput& ci) {
+  const uint32_t n = P.n;
+  ci.chunk = (uint32_t)std::min<uint64_t>(n, (want + kHostPart - 1) / kHostPart * kHostPart);
+  ci.nch = (n + ci.chunk - 1) / ci.chunk;
+  const uint64_t wlim = P.win_seq ? P.win_seq_bytes : ctx->ref_len;
+  const uint32_t parts = host_parts(n);
+  std::vector<uint64_t> rend(parts, 0), wend(parts, 0);
+  std::vector<int64_t> bad(parts, -1);
+  host_for(ctx, n, [&](uint32_t lo, uint32_t hi, uint32_t k) {
+    uint64_t re_max = 0, we_max = 0;
+    for (uint32_t i = lo; i < hi; ++i) {
+      const uint64_t re = P.read_off[i] + P.read_len[i], we = P.win_off[i] + P.win_len[i];
+      re_max = re > re_max ? re : re_max;
+      we_max = we > we_max ? we : we_max;
+    }
+    rend[k] = re_max;
+    wend[k] = we_max;
+    if (re_max <= P.read_seq_bytes && we_max <= wlim) return;
+    for (uint32_t i = lo; i < hi; ++i)
+      if (P.read_off[i] + P.read_len[i] > P.read_seq_bytes || P.win_off[i] + P.win_len[i] > wlim) {
+        bad[k] = i;
+        return;
+      }
+  });
+  for (const int64_t i : bad) {
+    if (i < 0) continue;
+    if (P.read_off[i] + P.read_len[i] > P.read_seq_bytes)
+      return fail(ctx, KIRA_ERR_INVALID, "pair %u: read outside read_seq", (uint32_t)i);
+    return fail(ctx, KIRA_ERR_INVALID, "pair %u: window outside %s", (uint32_t)i,
+                P.win_seq ? "win_seq" : "the resident reference");
+  }
+  ci.rend.assign(ci.nch, 0);
+  ci.wend.assign(ci.nch, 0);
+  uint64_t r = 0, w = 0;
+  for (uint32_t c = 0; c < ci.nch; ++c) {  // cumulative: later chunks never shrink the range
+    const uint32_t k0 = c * (ci.chunk / kHostPart), k1 = std::min(parts, k0 + ci.chunk / kHostPart);
+    for (uint32_t k = k0; k < k1; ++k) r = std::max(r, rend[k]), w = std::max(w, wend[k]);
+    ci.rend[c] = r;
+    ci.wend[c] = w;
+  }
+  cudaError_t cerr = cudaSuccess;
+  KIRA_DBUF(rs, uint8_t, B_READ_SEQ, P.read_seq_bytes);
+  KIRA_DBUF(ro, uint64_t, B_READ_OFF, n);
+  KIRA_DBUF(rl, uint32_t, B_READ_LEN, n);
+  KIRA_DBUF(wo, uint64_t, B_WIN_OFF, n);
+  KIRA_DBUF(wl, uint32_t, B_WIN_LEN, n);
+  const uint8_t* ws = ctx->ref_dev;
+  if (P.win_seq) {
+    KIRA_DBUF(wb, uint8_t, B_WIN_SEQ, P.win_seq_bytes);
+    ws = wb;
+  }
+  ci.D = DevPairs{n, rs, ro, rl, ws, wo, wl, nullptr, nullptr, nullptr, nullptr, nullptr};
+  if (!ctx->h2d) KIRA_CUDA(cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
+  if (!ctx->d2h) KIRA_CUDA(cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
+  while (ctx->ev_up.size() < ci.nch + 1) {
+    cudaEvent_t e[4] = {};
+    for (auto& x : e) KIRA_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    ctx->ev_up.push_back(e[0]);
+    ctx->ev_comp.push_back(e[1]);
+    ctx->ev_pack.push_back(e[2]);
+    ctx->ev_scan.push_back(e[3]);
+  }
+  return KIRA_OK;
+}
+
+// Enqueues chunk c's copies on the copy-in stream (extra copies the caller adds
+// through `extra(lo, m, stream)`) and makes the compute stream wait for them.
+template <class F>
+int chunked_upload(kira_ctx* ctx, const kira_pairs& P, ChunkedInput& ci, uint32_t c, F&& extra) {
+  const uint32_t lo = c * ci.chunk, m = std::min(P.n, lo + ci.chunk) - lo;
+  cudaStream_t up = ctx->h2d;
+  const DevPairs& D = ci.D;
+  KIRA_CUDA(cudaMemcpyAsync((uint64_t*)D.read_off + lo, P.read_off + lo, 8ull * m,
+                            cudaMemcpyHostToDevice, up));
+  KIRA_CUDA(cudaMemcpyAsync((uint32_t*)D.read_len + lo, P.read_len + lo, 4ull * m,
+                            cudaMemcpyHostToDevice, up));
+  KIRA_CUDA(cudaMemcpyAsync((uint64_t*)D.win_off + lo, P.win_off + lo, 8ull * m,
+                            cudaMemcpyHostToDevice, up));
+  KIRA_CUDA(cudaMemcpyAsync((uint32_t*)D.win_len + lo, P.win_len + lo, 4ull * m,
+                            cudaMemcpyHostToDevice, up));
+  if (ci.rend[c] > ci.rdone) {
+    KIRA_CUDA(cudaMemcpyAsync((uint8_t*)D.read_seq + ci.rdone, P.read_seq + ci.rdone,
+                              ci.rend[c] - ci.rdone, cudaMemcpyHostToDevice, up));
+    ci.rdone = ci.rend[c];
+  }
+  if (P.win_seq && ci.wend[c] > ci.wdone) {
+    KIRA_CUDA(cudaMemcpyAsync((uint8_t*)D.win_seq + ci.wdone, P.win_seq + ci.wdone,
+                              ci.wend[c] - ci.wdone, cudaMemcpyHostToDevice, up));
+    ci.wdone = ci.wend[c];
+  }
+  const int rc = extra(lo, m, up);
+  if (rc) return rc;
+  KIRA_CUDA(cudaEventRecord(ctx->ev_up[c], up));
+  KIRA_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_up[c], 0));
+  return KIRA_OK;
+}
+
+// Device view of chunk [lo, lo + m) of a chunked input.
+DevPairs chunk_view(const DevPairs& D, uint32_t lo, uint32_t m) {
+  DevPairs v = D;
+  v.n = m;
+  v.read_off += lo;
+  v.read_len += lo;
+  v.win_off += lo;
+  v.win_len += lo;
+  return v;
+}
+
+// Chunk size of a host batch: the context's setting (-1: a quarter of the batch,
+// at least 2^18 pairs; 0: one shot); chunking needs at least two chunks and no
+// stage profiling.
+uint64_t host_chunk(const kira_ctx* ctx, uint32_t n) {
+  if (ctx->profile) return 0;
+  const uint64_t chunk = ctx->chunk_pairs < 0 ? std::max<uint64_t>(1u << 18, (n + 3ull) / 4)
+                                              : (uint64_t)ctx->chunk_pairs;
+  return chunk && n >= 2 * chunk ? chunk : 0;
+}
+
+}  // namespace
+
 extern "C" {
 
 int kira_gpu_is_available(void) {
@@ -1443,19 +1578,29 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
   cudaStream_t st = ctx->stream;
   ctx->ev_recorded = 0;
   mark(ctx, 0, st);
-  DevPairs D;
-  int rc = upload_pairs(ctx, P, D);
-  if (rc) return rc;
   cudaError_t cerr = cudaSuccess;
+  int32_t *dms = nullptr, *dtbf = nullptr;
   if (max_score) {
     KIRA_DBUF(b, int32_t, B_WFA_MAXS, n);
-    KIRA_CUDA(cudaMemcpyAsync(b, max_score, 4ull * n, cudaMemcpyHostToDevice, st));
-    L.max_score_pp = b;
+    dms = b;
   }
   if (text_begin_free) {
     KIRA_DBUF(b, int32_t, B_WFA_TBF, n);
-    KIRA_CUDA(cudaMemcpyAsync(b, text_begin_free, 4ull * n, cudaMemcpyHostToDevice, st));
-    L.tbf_pp = b;
+    dtbf = b;
+  }
+  // Large host batches go chunk by chunk (uploads, kernels and downloads of
+  // consecutive chunks overlap); CIGAR offsets continue through the running total.
+  const uint64_t chunked = host_chunk(ctx, n);
+  ChunkedInput ci;
+  DevPairs D;
+  int rc = chunked ? chunked_plan(ctx, P, chunked, ci) : upload_pairs(ctx, P, D);
+  if (rc) return rc;
+  if (chunked) {
+    D = ci.D;
+  } else {
+    if (dms) KIRA_CUDA(cudaMemcpyAsync(dms, max_score, 4ull * n, cudaMemcpyHostToDevice, st));
+    if (dtbf)
+      KIRA_CUDA(cudaMemcpyAsync(dtbf, text_begin_free, 4ull * n, cudaMemcpyHostToDevice, st));
   }
   // Launch shape: four warps per block while their staged bytes fit comfortably.
   const uint32_t groups_per_warp = 32u / (uint32_t)L.group;
@@ -1466,46 +1611,79 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
   int per_sm = 0;
   KIRA_CUDA(wfa_blocks_per_sm(L.group, tb, smem, (int)(32 * wpb), &per_sm));
   if (per_sm < 1) return fail(ctx, KIRA_ERR_INVALID, "WFA: %zu shared bytes per block", smem);
-  uint64_t blocks = std::min<uint64_t>((n + gpb - 1) / gpb, (uint64_t)ctx->sms * per_sm);
+  const uint32_t csz = chunked ? ci.chunk : n, nch = chunked ? ci.nch : 1;
+  uint64_t blocks = std::min<uint64_t>((csz + gpb - 1) / gpb, (uint64_t)ctx->sms * per_sm);
   blocks = std::min<uint64_t>(blocks,
                               std::max<uint64_t>(1, kWfaScratchBudget / (gpb * group_bytes)));
   KIRA_DBUF(scratch, uint8_t, B_WFA_SCRATCH, blocks * gpb * group_bytes);
   KIRA_DBUF(dout, kira_wfa_result, B_WFA_OUT, n);
   KIRA_DBUF(work, uint32_t, B_WORK, 2);
+  KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
   L.scratch = scratch;
-  L.out = dout;
   L.work = work;
   L.flags = work + 1;
-  uint32_t* ncig = nullptr;
+  uint32_t *ncig = nullptr, *off = nullptr, *sums = nullptr, *ops = nullptr;
   if (tb) {
     KIRA_DBUF(nc, uint32_t, B_WFA_NCIG, n);
     KIRA_DBUF(sl, uint32_t, B_WFA_SLOTS, (uint64_t)n * L.slot_cap);
-    ncig = nc;
-    L.ncig = nc;
+    KIRA_DBUF(of, uint32_t, B_CIG_OFF, n);
+    KIRA_DBUF(su, uint32_t, B_CHUNK_SUMS, n / 4096 + 2);
+    KIRA_DBUF(dops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
+    ncig = nc, off = of, sums = su, ops = dops;
     L.slots = sl;
   }
   KIRA_CUDA(cudaMemsetAsync(work, 0, 8, st));
+  KIRA_CUDA(cudaMemsetAsync(total_dev, 0, 8, st));
+  if (chunked) {  // copies start once the buffers exist and the counters are reset
+    KIRA_CUDA(cudaEventRecord(ctx->ev_up[nch], st));
+    KIRA_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->ev_up[nch], 0));
+  }
   mark(ctx, 1, st);
-  KIRA_CUDA(launch_wfa(D, L, (uint32_t)blocks, wpb, tb, st));
-  mark(ctx, 2, st);
-  uint64_t total = 0;
-  uint32_t* ops = nullptr;
-  if (tb) {
-    KIRA_DBUF(off, uint32_t, B_CIG_OFF, n);
-    KIRA_DBUF(sums, uint32_t, B_CHUNK_SUMS, n / 4096 + 2);
-    KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
-    KIRA_DBUF(dops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
-    ops = dops;
-    KIRA_CUDA(launch_cigar_scan(ncig, n, off, sums, total_dev, st));
-    WfaCompact C{n, dout, ncig, off, L.slots, L.slot_cap, dops, cigar->cap};
-    KIRA_CUDA(launch_wfa_compact(C, ctx->sms, st));
-    KIRA_CUDA(cudaMemcpyAsync(&total, total_dev, 8, cudaMemcpyDeviceToHost, st));
+  for (uint32_t c = 0; c < nch; ++c) {
+    const uint32_t lo = c * csz, m = std::min(n, lo + csz) - lo;
+    if (chunked) {
+      rc = chunked_upload(ctx, P, ci, c, [&](uint32_t l, uint32_t k, cudaStream_t up) -> int {
+        if (dms) KIRA_CUDA(cudaMemcpyAsync(dms + l, max_score + l, 4ull * k, cudaMemcpyHostToDevice, up));
+        if (dtbf)
+          KIRA_CUDA(cudaMemcpyAsync(dtbf + l, text_begin_free + l, 4ull * k, cudaMemcpyHostToDevice, up));
+        return KIRA_OK;
+      });
+      if (rc) return rc;
+      if (c) KIRA_CUDA(cudaMemsetAsync(work, 0, 4, st));
+    }
+    WfaLaunch Lc = L;
+    Lc.n = m;
+    Lc.out = dout + lo;
+    Lc.max_score_pp = dms ? dms + lo : nullptr;
+    Lc.tbf_pp = dtbf ? dtbf + lo : nullptr;
+    if (tb) {
+      Lc.ncig = ncig + lo;
+      Lc.slots = L.slots + (size_t)lo * L.slot_cap;
+    }
+    const uint32_t bl = (uint32_t)std::min<uint64_t>(blocks, (m + gpb - 1) / gpb);
+    KIRA_CUDA(launch_wfa(chunk_view(D, lo, m), Lc, bl, wpb, tb, st));
+    mark(ctx, 2, st);
+    if (tb) {
+      KIRA_CUDA(launch_cigar_scan(ncig + lo, m, off + lo, sums, total_dev, st, true));
+      WfaCompact C{m, dout + lo, ncig + lo, off + lo, Lc.slots, L.slot_cap, ops, cigar->cap};
+      KIRA_CUDA(launch_wfa_compact(C, ctx->sms, st));
+    }
+    if (chunked) {
+      KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], st));
+      KIRA_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->ev_comp[c], 0));
+      KIRA_CUDA(cudaMemcpyAsync(out + lo, dout + lo, sizeof(kira_wfa_result) * m,
+                                cudaMemcpyDeviceToHost, ctx->d2h));
+    }
   }
   mark(ctx, 3, st);
+  cudaStream_t dn = chunked ? ctx->d2h : st;
+  uint64_t total = 0;
   uint32_t flags = 0;
-  KIRA_CUDA(cudaMemcpyAsync(&flags, work + 1, 4, cudaMemcpyDeviceToHost, st));
-  KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_wfa_result) * n, cudaMemcpyDeviceToHost, st));
-  KIRA_CUDA(cudaStreamSynchronize(st));
+  KIRA_CUDA(cudaMemcpyAsync(&flags, work + 1, 4, cudaMemcpyDeviceToHost, dn));
+  if (tb) KIRA_CUDA(cudaMemcpyAsync(&total, total_dev, 8, cudaMemcpyDeviceToHost, dn));
+  if (!chunked)
+    KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_wfa_result) * n, cudaMemcpyDeviceToHost, dn));
+  KIRA_CUDA(cudaStreamSynchronize(dn));
   if (flags & 2u) return fail(ctx, KIRA_ERR_RUNTIME, "WFA history above its computed bound");
   if (flags & 1u) return fail(ctx, KIRA_ERR_RUNTIME, "WFA CIGAR above its computed bound");
   if (!tb) {
@@ -1516,9 +1694,9 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
   if (total > cigar->cap)
     return fail(ctx, KIRA_ERR_CAPACITY, "CIGAR buffer holds %llu ops, %llu needed",
                 (unsigned long long)cigar->cap, (unsigned long long)total);
-  if (total) KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * total, cudaMemcpyDeviceToHost, st));
+  if (total) KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * total, cudaMemcpyDeviceToHost, dn));
   mark(ctx, 4, st);
-  KIRA_CUDA(cudaStreamSynchronize(st));
+  KIRA_CUDA(cudaStreamSynchronize(dn));
   return KIRA_OK;
 }
 
@@ -1526,10 +1704,15 @@ namespace {
 
 // Chains that reach ungapped_extend must lie inside their read and window: the
 // reference's u32 subtractions and slices panic otherwise (prefilter.rs:362-364).
-int check_chains(kira_ctx* ctx, const kira_pairs& P, const kira_chain* chains) {
+int check_chains(kira_ctx* ctx, const kira_pairs& P, const kira_chain* chains,
+                 uint32_t* max_read_len) {
   std::vector<int64_t> bad(host_parts(P.n), -1);
   std::vector<int> kind(host_parts(P.n), 0);
+  std::vector<uint32_t> qmax(host_parts(P.n), 0);
   host_for(ctx, P.n, [&](uint32_t lo, uint32_t hi, uint32_t k) {
+    uint32_t q = 0;
+    for (uint32_t i = lo; i < hi; ++i) q = P.read_len[i] > q ? P.read_len[i] : q;
+    qmax[k] = q;
     for (uint32_t i = lo; i < hi; ++i) {
       const kira_chain& c = chains[i];
       const bool extends = P.read_len[i] > 0 && c.read_start <= c.read_end &&
@@ -1542,6 +1725,8 @@ int check_chains(kira_ctx* ctx, const kira_pairs& P, const kira_chain* chains) {
       }
     }
   });
+  *max_read_len = 0;
+  for (const uint32_t q : qmax) *max_read_len = std::max(*max_read_len, q);
   for (size_t k = 0; k < bad.size(); ++k) {
     if (bad[k] < 0) continue;
     if (kind[k] == 1)
@@ -1574,7 +1759,8 @@ int kira_gpu_prefilter_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_
   *md_used = 0;
   if (n == 0) return KIRA_OK;
   if ((cigar->cap && !cigar->ops) || (md_cap && !md)) return KIRA_ERR_INVALID;
-  int rc = check_chains(ctx, P, chains);
+  uint32_t q_max = 0;
+  int rc = check_chains(ctx, P, chains, &q_max);
   if (rc) return rc;
   PrefilterLaunch L{};
   L.match = cfg->match_score;
@@ -1595,22 +1781,31 @@ int kira_gpu_prefilter_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_
   cudaStream_t st = ctx->stream;
   ctx->ev_recorded = 0;
   mark(ctx, 0, st);
-  DevPairs D;
-  rc = upload_pairs(ctx, P, D);
-  if (rc) return rc;
   cudaError_t cerr = cudaSuccess;
+  // Large host batches go chunk by chunk (uploads, kernels and downloads overlap);
+  // CIGAR and MD offsets continue through running totals, and pass 2 writes only
+  // what fits the caller's buffers, so no chunk waits for the host.
+  const uint64_t chunked = host_chunk(ctx, n);
+  ChunkedInput ci;
+  DevPairs D;
+  rc = chunked ? chunked_plan(ctx, P, chunked, ci) : upload_pairs(ctx, P, D);
+  if (rc) return rc;
+  if (chunked) D = ci.D;
   KIRA_DBUF(dch, kira_chain, B_PF_CHAINS, n);
-  KIRA_CUDA(cudaMemcpyAsync(dch, chains, sizeof(kira_chain) * n, cudaMemcpyHostToDevice, st));
-  L.chains = dch;
+  uint8_t* dtop = nullptr;
+  int32_t* dmar = nullptr;
   if (is_top1) {
     KIRA_DBUF(b, uint8_t, B_PF_TOP1, n);
-    KIRA_CUDA(cudaMemcpyAsync(b, is_top1, n, cudaMemcpyHostToDevice, st));
-    L.is_top1 = b;
+    dtop = b;
   }
   if (score_margin) {
     KIRA_DBUF(b, int32_t, B_PF_MARGIN, n);
-    KIRA_CUDA(cudaMemcpyAsync(b, score_margin, 4ull * n, cudaMemcpyHostToDevice, st));
-    L.score_margin = b;
+    dmar = b;
+  }
+  if (!chunked) {
+    KIRA_CUDA(cudaMemcpyAsync(dch, chains, sizeof(kira_chain) * n, cudaMemcpyHostToDevice, st));
+    if (dtop) KIRA_CUDA(cudaMemcpyAsync(dtop, is_top1, n, cudaMemcpyHostToDevice, st));
+    if (dmar) KIRA_CUDA(cudaMemcpyAsync(dmar, score_margin, 4ull * n, cudaMemcpyHostToDevice, st));
   }
   KIRA_DBUF(dout, kira_prefilter_result, B_PF_OUT, n);
   KIRA_DBUF(ncig, uint32_t, B_PF_NCIG, n);
@@ -1620,47 +1815,84 @@ int kira_gpu_prefilter_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_
   KIRA_DBUF(sums, uint32_t, B_CHUNK_SUMS, n / 4096 + 2);
   KIRA_DBUF(totals, uint64_t, B_TOTAL, 2);
   KIRA_DBUF(flags, uint32_t, B_WORK, 1);
-  L.out = dout;
+  const uint64_t ops_cap = std::min<uint64_t>(cigar->cap, 3ull * n);
+  KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(ops_cap, 1));
+  // An ungapped span of L columns has at most 2L + 1 MD bytes (all mismatches).
+  const uint64_t md_dev = std::min<uint64_t>(md_cap, (uint64_t)n * (2ull * q_max + 8));
+  KIRA_DBUF(dmd, char, B_PF_MD, std::max<uint64_t>(md_dev, 1));
   L.ncig = ncig;
   L.mdlen = mdlen;
   L.flags = flags;
+  L.ops = ops;
+  L.cigar_cap = ops_cap;
+  L.md = dmd;
+  L.md_cap = md_dev;
   KIRA_CUDA(cudaMemsetAsync(flags, 0, 4, st));
+  KIRA_CUDA(cudaMemsetAsync(totals, 0, 16, st));
+  const uint32_t csz = chunked ? ci.chunk : n, nch = chunked ? ci.nch : 1;
+  if (chunked) {
+    KIRA_CUDA(cudaEventRecord(ctx->ev_up[nch], st));
+    KIRA_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->ev_up[nch], 0));
+  }
   mark(ctx, 1, st);
-  KIRA_CUDA(launch_prefilter(D, L, false, ctx->sms, st));
-  mark(ctx, 2, st);
-  KIRA_CUDA(launch_cigar_scan(ncig, n, cig_off, sums, totals, st));
-  KIRA_CUDA(launch_cigar_scan(mdlen, n, md_off, sums, totals + 1, st));
-  KIRA_CUDA(launch_prefilter_offsets(n, dout, cig_off, md_off, ctx->sms, st));
+  for (uint32_t c = 0; c < nch; ++c) {
+    const uint32_t lo = c * csz, m = std::min(n, lo + csz) - lo;
+    if (chunked) {
+      rc = chunked_upload(ctx, P, ci, c, [&](uint32_t l, uint32_t k, cudaStream_t up) -> int {
+        KIRA_CUDA(cudaMemcpyAsync(dch + l, chains + l, sizeof(kira_chain) * k,
+                                  cudaMemcpyHostToDevice, up));
+        if (dtop) KIRA_CUDA(cudaMemcpyAsync(dtop + l, is_top1 + l, k, cudaMemcpyHostToDevice, up));
+        if (dmar)
+          KIRA_CUDA(cudaMemcpyAsync(dmar + l, score_margin + l, 4ull * k, cudaMemcpyHostToDevice, up));
+        return KIRA_OK;
+      });
+      if (rc) return rc;
+    }
+    const DevPairs Dc = chunk_view(D, lo, m);
+    PrefilterLaunch Lc = L;
+    Lc.chains = dch + lo;
+    Lc.is_top1 = dtop ? dtop + lo : nullptr;
+    Lc.score_margin = dmar ? dmar + lo : nullptr;
+    Lc.out = dout + lo;
+    Lc.ncig = ncig + lo;
+    Lc.mdlen = mdlen + lo;
+    KIRA_CUDA(launch_prefilter(Dc, Lc, false, ctx->sms, st));
+    mark(ctx, 2, st);
+    KIRA_CUDA(launch_cigar_scan(ncig + lo, m, cig_off + lo, sums, totals, st, true));
+    KIRA_CUDA(launch_cigar_scan(mdlen + lo, m, md_off + lo, sums, totals + 1, st, true));
+    KIRA_CUDA(launch_prefilter_offsets(m, dout + lo, cig_off + lo, md_off + lo, ctx->sms, st));
+    mark(ctx, 3, st);
+    KIRA_CUDA(launch_prefilter(Dc, Lc, true, ctx->sms, st));
+    mark(ctx, 4, st);
+    if (chunked) {
+      KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], st));
+      KIRA_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->ev_comp[c], 0));
+      KIRA_CUDA(cudaMemcpyAsync(out + lo, dout + lo, sizeof(kira_prefilter_result) * m,
+                                cudaMemcpyDeviceToHost, ctx->d2h));
+    }
+  }
+  cudaStream_t dn = chunked ? ctx->d2h : st;
   uint64_t tot[2] = {0, 0};
   uint32_t hflags = 0;
-  KIRA_CUDA(cudaMemcpyAsync(tot, totals, 16, cudaMemcpyDeviceToHost, st));
-  KIRA_CUDA(cudaMemcpyAsync(&hflags, flags, 4, cudaMemcpyDeviceToHost, st));
-  KIRA_CUDA(cudaStreamSynchronize(st));
+  KIRA_CUDA(cudaMemcpyAsync(tot, totals, 16, cudaMemcpyDeviceToHost, dn));
+  KIRA_CUDA(cudaMemcpyAsync(&hflags, flags, 4, cudaMemcpyDeviceToHost, dn));
+  if (!chunked)
+    KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_prefilter_result) * n,
+                              cudaMemcpyDeviceToHost, dn));
+  KIRA_CUDA(cudaStreamSynchronize(dn));
   if (hflags & 1u) return fail(ctx, KIRA_ERR_RUNTIME, "a chain ended outside its read or window");
   cigar->used = tot[0];
   *md_used = tot[1];
-  if (tot[0] > cigar->cap || tot[1] > md_cap) {
-    KIRA_CUDA(cudaMemcpy(out, dout, sizeof(kira_prefilter_result) * n, cudaMemcpyDeviceToHost));
+  if (tot[0] > cigar->cap || tot[1] > md_cap)
     return fail(ctx, KIRA_ERR_CAPACITY, "CIGAR / MD buffers hold %llu ops / %llu bytes; "
                 "%llu / %llu needed", (unsigned long long)cigar->cap,
                 (unsigned long long)md_cap, (unsigned long long)tot[0],
                 (unsigned long long)tot[1]);
-  }
-  KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(tot[0], 1));
-  KIRA_DBUF(dmd, char, B_PF_MD, std::max<uint64_t>(tot[1], 1));
-  L.ops = ops;
-  L.cigar_cap = tot[0];
-  L.md = dmd;
-  mark(ctx, 3, st);
-  KIRA_CUDA(launch_prefilter(D, L, true, ctx->sms, st));
-  mark(ctx, 4, st);
-  KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_prefilter_result) * n, cudaMemcpyDeviceToHost,
-                            st));
   if (tot[0])
-    KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * tot[0], cudaMemcpyDeviceToHost, st));
-  if (tot[1]) KIRA_CUDA(cudaMemcpyAsync(md, dmd, tot[1], cudaMemcpyDeviceToHost, st));
+    KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * tot[0], cudaMemcpyDeviceToHost, dn));
+  if (tot[1]) KIRA_CUDA(cudaMemcpyAsync(md, dmd, tot[1], cudaMemcpyDeviceToHost, dn));
   mark(ctx, 5, st);
-  KIRA_CUDA(cudaStreamSynchronize(st));
+  KIRA_CUDA(cudaStreamSynchronize(dn));
   return KIRA_OK;
 }
 

@@ -171,6 +171,7 @@ struct PrefilterLaunch {
   uint32_t* ops;                // pass 2: CIGAR output
   uint64_t cigar_cap;
   char* md;                     // pass 2: MD output
+  uint64_t md_cap;              // pass 2: chains whose CIGAR or MD would pass a cap are skipped
   uint32_t* flags;              // bit 0: a chain outside its read / window
 };
 

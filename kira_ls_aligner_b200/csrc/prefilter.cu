@@ -106,19 +106,23 @@ __device__ uint32_t pf_md(const uint8_t* read, const uint8_t* ref, uint32_t rs, 
       run = (uint32_t)((int)i - prev - 1);
       tok = pf_digits(run) + 1u;
     }
-    uint32_t inc = tok;  // inclusive warp scan of the token lengths
+    if (!out) {  // sizing: the sum of the token lengths is enough
+      wpos += __reduce_add_sync(kFull, tok);
+    } else {
+      uint32_t inc = tok;  // inclusive warp scan of the token lengths places each token
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(kFull, inc, o);
-      if (lane >= o) inc += t;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc += t;
+      }
+      if (mm) {
+        const uint32_t at = wpos + inc - tok;
+        const uint32_t d = tok - 1u;
+        pf_put(out + at, run, d);
+        out[at + d] = (char)(((r >= 'A' && r <= 'Z') || (r >= 'a' && r <= 'z')) ? (r & 0xDFu) : 'N');
+      }
+      wpos += __shfl_sync(kFull, inc, 31);
     }
-    if (out && mm) {
-      const uint32_t at = wpos + inc - tok;
-      const uint32_t d = tok - 1u;
-      pf_put(out + at, run, d);
-      out[at + d] = (char)(((r >= 'A' && r <= 'Z') || (r >= 'a' && r <= 'z')) ? (r & 0xDFu) : 'N');
-    }
-    wpos += __shfl_sync(kFull, inc, 31);
     if (bm) last = (int)base + (31 - __clz(bm));
   }
   const uint32_t tail = (uint32_t)((int)span - last - 1);
@@ -139,9 +143,12 @@ __global__ void __launch_bounds__(256) prefilter_kernel(DevPairs P, PrefilterLau
     if (write) {
       const kira_prefilter_result r = L.out[p];
       if (r.n_cigar == 0) continue;
+      if ((uint64_t)r.md_off + r.md_len > L.md_cap ||
+          (uint64_t)r.cigar_off + r.n_cigar > L.cigar_cap)
+        continue;  // the call reports the capacity it needs
       uint32_t nm;
       pf_md(read, ref, r.read_start, r.ref_start, r.len, L.md + r.md_off, nm, lane);
-      if (lane == 0 && (uint64_t)r.cigar_off + r.n_cigar <= L.cigar_cap) {
+      if (lane == 0) {
         uint32_t* ops = L.ops + r.cigar_off;
         uint32_t k = 0;
         if (r.read_start > 0) ops[k++] = (r.read_start << 4) | 4u;

@@ -180,3 +180,37 @@ def test_invalid_and_capacity(ctx):
         ctx.prefilter_batch(b, ok, PrefilterConfig(), md_cap=2)
     res, ops, md = ctx.prefilter_batch(b, ok, PrefilterConfig())
     assert int(res["result"][0]) == 3 and md.tobytes() == b"150"
+
+
+def test_chunked_host_path(ctx):
+    # Several chunks (overlapped uploads / kernels / downloads, CIGAR and MD offsets
+    # through running totals, no host round trip between the passes) equal the
+    # one-shot call; a too-small MD buffer still reports the bytes needed.
+    from kira_ls_aligner_b200 import CapacityError, PairBatch, PrefilterConfig, _abi, synth
+    w = synth.prefilter_chains(90_000, seed=0xC4A1, err_hi=0.03, ref_len=2_000_000)
+    n = w.n_pairs
+    ctx.ref_upload(w.reference)
+    b = PairBatch(w.reads, w.read_off, w.read_len, None, np.zeros(n, np.uint64),
+                  np.full(n, len(w.reference), np.uint32))
+    cfg = PrefilterConfig()
+    L = _abi.lib()
+    try:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, 0))
+        one = ctx.prefilter_batch(b, w.chains, cfg, is_top1=w.is_top1, score_margin=w.score_margin)
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, 32768))
+        many = ctx.prefilter_batch(b, w.chains, cfg, is_top1=w.is_top1,
+                                   score_margin=w.score_margin)
+        with pytest.raises(CapacityError):
+            ctx.prefilter_batch(b, w.chains, cfg, is_top1=w.is_top1, score_margin=w.score_margin,
+                                md_cap=1000)
+    finally:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, -1))
+    for a, c in zip(one, many):
+        assert np.array_equal(a, c)
+    ref = w.reference.tobytes()
+    res, ops, md = many
+    for i in range(0, n, 89):
+        read = w.reads[i * 150:(i + 1) * 150].tobytes()
+        want = _want(read, ref, tuple(int(x) for x in w.chains[i]), cfg, int(w.is_top1[i]),
+                     int(w.score_margin[i]))
+        assert _got(res, ops, md, i) == want, i

@@ -260,3 +260,41 @@ def test_refused_costs_and_capacity(ctx):
         ctx.wfa_batch(_batch([(b"A" * 30001, b"A")]), _pen(max_score=5))
     assert "ReadTooLong" in str(ei.value) or "30000" in str(ei.value)
     del _abi
+
+
+@pytest.mark.parametrize("traceback", [True, False])
+def test_chunked_host_path(ctx, traceback):
+    # Host batches of several chunks (uploads / kernels / downloads overlapped, CIGAR
+    # offsets through the running total) equal the one-shot call; per-pair budgets
+    # and leading free text are sliced with the chunks.
+    from kira_ls_aligner_b200 import AlignmentConfig, PairBatch, WfaParams, _abi, synth
+    w = synth.wfa_cascade(90_000, seed=0x5CA1, err_hi=0.06, ref_len=3_000_000)
+    rng = np.random.default_rng(4)
+    ms = rng.integers(5, 120, w.n_pairs).astype(np.int32)
+    tbf = rng.integers(0, 6, w.n_pairs).astype(np.int32)
+    ref = w.reference
+    b = PairBatch(w.reads, w.read_off, w.read_len, ref, w.win_off, w.win_len)
+    p = WfaParams.scored_from(AlignmentConfig(), traceback=traceback)
+    L = _abi.lib()
+    try:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, 0))
+        one = ctx.wfa_batch(b, p, max_score=ms, text_begin_free=tbf)
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, 32768))
+        many = ctx.wfa_batch(b, p, max_score=ms, text_begin_free=tbf)
+    finally:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, -1))
+    assert np.array_equal(one[0], many[0]) and np.array_equal(one[1], many[1])
+    sel = list(range(0, w.n_pairs, 97))
+    pairs = [(w.reads[int(w.read_off[i]):int(w.read_off[i]) + 150].tobytes(),
+              ref[int(w.win_off[i]):int(w.win_off[i]) + int(w.win_len[i])].tobytes()) for i in sel]
+    want = _want(pairs, p, max_score=ms[sel], tbf=tbf[sel])
+    from kira_ls_aligner_b200 import decode_cigar
+    res, ops = many
+    for j, i in enumerate(sel):
+        r = res[i]
+        got = None
+        if r["found"]:
+            cig = decode_cigar(ops[int(r["cigar_off"]):int(r["cigar_off"]) + int(r["n_cigar"])])
+            got = (int(r["cost"]), int(r["score"]), int(r["text_start"]), int(r["text_end"]),
+                   [(a, c) for a, c in cig])
+        assert got == want[j], i
