@@ -31,7 +31,7 @@ enum BufId {
   B_DIST, B_END, B_SIEVE_OUT, B_SIEVE_JOBS, B_CELLS, B_TOTAL, B_READ_PLANES, B_WIN_PLANES,
   B_ROWKEYS, B_DONE_ROW, B_WORK, B_WFA_MAXS, B_WFA_TBF, B_WFA_OUT, B_WFA_NCIG, B_WFA_SLOTS,
   B_WFA_SCRATCH, B_WFA_FLAGS, B_PF_CHAINS, B_PF_TOP1, B_PF_MARGIN, B_PF_OUT, B_PF_NCIG,
-  B_PF_MDLEN, B_PF_MDOFF, B_PF_MD, B_PF_EXACT, B_COUNT
+  B_PF_MDLEN, B_PF_MDOFF, B_PF_MD, B_PF_EXACT, B_WFA_FB, B_WFA_WHIST, B_COUNT
 };
 
 struct DevBuf {
@@ -1573,6 +1573,37 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
   L.slot_cap = (uint32_t)(2 * (S / min_cost) + 2);
   L.max_score_pp = nullptr;
   L.tbf_pp = nullptr;
+  // Fixed-window fast path: 64 diagonals per pair (128 when 64 cover fewer than 32
+  // scores), placed so every cell of the highest score stays inside for this
+  // batch's leading free text; pairs still open at that score fall back to the
+  // general kernel with a warp per pair (their fronts are the wide ones).
+  // ctx->wfa_lanes != 0 forces the general kernel alone.
+  auto place = [&](int width, int* base) {
+    int best = -1;
+    for (int b = -(width - 1 - (int)tbf_max); b <= 0; ++b) {
+      const int64_t lo_s = (int64_t)L.o + (int64_t)L.ei * (1 - b) - 1;
+      const int64_t hi_s = (int64_t)L.o + (int64_t)L.ed * (b + width - tbf_max) - 1;
+      const int64_t sm = std::min<int64_t>(std::min(lo_s, hi_s), 1 << 20);
+      if (sm > best) best = (int)sm, *base = b;
+    }
+    return best;
+  };
+  int win_base = 0, win_segments = 2;
+  int win_smax = tbf_max <= 63 ? place(64, &win_base) : -1;
+  if (win_smax < std::min<int64_t>(S, 32) && tbf_max <= 127) {
+    int b4 = 0;
+    const int s4 = place(128, &b4);
+    if (s4 > win_smax) win_smax = s4, win_base = b4, win_segments = 4;
+  }
+  const bool use_window = ctx->wfa_lanes == 0 && win_smax >= 16 && L.ring_len <= 64;
+  if (use_window) {
+    win_smax = (int)std::min<int64_t>(win_smax, S);
+    L.win_base = win_base;
+    L.win_smax = win_smax;
+    L.win_segments = win_segments;
+    L.win_ring_bytes =
+        (uint32_t)((L.ring_len * 3u * (32u * (uint32_t)win_segments + 2u) * 2u + 15u) & ~15u);
+  }
 
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
@@ -1617,11 +1648,33 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
                               std::max<uint64_t>(1, kWfaScratchBudget / (gpb * group_bytes)));
   KIRA_DBUF(scratch, uint8_t, B_WFA_SCRATCH, blocks * gpb * group_bytes);
   KIRA_DBUF(dout, kira_wfa_result, B_WFA_OUT, n);
-  KIRA_DBUF(work, uint32_t, B_WORK, 2);
+  KIRA_DBUF(work, uint32_t, B_WORK, 4);  // window fetch, flags, general fetch, fallbacks
   KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
   L.scratch = scratch;
-  L.work = work;
   L.flags = work + 1;
+  uint64_t wblocks = 0;
+  uint32_t fwpb = 4;
+  if (use_window) {
+    const size_t wsmem = (size_t)4 * (L.win_ring_bytes + L.smem_group - L.ring_bytes);
+    int wper = 0;
+    KIRA_CUDA(wfa_window_blocks_per_sm(win_segments, tb, wsmem, &wper));
+    if (wper < 1) return fail(ctx, KIRA_ERR_INVALID, "WFA window: %zu shared bytes", wsmem);
+    wblocks = std::min<uint64_t>((csz + 3) / 4, (uint64_t)ctx->sms * wper);
+    KIRA_DBUF(fb, uint32_t, B_WFA_FB, csz);
+    L.fb_list = fb;
+    // Fallback launch shape: 32 lanes per pair, up to 4 warps (pairs) per block; it
+    // uses no more groups than the scratch above holds.
+    while (fwpb > 1 && (uint64_t)fwpb * L.smem_group > (160u << 10)) fwpb >>= 1;
+    int fper = 0;
+    KIRA_CUDA(wfa_blocks_per_sm(32, tb, (size_t)fwpb * L.smem_group, (int)(32 * fwpb), &fper));
+    if (fper < 1) return fail(ctx, KIRA_ERR_INVALID, "WFA fallback: %u shared bytes", L.smem_group);
+    L.fb_count = work + 3;
+    if (tb) {
+      KIRA_DBUF(wh, int16_t, B_WFA_WHIST,
+                wblocks * 4 * (uint64_t)(win_smax + 1) * 3 * 32 * win_segments);
+      L.win_hist = wh;
+    }
+  }
   uint32_t *ncig = nullptr, *off = nullptr, *sums = nullptr, *ops = nullptr;
   if (tb) {
     KIRA_DBUF(nc, uint32_t, B_WFA_NCIG, n);
@@ -1632,7 +1685,7 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
     ncig = nc, off = of, sums = su, ops = dops;
     L.slots = sl;
   }
-  KIRA_CUDA(cudaMemsetAsync(work, 0, 8, st));
+  KIRA_CUDA(cudaMemsetAsync(work, 0, 16, st));
   KIRA_CUDA(cudaMemsetAsync(total_dev, 0, 8, st));
   if (chunked) {  // copies start once the buffers exist and the counters are reset
     KIRA_CUDA(cudaEventRecord(ctx->ev_up[nch], st));
@@ -1649,7 +1702,10 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
         return KIRA_OK;
       });
       if (rc) return rc;
-      if (c) KIRA_CUDA(cudaMemsetAsync(work, 0, 4, st));
+    }
+    if (c) {  // fetch counters of both kernels and the fallback count
+      KIRA_CUDA(cudaMemsetAsync(work, 0, 4, st));
+      KIRA_CUDA(cudaMemsetAsync(work + 2, 0, 8, st));
     }
     WfaLaunch Lc = L;
     Lc.n = m;
@@ -1660,8 +1716,26 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
       Lc.ncig = ncig + lo;
       Lc.slots = L.slots + (size_t)lo * L.slot_cap;
     }
-    const uint32_t bl = (uint32_t)std::min<uint64_t>(blocks, (m + gpb - 1) / gpb);
-    KIRA_CUDA(launch_wfa(chunk_view(D, lo, m), Lc, bl, wpb, tb, st));
+    const DevPairs Dc = chunk_view(D, lo, m);
+    if (use_window) {
+      // Window kernel first; its fallbacks (pairs still open at win_smax) run
+      // through the general kernel over the fallback list.
+      Lc.work = work;
+      KIRA_CUDA(launch_wfa_window(Dc, Lc, (uint32_t)std::min<uint64_t>(wblocks, (m + 3) / 4), tb,
+                                  st));
+      Lc.list = L.fb_list;
+      Lc.list_count = L.fb_count;
+      Lc.group = 32;
+      Lc.work = work + 2;
+      KIRA_CUDA(launch_wfa(Dc, Lc,
+                           (uint32_t)std::max<uint64_t>(
+                               1, std::min<uint64_t>(blocks * gpb / fwpb, (m + fwpb - 1) / fwpb)),
+                           fwpb, tb, st));
+    } else {
+      Lc.work = work + 2;
+      const uint32_t bl = (uint32_t)std::min<uint64_t>(blocks, (m + gpb - 1) / gpb);
+      KIRA_CUDA(launch_wfa(Dc, Lc, bl, wpb, tb, st));
+    }
     mark(ctx, 2, st);
     if (tb) {
       KIRA_CUDA(launch_cigar_scan(ncig + lo, m, off + lo, sums, total_dev, st, true));

@@ -143,6 +143,18 @@ struct WfaLaunch {
   uint32_t* slots;             // traceback: slot_cap ops per pair, newest first
   uint32_t slot_cap;
   uint32_t* flags;             // bit 0: CIGAR slot overflow, bit 1: history overflow
+  // General kernel over a pair list (the window kernel's fallbacks): pair list[q]
+  // for q < *list_count; null: every pair of [0, n).
+  const uint32_t* list;
+  const uint32_t* list_count;
+  // Window kernel (wfa_window_kernel): 32 x win_segments diagonals from win_base
+  // per pair, exact for every pair done by score win_smax; later pairs are
+  // appended to fb_list for the general kernel.
+  int32_t win_base, win_smax, win_segments;
+  uint32_t win_ring_bytes;     // shared bytes of the score ring per warp
+  uint32_t* fb_list;
+  uint32_t* fb_count;
+  int16_t* win_hist;           // traceback: per warp (win_smax + 1) x 3 x window offsets
 };
 
 struct WfaCompact {
@@ -237,6 +249,9 @@ cudaError_t launch_nm_md(const DevPairs& P, const NmMdLaunch& L, bool write, int
                          cudaStream_t st);
 
 cudaError_t wfa_blocks_per_sm(int group, bool traceback, size_t smem, int threads, int* per_sm);
+cudaError_t wfa_window_blocks_per_sm(int segments, bool traceback, size_t smem, int* per_sm);
+cudaError_t launch_wfa_window(const DevPairs& P, const WfaLaunch& L, uint32_t blocks,
+                              bool traceback, cudaStream_t st);
 cudaError_t launch_wfa(const DevPairs& P, const WfaLaunch& L, uint32_t blocks,
                        uint32_t warps_per_block, bool traceback, cudaStream_t st);
 cudaError_t launch_wfa_compact(const WfaCompact& C, int sms, cudaStream_t st);

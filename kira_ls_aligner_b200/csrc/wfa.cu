@@ -23,15 +23,12 @@ __device__ __forceinline__ int wfa_high_bit(unsigned b) { return 31 - __clz(b); 
 
 // Traceback in one lane (build_cigar, wfa.rs:762-952). Ops are pushed in reverse
 // order into the pair's slot with push_cigar's merging (wfa.rs:954-962); returns
-// the diagonal at termination (the alignment's text start).
-__device__ int wfa_traceback(const WfaLaunch& L, const int2* __restrict__ meta,
-                             const int16_t* __restrict__ H, const uint32_t* pw,
-                             const uint32_t* tw, int m, int n, int s, int k,
-                             uint32_t* __restrict__ slot, uint32_t& nops, bool& overflow) {
-  auto get = [&](int layer, int sc, int kk) -> int {
-    if (sc < 0) return kWfaNone;
-    return wfa_get(H, wfa_unpack(meta[(uint32_t)sc * 3u + layer]), kk);
-  };
+// the diagonal at termination (the alignment's text start). get(layer, score, k)
+// returns the stored offset or kWfaNone.
+template <class Get>
+__device__ int wfa_traceback_t(const WfaLaunch& L, Get get, const uint32_t* pw,
+                               const uint32_t* tw, int m, int n, int s, int k,
+                               uint32_t* __restrict__ slot, uint32_t& nops, bool& overflow) {
   uint32_t last = 0xFFFFFFFFu;  // op of the newest entry
   auto push = [&](uint32_t op, uint32_t len) {
     if (last == op) {
@@ -104,6 +101,17 @@ __device__ int wfa_traceback(const WfaLaunch& L, const int2* __restrict__ meta,
   return k;
 }
 
+__device__ int wfa_traceback(const WfaLaunch& L, const int2* __restrict__ meta,
+                             const int16_t* __restrict__ H, const uint32_t* pw,
+                             const uint32_t* tw, int m, int n, int s, int k,
+                             uint32_t* __restrict__ slot, uint32_t& nops, bool& overflow) {
+  auto get = [&](int layer, int sc, int kk) -> int {
+    if (sc < 0) return kWfaNone;
+    return wfa_get(H, wfa_unpack(meta[(uint32_t)sc * 3u + layer]), kk);
+  };
+  return wfa_traceback_t(L, get, pw, tw, m, n, s, k, slot, nops, overflow);
+}
+
 // G lanes align one pair; the 32 / G groups of a warp step in lockstep through
 // an outer loop of three phases so that their warp instructions are shared:
 //   fetch   -- groups without a pair take the next one and stage its bytes;
@@ -143,10 +151,10 @@ __global__ void __launch_bounds__(128) wfa_kernel(DevPairs P, WfaLaunch L) {
       uint32_t q = 0;
       if (gl == 0) q = atomicAdd(L.work, 1u);
       q = __shfl_sync(gmask, q, gbase);
-      if (q >= L.n) {
+      if (q >= (L.list ? min(*L.list_count, L.n) : L.n)) {
         phase = 2;
       } else {
-        p = q;
+        p = L.list ? L.list[q] : q;
         m = (int)P.read_len[p];
         n = (int)P.win_len[p];
         if (!L.valid || m == 0) {  // WfaCosts::scored refused: None; empty read: wfa.rs:555-563
@@ -371,6 +379,218 @@ __global__ void __launch_bounds__(128) wfa_kernel(DevPairs P, WfaLaunch L) {
   }
 }
 
+// Fixed-window WFA: one warp per pair, lane l owns diagonals win_base + 32 j + l
+// (j < NH) for the whole search. Every cell the recurrence can reach by score
+// win_smax lies in the window (an inserted base moves one diagonal down for at
+// least ei, a deleted base one up for at least ed, the seeds sit on
+// 0..text_begin_free), so up to that score the window is the whole wavefront and
+// no range is tracked; a 32-diagonal segment that no reached diagonal can touch
+// this score (new cells lie within one diagonal of the reached range) stays
+// "none" without being computed. The last lookback + 1 scores live in a shared
+// ring of int16 rows with a guard column on each side (the k - 1 / k + 1
+// neighbours of the edge diagonals read "none"); "none" is any negative value, so
+// the reference's checks become plain max / select: an unreached source stays
+// negative through the +1s of a search. A pair not done by win_smax (and not
+// exhausted) goes to fb_list for the general kernel, which redoes it from scratch.
+template <int NH, bool TB>
+__global__ void __launch_bounds__(128) wfa_window_kernel(DevPairs P, WfaLaunch L) {
+  constexpr int kW = 32 * NH;  // diagonals of the window
+  constexpr int kRow = kW + 2; // + 2 guards
+  constexpr int kNone16 = -32000;
+  extern __shared__ __align__(16) uint8_t wfa_smem[];
+  const int lane = threadIdx.x & 31;
+  const uint32_t wib = threadIdx.x >> 5;
+  const uint32_t stage = L.smem_group - L.ring_bytes;  // pattern + text bytes per warp
+  uint8_t* my = wfa_smem + (size_t)wib * (L.win_ring_bytes + stage);
+  int16_t* ring = (int16_t*)my;
+  uint32_t* pw = (uint32_t*)(my + L.win_ring_bytes + 16);
+  uint32_t* tw = (uint32_t*)(my + L.win_ring_bytes + L.pat_region + 16);
+  uint8_t* pb = (uint8_t*)pw;
+  uint8_t* tb = (uint8_t*)tw;
+  const uint32_t warp = blockIdx.x * (blockDim.x >> 5) + wib;
+  int16_t* hist = TB ? L.win_hist + (size_t)warp * (L.win_smax + 1) * 3 * kW : nullptr;
+  const int R = (int)L.ring_len;
+  const int x = L.x, oi = L.o + L.ei, od = L.o + L.ed, ei = L.ei, ed = L.ed;
+  const int xr = x % R, oir = oi % R, odr = od % R, eir = ei % R, edr = ed % R;
+  const int base = L.win_base;
+  for (int r = lane; r < R * 3; r += 32) {  // guard columns stay "none"
+    ring[r * kRow] = (int16_t)kNone16;
+    ring[r * kRow + kRow - 1] = (int16_t)kNone16;
+  }
+  for (;;) {
+    uint32_t p = 0;
+    if (lane == 0) p = atomicAdd(L.work, 1u);
+    p = __shfl_sync(kFull, p, 0);
+    if (p >= L.n) break;
+    const int m = (int)P.read_len[p], n = (int)P.win_len[p];
+    if (!L.valid || m == 0) {  // WfaCosts::scored refused: None; empty read: wfa.rs:555-563
+      if (lane == 0) {
+        kira_wfa_result res{};
+        res.cost = L.valid ? 0 : -1;
+        res.found = L.valid ? 1u : 0u;
+        L.out[p] = res;
+        if (TB) L.ncig[p] = 0;
+      }
+      continue;
+    }
+    const uint8_t* rs = P.read_seq + P.read_off[p];
+    const uint8_t* ws = P.win_seq + P.win_off[p];
+    __syncwarp();
+    for (int i = lane; i < m; i += 32) pb[i] = __ldg(rs + i);
+    for (int i = lane; i < n; i += 32) tb[i] = __ldg(ws + i);
+    int S = L.max_score_pp ? L.max_score_pp[p] : L.max_score;
+    if (!L.max_score_pp && S < 0) S = wfa_budget(m, L);
+    const int64_t cap = L.drop < 0 ? (int64_t)L.o + (int64_t)L.ei * m
+                                   : (int64_t)max(x, oi) * (2 * m + n + 2);
+    const int S_loop = (int)max((int64_t)0, min((int64_t)S, cap));
+    const int s_lim = min(S_loop, L.win_smax);
+    int tbf = L.tbf_pp ? L.tbf_pp[p] : L.tbf;
+    tbf = min(max(tbf, 0), max(n - 1, 0));
+    __syncwarp();
+    int done_s = -1, k_end = 0, last_live = 0, slot = 0;
+    int lo_seen = 0, hi_seen = tbf;  // reached diagonals so far (the seeds: 0 .. tbf)
+    bool dead = false;
+    for (int s = 0; s <= s_lim; ++s) {
+      bool need[NH];
+#pragma unroll
+      for (int h = 0; h < NH; ++h)
+        need[h] = lo_seen - 1 <= base + 32 * h + 31 && hi_seen + 1 >= base + 32 * h;
+      auto row = [&](int back, int backr, int layer) -> const int16_t* {
+        int sl = slot - backr;
+        if (sl < 0) sl += R;
+        return (s - back >= 0) ? ring + (sl * 3 + layer) * kRow : nullptr;
+      };
+      const int16_t* rMx = row(x, xr, 0);
+      const int16_t* rMoi = row(oi, oir, 0);
+      const int16_t* rMod = row(od, odr, 0);
+      const int16_t* rIe = row(ei, eir, 1);
+      const int16_t* rDe = row(ed, edr, 2);
+      int16_t* wM = ring + (slot * 3 + 0) * kRow;
+      int16_t* wI = ring + (slot * 3 + 1) * kRow;
+      int16_t* wD = ring + (slot * 3 + 2) * kRow;
+      int vm2[NH], vi2[NH], vd2[NH];
+#pragma unroll
+      for (int h = 0; h < NH; ++h) {
+        const int col = 1 + h * 32 + lane;
+        const int k = base + h * 32 + lane;
+        int vi = kNone16, vd = kNone16, vm = kNone16;
+        if (!need[h]) {
+          // this segment stays "none"
+        } else if (s == 0) {
+          vm = (k >= 0 && k <= tbf) ? 0 : kNone16;
+        } else {
+          if (rMoi) {
+            const int a = rMoi[col + 1];
+            vi = a < m ? a + 1 : kNone16;
+          }
+          if (rIe) {
+            const int b = rIe[col + 1];
+            vi = max(vi, b < m ? b + 1 : kNone16);
+          }
+          if (rMod) {
+            const int a = rMod[col - 1];
+            vd = a + k <= n ? a : kNone16;
+          }
+          if (rDe) {
+            const int b = rDe[col - 1];
+            vd = max(vd, b + k <= n ? b : kNone16);
+          }
+          if (rMx) {
+            const int a = rMx[col];
+            vm = (a < m && a + k < n) ? a + 1 : kNone16;
+          }
+          vm = max(vm, max(vi, vd));
+        }
+        if (vm >= 0) vm = wfa_extend(pw, tw, m, n, k, vm);
+        vm2[h] = vm, vi2[h] = vi, vd2[h] = vd;
+      }
+#pragma unroll
+      for (int h = 0; h < NH; ++h) {  // extend the reached range by this score's cells
+        const unsigned q = __ballot_sync(kFull, vm2[h] >= 0 || vi2[h] >= 0 || vd2[h] >= 0);
+        if (q) {
+          lo_seen = min(lo_seen, base + 32 * h + wfa_low_bit(q));
+          hi_seen = max(hi_seen, base + 32 * h + wfa_high_bit(q));
+        }
+      }
+      if (L.drop >= 0) {  // prune_wavefront (wfa.rs:293-346) on the extended M
+        int mad = INT32_MIN;
+#pragma unroll
+        for (int h = 0; h < NH; ++h)
+          if (vm2[h] >= 0) mad = max(mad, 2 * vm2[h] + base + h * 32 + lane);
+        mad = __reduce_max_sync(kFull, mad);
+        if (mad != INT32_MIN) {
+          const int th = mad - L.drop;
+#pragma unroll
+          for (int h = 0; h < NH; ++h)
+            if (vm2[h] >= 0 && 2 * vm2[h] + base + h * 32 + lane < th) vm2[h] = kNone16;
+        }
+      }
+      int kd = INT32_MAX;  // lowest done diagonal
+      bool live = false;
+#pragma unroll
+      for (int h = 0; h < NH; ++h) {
+        const int col = 1 + h * 32 + lane;
+        wM[col] = (int16_t)vm2[h];
+        wI[col] = (int16_t)vi2[h];
+        wD[col] = (int16_t)vd2[h];
+        if (TB) {
+          int16_t* hs = hist + (size_t)s * 3 * kW + h * 32 + lane;
+          hs[0] = (int16_t)vm2[h];
+          hs[kW] = (int16_t)vi2[h];
+          hs[2 * kW] = (int16_t)vd2[h];
+        }
+        const unsigned bd = __ballot_sync(kFull, vm2[h] >= m);
+        if (bd && kd == INT32_MAX) kd = base + 32 * h + wfa_low_bit(bd);
+        live |= (vm2[h] & vi2[h] & vd2[h]) >= 0;  // some value >= 0 unless all negative
+      }
+      live = __any_sync(kFull, live);
+      __syncwarp();
+      if (kd != INT32_MAX) {
+        done_s = s;
+        k_end = kd;
+        break;
+      }
+      // Nothing reached within the look-back window: no later score reaches anything.
+      if (live) last_live = s;
+      else if (s - last_live > L.lookback) {
+        dead = true;
+        break;
+      }
+      if (++slot == R) slot = 0;
+    }
+    if (lane == 0) {
+      if (done_s < 0 && !dead && S_loop > s_lim) {
+        L.fb_list[atomicAdd(L.fb_count, 1u)] = p;  // the general kernel redoes it
+      } else {
+        kira_wfa_result res{};
+        res.cost = -1;
+        uint32_t nops = 0;
+        if (done_s >= 0) {
+          res.found = 1;
+          res.cost = done_s;
+          res.score = L.scored ? m * L.match - done_s : done_s;
+          res.text_end = (uint32_t)(m + k_end);
+          if (TB) {
+            auto get = [&](int layer, int sc, int kk) -> int {
+              if (sc < 0 || kk < base || kk > base + kW - 1) return kWfaNone;
+              const int v = hist[(size_t)sc * 3 * kW + layer * kW + (kk - base)];
+              return v >= 0 ? v : kWfaNone;
+            };
+            bool ovf = false;
+            uint32_t* sl = L.slots + (size_t)p * L.slot_cap;
+            const int k0 = wfa_traceback_t(L, get, pw, tw, m, n, done_s, k_end, sl, nops, ovf);
+            res.text_start = (uint32_t)max(k0, 0);
+            if (ovf) atomicOr(L.flags, 1u);
+          }
+        }
+        if (TB) L.ncig[p] = nops;
+        L.out[p] = res;
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // cigar_off / n_cigar of every result and the ops in pair order (each pair's
 // slot holds its ops in reverse).
 __global__ void __launch_bounds__(256) wfa_compact_kernel(WfaCompact C) {
@@ -421,6 +641,27 @@ cudaError_t launch_wfa(const DevPairs& P, const WfaLaunch& L, uint32_t blocks,
     case 16: wfa_launch_g<16>(P, L, blocks, threads, smem, traceback, st); break;
     case 32: wfa_launch_g<32>(P, L, blocks, threads, smem, traceback, st); break;
     default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t wfa_window_blocks_per_sm(int segments, bool traceback, size_t smem, int* per_sm) {
+  auto kern = segments == 4 ? (traceback ? wfa_window_kernel<4, true> : wfa_window_kernel<4, false>)
+                            : (traceback ? wfa_window_kernel<2, true> : wfa_window_kernel<2, false>);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, 128, smem);
+}
+
+cudaError_t launch_wfa_window(const DevPairs& P, const WfaLaunch& L, uint32_t blocks,
+                              bool traceback, cudaStream_t st) {
+  const size_t smem = (size_t)4 * (L.win_ring_bytes + L.smem_group - L.ring_bytes);
+  if (L.win_segments == 4) {
+    if (traceback) wfa_window_kernel<4, true><<<blocks, 128, smem, st>>>(P, L);
+    else wfa_window_kernel<4, false><<<blocks, 128, smem, st>>>(P, L);
+  } else {
+    if (traceback) wfa_window_kernel<2, true><<<blocks, 128, smem, st>>>(P, L);
+    else wfa_window_kernel<2, false><<<blocks, 128, smem, st>>>(P, L);
   }
   return cudaGetLastError();
 }
