@@ -217,12 +217,13 @@ int kira_gpu_set_trace_budget(kira_ctx* ctx, uint64_t bytes);
  * Results are identical with and without graphs. */
 int kira_gpu_set_graphs(kira_ctx* ctx, int enable, uint64_t* captures, uint64_t* replays);
 
-/* kira_gpu_verify_batch on batches of at least 2 chunks runs chunk by chunk
- * through separate copy-in, compute and copy-out streams, so uploads, kernels and
- * downloads of consecutive chunks overlap (pinned host buffers make the copies
- * asynchronous). pairs < 0: automatic (a quarter of the batch, at least 2^18
- * pairs; the default), 0: off, else the chunk size. Results are identical either
- * way. */
+/* Host batches of at least 2 chunks run chunk by chunk through separate copy-in,
+ * compute and copy-out streams, so uploads, kernels and downloads of consecutive
+ * chunks overlap (pinned host buffers make the copies asynchronous); this applies
+ * to kira_gpu_verify_batch, kira_gpu_wfa_batch and kira_gpu_prefilter_batch.
+ * pairs < 0: automatic (the default: a quarter of the batch, at least 2^18
+ * pairs; verification batches of at least 2^20 pairs in chunks of 1/8, 3/8, 3/8
+ * and 1/8), 0: off, else the chunk size. Results are identical either way. */
 int kira_gpu_set_chunk_pairs(kira_ctx* ctx, int64_t pairs);
 
 /* Upload the reference as ASCII bases (Index::ref_bases, src/index/mod.rs:1098);

@@ -754,10 +754,10 @@ int plan_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const k
 // Results are identical to the one-shot path.
 int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_params& p,
                          kira_sw_result* out, kira_cigar_buf* cigar, kira_verify_detail* detail,
-                         uint64_t* cells, uint32_t chunk) {
+                         uint64_t* cells, const std::vector<uint32_t>& bounds) {
   cudaError_t cerr = cudaSuccess;
   const uint32_t n = P.n;
-  const uint32_t nch = (n + chunk - 1) / chunk;
+  const uint32_t nch = (uint32_t)bounds.size() - 1;  // chunk c: pairs [bounds[c], bounds[c + 1])
   cudaStream_t st = ctx->stream;
   const bool host_w = P.win_seq != nullptr;
   if (!host_w && !ctx->ref_dev) return fail(ctx, KIRA_ERR_INVALID, "no resident reference uploaded");
@@ -808,7 +808,7 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
   std::vector<uint32_t> sub_lo, sub_chunk, first_sub(nch + 1);
   for (uint32_t c = 0; c < nch; ++c) {
     first_sub[c] = (uint32_t)sub_lo.size();
-    const uint32_t lo = c * chunk, hi = std::min(n, lo + chunk);
+    const uint32_t lo = bounds[c], hi = bounds[c + 1];
     for (uint32_t x = lo; x < hi; x += kSub) sub_lo.push_back(x), sub_chunk.push_back(c);
   }
   first_sub[nch] = (uint32_t)sub_lo.size();
@@ -821,7 +821,7 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
     const uint32_t sidx = next.fetch_add(1, std::memory_order_relaxed);
     if (sidx >= nsub) return false;
     const uint32_t c = sub_chunk[sidx];
-    const uint32_t hi = std::min(std::min(n, c * chunk + chunk), sub_lo[sidx] + kSub);
+    const uint32_t hi = std::min(bounds[c + 1], sub_lo[sidx] + kSub);
     scan_range(sub_lo[sidx], hi, subs[sidx]);
     left[c].fetch_sub(1, std::memory_order_release);
     return true;
@@ -934,7 +934,7 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
       cudaStreamSynchronize(ctx->d2h);
       return rc;
     }
-    const uint32_t lo = c * chunk, hi = std::min(n, lo + chunk), m = hi - lo;
+    const uint32_t lo = bounds[c], hi = bounds[c + 1], m = hi - lo;
     const Maxes mx = scans[c].mx;
     const uint64_t rneed = std::max(rdone, scans[c].rend), wneed = std::max(wdone, scans[c].wend);
     cudaStream_t up = ctx->h2d;
@@ -2321,13 +2321,25 @@ int kira_gpu_verify_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_ver
   cudaSetDevice(ctx->device);
   // Chunks alternate between two compute streams so each chunk's row-serial DP and
   // traceback tail overlaps the next chunk; a few large chunks still do best
-  // (each pays some fixed launch and tail cost): by default a quarter of the
-  // batch, at least 2^18 pairs.
-  const uint64_t chunk = ctx->chunk_pairs < 0
-                             ? std::max<uint64_t>(1u << 18, (P.n + 3ull) / 4)
-                             : (uint64_t)ctx->chunk_pairs;
-  if (!ctx->profile && chunk && P.n >= 2 * chunk)
-    return verify_batch_chunked(ctx, P, *p, out, cigar, detail, cells, (uint32_t)chunk);
+  // (each pays some fixed launch and tail cost). Automatic: batches of at least
+  // 2^20 pairs in chunks of 1/8, 3/8, 3/8, 1/8 of the batch (a small first chunk
+  // starts the GPU sooner, a small last one drains sooner), smaller ones in
+  // quarters of at least 2^18 pairs; chunk_pairs > 0: equal chunks of that size.
+  std::vector<uint32_t> bounds;
+  if (!ctx->profile) {
+    const uint64_t n = P.n;
+    if (ctx->chunk_pairs < 0 && n >= (1u << 20)) {
+      bounds = {0u, (uint32_t)(n / 8), (uint32_t)(n / 2), (uint32_t)(n - n / 8), (uint32_t)n};
+    } else {
+      const uint64_t chunk = ctx->chunk_pairs < 0 ? std::max<uint64_t>(1u << 18, (n + 3) / 4)
+                                                  : (uint64_t)ctx->chunk_pairs;
+      if (chunk && n >= 2 * chunk)
+        for (uint64_t lo = 0; lo <= n; lo += chunk) bounds.push_back((uint32_t)std::min(lo, n));
+      if (!bounds.empty() && bounds.back() != n) bounds.push_back((uint32_t)n);
+    }
+  }
+  if (bounds.size() >= 3)
+    return verify_batch_chunked(ctx, P, *p, out, cigar, detail, cells, bounds);
   const Maxes mx = host_maxes(ctx, P, p->sw.bandwidth);
   DevPairs D;
   int rc = upload_pairs(ctx, P, D);

@@ -191,3 +191,22 @@ def test_chunked_host_checks_in_sub_ranges(ctx):
     finally:
         ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, -1))
     assert np.array_equal(one[0], chunked[0]) and np.array_equal(one[1], chunked[1])
+
+
+def test_uneven_automatic_chunks(ctx):
+    # Batches of at least 2^20 pairs go in chunks of 1/8, 3/8, 3/8, 1/8 of the batch
+    # by default; results equal the one-shot path.
+    from kira_ls_aligner_b200 import PairBatch, VerifyParams, _abi, synth
+    w = synth.make_workload("u", 270_000, 5_000_000, cands=4, sub_lo=0.0, sub_hi=0.03, seed=80)
+    assert w.n_pairs >= 1 << 20
+    ctx.ref_upload(w.reference)
+    b = PairBatch(w.reads, w.read_off, w.read_len, None, w.win_off, w.win_len)
+    params = VerifyParams(sieve_threshold=12, myers_k=8)
+    L = _abi.lib()
+    try:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, 0))
+        one = ctx.verify_batch(b, params)
+    finally:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, -1))
+    auto = ctx.verify_batch(b, params)
+    assert np.array_equal(one[0], auto[0]) and np.array_equal(one[1], auto[1]) and one[3] == auto[3]
