@@ -298,3 +298,26 @@ def test_chunked_host_path(ctx, traceback):
             got = (int(r["cost"]), int(r["score"]), int(r["text_start"]), int(r["text_end"]),
                    [(a, c) for a, c in cig])
         assert got == want[j], i
+
+
+@pytest.mark.parametrize("traceback", [True, False])
+def test_wide_window_and_fallbacks(ctx, traceback):
+    # Costs with a free gap open and unit extends: 64 diagonals cover fewer than 32
+    # scores, so the window kernel uses 128 diagonals (exact up to score 63), and
+    # pairs still open then go through the general kernel's fallback list. Every
+    # result equals the oracle; the general kernel alone (lanes 32) agrees too.
+    from kira_ls_aligner_b200 import WfaParams, _abi, synth
+    w = synth.wfa_cascade(3000, seed=0x64D, err_hi=0.3, ref_len=400_000)
+    ref = w.reference
+    pairs = [(w.reads[int(w.read_off[i]):int(w.read_off[i]) + 150].tobytes(),
+              ref[int(w.win_off[i]):int(w.win_off[i]) + int(w.win_len[i])].tobytes())
+             for i in range(w.n_pairs)]
+    p = WfaParams(2, 0, 1, max_score=120, traceback=traceback)
+    got = _check(ctx, pairs, p)
+    costs = [x[0] for x in got if x is not None]
+    assert max(costs) > 63 and min(costs) < 20  # both the window and the fallback ran
+    ctx.check(_abi.lib().kira_gpu_set_wfa_lanes(ctx.handle, 32))
+    try:
+        assert _gpu(ctx, pairs, p) == got
+    finally:
+        ctx.check(_abi.lib().kira_gpu_set_wfa_lanes(ctx.handle, 0))
