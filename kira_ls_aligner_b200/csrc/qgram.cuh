@@ -17,13 +17,39 @@
 //
 // Lane-per-pair: the window's 4-gram set is a 256-bit bitmap per lane in shared
 // memory laid out [word][lane] (each lane owns one bank); bases come from the
-// 2-bit + valid plane arenas, one 32-base word at a time.
+// 2-bit + valid plane arenas, one 32-base word at a time. A 4-gram's 8-bit code is
+// its four bit-0 plane bits and its four bit-1 plane bits (one bit-field extract
+// each, the previous word supplying the first three bases of a word); the
+// positions whose four bases are all valid come from one AND of shifted valid
+// masks per word. Window and read use the same code, so the count is the count.
 #pragma once
 
 #include "common.cuh"
 #include "planes.cuh"
 
 namespace kira {
+
+// Bits [b - 3, b] of the base stream ... prev | cur (b in 0..31, compile-time).
+template <int B>
+__device__ __forceinline__ uint32_t qgram_nibble(uint32_t prev, uint32_t cur) {
+  if constexpr (B >= 3) return (cur >> (B - 3)) & 0xFu;
+  else return __funnelshift_r(prev, cur, 29 + B) & 0xFu;
+}
+
+// Positions of a word whose 4-gram (this base and the three before) is all ACGT.
+__device__ __forceinline__ uint32_t qgram_valid4(uint32_t pv, uint32_t v, uint32_t lim) {
+  uint32_t v4 = v & __funnelshift_l(pv, v, 1) & __funnelshift_l(pv, v, 2) &
+                __funnelshift_l(pv, v, 3);
+  return lim < 32u ? v4 & ((1u << lim) - 1u) : v4;
+}
+
+template <int B>
+__device__ __forceinline__ void qgram_code(uint32_t p0, uint32_t c0, uint32_t p1, uint32_t c1,
+                                           uint32_t& word, uint32_t& bit) {
+  const uint32_t x0 = qgram_nibble<B>(p0, c0), x1 = qgram_nibble<B>(p1, c1);
+  word = x1 >> 1;
+  bit = ((x1 & 1u) << 4) | x0;
+}
 
 // True when the read provably has edit distance > k to every window substring.
 // `set` points at this lane's column of an [8][32] word bitmap in shared memory.
@@ -35,33 +61,46 @@ __device__ __forceinline__ bool qgram4_reject(const uint4* __restrict__ rplanes,
   if (need <= 0 || n < 4u) return false;
 #pragma unroll
   for (int w = 0; w < 8; ++w) set[w * 32] = 0u;
-  uint32_t code = 0, vrun = 0;
+  uint32_t p0 = 0, p1 = 0, pv = 0;
   for (uint32_t blk = 0; blk * 32u < n; ++blk) {
     const PlaneWord pw = plane_word_at(wplanes, wpos + 32u * blk);
-    const uint32_t lim = min(32u, n - 32u * blk);
-#pragma unroll
-    for (uint32_t b = 0; b < 32u; ++b) {
-      if (b < lim) {
-        code = ((code << 2) | (((pw.b1 >> b) & 1u) << 1) | ((pw.b0 >> b) & 1u)) & 0xFFu;
-        vrun = ((pw.v >> b) & 1u) ? vrun + 1u : 0u;
-        if (vrun >= 4u) set[(code >> 5) * 32u] |= 1u << (code & 31u);
-      }
-    }
+    const uint32_t v4 = qgram_valid4(pv, pw.v, min(32u, n - 32u * blk));
+#define KIRA_QG_SET(B)                                          \
+  if ((v4 >> (B)) & 1u) {                                       \
+    uint32_t word, bit;                                         \
+    qgram_code<(B)>(p0, pw.b0, p1, pw.b1, word, bit);           \
+    set[word * 32u] |= 1u << bit;                               \
+  }
+    KIRA_QG_SET(0) KIRA_QG_SET(1) KIRA_QG_SET(2) KIRA_QG_SET(3) KIRA_QG_SET(4) KIRA_QG_SET(5)
+    KIRA_QG_SET(6) KIRA_QG_SET(7) KIRA_QG_SET(8) KIRA_QG_SET(9) KIRA_QG_SET(10) KIRA_QG_SET(11)
+    KIRA_QG_SET(12) KIRA_QG_SET(13) KIRA_QG_SET(14) KIRA_QG_SET(15) KIRA_QG_SET(16)
+    KIRA_QG_SET(17) KIRA_QG_SET(18) KIRA_QG_SET(19) KIRA_QG_SET(20) KIRA_QG_SET(21)
+    KIRA_QG_SET(22) KIRA_QG_SET(23) KIRA_QG_SET(24) KIRA_QG_SET(25) KIRA_QG_SET(26)
+    KIRA_QG_SET(27) KIRA_QG_SET(28) KIRA_QG_SET(29) KIRA_QG_SET(30) KIRA_QG_SET(31)
+#undef KIRA_QG_SET
+    p0 = pw.b0, p1 = pw.b1, pv = pw.v;
   }
   int32_t count = 0;
-  code = 0;
-  vrun = 0;
+  p0 = p1 = pv = 0;
   for (uint32_t blk = 0; blk * 32u < m; ++blk) {
     const PlaneWord pw = plane_word_at(rplanes, rpos + 32u * blk);
     const uint32_t lim = min(32u, m - 32u * blk);
-#pragma unroll
-    for (uint32_t b = 0; b < 32u; ++b) {
-      if (b < lim) {
-        code = ((code << 2) | (((pw.b1 >> b) & 1u) << 1) | ((pw.b0 >> b) & 1u)) & 0xFFu;
-        vrun = ((pw.v >> b) & 1u) ? vrun + 1u : 0u;
-        if (vrun >= 4u) count += (int32_t)((set[(code >> 5) * 32u] >> (code & 31u)) & 1u);
-      }
-    }
+    const uint32_t v4 = qgram_valid4(pv, pw.v, lim);
+#define KIRA_QG_COUNT(B)                                        \
+  if ((v4 >> (B)) & 1u) {                                       \
+    uint32_t word, bit;                                         \
+    qgram_code<(B)>(p0, pw.b0, p1, pw.b1, word, bit);           \
+    count += (int32_t)((set[word * 32u] >> bit) & 1u);          \
+  }
+    KIRA_QG_COUNT(0) KIRA_QG_COUNT(1) KIRA_QG_COUNT(2) KIRA_QG_COUNT(3) KIRA_QG_COUNT(4)
+    KIRA_QG_COUNT(5) KIRA_QG_COUNT(6) KIRA_QG_COUNT(7) KIRA_QG_COUNT(8) KIRA_QG_COUNT(9)
+    KIRA_QG_COUNT(10) KIRA_QG_COUNT(11) KIRA_QG_COUNT(12) KIRA_QG_COUNT(13) KIRA_QG_COUNT(14)
+    KIRA_QG_COUNT(15) KIRA_QG_COUNT(16) KIRA_QG_COUNT(17) KIRA_QG_COUNT(18) KIRA_QG_COUNT(19)
+    KIRA_QG_COUNT(20) KIRA_QG_COUNT(21) KIRA_QG_COUNT(22) KIRA_QG_COUNT(23) KIRA_QG_COUNT(24)
+    KIRA_QG_COUNT(25) KIRA_QG_COUNT(26) KIRA_QG_COUNT(27) KIRA_QG_COUNT(28) KIRA_QG_COUNT(29)
+    KIRA_QG_COUNT(30) KIRA_QG_COUNT(31)
+#undef KIRA_QG_COUNT
+    p0 = pw.b0, p1 = pw.b1, pv = pw.v;
     // Decided either way once the count reaches the bound or can no longer.
     const int32_t left = (int32_t)m - (int32_t)(32u * blk + lim);
     if (count >= need) return false;
