@@ -413,7 +413,7 @@ uint64_t trace_budget(kira_ctx* ctx) {
 
 // Trace slot bytes of one item of a shape over reads of up to max_q bases.
 uint64_t trace_slot_bytes(int shape, uint32_t max_q) {
-  return (((uint64_t)(max_q + 1) * shape_row_stride(kBswShapes[shape])) + 15) & ~15ull;
+  return shape_slot_bytes(kBswShapes[shape], max_q);
 }
 
 // True when the trace arena already holds `slot_bytes` of slots and `meta_words`

@@ -257,65 +257,91 @@ __device__ __forceinline__ void bsw_group_sweep(
   cells_out = cells;
 }
 
-// One thread per item: the traceback state machine of mod.rs:1581-1627 over the
-// item's trace slot; CIGAR runs are written in reverse order into the item's
-// CIGAR slot (the compaction kernel reverses them).
-__device__ __forceinline__ uint32_t bsw_walk(const uint8_t* __restrict__ trace,
-                                             const uint32_t* __restrict__ meta, uint32_t k_cells,
-                                             uint32_t lane_bytes, uint32_t row_stride, int32_t& i,
-                                             int32_t& j, uint32_t* __restrict__ ops,
-                                             uint32_t cap, uint32_t& overflow) {
-  int state = 0;  // 0 H, 1 E, 2 F
+// Traceback state machine of mod.rs:1581-1627, one warp per item. The 32 lanes
+// read the next 32 cells of the current run at once (diagonal in H, up in E, left
+// in F) and a ballot finds the first cell that ends it, so a run costs one memory
+// round trip per 32 cells instead of one per cell; the moves, their tie order and
+// the CIGAR are those of the one-cell-at-a-time walk. `code(i, j)` gives a cell's
+// trace code: bits 0-1 the H move (0 stop, 1 diagonal, 2 E, 3 F), bit 2 E
+// extended, bit 3 F extended, 0xFF outside the row's band. CIGAR runs are written
+// in reverse order into `ops` by lane 0 (the compaction kernel reverses them).
+template <class Code>
+__device__ __forceinline__ uint32_t warp_walk(const Code& code, int32_t& i, int32_t& j,
+                                              uint32_t* __restrict__ ops, uint32_t cap,
+                                              uint32_t& overflow) {
+  const int32_t lane = (int32_t)(threadIdx.x & 31u);
+  uint32_t state = 0;  // 0 H, 1 E, 2 F; also the CIGAR op the state emits (M, I, D)
   uint32_t n = 0, cur_op = 0xFFu, cur_len = 0;
-  auto push = [&](uint32_t op) {
+  auto push = [&](uint32_t op, uint32_t cnt) {
+    if (!cnt) return;
     if (op == cur_op) {
-      ++cur_len;
+      cur_len += cnt;
       return;
     }
     if (cur_len) {
-      if (n < cap) ops[n] = (cur_len << 4) | cur_op;
-      else overflow = 1;
+      if (n < cap) {
+        if (lane == 0) ops[n] = (cur_len << 4) | cur_op;
+      } else {
+        overflow = 1;
+      }
       ++n;
     }
     cur_op = op;
-    cur_len = 1;
+    cur_len = cnt;
   };
   while (i > 0 && j > 0) {
-    const uint32_t m = __ldg(meta + i);
-    const int32_t rs = (int32_t)(m >> 11), rl = (int32_t)(m & 2047u);
-    const int32_t idx = j - rs;
-    if (idx < 0 || idx >= rl) break;
-    const uint32_t gi = (uint32_t)idx / k_cells, kk = (uint32_t)idx - gi * k_cells;
-    const uint32_t byte = trace[(size_t)i * row_stride + gi * lane_bytes + (kk >> 1)];
-    const uint32_t tr = (byte >> ((kk & 1u) * 4u)) & 15u;
-    if (state == 0) {
-      const uint32_t dd = tr & 3u;
-      if (dd == 0) break;
-      if (dd == 1) {
-        push(0);
-        --i;
-        --j;
-      } else if (dd == 2) {
-        state = 1;
-      } else {
-        state = 2;
-      }
-    } else if (state == 1) {
-      push(1);
-      --i;
-      state = (tr & 4u) ? 1 : 0;
-    } else {
-      push(2);
-      --j;
-      state = (tr & 8u) ? 2 : 0;
+    const int32_t di = state != 2u ? 1 : 0, dj = state != 1u ? 1 : 0;
+    const int32_t ci = i - lane * di, cj = j - lane * dj;
+    // A cell past row or column 0 ends the walk like the loop test does.
+    const uint32_t c = (ci > 0 && cj > 0) ? code(ci, cj) : 0xFFu;
+    const bool cont = c != 0xFFu && (state == 0u   ? (c & 3u) == 1u
+                                     : state == 1u ? (c & 4u) != 0u
+                                                   : (c & 8u) != 0u);
+    const uint32_t stop = __ballot_sync(0xffffffffu, !cont);
+    const uint32_t t = stop ? (uint32_t)(__ffs(stop) - 1) : 32u;
+    push(state, t);
+    i -= (int32_t)t * di;
+    j -= (int32_t)t * dj;
+    if (t == 32u) continue;
+    const uint32_t ct = __shfl_sync(0xffffffffu, c, (int)t);
+    if (ct == 0xFFu) break;
+    if (state == 0u) {
+      if ((ct & 3u) == 0u) break;  // H == 0
+      state = (ct & 3u) - 1u;      // E or F at the same cell
+    } else {                       // the gap's last cell, then back to H
+      push(state, 1u);
+      if (state == 1u) --i;
+      else --j;
+      state = 0u;
     }
   }
   if (cur_len) {
-    if (n < cap) ops[n] = (cur_len << 4) | cur_op;
-    else overflow = 1;
+    if (n < cap) {
+      if (lane == 0) ops[n] = (cur_len << 4) | cur_op;
+    } else {
+      overflow = 1;
+    }
     ++n;
   }
   return n;
 }
+
+// Trace codes of the int32 sweep of shape <G, K>: one nibble per cell, already in
+// warp_walk's code layout; lane gi of the row holds band cells gi*K .. +K-1.
+template <int G, int K>
+struct BswCode {
+  const uint8_t* __restrict__ trace;
+  const uint32_t* __restrict__ meta;
+  __device__ __forceinline__ uint32_t operator()(int32_t i, int32_t j) const {
+    constexpr uint32_t LB = BswShape<G, K>::kLaneBytes, S = BswShape<G, K>::kRowStride;
+    const uint32_t m = __ldg(meta + i);
+    const int32_t rs = (int32_t)(m >> 11), rl = (int32_t)(m & 2047u);
+    const int32_t idx = j - rs;
+    if (idx < 0 || idx >= rl) return 0xFFu;
+    const uint32_t gi = (uint32_t)idx / (uint32_t)K, kk = (uint32_t)idx - gi * (uint32_t)K;
+    const uint32_t byte = __ldg(trace + (size_t)i * S + gi * LB + (kk >> 1));
+    return (byte >> ((kk & 1u) * 4u)) & 15u;
+  }
+};
 
 }  // namespace kira

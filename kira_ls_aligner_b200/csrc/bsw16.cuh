@@ -41,6 +41,10 @@ struct Bsw16Shape {
   static constexpr int kSlabs = (kWords + 1) / 2;      // 8-byte stores per lane per row
   static constexpr int kLaneBytes = 8 * kSlabs;        // one code byte per cell
   static constexpr int kRowStride = G * kLaneBytes;
+  // Rows interleave in blocks of kInterleave: a block stores slab by slab, and in
+  // each slab row by row, so one 128-byte line holds one slab of kInterleave
+  // consecutive rows (the cells a diagonal traceback run reads next).
+  static constexpr int kInterleave = G >= 16 ? 1 : 16 / G;
 };
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
@@ -273,9 +277,12 @@ __device__ __forceinline__ void bsw16_group_sweep(
       pe[k] = ev[k] & act[k];
       ck += GE2S;
     }
-    // Row layout [slab][lane] of 8-byte words: a group's lanes fill one contiguous
-    // G x 8-byte run per slab, so each store instruction writes whole sectors.
-    uint2* trow = reinterpret_cast<uint2*>(trace + (size_t)i * S) + g;
+    // Layout [row block][slab][row in block][lane] of 8-byte words: a group's
+    // lanes fill one contiguous G x 8-byte run per slab, so each store
+    // instruction writes whole sectors.
+    constexpr int R = Bsw16Shape<G, K>::kInterleave;
+    uint2* trow = reinterpret_cast<uint2*>(trace + (size_t)(i & ~(R - 1)) * S +
+                                           (size_t)(i & (R - 1)) * (G * 8)) + g;
 #pragma unroll
     for (int x2 = 0; x2 < NS; ++x2) {
       constexpr int kLast = K - 1;
@@ -283,7 +290,7 @@ __device__ __forceinline__ void bsw16_group_sweep(
                 d = a + 3 <= kLast ? a + 3 : kLast;
       const uint32_t w0 = prmt(code[a], code[b], 0x7531u);
       const uint32_t w1 = 2 * x2 + 1 < NW ? prmt(code[c], code[d], 0x7531u) : 0u;
-      trow[x2 * G] = make_uint2(w0, w1);
+      trow[x2 * R * G] = make_uint2(w0, w1);
     }
     if (g == 0) meta[i] = ((uint32_t)js << 11) | (uint32_t)row_len;
 
@@ -345,69 +352,35 @@ __device__ __forceinline__ void bsw16_group_sweep(
   cells_out = cells;
 }
 
-// Traceback over the packed kernel's byte codes (state machine of
-// mod.rs:1581-1627). Code byte of a cell: bit 7 H > 0, bit 6 diag >= E,
-// bit 5 max(diag, E) >= F, bit 4 E extended, bit 3 F NOT extended.
-__device__ __forceinline__ uint32_t bsw16_walk(const uint8_t* __restrict__ trace,
-                                               const uint32_t* __restrict__ meta, uint32_t k_words,
-                                               uint32_t half, uint32_t lane_bytes,
-                                               uint32_t row_stride, int32_t go, int32_t& i,
-                                               int32_t& j, uint32_t* __restrict__ ops,
-                                               uint32_t cap, uint32_t& overflow) {
-  int state = 0;  // 0 H, 1 E, 2 F
-  uint32_t n = 0, cur_op = 0xFFu, cur_len = 0;
-  auto push = [&](uint32_t op) {
-    if (op == cur_op) {
-      ++cur_len;
-      return;
-    }
-    if (cur_len) {
-      if (n < cap) ops[n] = (cur_len << 4) | cur_op;
-      else overflow = 1;
-      ++n;
-    }
-    cur_op = op;
-    cur_len = 1;
-  };
-  while (i > 0 && j > 0) {
+// Trace codes of the packed sweep (state machine of mod.rs:1581-1627). Code byte
+// of a cell: bit 7 H > 0, bit 6 diag >= E, bit 5 max(diag, E) >= F, bit 4 E
+// extended, bit 3 F NOT extended (F always closes after one cell when the gap open
+// is 0). The row holds two halves of G*K band cells; in each, lane gi keeps cells
+// gi*K .. +K-1, word kk/2 of lane gi in slab kk/4, stored as [row block][slab][row
+// in block][lane] of 8-byte words (Bsw16Shape::kInterleave rows per block).
+// Decoded into warp_walk's code layout.
+template <int G, int K>
+struct Bsw16Code {
+  const uint8_t* __restrict__ trace;
+  const uint32_t* __restrict__ meta;
+  int32_t go;
+  __device__ __forceinline__ uint32_t operator()(int32_t i, int32_t j) const {
+    constexpr uint32_t H = Bsw16Shape<G, K>::kHalf, S = Bsw16Shape<G, K>::kRowStride;
+    constexpr uint32_t R = Bsw16Shape<G, K>::kInterleave;
     const uint32_t m = __ldg(meta + i);
     const int32_t rs = (int32_t)(m >> 11), rl = (int32_t)(m & 2047u);
     const int32_t idx = j - rs;
-    if (idx < 0 || idx >= rl) break;
-    const uint32_t hi = (uint32_t)idx >= half ? 1u : 0u;
-    const uint32_t c = (uint32_t)idx - hi * half;
-    const uint32_t gi = c / k_words, kk = c - gi * k_words;
-    // [slab][lane] rows of 8-byte words: word kk/2 of lane gi sits in slab kk/4.
-    const uint32_t lanes = half / k_words;
-    const uint32_t b = trace[(size_t)i * row_stride + (kk >> 2) * lanes * 8u + gi * 8u +
-                             ((kk >> 1) & 1u) * 4u + (kk & 1u) * 2u + hi];
-    if (state == 0) {
-      if (!(b & 0x80u)) break;  // H == 0
-      if ((b & 0x60u) == 0x60u) {
-        push(0);
-        --i;
-        --j;
-      } else if (b & 0x20u) {
-        state = 1;
-      } else {
-        state = 2;
-      }
-    } else if (state == 1) {
-      push(1);
-      --i;
-      state = (b & 0x10u) ? 1 : 0;
-    } else {
-      push(2);
-      --j;
-      state = (go > 0 && !(b & 0x08u)) ? 2 : 0;
-    }
+    if (idx < 0 || idx >= rl) return 0xFFu;
+    const uint32_t hi = (uint32_t)idx >= H ? 1u : 0u;
+    const uint32_t c = (uint32_t)idx - hi * H;
+    const uint32_t gi = c / (uint32_t)K, kk = c - gi * (uint32_t)K;
+    const uint32_t ib = (uint32_t)i & (R - 1u);
+    const uint32_t b = __ldg(trace + (size_t)((uint32_t)i - ib) * S +
+                             ((kk >> 2) * R + ib) * (G * 8u) + gi * 8u +
+                             ((kk >> 1) & 1u) * 4u + (kk & 1u) * 2u + hi);
+    const uint32_t h = !(b & 0x80u) ? 0u : (b & 0x60u) == 0x60u ? 1u : (b & 0x20u) ? 2u : 3u;
+    return h | ((b >> 2) & 4u) | ((go > 0 && !(b & 0x08u)) ? 8u : 0u);
   }
-  if (cur_len) {
-    if (n < cap) ops[n] = (cur_len << 4) | cur_op;
-    else overflow = 1;
-    ++n;
-  }
-  return n;
-}
+};
 
 }  // namespace kira

@@ -203,6 +203,17 @@ inline uint32_t shape_lane_bytes(const BswShapeInfo& s) {
 inline uint32_t shape_row_stride(const BswShapeInfo& s) {
   return (uint32_t)s.g * shape_lane_bytes(s);
 }
+// Rows per interleave block of the packed trace (Bsw16Shape::kInterleave).
+inline uint32_t shape_row_interleave(const BswShapeInfo& s) {
+  return s.packed && s.g < 16 ? 16u / (uint32_t)s.g : 1u;
+}
+// Bytes of one item's trace slot for reads of up to `max_q` bases: rows 0..max_q
+// rounded up to whole interleave blocks, then to 16 bytes.
+inline uint64_t shape_slot_bytes(const BswShapeInfo& s, uint32_t max_q) {
+  const uint64_t r = shape_row_interleave(s);
+  const uint64_t rows = ((uint64_t)max_q + 1 + r - 1) / r * r;
+  return (rows * shape_row_stride(s) + 15) & ~15ull;
+}
 inline TraceGeom shape_trace_geom(const BswShapeInfo& s, uint8_t* trace, uint32_t* meta,
                                   uint64_t slot_bytes, uint32_t meta_stride) {
   return TraceGeom{trace, meta, slot_bytes, shape_row_stride(s), shape_lane_bytes(s),

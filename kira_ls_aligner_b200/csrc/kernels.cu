@@ -471,11 +471,15 @@ __global__ void __launch_bounds__(T, MINB) bsw16_dp_kernel(DevPairs P, BswLaunch
   }
 }
 
+// One warp per item (warp_walk over the trace of shape <G, K>, packed or int32);
+// lane 0 writes the item's result row.
+template <int G, int K, bool PACKED>
 __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
   const uint32_t count = bsw_round_end(B);
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t item = B.item_lo + blockIdx.x * blockDim.x + threadIdx.x; item < count;
-       item += stride) {
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  const bool lead = (threadIdx.x & 31u) == 0u;
+  for (uint32_t item = B.item_lo + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+       item < count; item += warps) {
     const uint32_t pair = B.list ? B.list[item] : item;
     const DpEnd e = B.ends[item];
     int32_t i = e.end_i, j = e.end_j;
@@ -484,11 +488,12 @@ __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
     const uint8_t* tr = B.tg.trace + (size_t)slot_item * B.tg.slot_bytes;
     const uint32_t* mt = B.tg.meta + (size_t)slot_item * B.tg.meta_stride;
     uint32_t* ops = B.cig_slots + (size_t)item * B.slot_cap;
-    const uint32_t n =
-        B.tg.half ? bsw16_walk(tr, mt, B.tg.k_cells, B.tg.half, B.tg.lane_bytes, B.tg.row_stride,
-                               B.sp.gap_open, i, j, ops, B.slot_cap, overflow)
-                  : bsw_walk(tr, mt, B.tg.k_cells, B.tg.lane_bytes, B.tg.row_stride, i, j, ops,
-                             B.slot_cap, overflow);
+    uint32_t n;
+    if constexpr (PACKED)
+      n = warp_walk(Bsw16Code<G, K>{tr, mt, B.sp.gap_open}, i, j, ops, B.slot_cap, overflow);
+    else
+      n = warp_walk(BswCode<G, K>{tr, mt}, i, j, ops, B.slot_cap, overflow);
+    if (!lead) continue;
     kira_sw_result r;
     r.score = e.score;
     r.ref_start = (uint32_t)j;
@@ -767,8 +772,8 @@ static cudaError_t launch_bsw_shape(const DevPairs& P, const BswLaunch& B, uint3
   }
   if (between) cudaEventRecord(between, st);
   if (parts & kBswPartTb) {
-    const int tb_blocks = grid_for(max_items, 128, sms * 16);
-    bsw_tb_kernel<<<tb_blocks, 128, 0, st>>>(P, B);
+    const int tb_blocks = grid_for(max_items, 4, sms * 16);  // a warp per item
+    bsw_tb_kernel<G, K, false><<<tb_blocks, 128, 0, st>>>(P, B);
     e = cudaGetLastError();
   }
   return e;
@@ -792,8 +797,8 @@ static cudaError_t launch_bsw16_shape(const DevPairs& P, const BswLaunch& B, uin
   }
   if (between) cudaEventRecord(between, st);
   if (parts & kBswPartTb) {
-    const int tb_blocks = grid_for(max_items, 128, sms * 16);
-    bsw_tb_kernel<<<tb_blocks, 128, 0, st>>>(P, B);
+    const int tb_blocks = grid_for(max_items, 4, sms * 16);  // a warp per item
+    bsw_tb_kernel<G, K, true><<<tb_blocks, 128, 0, st>>>(P, B);
     e = cudaGetLastError();
   }
   return e;

@@ -99,8 +99,7 @@ extern "C" int kira_gpu_bsw_batch_noalloc(const kira_pairs* pairs, const kira_sw
   if (scratch_address(&sp) != cudaSuccess) return KIRA_ERR_RUNTIME;
   const uint32_t n = P.n;
   const BswShapeInfo sh = kBswShapes[shape];
-  const uint32_t row_stride = shape_row_stride(sh);
-  const uint64_t slot = (((uint64_t)(max_q + 1) * row_stride) + 15) & ~15ull;
+  const uint64_t slot = shape_slot_bytes(sh, max_q);
   const uint32_t meta_stride = max_q + 1;
   const uint32_t slot_cap = max_q + max_w + 2;
   Carve cv{static_cast<unsigned char*>(sp), 0, KIRA_NOALLOC_SCRATCH_BYTES};
