@@ -31,7 +31,7 @@ enum BufId {
   B_DIST, B_END, B_SIEVE_OUT, B_SIEVE_JOBS, B_CELLS, B_TOTAL, B_READ_PLANES, B_WIN_PLANES,
   B_ROWKEYS, B_DONE_ROW, B_WORK, B_WFA_MAXS, B_WFA_TBF, B_WFA_OUT, B_WFA_NCIG, B_WFA_SLOTS,
   B_WFA_SCRATCH, B_WFA_FLAGS, B_PF_CHAINS, B_PF_TOP1, B_PF_MARGIN, B_PF_OUT, B_PF_NCIG,
-  B_PF_MDLEN, B_PF_MDOFF, B_PF_MD, B_PF_EXACT, B_WFA_FB, B_WFA_WHIST, B_COUNT
+  B_PF_MDLEN, B_PF_MDOFF, B_PF_MD, B_PF_EXACT, B_WFA_FB, B_WFA_WHIST, B_SIEVE_LIST, B_COUNT
 };
 
 struct DevBuf {
@@ -523,7 +523,13 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
   KIRA_DBUF(counters, uint32_t, B_COUNTERS, 4);
   KIRA_CUDA(cudaMemsetAsync(counters, 0, cm.first ? 16 : 8, st));
   VerifyDev V{p.sieve_threshold, p.cert_strict, sp,       out,       detail, ncig,
-              swoff,             mlist,         counters, p.myers_k, (p.flags & KIRA_VERIFY_NO_QGRAM) ? 0 : 1};
+              swoff,             mlist,         counters, p.myers_k, (p.flags & KIRA_VERIFY_NO_QGRAM) ? 0 : 1,
+              nullptr,           nullptr};
+  if (!detail && V.qgram) {  // filter-first sieve: survivor list after its count word
+    KIRA_DBUF(sl, uint32_t, B_SIEVE_LIST, (uint64_t)n + 1);
+    V.sieve_count = sl;
+    V.sieve_list = sl + 1;
+  }
   ctx->ev_recorded = 0;
   mark(ctx, 0, st);
   if (!cm.planes_ready) {
@@ -925,19 +931,22 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
   KIRA_CUDA(cudaEventRecord(ctx->ev_up[nch], st));
   KIRA_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->ev_up[nch], 0));
   KIRA_CUDA(cudaStreamWaitEvent(twin->stream, ctx->ev_up[nch], 0));
+  // Enqueue order: every chunk's uploads (each as soon as its host checks pass),
+  // then every chunk's kernels, then every chunk's downloads. Streams can share a
+  // hardware work queue, in which a command that waits (a download waiting for its
+  // chunk's kernels, a kernel waiting for its upload) holds up what was enqueued
+  // after it; in this order no upload is queued behind such a wait.
+  std::vector<uint64_t> r_from(nch), r_to(nch), w_from(nch), w_to(nch);
   uint64_t rdone = 0, wdone = 0;
+  cudaStream_t up = ctx->h2d;
   for (uint32_t c = 0; c < nch; ++c) {
     if (int rc = checked(c)) {
-      // Nothing of chunk c or later is enqueued; let the queued chunks finish first.
-      cudaStreamSynchronize(st);
-      cudaStreamSynchronize(twin->stream);
-      cudaStreamSynchronize(ctx->d2h);
+      // Only uploads of earlier chunks are enqueued; let them finish first.
+      cudaStreamSynchronize(up);
       return rc;
     }
     const uint32_t lo = bounds[c], hi = bounds[c + 1], m = hi - lo;
-    const Maxes mx = scans[c].mx;
     const uint64_t rneed = std::max(rdone, scans[c].rend), wneed = std::max(wdone, scans[c].wend);
-    cudaStream_t up = ctx->h2d;
     KIRA_CUDA(cudaMemcpyAsync(ro + lo, P.read_off + lo, 8ull * m, cudaMemcpyHostToDevice, up));
     KIRA_CUDA(cudaMemcpyAsync(rl + lo, P.read_len + lo, 4ull * m, cudaMemcpyHostToDevice, up));
     KIRA_CUDA(cudaMemcpyAsync(wo + lo, P.win_off + lo, 8ull * m, cudaMemcpyHostToDevice, up));
@@ -951,21 +960,24 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
     if (host_w && wneed > wdone)
       KIRA_CUDA(cudaMemcpyAsync(ws + wdone, P.win_seq + wdone, wneed - wdone,
                                 cudaMemcpyHostToDevice, up));
+    KIRA_CUDA(cudaEventRecord(ctx->ev_up[c], up));
+    r_from[c] = rdone, r_to[c] = rneed, w_from[c] = wdone, w_to[c] = wneed;
+    rdone = rneed, wdone = wneed;
+  }
+  for (uint32_t c = 0; c < nch; ++c) {
+    const uint32_t lo = bounds[c], hi = bounds[c + 1], m = hi - lo;
     kira_ctx* const cx = cxs[c & 1];
     cudaStream_t cs = cx->stream;
-    KIRA_CUDA(cudaEventRecord(ctx->ev_up[c], up));
     KIRA_CUDA(cudaStreamWaitEvent(cs, ctx->ev_up[c], 0));
     if (c) KIRA_CUDA(cudaStreamWaitEvent(cs, ctx->ev_pack[c - 1], 0));
     // Planes of the newly arrived range, from its first (possibly partial) block.
-    if (rneed > rdone) {
-      const uint64_t b0 = rdone / 32, nb = plane_blocks(rneed);
-      KIRA_CUDA(launch_pack_planes(rs + b0 * 32, rneed - b0 * 32, rp + b0, nb - b0, ctx->sms, cs));
-      rdone = rneed;
+    if (r_to[c] > r_from[c]) {
+      const uint64_t b0 = r_from[c] / 32, nb = plane_blocks(r_to[c]);
+      KIRA_CUDA(launch_pack_planes(rs + b0 * 32, r_to[c] - b0 * 32, rp + b0, nb - b0, ctx->sms, cs));
     }
-    if (host_w && wneed > wdone) {
-      const uint64_t b0 = wdone / 32, nb = plane_blocks(wneed);
-      KIRA_CUDA(launch_pack_planes(ws + b0 * 32, wneed - b0 * 32, wp + b0, nb - b0, ctx->sms, cs));
-      wdone = wneed;
+    if (host_w && w_to[c] > w_from[c]) {
+      const uint64_t b0 = w_from[c] / 32, nb = plane_blocks(w_to[c]);
+      KIRA_CUDA(launch_pack_planes(ws + b0 * 32, w_to[c] - b0 * 32, wp + b0, nb - b0, ctx->sms, cs));
     }
     KIRA_CUDA(cudaEventRecord(ctx->ev_pack[c], cs));
     DevPairs D{m,       rs,      ro + lo, rl + lo, ws,
@@ -977,16 +989,20 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
     cm.accumulate = true;
     cm.before_scan = c ? ctx->ev_scan[c - 1] : nullptr;
     cm.after_scan = ctx->ev_scan[c];
-    int rc = verify_pipeline(cx, D, mx, p, P.read_seq_bytes, P.win_seq_bytes, !host_w, dout + lo,
-                             ops, cigar->cap, total_dev, ddet ? ddet + lo : nullptr, cells_dev, cs,
-                             cm);
+    int rc = verify_pipeline(cx, D, scans[c].mx, p, P.read_seq_bytes, P.win_seq_bytes, !host_w,
+                             dout + lo, ops, cigar->cap, total_dev, ddet ? ddet + lo : nullptr,
+                             cells_dev, cs, cm);
     if (rc) {
       if (cx != ctx) ctx->last_error = cx->last_error;
+      cudaStreamSynchronize(up);
       cudaStreamSynchronize(st);
       cudaStreamSynchronize(twin->stream);
       return rc;
     }
     KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], cs));
+  }
+  for (uint32_t c = 0; c < nch; ++c) {
+    const uint32_t lo = bounds[c], m = bounds[c + 1] - lo;
     KIRA_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->ev_comp[c], 0));
     KIRA_CUDA(cudaMemcpyAsync(out + lo, dout + lo, sizeof(kira_sw_result) * m,
                               cudaMemcpyDeviceToHost, ctx->d2h));
@@ -1093,6 +1109,10 @@ namespace {
 // the read / window arenas go up chunk by chunk on the copy-in stream (the arenas
 // as far as each chunk needs them), and each chunk's kernels wait for its own
 // copies, so uploads, kernels and result downloads of consecutive chunks overlap.
+// Every chunk's uploads are enqueued before any chunk's kernels, and the downloads
+// after all kernels: streams can share a hardware work queue, where a command that
+// waits (kernels waiting for their upload, a download for its kernels) holds up
+// what was enqueued after it.
 struct ChunkedInput {
   uint32_t chunk = 0, nch = 0;
   std::vector<uint64_t> rend, wend;  // per chunk: arena bytes needed up to it
@@ -1168,7 +1188,7 @@ int chunked_plan(kira_ctx* ctx, const kira_pairs& P, uint64_t want, ChunkedInput
 }
 
 // Enqueues chunk c's copies on the copy-in stream (extra copies the caller adds
-// through `extra(lo, m, stream)`) and makes the compute stream wait for them.
+// through `extra(lo, m, stream)`) and records ev_up[c] after them.
 template <class F>
 int chunked_upload(kira_ctx* ctx, const kira_pairs& P, ChunkedInput& ci, uint32_t c, F&& extra) {
   const uint32_t lo = c * ci.chunk, m = std::min(P.n, lo + ci.chunk) - lo;
@@ -1195,7 +1215,6 @@ int chunked_upload(kira_ctx* ctx, const kira_pairs& P, ChunkedInput& ci, uint32_
   const int rc = extra(lo, m, up);
   if (rc) return rc;
   KIRA_CUDA(cudaEventRecord(ctx->ev_up[c], up));
-  KIRA_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_up[c], 0));
   return KIRA_OK;
 }
 
@@ -1692,17 +1711,18 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
     KIRA_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->ev_up[nch], 0));
   }
   mark(ctx, 1, st);
+  for (uint32_t c = 0; chunked && c < nch; ++c) {
+    rc = chunked_upload(ctx, P, ci, c, [&](uint32_t l, uint32_t k, cudaStream_t up) -> int {
+      if (dms) KIRA_CUDA(cudaMemcpyAsync(dms + l, max_score + l, 4ull * k, cudaMemcpyHostToDevice, up));
+      if (dtbf)
+        KIRA_CUDA(cudaMemcpyAsync(dtbf + l, text_begin_free + l, 4ull * k, cudaMemcpyHostToDevice, up));
+      return KIRA_OK;
+    });
+    if (rc) return rc;
+  }
   for (uint32_t c = 0; c < nch; ++c) {
     const uint32_t lo = c * csz, m = std::min(n, lo + csz) - lo;
-    if (chunked) {
-      rc = chunked_upload(ctx, P, ci, c, [&](uint32_t l, uint32_t k, cudaStream_t up) -> int {
-        if (dms) KIRA_CUDA(cudaMemcpyAsync(dms + l, max_score + l, 4ull * k, cudaMemcpyHostToDevice, up));
-        if (dtbf)
-          KIRA_CUDA(cudaMemcpyAsync(dtbf + l, text_begin_free + l, 4ull * k, cudaMemcpyHostToDevice, up));
-        return KIRA_OK;
-      });
-      if (rc) return rc;
-    }
+    if (chunked) KIRA_CUDA(cudaStreamWaitEvent(st, ctx->ev_up[c], 0));
     if (c) {  // fetch counters of both kernels and the fallback count
       KIRA_CUDA(cudaMemsetAsync(work, 0, 4, st));
       KIRA_CUDA(cudaMemsetAsync(work + 2, 0, 8, st));
@@ -1742,12 +1762,13 @@ int kira_gpu_wfa_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_wfa_pa
       WfaCompact C{m, dout + lo, ncig + lo, off + lo, Lc.slots, L.slot_cap, ops, cigar->cap};
       KIRA_CUDA(launch_wfa_compact(C, ctx->sms, st));
     }
-    if (chunked) {
-      KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], st));
-      KIRA_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->ev_comp[c], 0));
-      KIRA_CUDA(cudaMemcpyAsync(out + lo, dout + lo, sizeof(kira_wfa_result) * m,
-                                cudaMemcpyDeviceToHost, ctx->d2h));
-    }
+    if (chunked) KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], st));
+  }
+  for (uint32_t c = 0; chunked && c < nch; ++c) {
+    const uint32_t lo = c * csz, m = std::min(n, lo + csz) - lo;
+    KIRA_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->ev_comp[c], 0));
+    KIRA_CUDA(cudaMemcpyAsync(out + lo, dout + lo, sizeof(kira_wfa_result) * m,
+                              cudaMemcpyDeviceToHost, ctx->d2h));
   }
   mark(ctx, 3, st);
   cudaStream_t dn = chunked ? ctx->d2h : st;
@@ -1909,19 +1930,20 @@ int kira_gpu_prefilter_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_
     KIRA_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->ev_up[nch], 0));
   }
   mark(ctx, 1, st);
+  for (uint32_t c = 0; chunked && c < nch; ++c) {
+    rc = chunked_upload(ctx, P, ci, c, [&](uint32_t l, uint32_t k, cudaStream_t up) -> int {
+      KIRA_CUDA(cudaMemcpyAsync(dch + l, chains + l, sizeof(kira_chain) * k,
+                                cudaMemcpyHostToDevice, up));
+      if (dtop) KIRA_CUDA(cudaMemcpyAsync(dtop + l, is_top1 + l, k, cudaMemcpyHostToDevice, up));
+      if (dmar)
+        KIRA_CUDA(cudaMemcpyAsync(dmar + l, score_margin + l, 4ull * k, cudaMemcpyHostToDevice, up));
+      return KIRA_OK;
+    });
+    if (rc) return rc;
+  }
   for (uint32_t c = 0; c < nch; ++c) {
     const uint32_t lo = c * csz, m = std::min(n, lo + csz) - lo;
-    if (chunked) {
-      rc = chunked_upload(ctx, P, ci, c, [&](uint32_t l, uint32_t k, cudaStream_t up) -> int {
-        KIRA_CUDA(cudaMemcpyAsync(dch + l, chains + l, sizeof(kira_chain) * k,
-                                  cudaMemcpyHostToDevice, up));
-        if (dtop) KIRA_CUDA(cudaMemcpyAsync(dtop + l, is_top1 + l, k, cudaMemcpyHostToDevice, up));
-        if (dmar)
-          KIRA_CUDA(cudaMemcpyAsync(dmar + l, score_margin + l, 4ull * k, cudaMemcpyHostToDevice, up));
-        return KIRA_OK;
-      });
-      if (rc) return rc;
-    }
+    if (chunked) KIRA_CUDA(cudaStreamWaitEvent(st, ctx->ev_up[c], 0));
     const DevPairs Dc = chunk_view(D, lo, m);
     PrefilterLaunch Lc = L;
     Lc.chains = dch + lo;
@@ -1938,12 +1960,13 @@ int kira_gpu_prefilter_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_
     mark(ctx, 3, st);
     KIRA_CUDA(launch_prefilter(Dc, Lc, true, ctx->sms, st));
     mark(ctx, 4, st);
-    if (chunked) {
-      KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], st));
-      KIRA_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->ev_comp[c], 0));
-      KIRA_CUDA(cudaMemcpyAsync(out + lo, dout + lo, sizeof(kira_prefilter_result) * m,
-                                cudaMemcpyDeviceToHost, ctx->d2h));
-    }
+    if (chunked) KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], st));
+  }
+  for (uint32_t c = 0; chunked && c < nch; ++c) {
+    const uint32_t lo = c * csz, m = std::min(n, lo + csz) - lo;
+    KIRA_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->ev_comp[c], 0));
+    KIRA_CUDA(cudaMemcpyAsync(out + lo, dout + lo, sizeof(kira_prefilter_result) * m,
+                              cudaMemcpyDeviceToHost, ctx->d2h));
   }
   cudaStream_t dn = chunked ? ctx->d2h : st;
   uint64_t tot[2] = {0, 0};

@@ -33,6 +33,11 @@ struct VerifyDev {
   uint32_t* counters;          // [0] myers items, [1] sw items
   int32_t myers_k;             // < 0: router bound per read (myers_k_for)
   int32_t qgram;               // exact 4-gram prefilter before Myers (qgram.cuh)
+  // Filter-first form (no detail rows, filter on): pairs the 4-gram count does not
+  // settle, as pair | 1 << 31 when the count already rejects them unless they
+  // certify; *sieve_count entries. Null: one kernel sieves every pair.
+  uint32_t* sieve_list;
+  uint32_t* sieve_count;
 };
 
 struct MyersLaunch {

@@ -183,7 +183,60 @@ __device__ __forceinline__ uint32_t myers_k_for(int32_t k, uint32_t q) {
   return k < 0 ? (q * 15u) / 100u + 4u : (uint32_t)k;
 }
 
-// Stage 1 of the composed path: sieve + certificate, one lane per pair.
+// Result rows of the sieve stage.
+__device__ __forceinline__ void write_myers_reject(const VerifyDev& V, uint32_t p) {
+  kira_sw_result r{};
+  r.status = KIRA_PAIR_MYERS_REJECT;
+  V.out[p] = r;
+  V.ncig[p] = 0;
+}
+
+// build_certified_spectral_alignment (mod.rs:636-686).
+__device__ __forceinline__ void write_certified(const VerifyDev& V, uint32_t p, uint32_t q,
+                                                const LaneSieve& so) {
+  kira_sw_result r;
+  r.score = (int32_t)(q - so.mism) * V.sw.match - (int32_t)so.mism * V.sw.mismatch;
+  r.ref_start = so.shift;
+  r.ref_end = so.shift + q;
+  r.read_start = 0;
+  r.read_end = (int32_t)q;
+  r.cigar_off = 0;
+  r.n_cigar = 1;
+  r.status = KIRA_PAIR_CERTIFIED;
+  r.early_abort = 0;
+  r.reserved = 0;
+  V.out[p] = r;
+  V.ncig[p] = 1;
+}
+
+// Warp-aggregated append of `value` for the lanes with `take` (all 32 lanes call).
+__device__ __forceinline__ void warp_append(bool take, uint32_t value, uint32_t* count,
+                                            uint32_t* list) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t need = __ballot_sync(0xFFFFFFFFu, take);
+  uint32_t slot0 = 0;
+  if (lane == 0 && need) slot0 = atomicAdd(count, (uint32_t)__popc(need));
+  slot0 = __shfl_sync(0xFFFFFFFFu, slot0, 0);
+  if (take) list[slot0 + __popc(need & ((1u << lane) - 1u))] = value;
+}
+
+// Sieve + certificate of pair p (scan_best_with_second_raw, then the certificate
+// of mod.rs:636-686); writes the certified row when it certifies.
+template <int RWMAX>
+__device__ __forceinline__ bool sieve_certify(const DevPairs& P, const VerifyDev& V, uint32_t p,
+                                              uint32_t q, LaneSieve& so) {
+  so = sieve_lane<RWMAX>(P.read_planes, P.read_off[p], q, P.win_planes, P.win_off[p],
+                         P.win_len[p]);
+  const uint32_t thr = sieve_threshold_for(V.sieve_threshold, q);
+  const bool cert = so.hit && so.mism <= thr &&
+                    lane_certify(P.read_seq + P.read_off[p], P.win_seq + P.win_off[p] + so.shift,
+                                 q, so.mism, so.second, thr, V.cert_strict != 0);
+  if (cert) write_certified(V, p, q, so);
+  return cert;
+}
+
+// Stage 1 of the composed path when detail rows are asked for or the filter is
+// off: sieve + certificate of every pair, then the 4-gram filter, one lane per pair.
 template <int RWMAX>
 __global__ void __launch_bounds__(256) verify_sieve_kernel(DevPairs P, VerifyDev V) {
   __shared__ uint32_t qset[8][8 * 32];  // per warp: 4-gram bitmap [word][lane]
@@ -194,16 +247,11 @@ __global__ void __launch_bounds__(256) verify_sieve_kernel(DevPairs P, VerifyDev
     const uint32_t p = base + threadIdx.x;
     const bool valid = p < P.n;
     bool cert = false;
-    LaneSieve so{false, 0, 0, 0xFFFFFFFFu};
     uint32_t q = 0;
     if (valid) {
       q = P.read_len[p];
-      const uint32_t w = P.win_len[p];
-      so = sieve_lane<RWMAX>(P.read_planes, P.read_off[p], q, P.win_planes, P.win_off[p], w);
-      const uint32_t thr = sieve_threshold_for(V.sieve_threshold, q);
-      if (so.hit && so.mism <= thr)
-        cert = lane_certify(P.read_seq + P.read_off[p], P.win_seq + P.win_off[p] + so.shift, q,
-                            so.mism, so.second, thr, V.cert_strict != 0);
+      LaneSieve so{false, 0, 0, 0xFFFFFFFFu};
+      cert = sieve_certify<RWMAX>(P, V, p, q, so);
       if (V.detail) {
         kira_verify_detail dt;
         dt.sieve_shift = so.hit ? (int32_t)so.shift : -1;
@@ -213,23 +261,7 @@ __global__ void __launch_bounds__(256) verify_sieve_kernel(DevPairs P, VerifyDev
         dt.myers_end = -1;
         V.detail[p] = dt;
       }
-      if (cert) {  // build_certified_spectral_alignment (mod.rs:636-686)
-        kira_sw_result r;
-        r.score = (int32_t)(q - so.mism) * V.sw.match - (int32_t)so.mism * V.sw.mismatch;
-        r.ref_start = so.shift;
-        r.ref_end = so.shift + q;
-        r.read_start = 0;
-        r.read_end = (int32_t)q;
-        r.cigar_off = 0;
-        r.n_cigar = 1;
-        r.status = KIRA_PAIR_CERTIFIED;
-        r.early_abort = 0;
-        r.reserved = 0;
-        V.out[p] = r;
-        V.ncig[p] = 1;
-      } else {
-        V.sw_offset[p] = so.hit ? (int32_t)so.shift : 0;
-      }
+      if (!cert) V.sw_offset[p] = so.hit ? (int32_t)so.shift : 0;
     }
     // Exact 4-gram prefilter: a pair it rejects is a Myers None (same result).
     bool gone = false;
@@ -237,20 +269,70 @@ __global__ void __launch_bounds__(256) verify_sieve_kernel(DevPairs P, VerifyDev
       const uint32_t k = myers_k_for(V.myers_k, q);
       gone = qgram4_reject(P.read_planes, P.read_off[p], q, P.win_planes, P.win_off[p],
                            P.win_len[p], k, myset);
-      if (gone) {
-        kira_sw_result r{};
-        r.status = KIRA_PAIR_MYERS_REJECT;
-        V.out[p] = r;
-        V.ncig[p] = 0;
+      if (gone) write_myers_reject(V, p);
+    }
+    warp_append(valid && !cert && !gone, p, V.counters + 0, V.myers_list);
+  }
+}
+
+// Stage 1, filter first (no detail rows): the 4-gram count of every pair decides
+// two things. Myers rejects the pair when count < m - 3 - 4k (qgram.cuh). And the
+// certificate needs a shift with at most min(threshold, 2) mismatches
+// (lane_certify): a shift with d mismatches leaves at least m - 3 - 4d read
+// 4-grams untouched, each found verbatim in the window, so count < m - 3 -
+// 4 min(threshold, 2) proves no shift certifies. A pair below both bounds is a
+// Myers reject whatever its sieve says, and its sieve is never run; the others go
+// to verify_sieve_list_kernel, tagged when the count already rejects them unless
+// they certify. Rows are those of verify_sieve_kernel.
+__global__ void __launch_bounds__(256) verify_filter_kernel(DevPairs P, VerifyDev V) {
+  __shared__ uint32_t qset[8][8 * 32];
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t* myset = &qset[threadIdx.x >> 5][lane];
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < P.n; base += stride) {
+    const uint32_t p = base + threadIdx.x;
+    const bool valid = p < P.n;
+    uint32_t verdict = 0;
+    if (valid) {
+      const uint32_t q = P.read_len[p];
+      const int32_t thr2 = (int32_t)min(sieve_threshold_for(V.sieve_threshold, q), 2u);
+      const int32_t hi = (int32_t)q - 3 - 4 * (int32_t)myers_k_for(V.myers_k, q);
+      const int32_t lo = min(hi, (int32_t)q - 3 - 4 * thr2);
+      verdict = qgram4_verdict(P.read_planes, P.read_off[p], q, P.win_planes, P.win_off[p],
+                               P.win_len[p], lo, hi, myset);
+      if (verdict == 2u) write_myers_reject(V, p);
+    }
+    warp_append(valid && verdict != 2u, p | (verdict == 1u ? 0x80000000u : 0u), V.sieve_count,
+                V.sieve_list);
+  }
+}
+
+// Stage 1, second pass: sieve + certificate of the listed pairs; a pair that does
+// not certify is a Myers reject when tagged, else it goes to the Myers list with
+// its sieve shift as the banded-SW offset.
+template <int RWMAX>
+__global__ void __launch_bounds__(256) verify_sieve_list_kernel(DevPairs P, VerifyDev V) {
+  const uint32_t count = *V.sieve_count;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += stride) {
+    const uint32_t idx = base + threadIdx.x;
+    const bool valid = idx < count;
+    bool to_myers = false;
+    uint32_t p = 0;
+    if (valid) {
+      const uint32_t e = V.sieve_list[idx];
+      p = e & 0x7FFFFFFFu;
+      LaneSieve so{false, 0, 0, 0xFFFFFFFFu};
+      if (!sieve_certify<RWMAX>(P, V, p, P.read_len[p], so)) {
+        if (e >> 31) {
+          write_myers_reject(V, p);
+        } else {
+          V.sw_offset[p] = so.hit ? (int32_t)so.shift : 0;
+          to_myers = true;
+        }
       }
     }
-    // Warp-aggregated append of the remaining pairs to the Myers list.
-    const bool to_myers = valid && !cert && !gone;
-    const uint32_t need = __ballot_sync(0xFFFFFFFFu, to_myers);
-    uint32_t slot0 = 0;
-    if (lane == 0 && need) slot0 = atomicAdd(V.counters + 0, (uint32_t)__popc(need));
-    slot0 = __shfl_sync(0xFFFFFFFFu, slot0, 0);
-    if (to_myers) V.myers_list[slot0 + __popc(need & ((1u << lane) - 1u))] = p;
+    warp_append(to_myers, p, V.counters + 0, V.myers_list);
   }
 }
 
@@ -729,6 +811,15 @@ cudaError_t launch_verify_sieve(const DevPairs& P, const VerifyDev& V, uint32_t 
                                 cudaStream_t st) {
   const int blocks = grid_for(P.n, 256, sms * 8);
   const uint32_t rw = (max_q + 31) / 32;
+  if (V.sieve_list && !V.detail && V.qgram && P.n < 0x80000000u) {
+    cudaError_t e = cudaMemsetAsync(V.sieve_count, 0, 4, st);
+    if (e != cudaSuccess) return e;
+    verify_filter_kernel<<<blocks, 256, 0, st>>>(P, V);
+    if (rw <= 5) verify_sieve_list_kernel<5><<<blocks, 256, 0, st>>>(P, V);
+    else if (rw <= 8) verify_sieve_list_kernel<8><<<blocks, 256, 0, st>>>(P, V);
+    else verify_sieve_list_kernel<16><<<blocks, 256, 0, st>>>(P, V);
+    return cudaGetLastError();
+  }
   if (rw <= 5) verify_sieve_kernel<5><<<blocks, 256, 0, st>>>(P, V);
   else if (rw <= 8) verify_sieve_kernel<8><<<blocks, 256, 0, st>>>(P, V);
   else verify_sieve_kernel<16><<<blocks, 256, 0, st>>>(P, V);

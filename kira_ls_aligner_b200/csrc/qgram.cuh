@@ -51,14 +51,17 @@ __device__ __forceinline__ void qgram_code(uint32_t p0, uint32_t c0, uint32_t p1
   bit = ((x1 & 1u) << 4) | x0;
 }
 
-// True when the read provably has edit distance > k to every window substring.
-// `set` points at this lane's column of an [8][32] word bitmap in shared memory.
-__device__ __forceinline__ bool qgram4_reject(const uint4* __restrict__ rplanes, uint64_t rpos,
-                                              uint32_t m, const uint4* __restrict__ wplanes,
-                                              uint64_t wpos, uint32_t n, uint32_t k,
-                                              uint32_t* set) {
-  const int32_t need = (int32_t)m - 3 - 4 * (int32_t)k;
-  if (need <= 0 || n < 4u) return false;
+// Where the count of read 4-grams found in the window falls against two bounds
+// lo <= hi: 0 when count >= hi, 1 when lo <= count < hi, 2 when count < lo; the
+// read walk stops as soon as that is decided. With hi <= 0 or a window of fewer
+// than four bases the answer is 0 (nothing is proved). `set` points at this
+// lane's column of an [8][32] word bitmap in shared memory.
+__device__ __forceinline__ uint32_t qgram4_verdict(const uint4* __restrict__ rplanes,
+                                                   uint64_t rpos, uint32_t m,
+                                                   const uint4* __restrict__ wplanes,
+                                                   uint64_t wpos, uint32_t n, int32_t lo,
+                                                   int32_t hi, uint32_t* set) {
+  if (hi <= 0 || n < 4u) return 0u;
 #pragma unroll
   for (int w = 0; w < 8; ++w) set[w * 32] = 0u;
   uint32_t p0 = 0, p1 = 0, pv = 0;
@@ -101,12 +104,22 @@ __device__ __forceinline__ bool qgram4_reject(const uint4* __restrict__ rplanes,
     KIRA_QG_COUNT(30) KIRA_QG_COUNT(31)
 #undef KIRA_QG_COUNT
     p0 = pw.b0, p1 = pw.b1, pv = pw.v;
-    // Decided either way once the count reaches the bound or can no longer.
+    // Decided once the count reaches a bound or can no longer reach it.
     const int32_t left = (int32_t)m - (int32_t)(32u * blk + lim);
-    if (count >= need) return false;
-    if (count + left < need) return true;
+    if (count >= hi) return 0u;
+    if (count + left < lo) return 2u;
+    if (count >= lo && count + left < hi) return 1u;
   }
-  return count < need;
+  return count < lo ? 2u : count < hi ? 1u : 0u;
+}
+
+// True when the read provably has edit distance > k to every window substring.
+__device__ __forceinline__ bool qgram4_reject(const uint4* __restrict__ rplanes, uint64_t rpos,
+                                              uint32_t m, const uint4* __restrict__ wplanes,
+                                              uint64_t wpos, uint32_t n, uint32_t k,
+                                              uint32_t* set) {
+  const int32_t need = (int32_t)m - 3 - 4 * (int32_t)k;
+  return qgram4_verdict(rplanes, rpos, m, wplanes, wpos, n, need, need, set) != 0u;
 }
 
 }  // namespace kira

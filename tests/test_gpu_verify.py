@@ -109,6 +109,46 @@ def test_qgram_prefilter_changes_nothing(ctx, myers_k, sub_hi, indel):
     _compare(on[0], on[1], on[2], out, cig, sel)
 
 
+@pytest.mark.parametrize("myers_k,thr,sub_hi,indel", [(8, 12, 0.05, 0.002), (0, 12, 0.02, 0.0),
+                                                      (1, 3, 0.03, 0.001), (-1, -1, 0.08, 0.004),
+                                                      (30, 2, 0.10, 0.005)])
+def test_filter_first_sieve_equals_full_sieve(ctx, myers_k, thr, sub_hi, indel):
+    # Without detail rows the 4-gram count runs first and the sieve only for the
+    # pairs it leaves open (k = 0 or 1 puts the certificate's bound below the
+    # filter's, so some pairs are tagged "reject unless certified"). Results equal
+    # the detail path, which sieves every pair, in one shot and in chunks, and the
+    # oracle on a sample; reads and windows carry some N bases.
+    from kira_ls_aligner_b200 import PairBatch, VerifyParams, _abi, synth
+    w = synth.make_workload("f", 2500, 400_000, cands=8, sub_lo=0.0, sub_hi=sub_hi,
+                            indel_rate=indel, repeat_frac=0.2, seed=3000 + max(myers_k, 0))
+    rng = np.random.default_rng(7)
+    reads = w.reads.copy()
+    for r in rng.choice(2500, 40, replace=False):
+        reads[int(w.read_off[8 * r]) + int(rng.integers(0, 150))] = ord("N")
+    arena, woffs = w.windows_arena()
+    arena = arena.copy()
+    arena[rng.choice(len(arena), 60, replace=False)] = ord("N")
+    w.reads = reads
+    b = PairBatch(reads, w.read_off, w.read_len, arena, woffs, w.win_len)
+    params = VerifyParams(sieve_threshold=thr, myers_k=myers_k)
+    full = ctx.verify_batch(b, params, detail=True)
+    fast = ctx.verify_batch(b, params)
+    assert np.array_equal(full[0], fast[0]) and np.array_equal(full[1], fast[1])
+    assert full[3] == fast[3]
+    st = np.bincount(fast[0]["status"], minlength=4)
+    assert st[1] > 0 and st[2] > 0, st
+    L = _abi.lib()
+    try:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, 3000))
+        chunked = ctx.verify_batch(b, params)
+    finally:
+        ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, -1))
+    assert np.array_equal(full[0], chunked[0]) and np.array_equal(full[1], chunked[1])
+    sel = np.arange(0, w.n_pairs, 17)
+    out, cig = _oracle(w, arena, woffs, params, sel)
+    _compare(fast[0], fast[1], full[2], out, cig, sel)
+
+
 @pytest.mark.parametrize("resident,shuffle", [(False, False), (True, False), (True, True)])
 def test_chunked_host_path_equals_one_shot(ctx, resident, shuffle):
     # kira_gpu_verify_batch in chunks (copy-in / compute / copy-out streams, read
