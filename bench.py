@@ -894,8 +894,9 @@ def run_ours(args, rank, local, world, dist):
     }[dom]
     # DRAM bytes per unit from the ncu captures of the same kernels (800k-pair case,
     # scaled by units processed): profiles/bsw16_dp_batched_800k.md (1.496 B per DP
-    # cell) and profiles/verify_sieve_batched_800k.md (169.3 B per pair).
-    traffic = {0: 169.3 * n, 2: 1.496 * cells_step if packed else None}.get(dom)
+    # cell) and profiles/verify_sieve_batched_800k.md (209.5 B per pair over the
+    # filter and survivor-sieve kernels).
+    traffic = {0: 209.5 * n, 2: 1.496 * cells_step if packed else None}.get(dom)
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     dp_ms = stage_ms[2] / args.steps
     roofline = {"bound": "hbm", "kernel": _abi.STAGES[dom], "achieved": achieved, "peak": peak,
@@ -908,8 +909,8 @@ def run_ours(args, rank, local, world, dist):
                 # 77-85 % of peak, DRAM < 10 %); their binding roofline is the ALU pipe.
                 "int_pipe": {"kernel": "bsw_dp", "gcups": cells_step / (dp_ms / 1e3) / 1e9
                              if dp_ms > 0 else None,
-                             "alu_pipe_frac_ncu": 0.770 if packed else 0.757,
-                             "thread_inst_per_cell_ncu": 28.3 if packed else 90.8,
+                             "alu_pipe_frac_ncu": 0.759 if packed else 0.757,
+                             "thread_inst_per_cell_ncu": 28.4 if packed else 90.8,
                              "source": "profiles/bsw16_dp_batched_800k.md"}}
 
     cpu = None

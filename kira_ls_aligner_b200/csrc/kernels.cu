@@ -239,7 +239,7 @@ __device__ __forceinline__ bool sieve_certify(const DevPairs& P, const VerifyDev
 // off: sieve + certificate of every pair, then the 4-gram filter, one lane per pair.
 template <int RWMAX>
 __global__ void __launch_bounds__(256) verify_sieve_kernel(DevPairs P, VerifyDev V) {
-  __shared__ uint32_t qset[8][8 * 32];  // per warp: 4-gram bitmap [word][lane]
+  __shared__ uint32_t qset[8][16 * 32];  // per warp: 4-gram bitmap [word][lane]
   const uint32_t lane = threadIdx.x & 31u;
   uint32_t* myset = &qset[threadIdx.x >> 5][lane];
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(256) verify_sieve_kernel(DevPairs P, VerifyDev
 // to verify_sieve_list_kernel, tagged when the count already rejects them unless
 // they certify. Rows are those of verify_sieve_kernel.
 __global__ void __launch_bounds__(256) verify_filter_kernel(DevPairs P, VerifyDev V) {
-  __shared__ uint32_t qset[8][8 * 32];
+  __shared__ uint32_t qset[8][16 * 32];
   const uint32_t lane = threadIdx.x & 31u;
   uint32_t* myset = &qset[threadIdx.x >> 5][lane];
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(256) verify_filter_kernel(DevPairs P, VerifyDe
 // not certify is a Myers reject when tagged, else it goes to the Myers list with
 // its sieve shift as the banded-SW offset.
 template <int RWMAX>
-__global__ void __launch_bounds__(256) verify_sieve_list_kernel(DevPairs P, VerifyDev V) {
+__global__ void __launch_bounds__(256, 4) verify_sieve_list_kernel(DevPairs P, VerifyDev V) {
   const uint32_t count = *V.sieve_count;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += stride) {

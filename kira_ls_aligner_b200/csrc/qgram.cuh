@@ -16,12 +16,13 @@
 // output is unchanged; survivors still run Myers.
 //
 // Lane-per-pair: the window's 4-gram set is a 256-bit bitmap per lane in shared
-// memory laid out [word][lane] (each lane owns one bank); bases come from the
-// 2-bit + valid plane arenas, one 32-base word at a time. A 4-gram's 8-bit code is
-// its four bit-0 plane bits and its four bit-1 plane bits (one bit-field extract
-// each, the previous word supplying the first three bases of a word); the
-// positions whose four bases are all valid come from one AND of shifted valid
-// masks per word. Window and read use the same code, so the count is the count.
+// memory, 16 words of 16 used bits laid out [word][lane] (each lane owns one
+// bank); bases come from the 2-bit + valid plane arenas, one 32-base word at a
+// time. A 4-gram is its four bit-1 plane bits (the word) and its four bit-0 plane
+// bits (the bit in it), each one bit-field extract, the previous word supplying
+// the first three bases of a word; the positions whose four bases are all valid
+// come from one AND of shifted valid masks per word. Window and read use the same
+// index, so the count is the count.
 #pragma once
 
 #include "common.cuh"
@@ -43,19 +44,12 @@ __device__ __forceinline__ uint32_t qgram_valid4(uint32_t pv, uint32_t v, uint32
   return lim < 32u ? v4 & ((1u << lim) - 1u) : v4;
 }
 
-template <int B>
-__device__ __forceinline__ void qgram_code(uint32_t p0, uint32_t c0, uint32_t p1, uint32_t c1,
-                                           uint32_t& word, uint32_t& bit) {
-  const uint32_t x0 = qgram_nibble<B>(p0, c0), x1 = qgram_nibble<B>(p1, c1);
-  word = x1 >> 1;
-  bit = ((x1 & 1u) << 4) | x0;
-}
 
 // Where the count of read 4-grams found in the window falls against two bounds
 // lo <= hi: 0 when count >= hi, 1 when lo <= count < hi, 2 when count < lo; the
 // read walk stops as soon as that is decided. With hi <= 0 or a window of fewer
 // than four bases the answer is 0 (nothing is proved). `set` points at this
-// lane's column of an [8][32] word bitmap in shared memory.
+// lane's column of a [16][32] word bitmap in shared memory.
 __device__ __forceinline__ uint32_t qgram4_verdict(const uint4* __restrict__ rplanes,
                                                    uint64_t rpos, uint32_t m,
                                                    const uint4* __restrict__ wplanes,
@@ -63,17 +57,14 @@ __device__ __forceinline__ uint32_t qgram4_verdict(const uint4* __restrict__ rpl
                                                    int32_t hi, uint32_t* set) {
   if (hi <= 0 || n < 4u) return 0u;
 #pragma unroll
-  for (int w = 0; w < 8; ++w) set[w * 32] = 0u;
+  for (int w = 0; w < 16; ++w) set[w * 32] = 0u;
   uint32_t p0 = 0, p1 = 0, pv = 0;
   for (uint32_t blk = 0; blk * 32u < n; ++blk) {
     const PlaneWord pw = plane_word_at(wplanes, wpos + 32u * blk);
     const uint32_t v4 = qgram_valid4(pv, pw.v, min(32u, n - 32u * blk));
-#define KIRA_QG_SET(B)                                          \
-  if ((v4 >> (B)) & 1u) {                                       \
-    uint32_t word, bit;                                         \
-    qgram_code<(B)>(p0, pw.b0, p1, pw.b1, word, bit);           \
-    set[word * 32u] |= 1u << bit;                               \
-  }
+#define KIRA_QG_SET(B)                                                      \
+  if ((v4 >> (B)) & 1u)                                                     \
+    set[qgram_nibble<(B)>(p1, pw.b1) * 32u] |= 1u << qgram_nibble<(B)>(p0, pw.b0);
     KIRA_QG_SET(0) KIRA_QG_SET(1) KIRA_QG_SET(2) KIRA_QG_SET(3) KIRA_QG_SET(4) KIRA_QG_SET(5)
     KIRA_QG_SET(6) KIRA_QG_SET(7) KIRA_QG_SET(8) KIRA_QG_SET(9) KIRA_QG_SET(10) KIRA_QG_SET(11)
     KIRA_QG_SET(12) KIRA_QG_SET(13) KIRA_QG_SET(14) KIRA_QG_SET(15) KIRA_QG_SET(16)
@@ -89,12 +80,9 @@ __device__ __forceinline__ uint32_t qgram4_verdict(const uint4* __restrict__ rpl
     const PlaneWord pw = plane_word_at(rplanes, rpos + 32u * blk);
     const uint32_t lim = min(32u, m - 32u * blk);
     const uint32_t v4 = qgram_valid4(pv, pw.v, lim);
-#define KIRA_QG_COUNT(B)                                        \
-  if ((v4 >> (B)) & 1u) {                                       \
-    uint32_t word, bit;                                         \
-    qgram_code<(B)>(p0, pw.b0, p1, pw.b1, word, bit);           \
-    count += (int32_t)((set[word * 32u] >> bit) & 1u);          \
-  }
+#define KIRA_QG_COUNT(B)                                                              \
+  if ((v4 >> (B)) & 1u)                                                               \
+    count += (int32_t)((set[qgram_nibble<(B)>(p1, pw.b1) * 32u] >> qgram_nibble<(B)>(p0, pw.b0)) & 1u);
     KIRA_QG_COUNT(0) KIRA_QG_COUNT(1) KIRA_QG_COUNT(2) KIRA_QG_COUNT(3) KIRA_QG_COUNT(4)
     KIRA_QG_COUNT(5) KIRA_QG_COUNT(6) KIRA_QG_COUNT(7) KIRA_QG_COUNT(8) KIRA_QG_COUNT(9)
     KIRA_QG_COUNT(10) KIRA_QG_COUNT(11) KIRA_QG_COUNT(12) KIRA_QG_COUNT(13) KIRA_QG_COUNT(14)
