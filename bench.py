@@ -870,7 +870,12 @@ def run_ours(args, rank, local, world, dist):
             tt = torch.tensor([el], device=dev, dtype=torch.float64)
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             el = float(tt.item())
-        h2d = int(w.reads.nbytes) + n * (8 + 4 + 8 + 4)
+        # Bytes the call copies up: the read arena plus the pair descriptors, packed to
+        # 12 bytes a pair (u32 offsets, u16 lengths) when the read arena and the
+        # reference are below 4 GiB and every length fits 16 bits, else 24.
+        packed = (w.reads.nbytes < 1 << 32 and len(w.reference) < 1 << 32
+                  and max(int(w.read_len.max()), int(w.win_len.max())) < 1 << 16)
+        h2d = int(w.reads.nbytes) + n * (12 if packed else 8 + 4 + 8 + 4)
         d2h = n * 32 + 4 * int(cb.used) + 8 + 8 + 16
         e2e = {"value": n * world * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * el / args.steps}

@@ -31,7 +31,7 @@ enum BufId {
   B_DIST, B_END, B_SIEVE_OUT, B_SIEVE_JOBS, B_CELLS, B_TOTAL, B_READ_PLANES, B_WIN_PLANES,
   B_ROWKEYS, B_DONE_ROW, B_WORK, B_WFA_MAXS, B_WFA_TBF, B_WFA_OUT, B_WFA_NCIG, B_WFA_SLOTS,
   B_WFA_SCRATCH, B_WFA_FLAGS, B_PF_CHAINS, B_PF_TOP1, B_PF_MARGIN, B_PF_OUT, B_PF_NCIG,
-  B_PF_MDLEN, B_PF_MDOFF, B_PF_MD, B_PF_EXACT, B_WFA_FB, B_WFA_WHIST, B_SIEVE_LIST, B_COUNT
+  B_PF_MDLEN, B_PF_MDOFF, B_PF_MD, B_PF_EXACT, B_WFA_FB, B_WFA_WHIST, B_SIEVE_LIST, B_PACKED, B_COUNT
 };
 
 struct DevBuf {
@@ -131,6 +131,8 @@ struct kira_ctx {
   std::unique_ptr<HostPool> pool;   // host threads of the chunked path's pair checks
   kira_ctx* twin = nullptr;          // second compute stream + scratch of the chunked path
   std::vector<cudaEvent_t> ev_pack, ev_scan;  // per chunk: planes packed / CIGARs placed
+  PackedPair* stage = nullptr;  // pinned: packed descriptors of the chunked host path
+  uint64_t stage_cap = 0;       // pairs
   DevBuf bufs[B_COUNT];
 };
 
@@ -780,6 +782,24 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
     int kind = 0;      // 1: read outside read_seq, 2: window outside
   };
   const int32_t cfg_band = std::max(p.sw.bandwidth, 1);
+  // Descriptors go up packed (12 bytes a pair instead of 24) when every offset that
+  // passes the bounds check fits 32 bits; the check pass writes them to the
+  // context's pinned staging buffer.
+  PackedPair* stage = nullptr;
+  if (P.read_seq_bytes <= UINT32_MAX && wlim <= UINT32_MAX) {
+    if (ctx->stage_cap < n) {
+      const uint64_t cap = std::max<uint64_t>(n, ctx->stage_cap + ctx->stage_cap / 4);
+      if (ctx->stage) cudaFreeHost(ctx->stage);
+      ctx->stage = nullptr;
+      ctx->stage_cap = 0;
+      if (cudaHostAlloc(reinterpret_cast<void**>(&ctx->stage), cap * sizeof(PackedPair),
+                        cudaHostAllocDefault) == cudaSuccess)
+        ctx->stage_cap = cap;
+      else
+        cudaGetLastError(), ctx->stage = nullptr;
+    }
+    stage = ctx->stage;
+  }
   auto scan_range = [&](uint32_t lo, uint32_t hi, Scan& sc) {
     uint64_t rend = 0, wend = 0;
     uint32_t q = 0, w = 0, band = 0;
@@ -790,6 +810,10 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
       q = P.read_len[i] > q ? P.read_len[i] : q;
       w = P.win_len[i] > w ? P.win_len[i] : w;
     }
+    if (stage)
+      for (uint32_t i = lo; i < hi; ++i)
+        stage[i] = PackedPair{(uint32_t)P.read_off[i], (uint32_t)P.win_off[i],
+                              (uint16_t)P.read_len[i], (uint16_t)P.win_len[i]};
     if (P.bandwidth) {
       for (uint32_t i = lo; i < hi; ++i) {
         const uint32_t b = (uint32_t)std::max(P.bandwidth[i], 1);
@@ -904,6 +928,11 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
   KIRA_DBUF(rl, uint32_t, B_READ_LEN, n);
   KIRA_DBUF(wo, uint64_t, B_WIN_OFF, n);
   KIRA_DBUF(wl, uint32_t, B_WIN_LEN, n);
+  PackedPair* dpk = nullptr;
+  if (stage) {
+    KIRA_DBUF(d, PackedPair, B_PACKED, n);
+    dpk = d;
+  }
   int32_t *bo = nullptr, *ab = nullptr, *bw = nullptr;
   if (P.band_offset) {
     KIRA_DBUF(b, int32_t, B_BAND_OFF, n);
@@ -947,10 +976,18 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
     }
     const uint32_t lo = bounds[c], hi = bounds[c + 1], m = hi - lo;
     const uint64_t rneed = std::max(rdone, scans[c].rend), wneed = std::max(wdone, scans[c].wend);
-    KIRA_CUDA(cudaMemcpyAsync(ro + lo, P.read_off + lo, 8ull * m, cudaMemcpyHostToDevice, up));
-    KIRA_CUDA(cudaMemcpyAsync(rl + lo, P.read_len + lo, 4ull * m, cudaMemcpyHostToDevice, up));
-    KIRA_CUDA(cudaMemcpyAsync(wo + lo, P.win_off + lo, 8ull * m, cudaMemcpyHostToDevice, up));
-    KIRA_CUDA(cudaMemcpyAsync(wl + lo, P.win_len + lo, 4ull * m, cudaMemcpyHostToDevice, up));
+    const bool short_lens = scans[c].mx.q <= UINT16_MAX && scans[c].mx.w <= UINT16_MAX;
+    if (dpk) {
+      KIRA_CUDA(cudaMemcpyAsync(dpk + lo, stage + lo, sizeof(PackedPair) * m,
+                                cudaMemcpyHostToDevice, up));
+    } else {
+      KIRA_CUDA(cudaMemcpyAsync(ro + lo, P.read_off + lo, 8ull * m, cudaMemcpyHostToDevice, up));
+      KIRA_CUDA(cudaMemcpyAsync(wo + lo, P.win_off + lo, 8ull * m, cudaMemcpyHostToDevice, up));
+    }
+    if (!dpk || !short_lens) {
+      KIRA_CUDA(cudaMemcpyAsync(rl + lo, P.read_len + lo, 4ull * m, cudaMemcpyHostToDevice, up));
+      KIRA_CUDA(cudaMemcpyAsync(wl + lo, P.win_len + lo, 4ull * m, cudaMemcpyHostToDevice, up));
+    }
     if (bo) KIRA_CUDA(cudaMemcpyAsync(bo + lo, P.band_offset + lo, 4ull * m, cudaMemcpyHostToDevice, up));
     if (ab) KIRA_CUDA(cudaMemcpyAsync(ab + lo, P.abort_score + lo, 4ull * m, cudaMemcpyHostToDevice, up));
     if (bw) KIRA_CUDA(cudaMemcpyAsync(bw + lo, P.bandwidth + lo, 4ull * m, cudaMemcpyHostToDevice, up));
@@ -969,6 +1006,11 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
     kira_ctx* const cx = cxs[c & 1];
     cudaStream_t cs = cx->stream;
     KIRA_CUDA(cudaStreamWaitEvent(cs, ctx->ev_up[c], 0));
+    if (dpk) {
+      const bool short_lens = scans[c].mx.q <= UINT16_MAX && scans[c].mx.w <= UINT16_MAX;
+      KIRA_CUDA(launch_unpack_pairs(dpk + lo, m, ro + lo, rl + lo, wo + lo, wl + lo, short_lens,
+                                    ctx->sms, cs));
+    }
     if (c) KIRA_CUDA(cudaStreamWaitEvent(cs, ctx->ev_pack[c - 1], 0));
     // Planes of the newly arrived range, from its first (possibly partial) block.
     if (r_to[c] > r_from[c]) {
@@ -1295,6 +1337,7 @@ void kira_gpu_destroy(kira_ctx* ctx) {
   for (auto e : ctx->ev_scan) cudaEventDestroy(e);
   if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
   if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
+  if (ctx->stage) cudaFreeHost(ctx->stage);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
 }

@@ -247,6 +247,19 @@ cudaError_t launch_sieve_dropin(const SieveJobsDev& J, kira_sieve_result* out, i
 cudaError_t launch_pack_planes(const uint8_t* seq, uint64_t len, uint4* out, uint64_t nblocks,
                                int sms, cudaStream_t st);
 inline uint64_t plane_blocks(uint64_t len) { return (len + 31) / 32 + 4; }
+// Pair descriptors as the chunked host path uploads them when the read arena and
+// the window source are below 4 GiB (every checked offset then fits 32 bits).
+struct PackedPair {
+  uint32_t read_off, win_off;
+  uint16_t read_len, win_len;
+};
+static_assert(sizeof(PackedPair) == 12, "PackedPair layout");
+
+// Expands n packed descriptors into the pipeline's arrays; with lens == false the
+// length arrays are left as they are (uploaded separately).
+cudaError_t launch_unpack_pairs(const PackedPair* src, uint32_t n, uint64_t* read_off,
+                                uint32_t* read_len, uint64_t* win_off, uint32_t* win_len,
+                                bool lens, int sms, cudaStream_t st);
 cudaError_t launch_verify_sieve(const DevPairs& P, const VerifyDev& V, uint32_t max_q, int sms,
                                 cudaStream_t st);
 cudaError_t launch_myers(const DevPairs& P, const MyersLaunch& M, uint32_t max_items, int sms,

@@ -336,6 +336,23 @@ __global__ void __launch_bounds__(256, 4) verify_sieve_list_kernel(DevPairs P, V
   }
 }
 
+// One thread per pair: 12-byte packed descriptors -> the pipeline's arrays.
+__global__ void __launch_bounds__(256) unpack_pairs_kernel(const PackedPair* __restrict__ src,
+                                                           uint32_t n, uint64_t* read_off,
+                                                           uint32_t* read_len, uint64_t* win_off,
+                                                           uint32_t* win_len, int lens) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+    const PackedPair d = src[p];
+    read_off[p] = d.read_off;
+    win_off[p] = d.win_off;
+    if (lens) {
+      read_len[p] = d.read_len;
+      win_len[p] = d.win_len;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Myers over a work list (one pair per lane; 32 pairs per warp).
 // ---------------------------------------------------------------------------
@@ -804,6 +821,15 @@ cudaError_t launch_pack_planes(const uint8_t* seq, uint64_t len, uint4* out, uin
                                int sms, cudaStream_t st) {
   const int blocks = grid_for((nblocks + 31) / 32, 8, sms * 16);
   pack_planes_kernel<<<blocks, 256, 0, st>>>(seq, len, out, nblocks);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_pairs(const PackedPair* src, uint32_t n, uint64_t* read_off,
+                                uint32_t* read_len, uint64_t* win_off, uint32_t* win_len,
+                                bool lens, int sms, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  unpack_pairs_kernel<<<grid_for(n, 256, sms * 8), 256, 0, st>>>(src, n, read_off, read_len,
+                                                                 win_off, win_len, lens ? 1 : 0);
   return cudaGetLastError();
 }
 
