@@ -222,8 +222,8 @@ int kira_gpu_set_graphs(kira_ctx* ctx, int enable, uint64_t* captures, uint64_t*
  * chunks overlap (pinned host buffers make the copies asynchronous); this applies
  * to kira_gpu_verify_batch, kira_gpu_wfa_batch and kira_gpu_prefilter_batch.
  * pairs < 0: automatic (the default: a quarter of the batch, at least 2^18
- * pairs; verification batches of at least 2^20 pairs in chunks of 1/8, 3/8, 3/8
- * and 1/8), 0: off, else the chunk size. Results are identical either way. */
+ * pairs; verification batches of at least 2^20 pairs in chunks of 1/8, 1/4, 1/4,
+ * 1/4 and 1/8), 0: off, else the chunk size. Results are identical either way. */
 int kira_gpu_set_chunk_pairs(kira_ctx* ctx, int64_t pairs);
 
 /* Upload the reference as ASCII bases (Index::ref_bases, src/index/mod.rs:1098);

@@ -2388,14 +2388,15 @@ int kira_gpu_verify_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_ver
   // Chunks alternate between two compute streams so each chunk's row-serial DP and
   // traceback tail overlaps the next chunk; a few large chunks still do best
   // (each pays some fixed launch and tail cost). Automatic: batches of at least
-  // 2^20 pairs in chunks of 1/8, 3/8, 3/8, 1/8 of the batch (a small first chunk
-  // starts the GPU sooner, a small last one drains sooner), smaller ones in
+  // 2^20 pairs in chunks of 1/8, 1/4, 1/4, 1/4, 1/8 of the batch (a small first
+  // chunk starts the GPU sooner, a small last one drains sooner), smaller ones in
   // quarters of at least 2^18 pairs; chunk_pairs > 0: equal chunks of that size.
   std::vector<uint32_t> bounds;
   if (!ctx->profile) {
     const uint64_t n = P.n;
     if (ctx->chunk_pairs < 0 && n >= (1u << 20)) {
-      bounds = {0u, (uint32_t)(n / 8), (uint32_t)(n / 2), (uint32_t)(n - n / 8), (uint32_t)n};
+      bounds = {0u, (uint32_t)(n / 8), (uint32_t)(3 * n / 8), (uint32_t)(5 * n / 8),
+                (uint32_t)(n - n / 8), (uint32_t)n};
     } else {
       const uint64_t chunk = ctx->chunk_pairs < 0 ? std::max<uint64_t>(1u << 18, (n + 3) / 4)
                                                   : (uint64_t)ctx->chunk_pairs;

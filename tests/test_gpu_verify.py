@@ -234,7 +234,7 @@ def test_chunked_host_checks_in_sub_ranges(ctx):
 
 
 def test_uneven_automatic_chunks(ctx):
-    # Batches of at least 2^20 pairs go in chunks of 1/8, 3/8, 3/8, 1/8 of the batch
+    # Batches of at least 2^20 pairs go in chunks of 1/8, 1/4, 1/4, 1/4, 1/8 of the batch
     # by default; results equal the one-shot path.
     from kira_ls_aligner_b200 import PairBatch, VerifyParams, _abi, synth
     w = synth.make_workload("u", 270_000, 5_000_000, cands=4, sub_lo=0.0, sub_hi=0.03, seed=80)
