@@ -941,8 +941,9 @@ def run_ours(args, rank, local, world, dist):
             "status_counts": {"certified": statuses[1], "myers_reject": statuses[2],
                               "sw": statuses[3]},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            # per step: planes pack, sieve, Myers, SW DP, traceback, 3 scan, compaction
-            "gpu_launches": 9 * args.steps,
+            # per step: planes pack, 4-gram filter, survivor sieve, Myers, SW DP,
+            # traceback, 3 scan, compaction
+            "gpu_launches": 10 * args.steps,
         }
         print(json.dumps(out))
     ctx.close()
