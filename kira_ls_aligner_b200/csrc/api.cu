@@ -793,10 +793,12 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
       ctx->stage = nullptr;
       ctx->stage_cap = 0;
       if (cudaHostAlloc(reinterpret_cast<void**>(&ctx->stage), cap * sizeof(PackedPair),
-                        cudaHostAllocDefault) == cudaSuccess)
+                        cudaHostAllocDefault) == cudaSuccess) {
         ctx->stage_cap = cap;
-      else
-        cudaGetLastError(), ctx->stage = nullptr;
+      } else {  // no pinned staging: the descriptors go up unpacked
+        cudaGetLastError();
+        ctx->stage = nullptr;
+      }
     }
     stage = ctx->stage;
   }
