@@ -62,16 +62,22 @@ __device__ __forceinline__ uint32_t qgram4_verdict(const uint4* __restrict__ rpl
   for (uint32_t blk = 0; blk * 32u < n; ++blk) {
     const PlaneWord pw = plane_word_at(wplanes, wpos + 32u * blk);
     const uint32_t v4 = qgram_valid4(pv, pw.v, min(32u, n - 32u * blk));
-#define KIRA_QG_SET(B)                                                      \
-  if ((v4 >> (B)) & 1u)                                                     \
-    set[qgram_nibble<(B)>(p1, pw.b1) * 32u] |= 1u << qgram_nibble<(B)>(p0, pw.b0);
-    KIRA_QG_SET(0) KIRA_QG_SET(1) KIRA_QG_SET(2) KIRA_QG_SET(3) KIRA_QG_SET(4) KIRA_QG_SET(5)
-    KIRA_QG_SET(6) KIRA_QG_SET(7) KIRA_QG_SET(8) KIRA_QG_SET(9) KIRA_QG_SET(10) KIRA_QG_SET(11)
-    KIRA_QG_SET(12) KIRA_QG_SET(13) KIRA_QG_SET(14) KIRA_QG_SET(15) KIRA_QG_SET(16)
-    KIRA_QG_SET(17) KIRA_QG_SET(18) KIRA_QG_SET(19) KIRA_QG_SET(20) KIRA_QG_SET(21)
-    KIRA_QG_SET(22) KIRA_QG_SET(23) KIRA_QG_SET(24) KIRA_QG_SET(25) KIRA_QG_SET(26)
-    KIRA_QG_SET(27) KIRA_QG_SET(28) KIRA_QG_SET(29) KIRA_QG_SET(30) KIRA_QG_SET(31)
+#define KIRA_QG_INS(B) \
+  set[qgram_nibble<(B)>(p1, pw.b1) * 32u] |= 1u << qgram_nibble<(B)>(p0, pw.b0);
+#define KIRA_QG_SET(B) \
+  if ((v4 >> (B)) & 1u) KIRA_QG_INS(B)
+#define KIRA_QG_ALL(M)                                                                   \
+  M(0) M(1) M(2) M(3) M(4) M(5) M(6) M(7) M(8) M(9) M(10) M(11) M(12) M(13) M(14) M(15) \
+  M(16) M(17) M(18) M(19) M(20) M(21) M(22) M(23) M(24) M(25) M(26) M(27) M(28) M(29)   \
+  M(30) M(31)
+    // A word whose 32 positions are all valid (no N near it) skips the per-position tests.
+    if (v4 == 0xFFFFFFFFu) {
+      KIRA_QG_ALL(KIRA_QG_INS)
+    } else {
+      KIRA_QG_ALL(KIRA_QG_SET)
+    }
 #undef KIRA_QG_SET
+#undef KIRA_QG_INS
     p0 = pw.b0, p1 = pw.b1, pv = pw.v;
   }
   int32_t count = 0;
@@ -80,17 +86,17 @@ __device__ __forceinline__ uint32_t qgram4_verdict(const uint4* __restrict__ rpl
     const PlaneWord pw = plane_word_at(rplanes, rpos + 32u * blk);
     const uint32_t lim = min(32u, m - 32u * blk);
     const uint32_t v4 = qgram_valid4(pv, pw.v, lim);
-#define KIRA_QG_COUNT(B)                                                              \
-  if ((v4 >> (B)) & 1u)                                                               \
-    count += (int32_t)((set[qgram_nibble<(B)>(p1, pw.b1) * 32u] >> qgram_nibble<(B)>(p0, pw.b0)) & 1u);
-    KIRA_QG_COUNT(0) KIRA_QG_COUNT(1) KIRA_QG_COUNT(2) KIRA_QG_COUNT(3) KIRA_QG_COUNT(4)
-    KIRA_QG_COUNT(5) KIRA_QG_COUNT(6) KIRA_QG_COUNT(7) KIRA_QG_COUNT(8) KIRA_QG_COUNT(9)
-    KIRA_QG_COUNT(10) KIRA_QG_COUNT(11) KIRA_QG_COUNT(12) KIRA_QG_COUNT(13) KIRA_QG_COUNT(14)
-    KIRA_QG_COUNT(15) KIRA_QG_COUNT(16) KIRA_QG_COUNT(17) KIRA_QG_COUNT(18) KIRA_QG_COUNT(19)
-    KIRA_QG_COUNT(20) KIRA_QG_COUNT(21) KIRA_QG_COUNT(22) KIRA_QG_COUNT(23) KIRA_QG_COUNT(24)
-    KIRA_QG_COUNT(25) KIRA_QG_COUNT(26) KIRA_QG_COUNT(27) KIRA_QG_COUNT(28) KIRA_QG_COUNT(29)
-    KIRA_QG_COUNT(30) KIRA_QG_COUNT(31)
+#define KIRA_QG_HIT(B) \
+  count += (int32_t)((set[qgram_nibble<(B)>(p1, pw.b1) * 32u] >> qgram_nibble<(B)>(p0, pw.b0)) & 1u);
+#define KIRA_QG_COUNT(B) \
+  if ((v4 >> (B)) & 1u) KIRA_QG_HIT(B)
+    if (v4 == 0xFFFFFFFFu) {
+      KIRA_QG_ALL(KIRA_QG_HIT)
+    } else {
+      KIRA_QG_ALL(KIRA_QG_COUNT)
+    }
 #undef KIRA_QG_COUNT
+#undef KIRA_QG_HIT
     p0 = pw.b0, p1 = pw.b1, pv = pw.v;
     // Decided once the count reaches a bound or can no longer reach it.
     const int32_t left = (int32_t)m - (int32_t)(32u * blk + lim);
@@ -100,6 +106,7 @@ __device__ __forceinline__ uint32_t qgram4_verdict(const uint4* __restrict__ rpl
   }
   return count < lo ? 2u : count < hi ? 1u : 0u;
 }
+#undef KIRA_QG_ALL
 
 // True when the read provably has edit distance > k to every window substring.
 __device__ __forceinline__ bool qgram4_reject(const uint4* __restrict__ rplanes, uint64_t rpos,
