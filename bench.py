@@ -899,9 +899,9 @@ def run_ours(args, rank, local, world, dist):
     }[dom]
     # DRAM bytes per unit from the ncu captures of the same kernels (800k-pair case,
     # scaled by units processed): profiles/bsw16_dp_batched_800k.md (1.496 B per DP
-    # cell) and profiles/verify_sieve_batched_800k.md (209.5 B per pair over the
+    # cell) and profiles/verify_sieve_batched_800k.md (213.7 B per pair over the
     # filter and survivor-sieve kernels).
-    traffic = {0: 209.5 * n, 2: 1.496 * cells_step if packed else None}.get(dom)
+    traffic = {0: 213.7 * n, 2: 1.496 * cells_step if packed else None}.get(dom)
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     dp_ms = stage_ms[2] / args.steps
     roofline = {"bound": "hbm", "kernel": _abi.STAGES[dom], "achieved": achieved, "peak": peak,
