@@ -292,17 +292,17 @@ __global__ void __launch_bounds__(256) verify_filter_kernel(DevPairs P, VerifyDe
   for (uint32_t base = blockIdx.x * blockDim.x; base < P.n; base += stride) {
     const uint32_t p = base + threadIdx.x;
     const bool valid = p < P.n;
-    uint32_t verdict = 0;
+    uint32_t outcome = 0;
     if (valid) {
       const uint32_t q = P.read_len[p];
       const int32_t thr2 = (int32_t)min(sieve_threshold_for(V.sieve_threshold, q), 2u);
       const int32_t hi = (int32_t)q - 3 - 4 * (int32_t)myers_k_for(V.myers_k, q);
       const int32_t lo = min(hi, (int32_t)q - 3 - 4 * thr2);
-      verdict = qgram4_verdict(P.read_planes, P.read_off[p], q, P.win_planes, P.win_off[p],
+      outcome = qgram4_outcome(P.read_planes, P.read_off[p], q, P.win_planes, P.win_off[p],
                                P.win_len[p], lo, hi, myset);
-      if (verdict == 2u) write_myers_reject(V, p);
+      if (outcome == 2u) write_myers_reject(V, p);
     }
-    warp_append(valid && verdict != 2u, p | (verdict == 1u ? 0x80000000u : 0u), V.sieve_count,
+    warp_append(valid && outcome != 2u, p | (outcome == 1u ? 0x80000000u : 0u), V.sieve_count,
                 V.sieve_list);
   }
 }

@@ -50,7 +50,7 @@ __device__ __forceinline__ uint32_t qgram_valid4(uint32_t pv, uint32_t v, uint32
 // read walk stops as soon as that is decided. With hi <= 0 or a window of fewer
 // than four bases the answer is 0 (nothing is proved). `set` points at this
 // lane's column of a [16][32] word bitmap in shared memory.
-__device__ __forceinline__ uint32_t qgram4_verdict(const uint4* __restrict__ rplanes,
+__device__ __forceinline__ uint32_t qgram4_outcome(const uint4* __restrict__ rplanes,
                                                    uint64_t rpos, uint32_t m,
                                                    const uint4* __restrict__ wplanes,
                                                    uint64_t wpos, uint32_t n, int32_t lo,
@@ -114,7 +114,7 @@ __device__ __forceinline__ bool qgram4_reject(const uint4* __restrict__ rplanes,
                                               uint64_t wpos, uint32_t n, uint32_t k,
                                               uint32_t* set) {
   const int32_t need = (int32_t)m - 3 - 4 * (int32_t)k;
-  return qgram4_verdict(rplanes, rpos, m, wplanes, wpos, n, need, need, set) != 0u;
+  return qgram4_outcome(rplanes, rpos, m, wplanes, wpos, n, need, need, set) != 0u;
 }
 
 }  // namespace kira
