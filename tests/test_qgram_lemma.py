@@ -53,3 +53,33 @@ def test_filter_rejects_only_myers_none(seed):
             rejected += 1
             assert O.bounded_edit_distance(read, win, k) is None, (read, win, k)
     assert rejected > 50
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_certified_pairs_meet_the_certificate_bound(seed):
+    # The filter-first verification skips the sieve of a pair whose 4-gram count is
+    # below m - 3 - 4 min(threshold, 2) (the certificate accepts at most two
+    # mismatches at its shift, each touching at most four read 4-grams). No pair
+    # the oracle certifies may fall below that bound. Planted reads with 0-3
+    # substitutions around the certificate's limit; mixed-case bases in one seed (an
+    # N only stops the certificate, so it cannot break the bound); thresholds from
+    # the router default up to 12.
+    rng = XorShift(0xCE27 + seed)
+    alpha = b"ACGT" if seed < 3 else b"ACGTACGTacgt"
+    certified = 0
+    for _ in range(500):
+        m = 40 + rng.next() % 110
+        n = m + rng.next() % 100
+        win = bytes(alpha[rng.next() % len(alpha)] for _ in range(n))
+        start = rng.next() % (n - m + 1)
+        read = mutate(rng, win[start:start + m], rng.next() % 4, 0)
+        thr = (-1, 1, 2, 3, 12)[rng.next() % 5]
+        out, _ = O.verify_pair(read, win, O.verify_params(O.cfg(), thr, 8))
+        if out.status != 1:
+            continue
+        certified += 1
+        t = O.spectral_max_mismatches(len(read)) if thr < 0 else thr
+        present = {c for _, c in grams(win)}
+        count = sum(1 for _, c in grams(read) if c in present)
+        assert count >= len(read) - 3 - 4 * min(t, 2), (read, win, thr)
+    assert certified > 40
