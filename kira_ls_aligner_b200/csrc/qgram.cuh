@@ -21,8 +21,9 @@
 // time. A 4-gram is its four bit-1 plane bits (the word) and its four bit-0 plane
 // bits (the bit in it), each one bit-field extract, the previous word supplying
 // the first three bases of a word; the positions whose four bases are all valid
-// come from one AND of shifted valid masks per word. Window and read use the same
-// index, so the count is the count.
+// come from one AND of shifted valid masks per word. An insert is one shared-memory
+// atomic OR (each lane owns its column, so nothing contends). Window and read use
+// the same index, so the count is the count.
 #pragma once
 
 #include "common.cuh"
@@ -63,7 +64,7 @@ __device__ __forceinline__ uint32_t qgram4_outcome(const uint4* __restrict__ rpl
     const PlaneWord pw = plane_word_at(wplanes, wpos + 32u * blk);
     const uint32_t v4 = qgram_valid4(pv, pw.v, min(32u, n - 32u * blk));
 #define KIRA_QG_INS(B) \
-  set[qgram_nibble<(B)>(p1, pw.b1) * 32u] |= 1u << qgram_nibble<(B)>(p0, pw.b0);
+  atomicOr(&set[qgram_nibble<(B)>(p1, pw.b1) * 32u], 1u << qgram_nibble<(B)>(p0, pw.b0));
 #define KIRA_QG_SET(B) \
   if ((v4 >> (B)) & 1u) KIRA_QG_INS(B)
 #define KIRA_QG_ALL(M)                                                                   \
