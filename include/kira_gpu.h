@@ -60,7 +60,10 @@ enum kira_pair_status {
   KIRA_PAIR_PENDING = 0,
   KIRA_PAIR_CERTIFIED = 1,    /* ungapped hit accepted by the certificate */
   KIRA_PAIR_MYERS_REJECT = 2, /* bounded edit distance above k */
-  KIRA_PAIR_SW = 3            /* banded SW alignment */
+  KIRA_PAIR_SW = 3,           /* banded SW alignment */
+  KIRA_PAIR_OUT_OF_BOUNDS = 4 /* banded SW: the pair exceeds the call's declared maxima
+                                 (read_len > max_read_len, or a band wider than the
+                                 launch shape); not aligned, n_cigar 0 */
 };
 
 /* Maximum packed read length of the sieve drop-in (src/cuda/mod.rs:35-37). */
@@ -168,7 +171,9 @@ typedef struct kira_sw_result {
   uint32_t n_cigar;
   uint8_t status;      /* kira_pair_status (verify) or KIRA_PAIR_SW */
   uint8_t early_abort;
-  uint16_t reserved;
+  uint16_t reserved;   /* banded SW: 1 when the pair's CIGAR overflowed its device slot
+                          (the row is then incomplete; the host entry points return an
+                          error for the call) */
 } kira_sw_result;
 
 /* Caller-owned CIGAR output: ops[cap]; *used receives the number of ops the
@@ -337,7 +342,14 @@ int kira_gpu_verify_dev(kira_ctx* ctx, const kira_pairs* pairs, const kira_verif
  *     work: split it into smaller batches.
  *   - Work is enqueued on `stream` (a cudaStream_t) and the call returns without
  *     synchronising; *cigar_used (device) receives the op count, and ops beyond
- *     cigar_cap are not written (the caller compares the two after syncing).
+ *     cigar_cap are not written (the caller compares the two after syncing; a
+ *     pair whose ops would cross cigar_cap gets none).
+ *   - Problems found on the device are reported per pair, since the call does
+ *     not wait for the GPU: a pair that exceeds the declared maxima (read_len >
+ *     max_read_len, or a per-pair band wider than max_bandwidth allows) is not
+ *     aligned and its row has status KIRA_PAIR_OUT_OF_BOUNDS and n_cigar 0; a
+ *     row with reserved == 1 lost part of its CIGAR (device slot overflow). Every
+ *     other row has status KIRA_PAIR_SW.
  *   - The first call on a device looks up the scratch array's device address on
  *     that device (cudaGetSymbolAddress, with the device current) and caches it;
  *     make that first call before any stream capture.

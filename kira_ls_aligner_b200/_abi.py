@@ -22,6 +22,8 @@ STATUS_NAMES = {
 KIRA_ERR_TIMEOUT = 6
 KIRA_ERR_SCRATCH_LIMIT = 10
 KIRA_PENDING = 11
+KIRA_PAIR_SW = 3
+KIRA_PAIR_OUT_OF_BOUNDS = 4
 NOALLOC_SCRATCH_BYTES = 32 << 20
 PAIR_PENDING, PAIR_CERTIFIED, PAIR_MYERS_REJECT, PAIR_SW = 0, 1, 2, 3
 READ_BYTES_MAX = 64

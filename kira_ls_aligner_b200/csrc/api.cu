@@ -206,21 +206,31 @@ SwParams resolve(const kira_sw_cfg& c) {
 
 // Domain of the GPU banded SW (exactness conditions of the F prefix scan and of
 // the packed row-argmax key).
-int check_sw_cfg(kira_ctx* ctx, const kira_sw_cfg& c, uint32_t max_q, uint32_t max_band) {
-  if (c.gap_open < 0 || c.gap_extend < 0)
-    return fail(ctx, KIRA_ERR_INVALID, "gap_open and gap_extend must be >= 0");
+}  // namespace
+
+// Domain of the banded-SW entry points (exactness of the F scan and of the row
+// keys); the reason when `c` is outside it, else null. Shared by every entry
+// point that runs the banded SW, so their domains cannot drift apart.
+const char* kira::sw_cfg_problem(const kira_sw_cfg& c, uint32_t max_q, uint32_t max_band) {
+  if (c.gap_open < 0 || c.gap_extend < 0) return "gap_open and gap_extend must be >= 0";
   if ((int64_t)c.gap_open + c.gap_extend > (1 << 24) || c.gap_extend > (1 << 16))
-    return fail(ctx, KIRA_ERR_INVALID, "gap costs above the supported range");
+    return "gap costs above the supported range";
   const int64_t step = std::max<int64_t>({(int64_t)c.match_score, -(int64_t)c.mismatch, 0});
-  if ((int64_t)max_q * step >= (1 << 21))
-    return fail(ctx, KIRA_ERR_INVALID, "read_len * max cell gain must be < 2^21");
+  if ((int64_t)max_q * step >= (1 << 21)) return "read_len * max cell gain must be < 2^21";
   if (std::abs((int64_t)c.match_score) > (1 << 20) || std::abs((int64_t)c.mismatch) > (1 << 20))
-    return fail(ctx, KIRA_ERR_INVALID, "match/mismatch above the supported range");
+    return "match/mismatch above the supported range";
   const int need = 2 * (int)std::max<uint32_t>(max_band, 1) + 1;
   int cap = 0;
   for (int s = 0; s < kNumBswShapes; ++s) cap = std::max(cap, shape_cap(kBswShapes[s]));
-  if (need > cap)
-    return fail(ctx, KIRA_ERR_INVALID, "bandwidth %u above the supported maximum", max_band);
+  if (need > cap) return "bandwidth above the supported maximum";
+  return nullptr;
+}
+
+namespace {
+
+int check_sw_cfg(kira_ctx* ctx, const kira_sw_cfg& c, uint32_t max_q, uint32_t max_band) {
+  const char* why = sw_cfg_problem(c, max_q, max_band);
+  if (why) return fail(ctx, KIRA_ERR_INVALID, "%s (band %u, read %u)", why, max_band, max_q);
   return KIRA_OK;
 }
 

@@ -56,8 +56,9 @@ struct DpEnd {
   int32_t score;
   int32_t end_i;
   int32_t end_j;
-  uint32_t early_abort;
+  uint32_t early_abort;  // kEndOutsideShape: the item was not run (outside the launch shape)
 };
+constexpr uint32_t kEndOutsideShape = 0xFFFFFFFFu;
 
 __device__ __forceinline__ int32_t sat_add(int32_t a, int32_t b) {
   int64_t s = (int64_t)a + (int64_t)b;

@@ -295,4 +295,7 @@ cudaError_t launch_exact_match(const DevPairs& P, const kira_chain* chains, uint
 
 int ctx_share_reference(kira_ctx* dst, const kira_ctx* src);
 
+// Why a banded-SW configuration is outside the supported domain (null: inside).
+const char* sw_cfg_problem(const kira_sw_cfg& c, uint32_t max_q, uint32_t max_band);
+
 }  // namespace kira

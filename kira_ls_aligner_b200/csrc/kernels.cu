@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B
     uint64_t cells = 0;
     if (q > B.max_q || (FULL ? (int32_t)w > CAP : 2 * band + 1 > CAP)) {  // outside the shape
       if (g == 0) {
-        B.ends[item] = DpEnd{0, 0, 0, 0};
+        B.ends[item] = DpEnd{0, 0, 0, kEndOutsideShape};
         atomicOr(B.flags, 2u);
       }
       if (!B.work) item += ngroups;
@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(T, MINB) bsw16_dp_kernel(DevPairs P, BswLaunch
     uint64_t cells = 0;
     if (q > B.max_q || 2 * band + 1 > CAP) {  // outside the shape
       if (g == 0) {
-        B.ends[item] = DpEnd{0, 0, 0, 0};
+        B.ends[item] = DpEnd{0, 0, 0, kEndOutsideShape};
         atomicOr(B.flags, 2u);
       }
       if (!B.work) item += ngroups;
@@ -587,11 +587,15 @@ __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
     const uint8_t* tr = B.tg.trace + (size_t)slot_item * B.tg.slot_bytes;
     const uint32_t* mt = B.tg.meta + (size_t)slot_item * B.tg.meta_stride;
     uint32_t* ops = B.cig_slots + (size_t)item * B.slot_cap;
-    uint32_t n;
-    if constexpr (PACKED)
+    uint32_t n = 0;
+    const bool outside = e.early_abort == kEndOutsideShape;  // uniform over the warp
+    if (outside) {
+      i = j = 0;
+    } else if constexpr (PACKED) {
       n = warp_walk(Bsw16Code<G, K>{tr, mt, B.sp.gap_open}, i, j, ops, B.slot_cap, overflow);
-    else
+    } else {
       n = warp_walk(BswCode<G, K>{tr, mt}, i, j, ops, B.slot_cap, overflow);
+    }
     if (!lead) continue;
     kira_sw_result r;
     r.score = e.score;
@@ -601,8 +605,8 @@ __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
     r.read_end = e.end_i;
     r.cigar_off = 0;
     r.n_cigar = n;
-    r.status = KIRA_PAIR_SW;
-    r.early_abort = (uint8_t)e.early_abort;
+    r.status = outside ? KIRA_PAIR_OUT_OF_BOUNDS : KIRA_PAIR_SW;
+    r.early_abort = outside ? 0 : (uint8_t)e.early_abort;
     r.reserved = overflow ? 1 : 0;
     B.out[pair] = r;
     B.ncig[pair] = n;

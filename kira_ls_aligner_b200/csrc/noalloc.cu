@@ -80,12 +80,8 @@ extern "C" int kira_gpu_bsw_batch_noalloc(const kira_pairs* pairs, const kira_sw
   const uint32_t max_q = P.max_read_len, max_w = P.max_win_len;
   const uint32_t max_band = P.bandwidth ? P.max_bandwidth : (uint32_t)std::max(c.bandwidth, 1);
   if (max_band == 0) return KIRA_ERR_INVALID;
-  // Same domain as kira_gpu_bsw_batch (exactness of the F scan and row keys).
-  if (c.gap_open < 0 || c.gap_extend < 0) return KIRA_ERR_INVALID;
-  if ((int64_t)c.gap_open + c.gap_extend > (1 << 24) || c.gap_extend > (1 << 16))
-    return KIRA_ERR_INVALID;
-  const int64_t step = std::max<int64_t>({(int64_t)c.match_score, -(int64_t)c.mismatch, 0});
-  if ((int64_t)max_q * step >= (1 << 21)) return KIRA_ERR_INVALID;
+  // Same domain as kira_gpu_bsw_batch (one shared check).
+  if (sw_cfg_problem(c, max_q, max_band)) return KIRA_ERR_INVALID;
   const int need = 2 * (int)max_band + 1;
   int shape = -1;
   for (int s = 0; s < kNumBswShapes; ++s)

@@ -233,9 +233,15 @@ void run_batch(kira_server* S, Slot& sl, std::vector<Request*>& b) {
     kira_gpu_last_error(sl.ctx, buf, sizeof(buf));
     err = buf;
   }
-  // Scatter: a request's pairs and CIGAR ops are contiguous in the batch.
+  // Scatter: a request's pairs and CIGAR ops are contiguous in the batch. The
+  // result rows and ops are written without the lock; each request's status and
+  // op count are published under it (with t_done), so a waiter that sees a final
+  // status also sees its outputs.
+  std::vector<int> fin(b.size());
+  std::vector<uint64_t> fin_used(b.size());
   at = 0;
-  for (Request* r : b) {
+  for (size_t ri = 0; ri < b.size(); ++ri) {
+    Request* r = b[ri];
     const uint32_t k = r->pairs.n;
     int st = rc;
     uint64_t used = 0;
@@ -254,13 +260,17 @@ void run_batch(kira_server* S, Slot& sl, std::vector<Request*>& b) {
         st = KIRA_ERR_CAPACITY;
       }
     }
-    r->cigar_used = used;
-    r->status = st;
+    fin[ri] = st;
+    fin_used[ri] = used;
     at += k;
   }
   std::lock_guard<std::mutex> lk(S->mu);
   const int64_t t = now_ns();
-  for (Request* r : b) r->t_done = t;
+  for (size_t ri = 0; ri < b.size(); ++ri) {
+    b[ri]->cigar_used = fin_used[ri];
+    b[ri]->t_done = t;
+    b[ri]->status = fin[ri];
+  }
   S->ms_stage += (t_staged - t_in) / 1e6;
   S->ms_run += (t_ran - t_staged) / 1e6;
   S->ms_scatter += (t - t_ran) / 1e6;

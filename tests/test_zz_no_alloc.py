@@ -46,10 +46,15 @@ def _dev_batch(cases, torch, dev):
     return b, p, keep
 
 
-def _noalloc(p, cfg, n, cap, torch, dev):
+SENTINEL = 0x5A5A5A5A
+
+
+def _noalloc(p, cfg, n, cap, torch, dev, ops_len=None, full=False):
+    """One call; returns (results, ops[:used]) or, with full=True, (results, every op
+    word of the buffer, used)."""
     from kira_ls_aligner_b200 import _abi
     out = torch.zeros(n * 32, dtype=torch.uint8, device=dev)
-    ops = torch.zeros(cap, dtype=torch.int32, device=dev)
+    ops = torch.full((ops_len or cap,), SENTINEL, dtype=torch.int32, device=dev)
     used = torch.zeros(1, dtype=torch.int64, device=dev)
     stream = torch.cuda.current_stream(dev)
     cc = cfg.to_c()
@@ -59,9 +64,12 @@ def _noalloc(p, cfg, n, cap, torch, dev):
     torch.cuda.synchronize(dev)
     assert rc == 0, rc
     u = int(used.item())
-    assert u <= cap
     res = np.frombuffer(out.cpu().numpy().tobytes(), _abi.SW_RESULT_DTYPE)
-    return res, ops.cpu().numpy().view(np.uint32)[:u]
+    allops = ops.cpu().numpy().view(np.uint32)
+    if full:
+        return res, allops, u
+    assert u <= cap
+    return res, allops[:u]
 
 
 def test_noalloc_matches_bsw_batch_on_two_calls():
@@ -103,3 +111,53 @@ def test_noalloc_rejects_batches_beyond_its_scratch():
     rc = _abi.lib().kira_gpu_bsw_batch_noalloc(C.byref(p), C.byref(cc), out.data_ptr(),
                                                 ops.data_ptr(), 16, used.data_ptr(), None)
     assert rc == _abi.KIRA_ERR_SCRATCH_LIMIT
+
+
+def test_noalloc_short_cigar_buffer_reports_the_need():
+    """With cigar_cap below the ops the batch produces, *cigar_used still gives the
+    full need and nothing is written past cigar_cap."""
+    torch = pytest.importorskip("torch")
+    from kira_ls_aligner_b200 import AlignmentConfig, GpuContext
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    cfg = AlignmentConfig(1, 4, 6, 1, 33, 100, 5, True, 16)
+    cases = sw_corpus(0x0A120, 200, qmin=40, qmax=160, pad=50, max_band=40)
+    b, p, keep = _dev_batch(cases, torch, dev)
+    with GpuContext(0) as ctx:
+        _, want_ops, _ = ctx.bsw_batch(b, cfg)
+    need = len(want_ops)
+    cap = need // 3
+    res, allops, used = _noalloc(p, cfg, b.n, cap, torch, dev, ops_len=need + 64, full=True)
+    assert used == need > cap
+    assert (allops[cap:] == SENTINEL).all()
+    # every pair whose ops lie wholly below the cap has them written in place (a pair
+    # that straddles the cap is skipped whole)
+    ends = res["cigar_off"].astype(np.int64) + res["n_cigar"].astype(np.int64)
+    inside = ends[ends <= cap]
+    end = int(inside.max()) if len(inside) else 0
+    assert end > 0
+    assert (allops[:end] == want_ops[:end]).all()
+
+
+def test_noalloc_reports_pairs_beyond_the_declared_maxima():
+    """A pair longer than max_read_len is not aligned: its row carries
+    KIRA_PAIR_OUT_OF_BOUNDS with no CIGAR, and every other pair is unchanged."""
+    torch = pytest.importorskip("torch")
+    from kira_ls_aligner_b200 import AlignmentConfig, GpuContext, _abi, results_to_list
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    cfg = AlignmentConfig(1, 4, 6, 1, 33, 100, 5, True, 16)
+    cases = sw_corpus(0x0A121, 64, qmin=30, qmax=100, pad=50, max_band=40)
+    long_read, long_win = cases[0][0] * 2, cases[0][1] * 2
+    cases[17] = (long_read[:150], long_win[:220], 0, 20, O.ABORT_DISABLED)
+    b, p, keep = _dev_batch(cases, torch, dev)
+    p.max_read_len = 100  # pair 17 (150 bases) exceeds it
+    with GpuContext(0) as ctx:
+        want_res, want_ops, _ = ctx.bsw_batch(b, cfg)
+    got_res, got_ops = _noalloc(p, cfg, b.n, 64 * b.n, torch, dev)
+    assert got_res["status"][17] == _abi.KIRA_PAIR_OUT_OF_BOUNDS
+    assert got_res["n_cigar"][17] == 0
+    got, want = results_to_list(got_res, got_ops), results_to_list(want_res, want_ops)
+    others = [i for i in range(b.n) if i != 17]
+    assert all(got_res["status"][i] == _abi.KIRA_PAIR_SW for i in others)
+    assert [got[i].key() for i in others] == [want[i].key() for i in others]
