@@ -40,10 +40,19 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--reads", type=int, default=250_000, help="reads per rank (x8 pairs)")
-    ap.add_argument("--cpu-sample", type=int, default=20_000, help="pairs in the CPU sample")
+    ap.add_argument("--reads", type=int, default=250_000,
+                    help="reads per GPU (x8 candidate windows = pairs per GPU)")
+    ap.add_argument("--ref-len", type=int, default=100_000_000, help="reference bases")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true",
+                    help="skip the oracle pass (parity check and cpu_baseline)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the uneven-batch and serving runs folded into the headline line")
+    ap.add_argument("--backend", choices=["nccl", "gloo"], default="nccl",
+                    help="process-group backend of a multi-GPU run")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="multi-rank plumbing only (launch, shards, gather, timing reduction), "
+                         "no GPU work; for CPU tests with --backend gloo")
     ap.add_argument("--shape", type=int, default=-1,
                     help="install this banded-SW launch shape instead of autotuning")
     ap.add_argument("--workload", choices=["batched", "uneven", "serving", "gapfill", "nmmd",
@@ -131,56 +140,105 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(w, nthreads: int, sample: int, repeat_min_s: float = 10.0):
-    """The oracle port of the reference CPU path on a bounded sample of the workload."""
+VERIFY_CFG = dict(match=1, mismatch=4, gap_open=6, gap_extend=1, band=33, xdrop=100, clip=5,
+                  sieve_threshold=12, myers_k=8)
+PARITY_FIELDS = ("status", "score", "ref_start", "ref_end", "read_start", "read_end", "n_cigar",
+                 "early_abort", "cigar", "cells")
+
+
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as O
-    arena, woffs = w.windows_arena()
-    idx = np.arange(min(sample, w.n_pairs))
-    op = O.verify_params(O.cfg(1, 4, 6, 1, 33, 100, 5), 12, 8)
-    args = (w.reads, w.read_off[idx].copy(), w.read_len[idx].copy(), arena, woffs[idx].copy(),
-            w.win_len[idx].copy())
-    done, t0 = 0, time.perf_counter()
-    while True:
-        O.verify_batch(*args, op, nthreads, 8)
-        done += len(idx)
-        el = time.perf_counter() - t0
-        if el >= repeat_min_s:
-            break
-    return done / el, el, len(idx)
+    c = VERIFY_CFG
+    op = O.verify_params(O.cfg(c["match"], c["mismatch"], c["gap_open"], c["gap_extend"],
+                               c["band"], c["xdrop"], c["clip"]), c["sieve_threshold"],
+                         c["myers_k"])
+    return O, op
+
+
+def oracle_verify(w, nthreads: int, cap: int = 16):
+    """The oracle port of the reference CPU path (sieve -> certificate -> Myers ->
+    banded_sw_with per pair) over every pair of `w`, on `nthreads` host threads;
+    windows read straight from the reference. Returns (rows, CIGAR ops per pair,
+    seconds). Pairs whose CIGAR exceeds `cap` ops are re-run with room for all."""
+    O, op = _oracle()
+    t = time.perf_counter()
+    out, cig = O.verify_batch(w.reads, w.read_off, w.read_len, w.reference, w.win_off, w.win_len,
+                              op, nthreads, cap)
+    el = time.perf_counter() - t
+    big = np.nonzero(out["n_cigar"] > cap)[0]
+    wide = {}
+    if len(big):
+        o2, c2 = O.verify_batch(w.reads, w.read_off[big].copy(), w.read_len[big].copy(),
+                                w.reference, w.win_off[big].copy(), w.win_len[big].copy(), op,
+                                nthreads, 1024)
+        wide = {int(p): c2[k] for k, p in enumerate(big)}
+    return out, cig, wide, el
+
+
+def parity_block(res, ops, cells, w, nthreads: int):
+    """Every pair of this rank's workload against the oracle, field by field, and the
+    CIGAR op by op; `cells` = the GPU's executed band cells of one step."""
+    out, cig, wide, el = oracle_verify(w, nthreads)
+    by = {}
+    for f in PARITY_FIELDS[:8]:
+        by[f] = int((res[f].astype(np.int64) != out[f].astype(np.int64)).sum())
+    n = res["n_cigar"].astype(np.int64)
+    sel = np.nonzero((n == out["n_cigar"].astype(np.int64)) & (n > 0))[0]
+    cnt = n[sel]
+    bad = set()
+    if len(sel):
+        pair = np.repeat(sel, cnt)
+        t = np.arange(int(cnt.sum())) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+        got = ops[res["cigar_off"][pair].astype(np.int64) + t]
+        narrow = cig.shape[1]
+        want = np.where(t < narrow, cig[pair, np.minimum(t, narrow - 1)], 0)
+        for k in np.nonzero(t >= narrow)[0]:
+            want[k] = wide[int(pair[k])][t[k]]
+        bad = set(np.unique(pair[got != want]).tolist())
+    by["cigar"] = len(bad)
+    by["cells"] = int(int(out["cells"].sum()) != int(cells))
+    return {"checked": int(len(res)), "mismatches": int(sum(by.values())), "by_field": by,
+            "fields": list(PARITY_FIELDS)}, el
 
 
 def run_reference(args, rank, world):
-    """Reference arm: the reference CPU path (oracle port, all host threads)."""
+    """Reference arm: the reference CPU path (the oracle port: the reference is Rust
+    and cannot be built here) on all host threads, over the same 2M-pair workload
+    as the GPU arm's rank 0, every pair every step. Under torchrun only rank 0 runs."""
     if rank != 0:
-        return
+        return None
     from kira_ls_aligner_b200 import synth
-    w = synth.batched(n_reads=max(args.reads // 10, 1000))
+    w = synth.batched(n_reads=args.reads, ref_len=args.ref_len)
     nthreads = os.cpu_count() or 1
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as O
-    arena, woffs = w.windows_arena()
-    n = min(args.cpu_sample, w.n_pairs)
-    op = O.verify_params(O.cfg(1, 4, 6, 1, 33, 100, 5), 12, 8)
-    a = (w.reads, w.read_off[:n].copy(), w.read_len[:n].copy(), arena, woffs[:n].copy(),
-         w.win_len[:n].copy())
+    O, op = _oracle()
+    a = (w.reads, w.read_off, w.read_len, w.reference, w.win_off, w.win_len)
     for _ in range(args.warmup):
-        O.verify_batch(*a, op, nthreads, 8)
+        O.verify_batch(*a, op, nthreads, 16)
     times = []
     for _ in range(args.steps):
         t = time.perf_counter()
-        O.verify_batch(*a, op, nthreads, 8)
+        O.verify_batch(*a, op, nthreads, 16)
         times.append(time.perf_counter() - t)
+    n = w.n_pairs
     v = n * len(times) / sum(times)
-    print(json.dumps({
+    return {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-        "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "pairs_per_step": n, "threads": nthreads},
+        "data": "synthetic (seeded; no public dataset)",
+        "config": _config(args, w, world, "reference CPU path on all host threads"),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
-                         "sample": f"{n} pairs of the batched workload per step"},
-        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+                         "sample": f"all {n} pairs of the workload every step"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def _config(args, w, world, parallelism):
+    return {"workload": WORKLOAD, "pairs_per_gpu": 8 * args.reads, "read_len": 150,
+            "window_len": 250, "candidates_per_read": 8, "band": 33, "sieve_threshold": 12,
+            "myers_k": 8, "scoring": "+1/-4/-6/-1, xdrop 100, clip 5, adaptive band (drift 16)",
+            "reference_bp": int(len(w.reference)), "seed": "0xB200",
+            "l2": "flushed between steps (256 MB write)", "parallelism": parallelism}
 
 
 def run_uneven(args, rank, local, world):
@@ -191,7 +249,7 @@ def run_uneven(args, rank, local, world):
 
     from kira_ls_aligner_b200 import AlignmentConfig, GpuContext, PairBatch, _abi, autotune, synth
     if rank != 0:
-        return
+        return None
     torch.cuda.set_device(local)
     w = synth.uneven()
     n = w.n_pairs
@@ -225,11 +283,14 @@ def run_uneven(args, rank, local, world):
         ctx.check(L.kira_gpu_profile(ctx.handle, 0))
         stages = dict(zip(("upload", "bucketing", "bsw_dp", "bsw_traceback", "cigar_compact"),
                           [round(float(x), 3) for x in buf[:k]]))
+        if mode == "bucketed":
+            graphs = graph_counts(ctx)
         out[mode] = {"stage_ms": stages, "pairs_per_s": n / (sum(ts) / len(ts) / 1e3),
                      "ms_per_call": sum(ts) / len(ts), "gcups": cells / (sum(ts) / len(ts) / 1e3) / 1e9,
                      "cells": int(cells), "checksum": int(res["score"].astype(np.int64).sum())}
     assert out["plain"]["checksum"] == out["bucketed"]["checksum"]
-    print(json.dumps({
+    ctx.close()
+    return {
         "metric": "pairs/s (uneven-length banded SW with CIGAR, bit-exact)",
         "value": out["bucketed"]["pairs_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": out["bucketed"]["ms_per_call"],
@@ -240,9 +301,8 @@ def run_uneven(args, rank, local, world):
                    "path": "host API, pinned inputs, H2D + D2H per call"},
         "bucketed": out["bucketed"], "plain": out["plain"],
         "speedup_vs_plain": out["bucketed"]["pairs_per_s"] / out["plain"]["pairs_per_s"],
-        "cuda_graphs": graph_counts(ctx),
-        "autotune": tuned}))
-    ctx.close()
+        "cuda_graphs": graphs,
+        "autotune": tuned}
 
 
 def run_nmmd(args, rank, local, world):
@@ -526,7 +586,7 @@ def run_serving(args, rank, local, world):
     from kira_ls_aligner_b200 import (AlignmentConfig, GpuContext, Server, VerifyParams, _abi,
                                       synth)
     if rank != 0:
-        return
+        return None
     torch.cuda.set_device(local)
     pool = synth.serving_pool()
     sched = synth.arrivals(0xA11, args.rate, args.duration)
@@ -615,7 +675,7 @@ def run_serving(args, rank, local, world):
     # saturated: every request submitted at once (capacity in pairs/s).
     srv_out, srv_sat = serve(True), serve(False)
     plain, plain_sat = plain_run(True), plain_run(False)
-    print(json.dumps({
+    return {
         "metric": "serving pairs/s with p50/p99 request latency (bit-exact)",
         "value": srv_out["pairs_per_s"], "unit": UNIT, "n_gpus": 1, "steps": len(reqs),
         "warmup": 4, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -633,7 +693,7 @@ def run_serving(args, rank, local, world):
                       "server_mean_requests_per_batch": srv_sat["mean_requests_per_batch"],
                       "server_host_ms": srv_sat["host_ms"], "server_submit_s": srv_sat["submit_s"]},
         "p99_ratio_plain_over_server": plain["p99_ms"] / srv_out["p99_ms"],
-        "p50_ratio_plain_over_server": plain["p50_ms"] / srv_out["p50_ms"]}))
+        "p50_ratio_plain_over_server": plain["p50_ms"] / srv_out["p50_ms"]}
 
 
 def run_gapfill(args, rank, local, world):
@@ -705,24 +765,39 @@ def _timed(fn) -> float:
     return (time.perf_counter() - t) * 1e3
 
 
+def relaunch(args) -> int:
+    """`--gpus N` without a launcher: run this script under torchrun, one rank per GPU
+    (rendezvous on 127.0.0.1); rank 0 prints the line."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1", "--master-port",
+           str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1 and args.impl == "ours":
+        sys.exit(relaunch(args))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
-    if world > 1:
+    if world > 1 and args.impl == "ours":
         import datetime
 
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
-                                timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(args.backend, timeout=datetime.timedelta(seconds=300))
+    out = None
     try:
         if args.workload == "uneven":
-            run_uneven(args, rank, local, world)
+            out = run_uneven(args, rank, local, world)
         elif args.workload == "serving":
-            run_serving(args, rank, local, world)
+            out = run_serving(args, rank, local, world)
         elif args.workload == "gapfill":
             run_gapfill(args, rank, local, world)
         elif args.workload == "nmmd":
@@ -732,23 +807,38 @@ def main():
         elif args.workload == "prefilter":
             run_prefilter(args, rank, local, world)
         elif args.impl == "reference":
-            run_reference(args, rank, world)
+            out = run_reference(args, rank, world)
         else:
-            run_ours(args, rank, local, world, dist)
+            out = run_ours(args, rank, local, world, dist)
     finally:
         if dist is not None:
             dist.barrier()
             dist.destroy_process_group()
+    if out is not None and rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def job_shard(args, rank, world):
+    """This rank's contiguous range of the job (world blocks of 8 x reads pairs on one
+    reference), cost-balanced by shard.shard_bounds, and its pairs."""
+    from kira_ls_aligner_b200 import shard, synth
+    block = 8 * args.reads
+    n = world * block
+    cost = shard.pair_cost(np.full(n, 150, np.uint32), np.full(n, 250, np.uint32), band=33)
+    lo, hi = shard.shard_bounds(cost, world)[rank]
+    return lo, hi, synth.batched_range(lo, hi, block_pairs=block, ref_len=args.ref_len)
 
 
 def run_ours(args, rank, local, world, dist):
+    lo, hi, w = job_shard(args, rank, world)
+    n = w.n_pairs
+    if args.dry_run:
+        return dry_run(args, rank, world, dist, w, lo, hi)
     import torch
 
-    from kira_ls_aligner_b200 import GpuContext, VerifyParams, _abi, synth
+    from kira_ls_aligner_b200 import GpuContext, VerifyParams, _abi, autotune, shard
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    w = synth.batched(seed=0xB200 + rank, n_reads=args.reads)
-    n = w.n_pairs
     params = VerifyParams(sieve_threshold=12, myers_k=8)
     ctx = GpuContext(local)
     L = _abi.lib()
@@ -784,7 +874,6 @@ def run_ours(args, rank, local, world, dist):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
-    from kira_ls_aligner_b200 import autotune
 
     def run_sync():
         step()
@@ -808,12 +897,15 @@ def run_ours(args, rank, local, world, dist):
     torch.cuda.synchronize(dev)
     total_ms = 0.0
     t_cells.zero_()
+    launches = 0
     for _ in range(args.steps):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0 = L.kira_gpu_launch_count()
         e0.record(stream)
         step()
         e1.record(stream)
+        launches += L.kira_gpu_launch_count() - c0
         e1.synchronize()
         total_ms += e0.elapsed_time(e1)
         buf = (C.c_float * 8)()
@@ -825,128 +917,266 @@ def run_ours(args, rank, local, world, dist):
     clocks = sampler.stop()
     L.kira_gpu_profile(ctx.handle, 0)
     cells = int(t_cells.item())
-    if dist is not None:
-        tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    cells_step = cells // max(args.steps, 1)
+    total_ms = _max_over_ranks(total_ms, dist, dev)
     ms_per_step = total_ms / args.steps
     value = n * world * args.steps / (total_ms / 1e3)
-    gcups = cells * world / (total_ms / 1e3) / 1e9
 
-    # Outcome summary of one step (for the record; parity is checked by the tests).
+    # This step's results on the host (outside the timed region).
     res = np.frombuffer(t_res.cpu().numpy().tobytes(), _abi.SW_RESULT_DTYPE)
+    used = int(t_used.item())
+    ops = t_ops[:used].cpu().numpy().view(np.uint32)
     statuses = np.bincount(res["status"], minlength=4).tolist()
 
     # e2e through the host API with pinned host inputs.
-    e2e = None
-    if not args.no_e2e:
-        pin = lambda a: torch.from_numpy(a).pin_memory()
-        h_reads = pin(np.concatenate([w.reads, np.zeros(16, np.uint8)]))
-        h_roff, h_rlen = pin(w.read_off.view(np.int64)), pin(w.read_len.view(np.int32))
-        h_woff, h_wlen = pin(w.win_off.view(np.int64)), pin(w.win_len.view(np.int32))
-        res_h = torch.empty(n * 32, dtype=torch.uint8).pin_memory()
-        ops_h = torch.empty(cap, dtype=torch.int32).pin_memory()
-        cb = _abi.CigarBuf(ops_h.data_ptr(), cap, 0)
-        hpc = _abi.Pairs()
-        hpc.n = n
-        hpc.read_seq, hpc.read_seq_bytes = h_reads.data_ptr(), int(w.reads.nbytes)
-        hpc.read_off, hpc.read_len = h_roff.data_ptr(), h_rlen.data_ptr()
-        hpc.win_seq, hpc.win_off, hpc.win_len = None, h_woff.data_ptr(), h_wlen.data_ptr()
-        cells_h = C.c_uint64()
+    e2e = None if args.no_e2e else e2e_run(args, ctx, L, vp, w, n, world, dist, dev)
 
-        def e2e_step():
-            ctx.check(L.kira_gpu_verify_batch(ctx.handle, C.byref(hpc), C.byref(vp),
-                                              res_h.data_ptr(), C.byref(cb), None,
-                                              C.byref(cells_h)))
-        for _ in range(max(1, args.warmup)):
-            e2e_step()
-        if dist is not None:
-            dist.barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            e2e_step()
-        el = time.perf_counter() - t0
-        if dist is not None:
-            tt = torch.tensor([el], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            el = float(tt.item())
-        # Bytes the call copies up: the read arena plus the pair descriptors, packed to
-        # 12 bytes a pair (u32 offsets, u16 lengths) when the read arena and the
-        # reference are below 4 GiB and every length fits 16 bits, else 24.
-        packed = (w.reads.nbytes < 1 << 32 and len(w.reference) < 1 << 32
-                  and max(int(w.read_len.max()), int(w.win_len.max())) < 1 << 16)
-        h2d = int(w.reads.nbytes) + n * (12 if packed else 8 + 4 + 8 + 4)
-        d2h = n * 32 + 4 * int(cb.used) + 8 + 8 + 16
-        e2e = {"value": n * world * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * el / args.steps}
+    # Every rank's results gathered on rank 0 (one collective, outside the timed
+    # region), checked against the per-rank checksums.
+    gathered = None
+    if dist is not None:
+        gdev = dev if args.backend == "nccl" else None
+        g_res, g_ops = shard.gather_results(res, ops, dist, device=gdev)
+        sums = _all_gather_ints([n, int(res["score"].astype(np.int64).sum()), len(ops),
+                                 int(ops.astype(np.int64).sum())], dist, gdev)
+        if rank == 0:
+            ok = (len(g_res) == sum(s[0] for s in sums) and len(g_ops) == sum(s[2] for s in sums)
+                  and int(g_res["score"].astype(np.int64).sum()) == sum(s[1] for s in sums)
+                  and int(g_ops.astype(np.int64).sum()) == sum(s[3] for s in sums))
+            gathered = {"pairs": int(len(g_res)), "cigar_ops": int(len(g_ops)),
+                        "checksums_match": bool(ok)}
 
-    # Roofline of the dominant stage.
+    # Parity: every pair of this rank's shard against the oracle (all ranks at once,
+    # host threads split between them); mismatch counts summed over ranks.
+    parity, cpu = None, None
+    if not args.no_cpu:
+        nthreads = max(1, (os.cpu_count() or 1) // world)
+        parity, el = parity_block(res, ops, cells_step, w, nthreads)
+        if dist is not None:
+            tot = _all_gather_ints([parity["checked"], parity["mismatches"]], dist,
+                                   dev if args.backend == "nccl" else None)
+            parity["checked_all_ranks"] = sum(t[0] for t in tot)
+            parity["mismatches_all_ranks"] = sum(t[1] for t in tot)
+        if world == 1:
+            cpu = {"value": n / el, "unit": UNIT, "cores": nthreads, "kind": "port",
+                   "sample": f"all {n} pairs of the workload, one pass (the parity check's "
+                             f"oracle run), {el:.2f} s"}
+
+    roofline = roofline_block(args, L, local, stage_ms, statuses, cells_step, n, tuning)
+
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        ctx.close()
+        ctx = None
+        extras = run_extras(args, local)
+
+    if ctx is not None:
+        ctx.close()
+    if rank != 0:
+        return None
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded; no public dataset)",
+        "config": _config(args, w, world,
+                          f"{world} rank(s), one job of {world} x {8 * args.reads} pairs in "
+                          f"contiguous cost-balanced shards, no data-path collective"),
+        "gcups": cells_step * world / (ms_per_step / 1e3) / 1e9, "cells_per_step": cells_step,
+        "autotune": tuning,
+        "status_counts": {"certified": statuses[1], "myers_reject": statuses[2],
+                          "sw": statuses[3]},
+        "parity": parity, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "clocks": clocks, "gpu_launches": int(launches),
+        "shard": {"rank0_pairs": [lo, hi], "gathered": gathered},
+    }
+    out.update(extras)
+    return out
+
+
+def _max_over_ranks(x: float, dist, dev) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _all_gather_ints(vals, dist, dev):
+    import torch
+    t = torch.tensor(vals, dtype=torch.int64, device=dev)
+    parts = [torch.zeros_like(t) for _ in range(dist.get_world_size())]
+    dist.all_gather(parts, t)
+    return [[int(v) for v in p.cpu()] for p in parts]
+
+
+def e2e_run(args, ctx, L, vp, w, n, world, dist, dev):
+    """The same metric through kira_gpu_verify_batch (the drop-in host API) with pinned
+    host inputs and outputs: H2D of reads and pair descriptors, D2H of result rows and
+    CIGAR ops inside the timed region."""
+    import torch
+
+    from kira_ls_aligner_b200 import _abi
+    pin = lambda a: torch.from_numpy(a).pin_memory()  # noqa: E731
+    h_reads = pin(np.concatenate([w.reads, np.zeros(16, np.uint8)]))
+    h_roff, h_rlen = pin(w.read_off.view(np.int64)), pin(w.read_len.view(np.int32))
+    h_woff, h_wlen = pin(w.win_off.view(np.int64)), pin(w.win_len.view(np.int32))
+    cap = 4 * n
+    res_h = torch.empty(n * 32, dtype=torch.uint8).pin_memory()
+    ops_h = torch.empty(cap, dtype=torch.int32).pin_memory()
+    cb = _abi.CigarBuf(ops_h.data_ptr(), cap, 0)
+    hpc = _abi.Pairs()
+    hpc.n = n
+    hpc.read_seq, hpc.read_seq_bytes = h_reads.data_ptr(), int(w.reads.nbytes)
+    hpc.read_off, hpc.read_len = h_roff.data_ptr(), h_rlen.data_ptr()
+    hpc.win_seq, hpc.win_off, hpc.win_len = None, h_woff.data_ptr(), h_wlen.data_ptr()
+    cells_h = C.c_uint64()
+
+    def e2e_step():
+        ctx.check(L.kira_gpu_verify_batch(ctx.handle, C.byref(hpc), C.byref(vp),
+                                          res_h.data_ptr(), C.byref(cb), None,
+                                          C.byref(cells_h)))
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    el = _max_over_ranks(time.perf_counter() - t0, dist, dev)
+    # Bytes the call copies up: the read arena plus the pair descriptors, packed to
+    # 12 bytes a pair (u32 offsets, u16 lengths) when the read arena and the
+    # reference are below 4 GiB and every length fits 16 bits, else 24.
+    packed = (w.reads.nbytes < 1 << 32 and len(w.reference) < 1 << 32
+              and max(int(w.read_len.max()), int(w.win_len.max())) < 1 << 16)
+    h2d = int(w.reads.nbytes) + n * (12 if packed else 8 + 4 + 8 + 4)
+    d2h = n * 32 + 4 * int(cb.used) + 8 + 8 + 16
+    return {"value": n * world * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * el / args.steps}
+
+
+def profile_figure(name: str, key: str):
+    """A figure recorded in a committed ncu summary (`key: value` line), or None."""
+    import re
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            m = re.search(rf"^{re.escape(key)}:\s*([0-9.eE+-]+)", f.read(), re.M)
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+ALU_PROBES = ("dpx_s16x2_addmax", "iadd3", "lop3")
+
+
+def roofline_block(args, L, local, stage_ms, statuses, cells_step, n, tuning):
+    """HBM roofline of the dominant stage (algorithmic bytes / CUDA-event time against
+    the measured copy bandwidth) and, beside it, the integer-pipe roofline of the DP
+    kernel: the reference recurrence's integer operations per cell (18; 9 on packed
+    int16 pairs) at the measured cell rate, against this GPU's integer instruction
+    rate measured in the same run (kira_gpu_alu_probe)."""
+    from kira_ls_aligner_b200 import _abi, autotune
     peak, peak_kind = measured_peaks()
     dom = int(np.argmax(stage_ms))
     dom_ms = stage_ms[dom] / args.steps
     n_sw = statuses[3]
     n_my = statuses[2] + statuses[3]
     q, wl = 150, 250
-    cells_step = cells // max(args.steps, 1)
-    packed = autotune.packed()[tuning["best"]]
-    trace_b = 1.0 if packed else 0.5  # trace bytes per DP cell (byte codes / nibbles)
-    alg_bytes = {  # algorithmic bytes per launch of each stage (sequences in, results out)
-        0: n * (q + wl + 24 + 32),
-        1: n_my * (q + wl + 8) + n_sw * 4,
-        2: int(n_sw * (q + wl + 16 + 4 * (q + 1)) + cells_step * trace_b),
-        3: int(n_sw * (32 + 16) + cells_step * trace_b / 50),
-        4: n * (32 + 8) + 4 * n,
-    }[dom]
-    # DRAM bytes per unit from the ncu captures of the same kernels (800k-pair case,
-    # scaled by units processed): profiles/bsw16_dp_batched_800k.md (1.496 B per DP
-    # cell) and profiles/verify_sieve_batched_800k.md (213.7 B per pair over the
-    # filter and survivor-sieve kernels).
-    traffic = {0: 213.7 * n, 2: 1.496 * cells_step if packed else None}.get(dom)
-    achieved = alg_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    packed = bool(autotune.packed()[tuning["best"]])
+    qp, wp = (q + 3) // 4, (wl + 3) // 4
+    # Algorithmic bytes per launch of each stage: 2-bit packed sequences and result
+    # rows for the sieve and Myers; for the DP the ASCII read and window of every SW
+    # pair, its end coordinates, and a 4-bit trace code per executed band cell.
+    alg = {0: n * (qp + wp + 12), 1: n_my * (qp + wp + 8), 2: n_sw * (q + wl + 16) + cells_step // 2,
+           3: n_sw * (32 + 16) + cells_step // 50, 4: n * (32 + 8) + 4 * n}
+    achieved = alg[dom] / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    per_cell = profile_figure("bsw16_dp_batched_800k.md" if packed else "bsw_dp_batched_800k.md",
+                              "dram_bytes_per_cell")
+    per_pair = profile_figure("verify_sieve_batched_800k.md", "dram_bytes_per_pair")
+    traffic = {2: None if per_cell is None else per_cell * cells_step,
+               0: None if per_pair is None else per_pair * n}.get(dom)
     dp_ms = stage_ms[2] / args.steps
-    roofline = {"bound": "hbm", "kernel": _abi.STAGES[dom], "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None if traffic is None else int(traffic),
-                "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs",
-                "stage_ms_per_step": {s: round(float(t) / args.steps, 4)
-                                      for s, t in zip(_abi.STAGES, stage_ms)},
-                # The sieve, Myers and DP kernels are integer-pipe bound (ncu: ALU pipe
-                # 77-85 % of peak, DRAM < 10 %); their binding roofline is the ALU pipe.
-                "int_pipe": {"kernel": "bsw_dp", "gcups": cells_step / (dp_ms / 1e3) / 1e9
-                             if dp_ms > 0 else None,
-                             "alu_pipe_frac_ncu": 0.759 if packed else 0.757,
-                             "thread_inst_per_cell_ncu": 28.4 if packed else 90.8,
-                             "source": "profiles/bsw16_dp_batched_800k.md"}}
+    probes = {}
+    for op, name in enumerate(ALU_PROBES):
+        v = C.c_double()
+        if L.kira_gpu_alu_probe(local, op, 200_000, C.byref(v)) == 0:
+            probes[name] = v.value / 1e12
+    ops_cell = 9 if packed else 18
+    cell_rate = cells_step / (dp_ms / 1e3) if dp_ms > 0 else 0.0
+    ipeak = max(probes.values()) if probes else None
+    return {"bound": "hbm", "kernel": _abi.STAGES[dom], "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "traffic": None if traffic is None
+            else int(traffic), "algorithmic_bytes": int(alg[dom]),
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic_source": "ncu DRAM bytes per unit (profiles/), scaled by this run's units",
+            "stage_ms_per_step": {s: round(float(t) / args.steps, 4)
+                                  for s, t in zip(_abi.STAGES, stage_ms)},
+            "int_pipe": {"kernel": "bsw_dp", "gcups": cell_rate / 1e9,
+                         "ops_per_cell": ops_cell,
+                         "achieved_tops": cell_rate * ops_cell / 1e12,
+                         "peak_tops": ipeak, "frac": None if not ipeak
+                         else cell_rate * ops_cell / 1e12 / ipeak,
+                         "probe_tops": probes,
+                         "peak_source": "kira_gpu_alu_probe in this run (fastest of "
+                                        "DPX add-max / IADD3 / LOP3 streams)"}}
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        nthreads = os.cpu_count() or 1
-        v, el, ns = cpu_baseline(w, nthreads, args.cpu_sample)
-        cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
-               "sample": f"first {ns} pairs of the workload, repeated for {el:.1f} s"}
 
-    if rank == 0:
-        out = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic (seeded; no public dataset)",
-            "config": {"workload": WORKLOAD, "pairs_per_gpu": n, "read_len": 150,
-                       "window_len": 250, "candidates_per_read": 8, "band": 33,
-                       "sieve_threshold": 12, "myers_k": 8, "reference_bp": int(len(w.reference)),
-                       "l2": "flushed between steps (256 MB write)",
-                       "parallelism": f"replicas x{world} (pairs sharded, no collective)"},
-            "gcups": gcups, "cells_per_step": cells // args.steps,
-            "autotune": tuning,
-            "status_counts": {"certified": statuses[1], "myers_reject": statuses[2],
-                              "sw": statuses[3]},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            # per step: planes pack, 4-gram filter, survivor sieve, Myers, SW DP,
-            # traceback, 3 scan, compaction
-            "gpu_launches": 10 * args.steps,
-        }
-        print(json.dumps(out))
-    ctx.close()
+def run_extras(args, local) -> dict:
+    """The batching and serving targets on the same GPU, folded into the headline
+    line: the uneven-length batch (bucketed persistent launches + graphs vs one
+    launch of the same kernel choice) and a short serving run (p50 / p99 latency,
+    server vs one request per call)."""
+    import argparse as _ap
+    ea = _ap.Namespace(**vars(args))
+    ea.steps, ea.warmup = 3, 2
+    out = {}
+    try:
+        u = run_uneven(ea, 0, local, 1)
+        out["uneven"] = {"config": u["config"], "pairs_per_s": u["value"],
+                         "plain_pairs_per_s": u["plain"]["pairs_per_s"],
+                         "speedup_vs_plain": u["speedup_vs_plain"],
+                         "bucketed_stage_ms": u["bucketed"]["stage_ms"],
+                         "plain_stage_ms": u["plain"]["stage_ms"], "cuda_graphs": u["cuda_graphs"]}
+    except Exception as e:  # noqa: BLE001 -- reported, the headline stands
+        out["uneven"] = {"error": repr(e)}
+    ea.rate, ea.duration = 200.0, 2.0
+    try:
+        v = run_serving(ea, 0, local, 1)
+        out["serving"] = {"config": v["config"], "pairs_per_s": v["value"],
+                          "p50_ms": v["server"]["p50_ms"], "p99_ms": v["server"]["p99_ms"],
+                          "plain_p50_ms": v["plain"]["p50_ms"],
+                          "plain_p99_ms": v["plain"]["p99_ms"],
+                          "speedup_vs_plain": v["saturated"]["speedup"],
+                          "saturated": v["saturated"]}
+    except Exception as e:  # noqa: BLE001
+        out["serving"] = {"error": repr(e)}
+    return out
+
+
+def dry_run(args, rank, world, dist, w, lo, hi):
+    """The multi-rank plumbing without a GPU: shard, stand-in results, gather on rank
+    0, max-over-ranks timing."""
+    from kira_ls_aligner_b200 import _abi, shard
+    n = w.n_pairs
+    res = np.zeros(n, _abi.SW_RESULT_DTYPE)
+    res["score"] = (w.win_off % 97).astype(np.int32)
+    res["n_cigar"] = 1
+    res["cigar_off"] = np.arange(n, dtype=np.uint32)
+    ops = (w.read_len.astype(np.uint32) << 4)
+    t = time.perf_counter()
+    el = _max_over_ranks(time.perf_counter() - t, dist, None)
+    gathered = None
+    if dist is not None:
+        g_res, g_ops = shard.gather_results(res, ops, dist)
+        if rank == 0:
+            gathered = {"pairs": int(len(g_res)), "cigar_ops": int(len(g_ops)),
+                        "offsets_rebased": bool((g_res["cigar_off"] ==
+                                                 np.arange(len(g_res))).all())}
+    if rank != 0:
+        return None
+    return {"metric": METRIC, "dry_run": True, "n_gpus": world, "steps": args.steps,
+            "shard": {"rank0_pairs": [lo, hi], "gathered": gathered}, "max_s": el}
 
 
 if __name__ == "__main__":

@@ -90,6 +90,19 @@ int kira_gpu_last_error(const kira_ctx* ctx, char* buf, size_t len);
 /* Bytes of device memory the ctx arena currently holds. */
 uint64_t kira_gpu_arena_bytes(const kira_ctx* ctx);
 
+/* No counterpart in the reference (launch accounting for benchmarks): the number
+ * of kernels this library has launched in this process, over all contexts and
+ * threads; a CUDA-graph replay adds the kernels of the replayed graph. */
+uint64_t kira_gpu_launch_count(void);
+
+/* No counterpart in the reference (the denominator of the integer roofline of
+ * the DP kernels): measures this GPU's integer instruction rate. Every thread of
+ * a full grid runs `rounds` rounds of 16 independent instructions of one kind --
+ * op 0 the DPX add-max on packed int16 pairs, op 1 a three-input add, op 2 a
+ * three-input logic op -- and *thread_ops_per_s receives the thread-instructions
+ * per second (CUDA events around one launch after a warm-up launch). */
+int kira_gpu_alu_probe(int device, int op, uint32_t rounds, double* thread_ops_per_s);
+
 /* ------------------------------------------------------- sieve (drop-in) */
 
 /* CudaJob (src/cuda/backend.rs:13-26). Only phase 0 of ref_shifted is read:
@@ -203,9 +216,11 @@ int kira_gpu_set_bsw_shape(kira_ctx* ctx, uint32_t band, int shape);
 
 /* kira_gpu_bsw_batch buckets pairs by band class (one tuned launch shape and trace
  * geometry per class, longest reads first, dynamic work fetching). plain = 1
- * selects the one-launch form instead (a single shape sized for the widest band,
- * static order), kept as the baseline the bucketed form is measured against.
- * Results are identical either way. */
+ * selects the one-launch form instead: the kernel the bucketed path would pick
+ * for the batch's widest band (packed int16 when the batch's scores fit, else
+ * int32), one launch over every pair in input order, no graph replay -- the
+ * baseline the bucketed form is measured against. Results are identical either
+ * way. */
 int kira_gpu_set_plain(kira_ctx* ctx, int plain);
 
 /* Device bytes the banded-SW trace arena (trace slots + row metadata) may hold at

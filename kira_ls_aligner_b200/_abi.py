@@ -43,7 +43,7 @@ EXPORTS = (
     "kira_server_create", "kira_server_destroy", "kira_server_ref_upload",
     "kira_server_submit_verify", "kira_server_submit_bsw", "kira_server_poll",
     "kira_server_wait", "kira_server_info", "kira_server_release", "kira_server_stats",
-    "kira_server_last_error", "kira_server_profile",
+    "kira_server_last_error", "kira_server_profile", "kira_gpu_launch_count", "kira_gpu_alu_probe",
 )
 SIMD_SCALAR, SIMD_AVX2, SIMD_AVX_VNNI, SIMD_NEON = 0, 1, 2, 3
 VERIFY_NO_QGRAM = 1
@@ -213,6 +213,9 @@ def lib():
     L.kira_gpu_destroy.restype = None
     L.kira_server_destroy.restype = None
     L.kira_gpu_arena_bytes.restype = C.c_uint64
+    L.kira_gpu_launch_count.argtypes = []
+    L.kira_gpu_launch_count.restype = C.c_uint64
+    L.kira_gpu_alu_probe.argtypes = [C.c_int, C.c_int, C.c_uint32, C.POINTER(C.c_double)]
     _lib = L
     return L
 

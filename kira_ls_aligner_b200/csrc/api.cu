@@ -114,6 +114,7 @@ struct kira_ctx {
   cudaGraphExec_t graph_exec = nullptr;
   std::vector<uint8_t> graph_key;  // launch parameters the cached graph was captured with
   uint64_t graph_replays = 0, graph_captures = 0;
+  unsigned long long graph_kernels = 0;  // kernels in the cached graph (launch accounting)
   cudaStream_t h2d = nullptr, d2h = nullptr;   // copy streams of the chunked host path
   int64_t chunk_pairs = -1;                    // chunked host path: -1 auto, 0 off, else pairs
   int wfa_lanes = 0;                           // WFA lanes per pair: 0 auto, else 8 / 16 / 32
@@ -1120,12 +1121,15 @@ cudaError_t run_as_graph(kira_ctx* ctx, const DevPairs& D, const BucketRun& R,
   put(CL.slot_cap), put(CL.ops), put(CL.cap), put(total_dev);
   if (ctx->graph_exec && key == ctx->graph_key) {
     ++ctx->graph_replays;
+    count_launch(ctx->graph_kernels);
     return cudaGraphLaunch(ctx->graph_exec, st);
   }
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return enqueue();
+  const unsigned long long launched = launch_count();
   cudaError_t ee = enqueue();
+  ctx->graph_kernels = launch_count() - launched;  // counted once here, run by the launch below
   e = cudaStreamEndCapture(st, &g);
   if (ee != cudaSuccess || e != cudaSuccess || !g) {
     if (g) cudaGraphDestroy(g);
@@ -2217,15 +2221,21 @@ int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg
   KIRA_CUDA(cudaMemsetAsync(counters, 0, 16, st));
   KIRA_CUDA(cudaMemsetAsync(cells_dev, 0, 8, st));
   BswLaunch B{};
-  if (ctx->plain) {  // one launch, one shape for the widest band, static order
-    const int shape = plain_shape(mx.band);
+  if (ctx->plain) {
+    // The one-launch comparator: the same kernel choice the bucketed path makes for
+    // the batch's widest band (the tuned shape of its class when the batch fits it,
+    // packed int16 wherever the scores fit, else int32), one launch over every pair
+    // in input order; only the bucketing, dynamic fetch and graph replay differ.
+    const SwParams sp = resolve(*cfg);
+    const int shape = pick_shape(ctx, mx.band, mx.q, sp);
     if (shape < 0)
-      return fail(ctx, KIRA_ERR_INVALID, "band %u above the int32 one-launch maximum", mx.band);
+      return fail(ctx, KIRA_ERR_INVALID, "band %u above the one-launch maximum", mx.band);
     const uint32_t per_round = round_items(ctx, n, shape, mx.q);
     rc = prepare_bsw(ctx, n, n, per_round, mx, shape, B);
     if (rc) return rc;
     B.count = n;
-    B.sp = resolve(*cfg);
+    B.sp = sp;
+    B.bias = packed_bias(kBswShapes[shape], sp);
     B.offset = D.band_offset;
     B.cells = cells_dev;
     B.out = dout;

@@ -295,6 +295,10 @@ cudaError_t launch_exact_match(const DevPairs& P, const kira_chain* chains, uint
 
 int ctx_share_reference(kira_ctx* dst, const kira_ctx* src);
 
+// Launch accounting (kernels.cu): every kernel launch of the library adds one.
+void count_launch(unsigned long long k = 1);
+unsigned long long launch_count();
+
 // Why a banded-SW configuration is outside the supported domain (null: inside).
 const char* sw_cfg_problem(const kira_sw_cfg& c, uint32_t max_q, uint32_t max_band);
 

@@ -1,4 +1,5 @@
 // kernels.cu -- device kernels of libkira_gpu and their launchers.
+#include <atomic>
 #include <cuda_runtime.h>
 
 #include "bsw.cuh"
@@ -807,6 +808,12 @@ __global__ void __launch_bounds__(128) nmmd_kernel(DevPairs P, NmMdLaunch L, int
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
+// Kernels launched by this library in this process (graph replays add the
+// kernels of the replayed graph); read by kira_gpu_launch_count.
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch(unsigned long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
 static int grid_for(uint64_t units, int per_block, int max_blocks) {
   uint64_t b = (units + per_block - 1) / per_block;
   if (b < 1) b = 1;
@@ -817,14 +824,14 @@ static int grid_for(uint64_t units, int per_block, int max_blocks) {
 cudaError_t launch_sieve_dropin(const SieveJobsDev& J, kira_sieve_result* out, int sms,
                                 cudaStream_t st) {
   const int blocks = grid_for(J.n, 8, sms * 16);
-  sieve_dropin_kernel<<<blocks, 256, 0, st>>>(J, out);
+  (sieve_dropin_kernel<<<blocks, 256, 0, st>>>(J, out), count_launch());
   return cudaGetLastError();
 }
 
 cudaError_t launch_pack_planes(const uint8_t* seq, uint64_t len, uint4* out, uint64_t nblocks,
                                int sms, cudaStream_t st) {
   const int blocks = grid_for((nblocks + 31) / 32, 8, sms * 16);
-  pack_planes_kernel<<<blocks, 256, 0, st>>>(seq, len, out, nblocks);
+  (pack_planes_kernel<<<blocks, 256, 0, st>>>(seq, len, out, nblocks), count_launch());
   return cudaGetLastError();
 }
 
@@ -832,8 +839,10 @@ cudaError_t launch_unpack_pairs(const PackedPair* src, uint32_t n, uint64_t* rea
                                 uint32_t* read_len, uint64_t* win_off, uint32_t* win_len,
                                 bool lens, int sms, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
-  unpack_pairs_kernel<<<grid_for(n, 256, sms * 8), 256, 0, st>>>(src, n, read_off, read_len,
-                                                                 win_off, win_len, lens ? 1 : 0);
+  const int blocks = grid_for(n, 256, sms * 8);
+  (unpack_pairs_kernel<<<blocks, 256, 0, st>>>(src, n, read_off, read_len, win_off, win_len,
+                                                lens ? 1 : 0),
+   count_launch());
   return cudaGetLastError();
 }
 
@@ -844,15 +853,15 @@ cudaError_t launch_verify_sieve(const DevPairs& P, const VerifyDev& V, uint32_t 
   if (V.sieve_list && !V.detail && V.qgram && P.n < 0x80000000u) {
     cudaError_t e = cudaMemsetAsync(V.sieve_count, 0, 4, st);
     if (e != cudaSuccess) return e;
-    verify_filter_kernel<<<blocks, 256, 0, st>>>(P, V);
-    if (rw <= 5) verify_sieve_list_kernel<5><<<blocks, 256, 0, st>>>(P, V);
-    else if (rw <= 8) verify_sieve_list_kernel<8><<<blocks, 256, 0, st>>>(P, V);
-    else verify_sieve_list_kernel<16><<<blocks, 256, 0, st>>>(P, V);
+    (verify_filter_kernel<<<blocks, 256, 0, st>>>(P, V), count_launch());
+    if (rw <= 5) (verify_sieve_list_kernel<5><<<blocks, 256, 0, st>>>(P, V), count_launch());
+    else if (rw <= 8) (verify_sieve_list_kernel<8><<<blocks, 256, 0, st>>>(P, V), count_launch());
+    else (verify_sieve_list_kernel<16><<<blocks, 256, 0, st>>>(P, V), count_launch());
     return cudaGetLastError();
   }
-  if (rw <= 5) verify_sieve_kernel<5><<<blocks, 256, 0, st>>>(P, V);
-  else if (rw <= 8) verify_sieve_kernel<8><<<blocks, 256, 0, st>>>(P, V);
-  else verify_sieve_kernel<16><<<blocks, 256, 0, st>>>(P, V);
+  if (rw <= 5) (verify_sieve_kernel<5><<<blocks, 256, 0, st>>>(P, V), count_launch());
+  else if (rw <= 8) (verify_sieve_kernel<8><<<blocks, 256, 0, st>>>(P, V), count_launch());
+  else (verify_sieve_kernel<16><<<blocks, 256, 0, st>>>(P, V), count_launch());
   return cudaGetLastError();
 }
 
@@ -860,10 +869,10 @@ cudaError_t launch_myers(const DevPairs& P, const MyersLaunch& M, uint32_t max_i
                          cudaStream_t st) {
   const size_t smem = (size_t)4 * M.lmax * 160 * sizeof(uint32_t);
   const int blocks = grid_for(max_items, 128, sms * 8);
-  if (M.lmax <= 5) myers_kernel<5><<<blocks, 128, smem, st>>>(P, M);
-  else if (M.lmax <= 8) myers_kernel<8><<<blocks, 128, smem, st>>>(P, M);
-  else if (M.lmax <= 12) myers_kernel<12><<<blocks, 128, smem, st>>>(P, M);
-  else myers_kernel<16><<<blocks, 128, smem, st>>>(P, M);
+  if (M.lmax <= 5) (myers_kernel<5><<<blocks, 128, smem, st>>>(P, M), count_launch());
+  else if (M.lmax <= 8) (myers_kernel<8><<<blocks, 128, smem, st>>>(P, M), count_launch());
+  else if (M.lmax <= 12) (myers_kernel<12><<<blocks, 128, smem, st>>>(P, M), count_launch());
+  else (myers_kernel<16><<<blocks, 128, smem, st>>>(P, M), count_launch());
   return cudaGetLastError();
 }
 
@@ -880,13 +889,13 @@ static cudaError_t launch_bsw_shape(const DevPairs& P, const BswLaunch& B, uint3
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
     if (per_sm < 1) per_sm = 1;
     const int blocks = grid_for(max_items, threads / G, sms * per_sm);
-    kern<<<blocks, threads, smem, st>>>(P, B);
+    (kern<<<blocks, threads, smem, st>>>(P, B), count_launch());
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (B.full && B.rowkeys) {
       const int rb = (int)((B.count + 127) / 128);
-      bsw_full_done_kernel<<<rb, 128, 0, st>>>(P, B);
-      bsw_full_resolve_kernel<<<rb, 128, 0, st>>>(P, B);
+      (bsw_full_done_kernel<<<rb, 128, 0, st>>>(P, B), count_launch());
+      (bsw_full_resolve_kernel<<<rb, 128, 0, st>>>(P, B), count_launch());
       e = cudaGetLastError();
       if (e != cudaSuccess) return e;
     }
@@ -894,7 +903,7 @@ static cudaError_t launch_bsw_shape(const DevPairs& P, const BswLaunch& B, uint3
   if (between) cudaEventRecord(between, st);
   if (parts & kBswPartTb) {
     const int tb_blocks = grid_for(max_items, 4, sms * 16);  // a warp per item
-    bsw_tb_kernel<G, K, false><<<tb_blocks, 128, 0, st>>>(P, B);
+    (bsw_tb_kernel<G, K, false><<<tb_blocks, 128, 0, st>>>(P, B), count_launch());
     e = cudaGetLastError();
   }
   return e;
@@ -912,14 +921,14 @@ static cudaError_t launch_bsw16_shape(const DevPairs& P, const BswLaunch& B, uin
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, smem);
     if (per_sm < 1) per_sm = 1;
     const int blocks = grid_for(max_items, T / G, sms * per_sm);
-    kern<<<blocks, T, smem, st>>>(P, B);
+    (kern<<<blocks, T, smem, st>>>(P, B), count_launch());
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   if (between) cudaEventRecord(between, st);
   if (parts & kBswPartTb) {
     const int tb_blocks = grid_for(max_items, 4, sms * 16);  // a warp per item
-    bsw_tb_kernel<G, K, true><<<tb_blocks, 128, 0, st>>>(P, B);
+    (bsw_tb_kernel<G, K, true><<<tb_blocks, 128, 0, st>>>(P, B), count_launch());
     e = cudaGetLastError();
   }
   return e;
@@ -962,23 +971,102 @@ cudaError_t launch_cigar_scan(const uint32_t* ncig, uint32_t n, uint32_t* off, u
                               uint64_t* total_dev, cudaStream_t st, bool accumulate) {
   const uint32_t chunks = (n + kScanChunk - 1) / kScanChunk;
   if (chunks == 0) return cudaSuccess;
-  scan_chunk_sums<<<chunks, kScanThreads, 0, st>>>(ncig, n, chunk_sums);
-  scan_sums<<<1, kScanThreads, 0, st>>>(chunk_sums, chunks, total_dev, accumulate ? 1 : 0);
-  scan_apply<<<chunks, kScanThreads, 0, st>>>(ncig, n, chunk_sums, off);
+  (scan_chunk_sums<<<chunks, kScanThreads, 0, st>>>(ncig, n, chunk_sums), count_launch());
+  (scan_sums<<<1, kScanThreads, 0, st>>>(chunk_sums, chunks, total_dev, accumulate ? 1 : 0), count_launch());
+  (scan_apply<<<chunks, kScanThreads, 0, st>>>(ncig, n, chunk_sums, off), count_launch());
   return cudaGetLastError();
 }
 
 cudaError_t launch_nm_md(const DevPairs& P, const NmMdLaunch& L, bool write, int sms,
                          cudaStream_t st) {
   const int blocks = grid_for(L.n, 128, sms * 16);
-  nmmd_kernel<<<blocks, 128, 0, st>>>(P, L, write ? 1 : 0);
+  (nmmd_kernel<<<blocks, 128, 0, st>>>(P, L, write ? 1 : 0), count_launch());
   return cudaGetLastError();
 }
 
 cudaError_t launch_cigar_compact(const CompactLaunch& C, int sms, cudaStream_t st) {
   const int blocks = grid_for(C.n, 256, sms * 8);
-  cigar_compact_kernel<<<blocks, 256, 0, st>>>(C);
+  (cigar_compact_kernel<<<blocks, 256, 0, st>>>(C), count_launch());
   return cudaGetLastError();
 }
 
 }  // namespace kira
+
+extern "C" uint64_t kira_gpu_launch_count(void) { return kira::launch_count(); }
+
+// ---------------------------------------------------------------------------
+// Integer issue-rate probe (the denominator of the DP kernels' integer roofline).
+// Every thread updates 16 independent packed words per round with one kind of
+// instruction: OP 0 the DPX add-max (__viaddmax_s16x2), OP 1 a three-input add,
+// OP 2 a three-input logic op. The result is folded into a sink that is written
+// only on an impossible value, which keeps every round live.
+// ---------------------------------------------------------------------------
+namespace kira {
+
+template <int OP>
+__global__ void __launch_bounds__(256) alu_probe_kernel(uint32_t rounds, uint32_t seed,
+                                                        uint32_t* sink) {
+  uint32_t x[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) x[k] = seed * (threadIdx.x + 977u * k + 31u * blockIdx.x + 1u);
+  uint32_t y = seed ^ threadIdx.x;
+  for (uint32_t r = 0; r < rounds; ++r) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const uint32_t nb = x[(k + 1) & 15];
+      if constexpr (OP == 0) x[k] = __viaddmax_s16x2(x[k], y, nb);
+      else if constexpr (OP == 1) x[k] = x[k] + nb + y;
+      else x[k] = (x[k] & nb) ^ y;
+    }
+    y += 0x00010001u;
+  }
+  uint32_t acc = 0;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) acc ^= x[k];
+  if (acc == 0x9E3779B9u) sink[0] = acc;
+}
+
+}  // namespace kira
+
+extern "C" int kira_gpu_alu_probe(int device, int op, uint32_t rounds, double* thread_ops_per_s) {
+  using namespace kira;
+  if (!thread_ops_per_s || op < 0 || op > 2 || rounds == 0) return KIRA_ERR_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return KIRA_ERR_NO_DEVICE;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    return KIRA_ERR_RUNTIME;
+  uint32_t* sink = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaStream_t st = nullptr;
+  int rc = KIRA_OK;
+  if (cudaMalloc(&sink, 16) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+      cudaEventCreate(&e1) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    rc = KIRA_ERR_RUNTIME;
+  } else {
+    const int blocks = sms * 8, threads = 256;
+    auto launch = [&](uint32_t n) {
+      const uint32_t seed = 0x2545F491u;
+      if (op == 0) alu_probe_kernel<0><<<blocks, threads, 0, st>>>(n, seed, sink);
+      else if (op == 1) alu_probe_kernel<1><<<blocks, threads, 0, st>>>(n, seed, sink);
+      else alu_probe_kernel<2><<<blocks, threads, 0, st>>>(n, seed, sink);
+      count_launch();
+    };
+    launch(rounds / 8 + 1);  // warm-up (clocks up, module loaded)
+    cudaEventRecord(e0, st);
+    launch(rounds);
+    cudaEventRecord(e1, st);
+    float ms = 0.f;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess ||
+        cudaGetLastError() != cudaSuccess || ms <= 0.f) {
+      rc = KIRA_ERR_RUNTIME;
+    } else {
+      *thread_ops_per_s = (double)blocks * threads * 16.0 * rounds / (ms * 1e-3);
+    }
+  }
+  if (st) cudaStreamDestroy(st);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (sink) cudaFree(sink);
+  return rc;
+}

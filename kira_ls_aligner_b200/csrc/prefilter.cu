@@ -298,7 +298,7 @@ int pf_grid(uint32_t n, int sms) {
 
 cudaError_t launch_prefilter(const DevPairs& P, const PrefilterLaunch& L, bool write, int sms,
                              cudaStream_t st) {
-  prefilter_kernel<<<pf_grid(P.n, sms), 256, 0, st>>>(P, L, write ? 1 : 0);
+  (prefilter_kernel<<<pf_grid(P.n, sms), 256, 0, st>>>(P, L, write ? 1 : 0), count_launch());
   return cudaGetLastError();
 }
 
@@ -308,13 +308,13 @@ cudaError_t launch_prefilter_offsets(uint32_t n, kira_prefilter_result* out,
   uint64_t b = ((uint64_t)n + 255) / 256;
   if (b < 1) b = 1;
   if (b > (uint64_t)sms * 8) b = (uint64_t)sms * 8;
-  prefilter_offsets_kernel<<<(int)b, 256, 0, st>>>(n, out, cig_off, md_off);
+  (prefilter_offsets_kernel<<<(int)b, 256, 0, st>>>(n, out, cig_off, md_off), count_launch());
   return cudaGetLastError();
 }
 
 cudaError_t launch_exact_match(const DevPairs& P, const kira_chain* chains, uint8_t* out, int sms,
                                cudaStream_t st) {
-  exact_match_kernel<<<pf_grid(P.n, sms), 256, 0, st>>>(P, chains, out);
+  (exact_match_kernel<<<pf_grid(P.n, sms), 256, 0, st>>>(P, chains, out), count_launch());
   return cudaGetLastError();
 }
 

@@ -627,8 +627,8 @@ cudaError_t wfa_blocks_per_sm(int group, bool traceback, size_t smem, int thread
 template <int G>
 static void wfa_launch_g(const DevPairs& P, const WfaLaunch& L, uint32_t blocks, uint32_t threads,
                          size_t smem, bool traceback, cudaStream_t st) {
-  if (traceback) wfa_kernel<G, true><<<blocks, threads, smem, st>>>(P, L);
-  else wfa_kernel<G, false><<<blocks, threads, smem, st>>>(P, L);
+  if (traceback) (wfa_kernel<G, true><<<blocks, threads, smem, st>>>(P, L), count_launch());
+  else (wfa_kernel<G, false><<<blocks, threads, smem, st>>>(P, L), count_launch());
 }
 
 cudaError_t launch_wfa(const DevPairs& P, const WfaLaunch& L, uint32_t blocks,
@@ -657,11 +657,11 @@ cudaError_t launch_wfa_window(const DevPairs& P, const WfaLaunch& L, uint32_t bl
                               bool traceback, cudaStream_t st) {
   const size_t smem = (size_t)4 * (L.win_ring_bytes + L.smem_group - L.ring_bytes);
   if (L.win_segments == 4) {
-    if (traceback) wfa_window_kernel<4, true><<<blocks, 128, smem, st>>>(P, L);
-    else wfa_window_kernel<4, false><<<blocks, 128, smem, st>>>(P, L);
+    if (traceback) (wfa_window_kernel<4, true><<<blocks, 128, smem, st>>>(P, L), count_launch());
+    else (wfa_window_kernel<4, false><<<blocks, 128, smem, st>>>(P, L), count_launch());
   } else {
-    if (traceback) wfa_window_kernel<2, true><<<blocks, 128, smem, st>>>(P, L);
-    else wfa_window_kernel<2, false><<<blocks, 128, smem, st>>>(P, L);
+    if (traceback) (wfa_window_kernel<2, true><<<blocks, 128, smem, st>>>(P, L), count_launch());
+    else (wfa_window_kernel<2, false><<<blocks, 128, smem, st>>>(P, L), count_launch());
   }
   return cudaGetLastError();
 }
@@ -670,7 +670,7 @@ cudaError_t launch_wfa_compact(const WfaCompact& C, int sms, cudaStream_t st) {
   uint64_t b = (C.n + 255) / 256;
   if (b < 1) b = 1;
   if (b > (uint64_t)sms * 8) b = (uint64_t)sms * 8;
-  wfa_compact_kernel<<<(int)b, 256, 0, st>>>(C);
+  (wfa_compact_kernel<<<(int)b, 256, 0, st>>>(C), count_launch());
   return cudaGetLastError();
 }
 

@@ -94,9 +94,18 @@ def _mutate(rng, frag: np.ndarray, read_len: int, sub_rate: float, indel_rate: f
 def make_workload(name: str, n_reads: int, ref_len: int, read_len: int = 150,
                   win_len: int = 250, cands: int = 4, sub_lo: float = 0.01,
                   sub_hi: float = 0.01, indel_rate: float = 0.001, repeat_frac: float = 0.0,
-                  seed: int = 0x5EED) -> Workload:
+                  seed: int = 0x5EED, block: int = 0, ref: np.ndarray | None = None) -> Workload:
+    """Reference from `seed`, then reads and candidate windows. Block 0 continues the
+    reference's random stream; block b > 0 draws its reads from the stream (seed, b),
+    so a job of several blocks shares one reference and block 0 is the one-block
+    workload itself. `ref` (the same seed's reference) skips regenerating it."""
     rng = np.random.default_rng(seed)
-    ref = random_reference(rng, ref_len, repeat_frac)
+    if ref is None:
+        ref = random_reference(rng, ref_len, repeat_frac)
+    elif block == 0:
+        raise ValueError("block 0 continues the reference's stream: pass ref=None")
+    if block:
+        rng = np.random.default_rng([seed, block])
     slack = win_len - read_len
     origins = rng.integers(slack, ref_len - win_len - 8, n_reads)
     sub = rng.uniform(sub_lo, sub_hi, n_reads)
@@ -127,10 +136,52 @@ def small(seed: int = 0x5EED) -> Workload:
                          sub_hi=0.01, seed=seed)
 
 
-def batched(seed: int = 0xB200, n_reads: int = 250_000, ref_len: int = 100_000_000) -> Workload:
-    """100 Mbp + 5 % repeats, 250k reads x 8 candidates = 2M pairs of 150 / 250 bp."""
+def batched(seed: int = 0xB200, n_reads: int = 250_000, ref_len: int = 100_000_000,
+            block: int = 0, ref: np.ndarray | None = None) -> Workload:
+    """100 Mbp + 5 % repeats, 250k reads x 8 candidates = 2M pairs of 150 / 250 bp.
+    Block b of a multi-block job (same reference, reads from the stream (seed, b))."""
     return make_workload("batched_2M_150x250", n_reads, ref_len, cands=8, sub_lo=0.005,
-                         sub_hi=0.02, repeat_frac=0.05, seed=seed)
+                         sub_hi=0.02, repeat_frac=0.05, seed=seed, block=block, ref=ref)
+
+
+def batched_reference(seed: int = 0xB200, ref_len: int = 100_000_000) -> np.ndarray:
+    """The reference of `batched` (the first draws of its seed's stream)."""
+    return random_reference(np.random.default_rng(seed), ref_len, 0.05)
+
+
+def batched_range(lo: int, hi: int, block_pairs: int = 2_000_000, seed: int = 0xB200,
+                  ref_len: int = 100_000_000) -> Workload:
+    """Pairs [lo, hi) of the job made of consecutive `batched` blocks of block_pairs
+    pairs each (8 candidates per read): the blocks that overlap the range are
+    generated and sliced, read arena compacted to the reads the range uses."""
+    cands = 8
+    if block_pairs % cands:
+        raise ValueError("block_pairs must be a multiple of 8")
+    n_reads = block_pairs // cands
+    first, last = lo // block_pairs, max(lo, hi - 1) // block_pairs
+    ref = None
+    parts = []
+    for b in range(first, last + 1):
+        w = batched(seed, n_reads, ref_len, block=b, ref=ref if b else None)
+        ref = w.reference if ref is None else ref
+        a, e = max(lo - b * block_pairs, 0), min(hi - b * block_pairs, block_pairs)
+        parts.append((w, a, e))
+    reads, roff, rlen, woff, wlen, tru = [], [], [], [], [], []
+    base = 0
+    for w, a, e in parts:
+        r0 = int(w.read_off[a]) if e > a else 0
+        r1 = int(w.read_off[e - 1]) + int(w.read_len[e - 1]) if e > a else 0
+        reads.append(w.reads[r0:r1])
+        roff.append(w.read_off[a:e] - np.uint64(r0) + np.uint64(base))
+        base += r1 - r0
+        rlen.append(w.read_len[a:e])
+        woff.append(w.win_off[a:e])
+        wlen.append(w.win_len[a:e])
+        tru.append(w.is_true[a:e])
+    cat = np.concatenate
+    return Workload(f"batched_pairs_{lo}_{hi}", ref if ref is not None else parts[0][0].reference,
+                    cat(reads), cat(roff).astype(np.uint64), cat(rlen), cat(woff), cat(wlen),
+                    cat(tru))
 
 
 def _mutate_matrix(rng, frag: np.ndarray, q: np.ndarray, rate: np.ndarray,

@@ -250,3 +250,48 @@ def test_uneven_automatic_chunks(ctx):
         ctx.check(L.kira_gpu_set_chunk_pairs(ctx.handle, -1))
     auto = ctx.verify_batch(b, params)
     assert np.array_equal(one[0], auto[0]) and np.array_equal(one[1], auto[1]) and one[3] == auto[3]
+
+
+def _compare_all(res, ops, det, out, cig):
+    """Vectorised form of _compare over every pair (rows, details and CIGAR ops)."""
+    for f in ("status", "score", "ref_start", "ref_end", "read_start", "read_end", "n_cigar",
+              "early_abort"):
+        bad = np.nonzero(res[f].astype(np.int64) != out[f].astype(np.int64))[0]
+        assert len(bad) == 0, (f, bad[:5], res[bad[:1]], out[bad[:1]])
+    if det is not None:
+        for f in ("sieve_shift", "sieve_mism", "sieve_second", "myers_dist", "myers_end"):
+            bad = np.nonzero(det[f].astype(np.int64) != out[f].astype(np.int64))[0]
+            assert len(bad) == 0, (f, bad[:5])
+    n = res["n_cigar"].astype(np.int64)
+    sel = np.nonzero(n)[0]
+    cnt = n[sel]
+    pair = np.repeat(sel, cnt)
+    t = np.arange(int(cnt.sum())) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+    got = ops[res["cigar_off"][pair].astype(np.int64) + t]
+    bad = np.nonzero(got != cig[pair, t])[0]
+    assert len(bad) == 0, ("cigar", np.unique(pair[bad])[:5])
+
+
+def test_batched_config_200k_all_pairs(ctx):
+    """The benchmark's own generator (100 Mbp with 5 % repeat families, 8 candidate
+    windows per read, seed 0xB200): 200k pairs, every pair against the oracle, in
+    the detail form and in the filter-first form the benchmark times."""
+    from kira_ls_aligner_b200 import PairBatch, VerifyParams, synth
+    w = synth.batched(n_reads=25_000)
+    params = VerifyParams(sieve_threshold=12, myers_k=8)
+    c = params.cfg
+    op = O.verify_params(O.cfg(c.match_score, c.mismatch, c.gap_open, c.gap_extend, c.bandwidth,
+                               c.xdrop, c.clip_penalty), 12, 8)
+    out, cig = O.verify_batch(w.reads, w.read_off, w.read_len, w.reference, w.win_off, w.win_len,
+                              op, NTHREADS, 64)
+    assert int(out["n_cigar"].max()) <= 64
+    ctx.ref_upload(w.reference)
+    b = PairBatch(w.reads, w.read_off, w.read_len, None, w.win_off, w.win_len)
+    res, ops, det, cells = ctx.verify_batch(b, params, detail=True)
+    _compare_all(res, ops, det, out, cig)
+    assert cells == int(out["cells"].sum())
+    res2, ops2, _, cells2 = ctx.verify_batch(b, params)
+    _compare_all(res2, ops2, None, out, cig)
+    assert cells2 == cells
+    counts = np.bincount(res["status"], minlength=4)
+    assert counts[1] > 0 and counts[2] > 0 and counts[3] > 0

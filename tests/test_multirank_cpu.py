@@ -119,3 +119,25 @@ def test_failed_rank_is_seen_by_the_other():
     errs = {o[1]: o for o in out if o[0] == "error"}
     assert 1 in errs and errs[1][2] == "RuntimeError"
     assert 0 in errs  # rank 0's gather ended with an error instead of hanging
+
+
+def test_bench_two_ranks_dry_run():
+    """bench.py --gpus 2 launches two ranks itself (torchrun, 127.0.0.1), shards one
+    job between them and gathers every rank's rows on rank 0, through the same code
+    the GPU run takes; --dry-run replaces the GPU step (gloo, CPU only)."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2",
+                        "--backend", "gloo", "--dry-run", "--reads", "2000", "--ref-len",
+                        "200000", "--steps", "1", "--warmup", "0"],
+                       capture_output=True, text=True, timeout=240)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1]
+    d = json.loads(line)
+    assert d["n_gpus"] == 2 and d["dry_run"]
+    assert d["shard"]["rank0_pairs"] == [0, 16000]
+    assert d["shard"]["gathered"] == {"pairs": 32000, "cigar_ops": 32000,
+                                      "offsets_rebased": True}
