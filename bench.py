@@ -68,7 +68,8 @@ def parse():
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=5.0, help="serving: seconds of arrivals")
     ap.add_argument("--slots", type=int, default=4, help="serving: concurrent batches")
-    ap.add_argument("--segments", type=int, default=20_000, help="gapfill: segments per call")
+    ap.add_argument("--long-reads", type=int, default=20_000,
+                    help="gapfill: simulated long reads (split into gap-fill segments)")
     ap.add_argument("--wfa-pairs", type=int, default=1_000_000, help="wfa: pairs per call")
     ap.add_argument("--wfa-drop", type=int, default=-1, help="wfa: adaptive drop (< 0 exact)")
     ap.add_argument("--chains", type=int, default=2_000_000, help="prefilter: chains per call")
@@ -697,18 +698,26 @@ def run_serving(args, rank, local, world):
 
 
 def run_gapfill(args, rank, local, world):
-    """Long-read gap-fill: segments U[200, 2000] bp at 5-12 % error, band 256, over a
-    resident reference; int32 lanes (scores exceed the packed range), traces in
-    rounds bounded by free device memory. Host API, H2D + D2H per call."""
+    """Long-read gap-fill at the configured size: 20k simulated long reads (lognormal
+    length, mean 10 kbp, sd 6 kbp, 1-50 kbp; 5-12 % error at 2:1:1) from a 1 Gbp
+    genome with 10 % repeat families, split at exact 15-mer anchors into segments of
+    200-2000 bases, each aligned with band 256 (int32 lanes: the scores leave the
+    packed int16 range) against the reference between its anchors. One host-API call
+    per step over every segment (H2D of the segment bases and descriptors, D2H of
+    rows and CIGARs); the trace arena runs in rounds sized by free device memory.
+    A sample of segments is checked against the oracle outside the timed region."""
     import torch
 
     from kira_ls_aligner_b200 import AlignmentConfig, GpuContext, PairBatch, _abi, synth
     if rank != 0:
         return
     torch.cuda.set_device(local)
-    g = synth.gapfill(args.segments)
-    b = PairBatch(g.reads, g.read_off, g.read_len, None, g.win_off, g.win_len, g.band_offset,
-                  None, g.bandwidth)
+    t0 = time.perf_counter()
+    g = synth.gapfill_reads(args.long_reads)
+    gen_s = time.perf_counter() - t0
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    b = PairBatch(pin(g.reads), pin(g.read_off), pin(g.read_len), None, pin(g.win_off),
+                  pin(g.win_len), pin(g.band_offset), None, pin(g.bandwidth))
     cfg = AlignmentConfig(1, 4, 6, 1, 256, 100, 5, True, 16)
     ctx = GpuContext(local)
     ctx.ref_upload(g.reference)
@@ -717,23 +726,52 @@ def run_gapfill(args, rank, local, world):
         res, ops, cells = ctx.bsw_batch(b, cfg)
     ts = [_timed(lambda: ctx.bsw_batch(b, cfg)) for _ in range(args.steps)]
     res, ops, cells = ctx.bsw_batch(b, cfg)
+    rounds = int(L.kira_gpu_bsw_rounds(ctx.handle))
     ctx.check(L.kira_gpu_profile(ctx.handle, 1))
     ctx.bsw_batch(b, cfg)
     buf = (C.c_float * 8)()
     k = L.kira_gpu_stage_times(ctx.handle, buf, 8)
     ctx.check(L.kira_gpu_profile(ctx.handle, 0))
+    stage = dict(zip(("upload", "bucketing", "bsw_dp", "bsw_traceback", "cigar_compact"),
+                     [round(float(x), 3) for x in buf[:k]]))
     ms = sum(ts) / len(ts)
+    n = g.n_pairs
+    parity = None
+    if not args.no_cpu:  # every 37th segment against the oracle's banded_sw_with
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as O
+        sel = np.arange(0, n, 37)
+        c = O.cfg(1, 4, 6, 1, 256, 100, 5)
+        out, cig = O.banded_sw_batch(g.reads, g.read_off[sel].copy(), g.read_len[sel].copy(),
+                                     g.reference, g.win_off[sel].copy(), g.win_len[sel].copy(),
+                                     g.band_offset[sel].copy(), c, os.cpu_count() or 1, 1024)
+        bad = 0
+        for t, p in enumerate(sel):
+            r = res[p]
+            same = all(int(r[f]) == int(out[f][t]) for f in
+                       ("score", "ref_start", "ref_end", "read_start", "read_end", "n_cigar",
+                        "early_abort"))
+            o, m = int(r["cigar_off"]), int(r["n_cigar"])
+            if not same or m > 1024 or not np.array_equal(ops[o:o + m], cig[t][:m]):
+                bad += 1
+        parity = {"checked": int(len(sel)), "mismatches": bad,
+                  "fields": ["score", "ref_start", "ref_end", "read_start", "read_end",
+                             "n_cigar", "early_abort", "cigar"]}
     print(json.dumps({
-        "metric": "pairs/s and GCUPS (gap-fill banded SW with CIGAR, bit-exact)",
-        "value": g.n_pairs / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "metric": "pairs/s and GCUPS (long-read gap-fill banded SW with CIGAR, bit-exact)",
+        "value": n / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
-        "config": {"workload": g.name, "segments": g.n_pairs, "band": 256,
-                   "errors": "U[5%,12%] 2:1:1", "reference_bp": int(len(g.reference)),
-                   "path": "host API, pinned-free inputs, H2D + D2H per call"},
-        "gcups": cells / (ms / 1e3) / 1e9, "cells": int(cells),
-        "stage_ms": dict(zip(("upload", "bucketing", "bsw_dp", "bsw_traceback",
-                              "cigar_compact"), [round(float(x), 3) for x in buf[:k]])),
+        "config": {"workload": g.name, "long_reads": g.n_reads, "read_bases": g.read_bases,
+                   "segments": n, "segment_bases": int(g.read_len.sum()),
+                   "segment_len": [int(g.read_len.min()), int(g.read_len.max())],
+                   "read_len": "lognormal mean 10 kbp sd 6 kbp, 1-50 kbp",
+                   "errors": "U[5%,12%] 2:1:1", "anchors": "exact 15-mers", "band": 256,
+                   "reference_bp": int(len(g.reference)), "repeats": "10 %",
+                   "path": "resident reference, host API (H2D segments + descriptors, "
+                           "D2H rows + CIGARs per call)", "generate_s": round(gen_s, 1)},
+        "gcups": cells / (ms / 1e3) / 1e9, "cells": int(cells), "trace_rounds": rounds,
+        "reads_per_s": g.n_reads / (ms / 1e3), "stage_ms": stage, "parity": parity,
         "checksum": int(res["score"].astype(np.int64).sum())}))
     ctx.close()
 
@@ -1012,9 +1050,11 @@ def _all_gather_ints(vals, dist, dev):
 
 
 def e2e_run(args, ctx, L, vp, w, n, world, dist, dev):
-    """The same metric through kira_gpu_verify_batch (the drop-in host API) with pinned
-    host inputs and outputs: H2D of reads and pair descriptors, D2H of result rows and
-    CIGAR ops inside the timed region."""
+    """The same metric through the host API with pinned host buffers: H2D of the
+    read arena and pair descriptors, D2H of the results inside the timed region.
+    Headline: kira_gpu_verify_batch_compact (a status byte per pair, full rows and
+    CIGARs of the aligned pairs); beside it kira_gpu_verify_batch (a 32-byte row for
+    every pair)."""
     import torch
 
     from kira_ls_aligner_b200 import _abi
@@ -1024,6 +1064,7 @@ def e2e_run(args, ctx, L, vp, w, n, world, dist, dev):
     h_woff, h_wlen = pin(w.win_off.view(np.int64)), pin(w.win_len.view(np.int32))
     cap = 4 * n
     res_h = torch.empty(n * 32, dtype=torch.uint8).pin_memory()
+    stat_h = torch.empty(n, dtype=torch.uint8).pin_memory()
     ops_h = torch.empty(cap, dtype=torch.int32).pin_memory()
     cb = _abi.CigarBuf(ops_h.data_ptr(), cap, 0)
     hpc = _abi.Pairs()
@@ -1031,29 +1072,45 @@ def e2e_run(args, ctx, L, vp, w, n, world, dist, dev):
     hpc.read_seq, hpc.read_seq_bytes = h_reads.data_ptr(), int(w.reads.nbytes)
     hpc.read_off, hpc.read_len = h_roff.data_ptr(), h_rlen.data_ptr()
     hpc.win_seq, hpc.win_off, hpc.win_len = None, h_woff.data_ptr(), h_wlen.data_ptr()
-    cells_h = C.c_uint64()
+    cells_h, rows_used = C.c_uint64(), C.c_uint64()
 
-    def e2e_step():
+    def full_step():
         ctx.check(L.kira_gpu_verify_batch(ctx.handle, C.byref(hpc), C.byref(vp),
                                           res_h.data_ptr(), C.byref(cb), None,
                                           C.byref(cells_h)))
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
-    if dist is not None:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
-    el = _max_over_ranks(time.perf_counter() - t0, dist, dev)
+
+    def compact_step():
+        ctx.check(L.kira_gpu_verify_batch_compact(ctx.handle, C.byref(hpc), C.byref(vp),
+                                                  stat_h.data_ptr(), res_h.data_ptr(), n,
+                                                  C.byref(rows_used), C.byref(cb),
+                                                  C.byref(cells_h)))
+
+    def timed(fn):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            fn()
+        return _max_over_ranks(time.perf_counter() - t0, dist, dev)
+    el_full = timed(full_step)
+    el = timed(compact_step)
     # Bytes the call copies up: the read arena plus the pair descriptors, packed to
     # 12 bytes a pair (u32 offsets, u16 lengths) when the read arena and the
     # reference are below 4 GiB and every length fits 16 bits, else 24.
     packed = (w.reads.nbytes < 1 << 32 and len(w.reference) < 1 << 32
               and max(int(w.read_len.max()), int(w.win_len.max())) < 1 << 16)
     h2d = int(w.reads.nbytes) + n * (12 if packed else 8 + 4 + 8 + 4)
-    d2h = n * 32 + 4 * int(cb.used) + 8 + 8 + 16
+    tail = 8 + 8 + 16  # op count, cells, flag words
+    d2h = n + 32 * int(rows_used.value) + 4 * int(cb.used) + tail + 8
     return {"value": n * world * args.steps / el, "unit": UNIT, "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * el / args.steps}
+            "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * el / args.steps,
+            "api": "kira_gpu_verify_batch_compact",
+            "full_rows": {"value": n * world * args.steps / el_full,
+                          "ms_per_step": 1e3 * el_full / args.steps,
+                          "d2h_bytes_per_step": 32 * n + 4 * int(cb.used) + tail,
+                          "api": "kira_gpu_verify_batch"}}
 
 
 def profile_figure(name: str, key: str):
@@ -1067,7 +1124,7 @@ def profile_figure(name: str, key: str):
         return None
 
 
-ALU_PROBES = ("dpx_s16x2_addmax", "iadd3", "lop3")
+ALU_PROBES = ("dpx_s16x2_addmax", "iadd3", "lop3", "imad", "lop3+imad", "dpx+imad")
 
 
 def roofline_block(args, L, local, stage_ms, statuses, cells_step, n, tuning):
@@ -1104,7 +1161,8 @@ def roofline_block(args, L, local, stage_ms, statuses, cells_step, n, tuning):
             probes[name] = v.value / 1e12
     ops_cell = 9 if packed else 18
     cell_rate = cells_step / (dp_ms / 1e3) if dp_ms > 0 else 0.0
-    ipeak = max(probes.values()) if probes else None
+    single = [probes[k] for k in ALU_PROBES[:4] if k in probes]
+    ipeak = max(single) if single else None
     return {"bound": "hbm", "kernel": _abi.STAGES[dom], "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak, "traffic": None if traffic is None
             else int(traffic), "algorithmic_bytes": int(alg[dom]),
@@ -1118,8 +1176,8 @@ def roofline_block(args, L, local, stage_ms, statuses, cells_step, n, tuning):
                          "peak_tops": ipeak, "frac": None if not ipeak
                          else cell_rate * ops_cell / 1e12 / ipeak,
                          "probe_tops": probes,
-                         "peak_source": "kira_gpu_alu_probe in this run (fastest of "
-                                        "DPX add-max / IADD3 / LOP3 streams)"}}
+                         "peak_source": "kira_gpu_alu_probe in this run (fastest single-kind "
+                                        "stream: DPX add-max / IADD3 / LOP3 / IMAD)"}}
 
 
 def run_extras(args, local) -> dict:

@@ -97,10 +97,12 @@ uint64_t kira_gpu_launch_count(void);
 
 /* No counterpart in the reference (the denominator of the integer roofline of
  * the DP kernels): measures this GPU's integer instruction rate. Every thread of
- * a full grid runs `rounds` rounds of 16 independent instructions of one kind --
- * op 0 the DPX add-max on packed int16 pairs, op 1 a three-input add, op 2 a
- * three-input logic op -- and *thread_ops_per_s receives the thread-instructions
- * per second (CUDA events around one launch after a warm-up launch). */
+ * a full grid runs `rounds` rounds of 16 independent instructions -- op 0 the
+ * DPX add-max on packed int16 pairs, op 1 a three-input add, op 2 a three-input
+ * logic op, op 3 an integer multiply-add, op 4 logic op and multiply-add
+ * alternating, op 5 DPX add-max and multiply-add alternating -- and
+ * *thread_ops_per_s receives the thread-instructions per second (CUDA events
+ * around one launch after a warm-up launch). */
 int kira_gpu_alu_probe(int device, int op, uint32_t rounds, double* thread_ops_per_s);
 
 /* ------------------------------------------------------- sieve (drop-in) */
@@ -229,6 +231,11 @@ int kira_gpu_set_plain(kira_ctx* ctx, int plain);
  * traceback in rounds over the same arena; results are identical. */
 int kira_gpu_set_trace_budget(kira_ctx* ctx, uint64_t bytes);
 
+/* No counterpart in the reference: the number of trace rounds (DP + traceback
+ * passes over the reused trace arena, summed over band classes) that the last
+ * kira_gpu_bsw_batch call on this ctx ran. */
+uint32_t kira_gpu_bsw_rounds(const kira_ctx* ctx);
+
 /* CUDA-graph replay of the bucketed banded-SW launches (per-class DP sweeps,
  * tracebacks, CIGAR scan and compaction) of kira_gpu_bsw_batch: a call whose
  * launch parameters (device buffers, per-class counts, shapes, rounds) equal the
@@ -320,6 +327,22 @@ typedef struct kira_verify_detail {
 int kira_gpu_verify_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_verify_params* p,
                           kira_sw_result* out, kira_cigar_buf* cigar, kira_verify_detail* detail,
                           uint64_t* cells);
+
+/* Compact result form of kira_gpu_verify_batch, for callers that use only the
+ * pairs with an alignment -- stage 4's consumer of the GPU sieve keeps the
+ * accepted hits and drops the rest (src/pipeline/stage4_alignment.rs:1317-1356).
+ * Same computation and the same rows; what comes back is
+ *   status[i]   the kira_pair_status of pair i (one byte per pair);
+ *   rows[0..k)  the full rows of the pairs whose status is KIRA_PAIR_CERTIFIED or
+ *               KIRA_PAIR_SW, in pair order (row r belongs to the r-th such pair);
+ *               *rows_used = k. Rows past rows_cap are not written and the call
+ *               returns KIRA_ERR_CAPACITY (the status bytes are complete);
+ *   cigar       as in kira_gpu_verify_batch (cigar_off of each row indexes it).
+ * On the 2M-pair short-read batch this moves about 11 MB back instead of 65 MB. */
+int kira_gpu_verify_batch_compact(kira_ctx* ctx, const kira_pairs* pairs,
+                                  const kira_verify_params* p, uint8_t* status,
+                                  kira_sw_result* rows, uint64_t rows_cap, uint64_t* rows_used,
+                                  kira_cigar_buf* cigar, uint64_t* cells);
 
 /* Device-pointer form of kira_gpu_verify_batch: every pointer in `pairs` and the
  * outputs are device pointers; work is enqueued on `stream` (a cudaStream_t) and

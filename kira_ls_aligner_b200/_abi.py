@@ -43,7 +43,8 @@ EXPORTS = (
     "kira_server_create", "kira_server_destroy", "kira_server_ref_upload",
     "kira_server_submit_verify", "kira_server_submit_bsw", "kira_server_poll",
     "kira_server_wait", "kira_server_info", "kira_server_release", "kira_server_stats",
-    "kira_server_last_error", "kira_server_profile", "kira_gpu_launch_count", "kira_gpu_alu_probe",
+    "kira_server_last_error", "kira_server_profile", "kira_gpu_launch_count",
+    "kira_gpu_alu_probe", "kira_gpu_verify_batch_compact", "kira_gpu_bsw_rounds",
 )
 SIMD_SCALAR, SIMD_AVX2, SIMD_AVX_VNNI, SIMD_NEON = 0, 1, 2, 3
 VERIFY_NO_QGRAM = 1
@@ -170,6 +171,9 @@ def lib():
                                      C.POINTER(CigarBuf), C.POINTER(C.c_uint64)]
     L.kira_gpu_verify_batch.argtypes = [vp, C.POINTER(Pairs), C.POINTER(VerifyParams), vp,
                                         C.POINTER(CigarBuf), vp, C.POINTER(C.c_uint64)]
+    L.kira_gpu_verify_batch_compact.argtypes = [vp, C.POINTER(Pairs), C.POINTER(VerifyParams),
+                                                vp, vp, C.c_uint64, C.POINTER(C.c_uint64),
+                                                C.POINTER(CigarBuf), C.POINTER(C.c_uint64)]
     L.kira_gpu_verify_dev.argtypes = [vp, C.POINTER(Pairs), C.POINTER(VerifyParams), vp, vp,
                                       C.c_uint64, vp, vp, vp, vp]
     L.kira_gpu_profile.argtypes = [vp, C.c_int]
@@ -215,6 +219,8 @@ def lib():
     L.kira_gpu_arena_bytes.restype = C.c_uint64
     L.kira_gpu_launch_count.argtypes = []
     L.kira_gpu_launch_count.restype = C.c_uint64
+    L.kira_gpu_bsw_rounds.argtypes = [vp]
+    L.kira_gpu_bsw_rounds.restype = C.c_uint32
     L.kira_gpu_alu_probe.argtypes = [C.c_int, C.c_int, C.c_uint32, C.POINTER(C.c_double)]
     _lib = L
     return L

@@ -31,7 +31,8 @@ enum BufId {
   B_DIST, B_END, B_SIEVE_OUT, B_SIEVE_JOBS, B_CELLS, B_TOTAL, B_READ_PLANES, B_WIN_PLANES,
   B_ROWKEYS, B_DONE_ROW, B_WORK, B_WFA_MAXS, B_WFA_TBF, B_WFA_OUT, B_WFA_NCIG, B_WFA_SLOTS,
   B_WFA_SCRATCH, B_WFA_FLAGS, B_PF_CHAINS, B_PF_TOP1, B_PF_MARGIN, B_PF_OUT, B_PF_NCIG,
-  B_PF_MDLEN, B_PF_MDOFF, B_PF_MD, B_PF_EXACT, B_WFA_FB, B_WFA_WHIST, B_SIEVE_LIST, B_PACKED, B_COUNT
+  B_PF_MDLEN, B_PF_MDOFF, B_PF_MD, B_PF_EXACT, B_WFA_FB, B_WFA_WHIST, B_SIEVE_LIST, B_PACKED, B_STATUS, B_KEEP, B_ROW_OFF,
+  B_ROWS, B_ROW_SUMS, B_ROW_TOTAL, B_COUNT
 };
 
 struct DevBuf {
@@ -115,6 +116,7 @@ struct kira_ctx {
   std::vector<uint8_t> graph_key;  // launch parameters the cached graph was captured with
   uint64_t graph_replays = 0, graph_captures = 0;
   unsigned long long graph_kernels = 0;  // kernels in the cached graph (launch accounting)
+  uint32_t last_rounds = 0;              // trace rounds of the last kira_gpu_bsw_batch
   cudaStream_t h2d = nullptr, d2h = nullptr;   // copy streams of the chunked host path
   int64_t chunk_pairs = -1;                    // chunked host path: -1 auto, 0 off, else pairs
   int wfa_lanes = 0;                           // WFA lanes per pair: 0 auto, else 8 / 16 / 32
@@ -718,6 +720,7 @@ int plan_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const k
     mwords = std::max<uint64_t>(mbase[kBandClasses], 1);
   }
   const uint32_t nwork = std::max<uint32_t>(rounds_before[kBandClasses], 1);
+  ctx->last_rounds = rounds_before[kBandClasses];
   const uint32_t cap = qall + wall + 2;
   KIRA_DBUF(dlist, uint32_t, B_SW_LIST, n);
   KIRA_DBUF(trace, uint8_t, B_TRACE, tbytes);
@@ -771,9 +774,59 @@ int plan_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const k
 // as far as each chunk needs it and its planes are packed for the new range
 // only; CIGAR offsets stay global through the running total in total_dev.
 // Results are identical to the one-shot path.
+// Compact result form (kira_gpu_verify_batch_compact): host outputs.
+struct CompactOut {
+  uint8_t* status;       // n bytes
+  kira_sw_result* rows;  // rows_cap rows: the pairs with an alignment, in pair order
+  uint64_t rows_cap;
+  uint64_t* rows_used;
+};
+
+// Device side of the compact form after every pair's row is final (stream `st`):
+// scan of the keep flags, kept rows to their slots, row count to rows_total_dev.
+int compact_rows_tail(kira_ctx* ctx, const kira_sw_result* dout, uint32_t n, const uint32_t* keep,
+                      kira_sw_result** rows_dev, uint64_t** rows_total_dev, uint64_t cap,
+                      cudaStream_t st) {
+  cudaError_t cerr = cudaSuccess;
+  KIRA_DBUF(off, uint32_t, B_ROW_OFF, std::max<uint32_t>(n, 1));
+  KIRA_DBUF(sums, uint32_t, B_ROW_SUMS, n / 4096 + 2);
+  KIRA_DBUF(total, uint64_t, B_ROW_TOTAL, 1);
+  KIRA_DBUF(rows, kira_sw_result, B_ROWS, std::max<uint64_t>(std::min<uint64_t>(cap, n), 1));
+  KIRA_CUDA(launch_cigar_scan(keep, n, off, sums, total, st));
+  KIRA_CUDA(launch_compact_rows(dout, n, keep, off, rows, std::min<uint64_t>(cap, n), ctx->sms,
+                                st));
+  *rows_dev = rows;
+  *rows_total_dev = total;
+  return KIRA_OK;
+}
+
+// Last copies of a composed host call once the counts are known: the CIGAR ops and,
+// in the compact form, the kept rows (as many as fit); the capacity checks.
+int finish_host_outputs(kira_ctx* ctx, kira_cigar_buf* cigar, const uint32_t* ops, uint64_t total,
+                        const CompactOut* co, const kira_sw_result* rows_dev, uint64_t rows_total,
+                        cudaStream_t st) {
+  if (co) *co->rows_used = rows_total;
+  const uint64_t nrows = co ? std::min(rows_total, co->rows_cap) : 0;
+  const uint64_t nops = std::min(total, cigar->cap);
+  if (nrows)
+    KIRA_CUDA(cudaMemcpyAsync(co->rows, rows_dev, sizeof(kira_sw_result) * nrows,
+                              cudaMemcpyDeviceToHost, st));
+  if (total <= cigar->cap && nops)
+    KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * nops, cudaMemcpyDeviceToHost, st));
+  if (nrows || (total <= cigar->cap && nops)) KIRA_CUDA(cudaStreamSynchronize(st));
+  if (total > cigar->cap)
+    return fail(ctx, KIRA_ERR_CAPACITY, "CIGAR buffer holds %llu ops, %llu needed",
+                (unsigned long long)cigar->cap, (unsigned long long)total);
+  if (co && rows_total > co->rows_cap)
+    return fail(ctx, KIRA_ERR_CAPACITY, "row buffer holds %llu rows, %llu needed",
+                (unsigned long long)co->rows_cap, (unsigned long long)rows_total);
+  return KIRA_OK;
+}
+
 int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_params& p,
                          kira_sw_result* out, kira_cigar_buf* cigar, kira_verify_detail* detail,
-                         uint64_t* cells, const std::vector<uint32_t>& bounds) {
+                         uint64_t* cells, const std::vector<uint32_t>& bounds,
+                         const CompactOut* co = nullptr) {
   cudaError_t cerr = cudaSuccess;
   const uint32_t n = P.n;
   const uint32_t nch = (uint32_t)bounds.size() - 1;  // chunk c: pairs [bounds[c], bounds[c + 1])
@@ -965,6 +1018,14 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
     KIRA_DBUF(dd, kira_verify_detail, B_DETAIL, n);
     ddet = dd;
   }
+  uint8_t* dstat = nullptr;
+  uint32_t* keep = nullptr;
+  if (co) {
+    KIRA_DBUF(a, uint8_t, B_STATUS, n);
+    KIRA_DBUF(b, uint32_t, B_KEEP, n);
+    dstat = a;
+    keep = b;
+  }
   KIRA_DBUF(cells_dev, unsigned long long, B_CELLS, 1);
   KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
   KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
@@ -1054,16 +1115,29 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
       cudaStreamSynchronize(twin->stream);
       return rc;
     }
+    if (co) KIRA_CUDA(launch_status_keep(dout + lo, m, dstat + lo, keep + lo, ctx->sms, cs));
     KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], cs));
   }
   for (uint32_t c = 0; c < nch; ++c) {
     const uint32_t lo = bounds[c], m = bounds[c + 1] - lo;
     KIRA_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->ev_comp[c], 0));
-    KIRA_CUDA(cudaMemcpyAsync(out + lo, dout + lo, sizeof(kira_sw_result) * m,
-                              cudaMemcpyDeviceToHost, ctx->d2h));
+    if (co)
+      KIRA_CUDA(cudaMemcpyAsync(co->status + lo, dstat + lo, m, cudaMemcpyDeviceToHost, ctx->d2h));
+    else
+      KIRA_CUDA(cudaMemcpyAsync(out + lo, dout + lo, sizeof(kira_sw_result) * m,
+                                cudaMemcpyDeviceToHost, ctx->d2h));
     if (detail)
       KIRA_CUDA(cudaMemcpyAsync(detail + lo, ddet + lo, sizeof(kira_verify_detail) * m,
                                 cudaMemcpyDeviceToHost, ctx->d2h));
+  }
+  kira_sw_result* rows_dev = nullptr;
+  uint64_t* rows_total_dev = nullptr;
+  uint64_t rows_total = 0;
+  if (co) {  // after every chunk's rows (the copy stream waited for all of them)
+    int rc = compact_rows_tail(ctx, dout, n, keep, &rows_dev, &rows_total_dev, co->rows_cap,
+                               ctx->d2h);
+    if (rc) return rc;
+    KIRA_CUDA(cudaMemcpyAsync(&rows_total, rows_total_dev, 8, cudaMemcpyDeviceToHost, ctx->d2h));
   }
   uint64_t total = 0;
   unsigned long long hcells = 0;
@@ -1080,14 +1154,7 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
   flags[2] |= flags2[2];
   if (flags[2] & 1u) return fail(ctx, KIRA_ERR_RUNTIME, "CIGAR slot overflow");
   if (flags[2] & 6u) return fail(ctx, KIRA_ERR_INVALID, "a pair exceeded the launch's length bounds");
-  if (total > cigar->cap)
-    return fail(ctx, KIRA_ERR_CAPACITY, "CIGAR buffer holds %llu ops, %llu needed",
-                (unsigned long long)cigar->cap, (unsigned long long)total);
-  if (total) {
-    KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * total, cudaMemcpyDeviceToHost, ctx->d2h));
-    KIRA_CUDA(cudaStreamSynchronize(ctx->d2h));
-  }
-  return KIRA_OK;
+  return finish_host_outputs(ctx, cigar, ops, total, co, rows_dev, rows_total, ctx->d2h);
 }
 
 // Runs `enqueue` on `st` through a CUDA graph: replays the cached executable
@@ -1295,6 +1362,91 @@ uint64_t host_chunk(const kira_ctx* ctx, uint32_t n) {
   const uint64_t chunk = ctx->chunk_pairs < 0 ? std::max<uint64_t>(1u << 18, (n + 3ull) / 4)
                                               : (uint64_t)ctx->chunk_pairs;
   return chunk && n >= 2 * chunk ? chunk : 0;
+}
+
+}  // namespace
+
+namespace {
+
+// The composed path on host buffers: full rows (`out`) or the compact form (`co`).
+int verify_host(kira_ctx* ctx, const kira_pairs& P, const kira_verify_params& prm,
+                kira_sw_result* out, kira_cigar_buf* cigar, kira_verify_detail* detail,
+                uint64_t* cells, const CompactOut* co) {
+  const kira_verify_params* p = &prm;
+  cigar->used = 0;
+  if (cells) *cells = 0;
+  if (P.n == 0) return KIRA_OK;
+  cudaSetDevice(ctx->device);
+  // Chunks alternate between two compute streams so each chunk's row-serial DP and
+  // traceback tail overlaps the next chunk; a few large chunks still do best
+  // (each pays some fixed launch and tail cost). Automatic: batches of at least
+  // 2^20 pairs in chunks of 1/8, 1/4, 1/4, 1/4, 1/8 of the batch (a small first
+  // chunk starts the GPU sooner, a small last one drains sooner), smaller ones in
+  // quarters of at least 2^18 pairs; chunk_pairs > 0: equal chunks of that size.
+  std::vector<uint32_t> bounds;
+  if (!ctx->profile) {
+    const uint64_t n = P.n;
+    if (ctx->chunk_pairs < 0 && n >= (1u << 20)) {
+      bounds = {0u, (uint32_t)(n / 8), (uint32_t)(3 * n / 8), (uint32_t)(5 * n / 8),
+                (uint32_t)(n - n / 8), (uint32_t)n};
+    } else {
+      const uint64_t chunk = ctx->chunk_pairs < 0 ? std::max<uint64_t>(1u << 18, (n + 3) / 4)
+                                                  : (uint64_t)ctx->chunk_pairs;
+      if (chunk && n >= 2 * chunk)
+        for (uint64_t lo = 0; lo <= n; lo += chunk) bounds.push_back((uint32_t)std::min(lo, n));
+      if (!bounds.empty() && bounds.back() != n) bounds.push_back((uint32_t)n);
+    }
+  }
+  if (bounds.size() >= 3)
+    return verify_batch_chunked(ctx, P, *p, out, cigar, detail, cells, bounds, co);
+  const Maxes mx = host_maxes(ctx, P, p->sw.bandwidth);
+  DevPairs D;
+  int rc = upload_pairs(ctx, P, D);
+  if (rc) return rc;
+  cudaError_t cerr = cudaSuccess;
+  cudaStream_t st = ctx->stream;
+  const uint32_t n = P.n;
+  KIRA_DBUF(dout, kira_sw_result, B_OUT, n);
+  kira_verify_detail* ddet = nullptr;
+  if (detail) {
+    KIRA_DBUF(dd, kira_verify_detail, B_DETAIL, n);
+    ddet = dd;
+  }
+  KIRA_DBUF(cells_dev, unsigned long long, B_CELLS, 1);
+  KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
+  KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
+  KIRA_CUDA(cudaMemsetAsync(cells_dev, 0, 8, st));
+  rc = verify_pipeline(ctx, D, mx, *p, P.read_seq_bytes, P.win_seq_bytes, P.win_seq == nullptr,
+                       dout, ops, cigar->cap, total_dev, ddet, cells_dev, st);
+  if (rc) return rc;
+  uint64_t total = 0, rows_total = 0;
+  unsigned long long hcells = 0;
+  uint32_t flags[4];
+  kira_sw_result* rows_dev = nullptr;
+  if (co) {
+    KIRA_DBUF(dstat, uint8_t, B_STATUS, n);
+    KIRA_DBUF(keep, uint32_t, B_KEEP, n);
+    KIRA_CUDA(launch_status_keep(dout, n, dstat, keep, ctx->sms, st));
+    uint64_t* rows_total_dev = nullptr;
+    rc = compact_rows_tail(ctx, dout, n, keep, &rows_dev, &rows_total_dev, co->rows_cap, st);
+    if (rc) return rc;
+    KIRA_CUDA(cudaMemcpyAsync(co->status, dstat, n, cudaMemcpyDeviceToHost, st));
+    KIRA_CUDA(cudaMemcpyAsync(&rows_total, rows_total_dev, 8, cudaMemcpyDeviceToHost, st));
+  } else {
+    KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_sw_result) * n, cudaMemcpyDeviceToHost, st));
+  }
+  if (detail)
+    KIRA_CUDA(cudaMemcpyAsync(detail, ddet, sizeof(kira_verify_detail) * n,
+                              cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(&total, total_dev, 8, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(&hcells, cells_dev, 8, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaMemcpyAsync(flags, ctx->bufs[B_COUNTERS].p, 16, cudaMemcpyDeviceToHost, st));
+  KIRA_CUDA(cudaStreamSynchronize(st));
+  cigar->used = total;
+  if (cells) *cells = hcells;
+  if (flags[2] & 1u) return fail(ctx, KIRA_ERR_RUNTIME, "CIGAR slot overflow");
+  if (flags[2] & 6u) return fail(ctx, KIRA_ERR_INVALID, "a pair exceeded the launch's length bounds");
+  return finish_host_outputs(ctx, cigar, ops, total, co, rows_dev, rows_total, st);
 }
 
 }  // namespace
@@ -2085,6 +2237,8 @@ int kira_gpu_set_chunk_pairs(kira_ctx* ctx, int64_t pairs) {
   return KIRA_OK;
 }
 
+uint32_t kira_gpu_bsw_rounds(const kira_ctx* ctx) { return ctx ? ctx->last_rounds : 0; }
+
 int kira_gpu_set_trace_budget(kira_ctx* ctx, uint64_t bytes) {
   if (!ctx) return KIRA_ERR_INVALID;
   ctx->trace_budget = bytes;
@@ -2231,6 +2385,7 @@ int kira_gpu_bsw_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_sw_cfg
     if (shape < 0)
       return fail(ctx, KIRA_ERR_INVALID, "band %u above the one-launch maximum", mx.band);
     const uint32_t per_round = round_items(ctx, n, shape, mx.q);
+    ctx->last_rounds = (n + per_round - 1) / per_round;
     rc = prepare_bsw(ctx, n, n, per_round, mx, shape, B);
     if (rc) return rc;
     B.count = n;
@@ -2402,76 +2557,18 @@ int kira_gpu_verify_batch(kira_ctx* ctx, const kira_pairs* pairs, const kira_ver
                           kira_sw_result* out, kira_cigar_buf* cigar, kira_verify_detail* detail,
                           uint64_t* cells) {
   if (!ctx || !pairs || !p || !out || !cigar) return KIRA_ERR_INVALID;
-  const kira_pairs& P = *pairs;
-  cigar->used = 0;
-  if (cells) *cells = 0;
-  if (P.n == 0) return KIRA_OK;
-  cudaSetDevice(ctx->device);
-  // Chunks alternate between two compute streams so each chunk's row-serial DP and
-  // traceback tail overlaps the next chunk; a few large chunks still do best
-  // (each pays some fixed launch and tail cost). Automatic: batches of at least
-  // 2^20 pairs in chunks of 1/8, 1/4, 1/4, 1/4, 1/8 of the batch (a small first
-  // chunk starts the GPU sooner, a small last one drains sooner), smaller ones in
-  // quarters of at least 2^18 pairs; chunk_pairs > 0: equal chunks of that size.
-  std::vector<uint32_t> bounds;
-  if (!ctx->profile) {
-    const uint64_t n = P.n;
-    if (ctx->chunk_pairs < 0 && n >= (1u << 20)) {
-      bounds = {0u, (uint32_t)(n / 8), (uint32_t)(3 * n / 8), (uint32_t)(5 * n / 8),
-                (uint32_t)(n - n / 8), (uint32_t)n};
-    } else {
-      const uint64_t chunk = ctx->chunk_pairs < 0 ? std::max<uint64_t>(1u << 18, (n + 3) / 4)
-                                                  : (uint64_t)ctx->chunk_pairs;
-      if (chunk && n >= 2 * chunk)
-        for (uint64_t lo = 0; lo <= n; lo += chunk) bounds.push_back((uint32_t)std::min(lo, n));
-      if (!bounds.empty() && bounds.back() != n) bounds.push_back((uint32_t)n);
-    }
-  }
-  if (bounds.size() >= 3)
-    return verify_batch_chunked(ctx, P, *p, out, cigar, detail, cells, bounds);
-  const Maxes mx = host_maxes(ctx, P, p->sw.bandwidth);
-  DevPairs D;
-  int rc = upload_pairs(ctx, P, D);
-  if (rc) return rc;
-  cudaError_t cerr = cudaSuccess;
-  cudaStream_t st = ctx->stream;
-  const uint32_t n = P.n;
-  KIRA_DBUF(dout, kira_sw_result, B_OUT, n);
-  kira_verify_detail* ddet = nullptr;
-  if (detail) {
-    KIRA_DBUF(dd, kira_verify_detail, B_DETAIL, n);
-    ddet = dd;
-  }
-  KIRA_DBUF(cells_dev, unsigned long long, B_CELLS, 1);
-  KIRA_DBUF(total_dev, uint64_t, B_TOTAL, 1);
-  KIRA_DBUF(ops, uint32_t, B_CIGAR_OUT, std::max<uint64_t>(cigar->cap, 1));
-  KIRA_CUDA(cudaMemsetAsync(cells_dev, 0, 8, st));
-  rc = verify_pipeline(ctx, D, mx, *p, P.read_seq_bytes, P.win_seq_bytes, P.win_seq == nullptr,
-                       dout, ops, cigar->cap, total_dev, ddet, cells_dev, st);
-  if (rc) return rc;
-  uint64_t total = 0;
-  unsigned long long hcells = 0;
-  uint32_t flags[4];
-  KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_sw_result) * n, cudaMemcpyDeviceToHost, st));
-  if (detail)
-    KIRA_CUDA(cudaMemcpyAsync(detail, ddet, sizeof(kira_verify_detail) * n,
-                              cudaMemcpyDeviceToHost, st));
-  KIRA_CUDA(cudaMemcpyAsync(&total, total_dev, 8, cudaMemcpyDeviceToHost, st));
-  KIRA_CUDA(cudaMemcpyAsync(&hcells, cells_dev, 8, cudaMemcpyDeviceToHost, st));
-  KIRA_CUDA(cudaMemcpyAsync(flags, ctx->bufs[B_COUNTERS].p, 16, cudaMemcpyDeviceToHost, st));
-  KIRA_CUDA(cudaStreamSynchronize(st));
-  cigar->used = total;
-  if (cells) *cells = hcells;
-  if (flags[2] & 1u) return fail(ctx, KIRA_ERR_RUNTIME, "CIGAR slot overflow");
-  if (flags[2] & 6u) return fail(ctx, KIRA_ERR_INVALID, "a pair exceeded the launch's length bounds");
-  if (total > cigar->cap)
-    return fail(ctx, KIRA_ERR_CAPACITY, "CIGAR buffer holds %llu ops, %llu needed",
-                (unsigned long long)cigar->cap, (unsigned long long)total);
-  if (total) {
-    KIRA_CUDA(cudaMemcpyAsync(cigar->ops, ops, 4ull * total, cudaMemcpyDeviceToHost, st));
-    KIRA_CUDA(cudaStreamSynchronize(st));
-  }
-  return KIRA_OK;
+  return verify_host(ctx, *pairs, *p, out, cigar, detail, cells, nullptr);
+}
+
+int kira_gpu_verify_batch_compact(kira_ctx* ctx, const kira_pairs* pairs,
+                                  const kira_verify_params* p, uint8_t* status,
+                                  kira_sw_result* rows, uint64_t rows_cap, uint64_t* rows_used,
+                                  kira_cigar_buf* cigar, uint64_t* cells) {
+  if (!ctx || !pairs || !p || !status || (!rows && rows_cap) || !rows_used || !cigar)
+    return KIRA_ERR_INVALID;
+  *rows_used = 0;
+  const CompactOut co{status, rows, rows_cap, rows_used};
+  return verify_host(ctx, *pairs, *p, nullptr, cigar, nullptr, cells, &co);
 }
 
 int kira_gpu_verify_dev(kira_ctx* ctx, const kira_pairs* pairs, const kira_verify_params* p,

@@ -274,6 +274,13 @@ cudaError_t launch_cigar_scan(const uint32_t* ncig, uint32_t n, uint32_t* off,
                               uint32_t* chunk_sums, uint64_t* total_dev, cudaStream_t st,
                               bool accumulate = false);
 cudaError_t launch_cigar_compact(const CompactLaunch& C, int sms, cudaStream_t st);
+// Compact result form of the composed path: status bytes + keep flags, then the
+// kept rows at their scan offsets (kira_gpu_verify_batch_compact).
+cudaError_t launch_status_keep(const kira_sw_result* rows, uint32_t n, uint8_t* status,
+                               uint32_t* keep, int sms, cudaStream_t st);
+cudaError_t launch_compact_rows(const kira_sw_result* rows, uint32_t n, const uint32_t* keep,
+                                const uint32_t* off, kira_sw_result* dst, uint64_t cap, int sms,
+                                cudaStream_t st);
 cudaError_t launch_nm_md(const DevPairs& P, const NmMdLaunch& L, bool write, int sms,
                          cudaStream_t st);
 

@@ -990,16 +990,60 @@ cudaError_t launch_cigar_compact(const CompactLaunch& C, int sms, cudaStream_t s
   return cudaGetLastError();
 }
 
+// Compact result form: one status byte per pair and a keep flag (1 for a pair
+// with an alignment: certified or banded SW).
+__global__ void __launch_bounds__(256) status_keep_kernel(const kira_sw_result* __restrict__ rows,
+                                                          uint32_t n, uint8_t* __restrict__ status,
+                                                          uint32_t* __restrict__ keep) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+    const uint8_t s = rows[p].status;
+    status[p] = s;
+    keep[p] = (s == KIRA_PAIR_CERTIFIED || s == KIRA_PAIR_SW) ? 1u : 0u;
+  }
+}
+
+// Kept rows to their exclusive-scan slots (pair order); slots at or past cap skipped.
+__global__ void __launch_bounds__(256) compact_rows_kernel(const kira_sw_result* __restrict__ rows,
+                                                           uint32_t n, const uint32_t* __restrict__ keep,
+                                                           const uint32_t* __restrict__ off,
+                                                           kira_sw_result* __restrict__ dst,
+                                                           uint64_t cap) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride)
+    if (keep[p] && off[p] < cap) dst[off[p]] = rows[p];
+}
+
+cudaError_t launch_status_keep(const kira_sw_result* rows, uint32_t n, uint8_t* status,
+                               uint32_t* keep, int sms, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const int blocks = grid_for(n, 256, sms * 8);
+  (status_keep_kernel<<<blocks, 256, 0, st>>>(rows, n, status, keep), count_launch());
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compact_rows(const kira_sw_result* rows, uint32_t n, const uint32_t* keep,
+                                const uint32_t* off, kira_sw_result* dst, uint64_t cap, int sms,
+                                cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const int blocks = grid_for(n, 256, sms * 8);
+  (compact_rows_kernel<<<blocks, 256, 0, st>>>(rows, n, keep, off, dst, cap), count_launch());
+  return cudaGetLastError();
+}
+
 }  // namespace kira
 
 extern "C" uint64_t kira_gpu_launch_count(void) { return kira::launch_count(); }
 
 // ---------------------------------------------------------------------------
 // Integer issue-rate probe (the denominator of the DP kernels' integer roofline).
-// Every thread updates 16 independent packed words per round with one kind of
-// instruction: OP 0 the DPX add-max (__viaddmax_s16x2), OP 1 a three-input add,
-// OP 2 a three-input logic op. The result is folded into a sink that is written
-// only on an impossible value, which keeps every round live.
+// Every thread updates 16 independent packed words per round: OP 0 the DPX
+// add-max (__viaddmax_s16x2), OP 1 a three-input add, OP 2 a three-input logic
+// op, OP 3 an integer multiply-add by one (the add form of the FMA pipe), OP 4
+// alternating logic op and multiply-add, OP 5 alternating DPX add-max and
+// multiply-add (the mixed forms show which kinds issue to separate pipes). The
+// result is folded into a sink that is written only on an impossible value, which
+// keeps every round live.
 // ---------------------------------------------------------------------------
 namespace kira {
 
@@ -1014,9 +1058,18 @@ __global__ void __launch_bounds__(256) alu_probe_kernel(uint32_t rounds, uint32_
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
       const uint32_t nb = x[(k + 1) & 15];
-      if constexpr (OP == 0) x[k] = __viaddmax_s16x2(x[k], y, nb);
-      else if constexpr (OP == 1) x[k] = x[k] + nb + y;
-      else x[k] = (x[k] & nb) ^ y;
+      const int kind = OP < 3 ? OP : OP == 3 ? 3 : (k & 1) ? 3 : (OP == 4 ? 2 : 0);
+      if (kind == 0) {
+        x[k] = __viaddmax_s16x2(x[k], y, nb);
+      } else if (kind == 1) {
+        x[k] = x[k] + nb + y;
+      } else if (kind == 2) {
+        x[k] = (x[k] & nb) ^ y;
+      } else {
+        uint32_t r;
+        asm volatile("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(nb), "r"(y | 1u), "r"(x[k]));
+        x[k] = r;
+      }
     }
     y += 0x00010001u;
   }
@@ -1030,7 +1083,7 @@ __global__ void __launch_bounds__(256) alu_probe_kernel(uint32_t rounds, uint32_
 
 extern "C" int kira_gpu_alu_probe(int device, int op, uint32_t rounds, double* thread_ops_per_s) {
   using namespace kira;
-  if (!thread_ops_per_s || op < 0 || op > 2 || rounds == 0) return KIRA_ERR_INVALID;
+  if (!thread_ops_per_s || op < 0 || op > 5 || rounds == 0) return KIRA_ERR_INVALID;
   if (cudaSetDevice(device) != cudaSuccess) return KIRA_ERR_NO_DEVICE;
   int sms = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
@@ -1049,7 +1102,10 @@ extern "C" int kira_gpu_alu_probe(int device, int op, uint32_t rounds, double* t
       const uint32_t seed = 0x2545F491u;
       if (op == 0) alu_probe_kernel<0><<<blocks, threads, 0, st>>>(n, seed, sink);
       else if (op == 1) alu_probe_kernel<1><<<blocks, threads, 0, st>>>(n, seed, sink);
-      else alu_probe_kernel<2><<<blocks, threads, 0, st>>>(n, seed, sink);
+      else if (op == 2) alu_probe_kernel<2><<<blocks, threads, 0, st>>>(n, seed, sink);
+      else if (op == 3) alu_probe_kernel<3><<<blocks, threads, 0, st>>>(n, seed, sink);
+      else if (op == 4) alu_probe_kernel<4><<<blocks, threads, 0, st>>>(n, seed, sink);
+      else alu_probe_kernel<5><<<blocks, threads, 0, st>>>(n, seed, sink);
       count_launch();
     };
     launch(rounds / 8 + 1);  // warm-up (clocks up, module loaded)

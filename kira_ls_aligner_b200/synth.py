@@ -291,6 +291,100 @@ def gapfill(n_segments: int = 20_000, seed: int = 0x6A9F, seg_lo: int = 200, seg
                       ref)
 
 
+@dataclass
+class LongReadSegments(SwWorkload):
+    """Gap-fill segments of simulated long reads (SwWorkload fields) plus, per
+    segment, the read it came from; `read_bases` = bases of the simulated reads."""
+    read_of: np.ndarray | None = None
+    n_reads: int = 0
+    read_bases: int = 0
+
+
+def simulate_long_read(rng, ref: np.ndarray, length: int, err: float, split=(2, 1, 1)):
+    """One long read drawn from `ref` at a random origin with error rate `err` split
+    subs:ins:del. Returns (bases, origin, src, exact): src[p] = reference offset (from
+    origin) of the base read position p copies or replaces, exact[p] = position p is
+    an error-free base on the alignment's diagonal (a match with no gap before it)."""
+    tot = float(sum(split))
+    u = rng.random(length)
+    sub = u < err * split[0] / tot
+    ins = (u >= err * split[0] / tot) & (u < err * (split[0] + split[1]) / tot)
+    dele = (u >= err * (split[0] + split[1]) / tot) & (u < err)
+    adv = np.where(ins, 0, np.where(dele, 2, 1)).astype(np.int64)
+    src = np.cumsum(adv) - adv + dele
+    span = int(src[-1]) + 2
+    origin = int(rng.integers(0, len(ref) - span - 1))
+    out = ref[origin + src].copy()
+    if sub.any():
+        out[sub] = BASES[(np.searchsorted(BASES, out[sub]) + rng.integers(1, 4, int(sub.sum())))
+                         % 4]
+    if ins.any():
+        out[ins] = BASES[rng.integers(0, 4, int(ins.sum()))]
+    return out, origin, src, ~(sub | ins | dele)
+
+
+def gapfill_reads(n_reads: int = 20_000, seed: int = 0x10C4, ref_len: int = 1_000_000_000,
+                  repeat_frac: float = 0.10, mean: float = 10_000.0, sd: float = 6_000.0,
+                  len_lo: int = 1_000, len_hi: int = 50_000, err_lo: float = 0.05,
+                  err_hi: float = 0.12, split=(2, 1, 1), k: int = 15, seg_lo: int = 200,
+                  seg_hi: int = 2_000, band: int = 256,
+                  reference: np.ndarray | None = None) -> LongReadSegments:
+    """Long-read gap-fill: reads of lognormal length (mean 10 kbp, sd 6 kbp, clipped to
+    1-50 kbp) at error U[5 %, 12 %] (subs:ins:del 2:1:1) from a genome with 10 % repeat
+    families, each split at exact k-mer anchors (k = 15 bases that match the reference
+    on the read's diagonal) into the segments between consecutive anchors. Walking
+    along a read, the next anchor is the first one that starts at least U[seg_lo,
+    seg_hi - 150] bases after the previous anchor's end, so segments run 200-2000
+    bases. Each segment is aligned with band `band` in a window of the reference gap
+    between the anchors plus `band` bases on either side (win_off: reference
+    coordinates; the segment starts at window offset `band`)."""
+    rng = np.random.default_rng(seed)
+    ref = reference if reference is not None else random_genome(rng, ref_len, repeat_frac)
+    sig2 = np.log(1.0 + (sd / mean) ** 2)
+    lengths = np.clip(rng.lognormal(np.log(mean) - sig2 / 2, np.sqrt(sig2), n_reads),
+                      len_lo, len_hi).astype(np.int64)
+    errs = rng.uniform(err_lo, err_hi, n_reads)
+    seg_bases, q, wstart, wlen, read_of = [], [], [], [], []
+    total = 0
+    kernel = np.ones(k, np.int64)
+    for r in range(n_reads):
+        bases, origin, src, exact = simulate_long_read(rng, ref, int(lengths[r]), float(errs[r]),
+                                                       split)
+        total += len(bases)
+        # run[p] = k: positions p-k+1..p are all exact (an anchor ends at p)
+        run = np.convolve(exact.astype(np.int64), kernel, mode="full")[:len(bases)]
+        ends = np.nonzero(run == k)[0]
+        if len(ends) < 2:
+            continue
+        a_end = int(ends[0])  # the first anchor
+        while True:
+            target = a_end + 1 + int(rng.integers(seg_lo, seg_hi - 150 + 1))
+            nxt = np.searchsorted(ends, target + k - 1)  # anchor starting at >= target
+            if nxt >= len(ends):
+                break
+            b_end = int(ends[nxt])
+            b_start = b_end - k + 1
+            s0, s1 = a_end + 1, b_start  # segment = read[s0:s1]
+            r0 = origin + int(src[a_end]) + 1  # reference gap [r0, r1)
+            r1 = origin + int(src[b_start])
+            if s1 > s0 and r1 > r0 and r0 - band >= 0 and r1 + band <= len(ref):
+                seg_bases.append(bases[s0:s1])
+                q.append(s1 - s0)
+                wstart.append(r0 - band)
+                wlen.append(r1 - r0 + 2 * band)
+                read_of.append(r)
+            a_end = b_end
+    q = np.asarray(q, np.int64)
+    read_off = np.zeros(len(q), np.uint64)
+    read_off[1:] = np.cumsum(q[:-1])
+    n = len(q)
+    return LongReadSegments(
+        f"gapfill_reads_{n_reads}_lognormal10k_band{band}",
+        np.concatenate(seg_bases + [np.zeros(16, np.uint8)]), read_off, q.astype(np.uint32), None,
+        np.asarray(wstart, np.uint64), np.asarray(wlen, np.uint32), np.full(n, band, np.int32),
+        np.full(n, band, np.int32), ref, np.asarray(read_of, np.int32), n_reads, int(total))
+
+
 def wfa_cascade(n_pairs: int = 2_000_000, seed: int = 0x3FA0, read_len: int = 150,
                 band: int = 33, err_hi: float = 0.04, split=(4, 1, 1),
                 reference: np.ndarray | None = None, ref_len: int = 50_000_000) -> SwWorkload:
