@@ -1582,7 +1582,10 @@ int kira_gpu_sieve_batch(kira_ctx* ctx, const kira_sieve_job* jobs, uint32_t n,
   KIRA_CUDA(cudaMemcpyAsync(dwn, wn.data(), 4ull * n, cudaMemcpyHostToDevice, st));
   KIRA_CUDA(cudaMemcpyAsync(dmm, mm.data(), 4ull * n, cudaMemcpyHostToDevice, st));
   SieveJobsDev J{n, drs, dro, drn, dws, dwo, dwn, dmm};
+  ctx->ev_recorded = 0;
+  mark(ctx, 0, st);  // stage 0 of kira_gpu_stage_times: the sieve kernel alone
   KIRA_CUDA(launch_sieve_dropin(J, dout, ctx->sms, st));
+  mark(ctx, 1, st);
   KIRA_CUDA(cudaMemcpyAsync(out, dout, sizeof(kira_sieve_result) * n, cudaMemcpyDeviceToHost, st));
   KIRA_CUDA(cudaStreamSynchronize(st));
   return KIRA_OK;

@@ -7,8 +7,9 @@
 //   in two halves: word k of lane g holds cell c = g*K + k in its low 16 bits and
 //   cell H + c in its high 16 bits, so every per-row quantity (band start, shift,
 //   argmax, x-drop) stays one scalar per pair while the DP arithmetic runs two
-//   cells per instruction with the DPX s16x2 forms (__viaddmax_s16x2,
-//   __vimax_s16x2_relu, __vibmax_s16x2).
+//   cells per instruction with the DPX 16x2 forms (__viaddmax_s16x2,
+//   __vimax_s16x2_relu, and the three-input __vimax3_s16x2_relu / __vimax3_u16x2
+//   for the scan operand's lane maximum and the row-max keys).
 //
 // Biased values
 //   Every DP value v is kept as v + B (B = bias >= gof + 2H*ge + mismatch + 1), so
@@ -16,8 +17,14 @@
 //   makes plain 32-bit IADD/IADD3 exact on packed words (no carry crosses the
 //   half boundary when each half's result stays in [0, 2^16)), and turns every
 //   comparison into the sign of a biased difference: 2^p + a - b has bit p set iff
-//   a >= b when |a - b| < 2^p. The five trace flags are produced that way at
-//   distinct bit positions (15..11) and merged with bit-select LOP3s.
+//   a >= b when |a - b| < 2^p. The four trace flags of a cell are produced that way
+//   at distinct bit positions and merged with bit-select LOP3s: diag >= E, max(diag,
+//   E) >= F, E extended, F not extended (bits 14..11 of words 0-1 of each group of
+//   four, 15..12 of words 2-3, so one PRMT per word pair and one shift and one LOP3
+//   per group pack them as 4-bit codes). Whether H > 0 is not stored: the traceback
+//   carries the exact H, E or F value of the cell it stands on (from the end score,
+//   the match / mismatch scores of its diagonal steps and the gap costs), and an H
+//   of 0 is the stop.
 //
 // Band edges
 //   Cells outside the previous row's band read as "neutral" (H = 0, E = the
@@ -37,14 +44,16 @@ template <int G, int K>
 struct Bsw16Shape {
   static constexpr int kHalf = G * K;                  // cells per half row
   static constexpr int kCap = 2 * kHalf;               // cells per row
-  static constexpr int kWords = (K + 1) / 2;           // code words per lane per row
-  static constexpr int kSlabs = (kWords + 1) / 2;      // 8-byte stores per lane per row
-  static constexpr int kLaneBytes = 8 * kSlabs;        // one code byte per cell
+  static constexpr int kWords = (K + 1) / 2;           // window-byte words per lane
+  static constexpr int kSlabs = (K + 3) / 4;           // 4-byte code stores per lane per row
+  static constexpr int kLaneBytes = 4 * kSlabs;        // a 4-bit code per cell
   static constexpr int kRowStride = G * kLaneBytes;
   // Rows interleave in blocks of kInterleave: a block stores slab by slab, and in
   // each slab row by row, so one 128-byte line holds one slab of kInterleave
   // consecutive rows (the cells a diagonal traceback run reads next).
-  static constexpr int kInterleave = G >= 16 ? 1 : 16 / G;
+  static constexpr int kInterleave = G >= 32 ? 1 : 32 / G;
+  // Bits of the word index in a row-max key ((h << kKeyBits) | (max - k) per half).
+  static constexpr int kKeyBits = K <= 2 ? 1 : K <= 4 ? 2 : K <= 8 ? 3 : K <= 16 ? 4 : 5;
 };
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
@@ -125,14 +134,13 @@ __device__ __forceinline__ void bsw16_group_sweep(
   const uint32_t MAT2 = pk2(match), MIS2 = pk2(-mism), NGE2 = pk2(-ge);
   const uint32_t GOFS = isum(gof, gof);
   const uint32_t FOFS = isum(ge - gof, ge - gof);              // f = run - C_k + (ge - gof)
-  const uint32_t NZC = isum(0x8000 - bias - 1, 0x8000 - bias - 1);
   const uint32_t C0 = isum(c0 * ge - gof, (H + c0) * ge - gof);  // C_k = idx*ge - gof
   const uint32_t GE2S = isum(ge, ge);
 
   int32_t prev_start = 1, prev_len = 0, act_len = -1;
   int32_t best = 0, bi = 0, bj = 0, bq = 0, bqj = 0;
   uint32_t early = 0;
-  uint64_t cells = 0;
+  uint32_t cells = 0;  // < 2^32: read_len * row length
   const int32_t drift = sp.adaptive ? sp.max_drift : 0;
   int32_t acenter = 1 + offset;
   const int32_t wl = (int32_t)w;
@@ -167,7 +175,7 @@ __device__ __forceinline__ void bsw16_group_sweep(
       continue;
     }
     const int32_t row_len = je - js + 1;
-    cells += (uint64_t)row_len;
+    cells += (uint32_t)row_len;
     const uint32_t qb = ldb(rd, (uint64_t)(i - 1));
     const int32_t sft = js - prev_start - 1;
     if (sft != 0 && prev_len > 0) bsw16_realign<G, K>(ph, pe, sft, prev_len, rowbuf, c0, B2, gmask);
@@ -208,41 +216,43 @@ __device__ __forceinline__ void bsw16_group_sweep(
         wb[j] = prmt(prmt(b0, b1, 0x0040u), prmt(b2, b3, 0x0040u), 0x5410u);
       }
     }
+    // Pass 1: E (+ extend flag), H_diag + s, the diag-vs-E flag, max(Hdiag+s, E)
+    // and the F-scan operand G = max(Hdiag+s, E, 0) - gof + idx*ge. E is final
+    // here, so the previous row's E of word k is replaced at once (word k reads
+    // only words k and k + 1 of the previous row).
     // Bit 7 of each byte of z: that cell's window base differs from the read base.
     const uint32_t qb4 = qb * 0x01010101u;
-    uint32_t z[NW];
-#pragma unroll
-    for (int j = 0; j < NW; ++j) {
-      const uint32_t x = wb[j] ^ qb4;
-      z[j] = x | ((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu);
-    }
-
-    // Pass 1: E (+ extend flag), H_diag + s, the diag-vs-E flag, max(Hdiag+s, E)
-    // and the F-scan operand G = max(Hdiag+s, E, 0) - gof + idx*ge.
-    uint32_t m1[K], gv[K], ev[K], code[K];
-    uint32_t lmax = 0u;
-    uint32_t ck = C0;
+    uint32_t m1[K], gv[K], code[K];
+    uint32_t ck = C0, z = 0u;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
+      if ((k & 1) == 0) {
+        const uint32_t x = wb[k >> 1] ^ qb4;
+        z = x | ((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu);
+      }
       const uint32_t uh = k + 1 < K ? ph[k + 1 < K ? k + 1 : 0] : nh;
       const uint32_t ue = k + 1 < K ? pe[k + 1 < K ? k + 1 : 0] : ne;
+      // Flag bits: 14..11 for words 0-1 of each group of four, 15..12 for words 2-3.
+      const uint32_t up = (k & 2) ? 1u : 0u;
       const uint32_t t = uh - GOFS;                      // H_up - gof
       const uint32_t e = __viaddmax_s16x2(ue, NGE2, t);  // max(E_up - ge, H_up - gof)
-      const uint32_t yee = e + 0x0FFF0FFFu - t;          // bit 12: e > t (E extended)
+      const uint32_t yee = e + (0x0FFF0FFFu << up | (up ? 0x00010001u : 0u)) - t;  // e > t
       // 0xFFFF per mismatching half (sign of the cell's byte replicated).
-      const uint32_t ms = prmt(z[k >> 1], 0u, (k & 1) ? 0xBBAAu : 0x9988u);
+      const uint32_t ms = prmt(z, 0u, (k & 1) ? 0xBBAAu : 0x9988u);
       const uint32_t s2 = bsel(MAT2, MIS2, ms);
       const uint32_t hm = __viaddmax_s16x2(ph[k], s2, B2);     // max(Hdiag + s, 0)
-      const uint32_t y1 = hm + 0x40004000u - e;          // bit 14: hm >= e
+      const uint32_t y1 = hm + (0x40004000u << up) - e;  // hm >= e
       const uint32_t mm = __vimax_s16x2_relu(hm, e);
-      const uint32_t gk = mm + ck;
-      code[k] = bsel(y1, yee, 0x10001000u);
+      code[k] = bsel(y1, yee, 0x10001000u << up);
       m1[k] = mm;
-      gv[k] = gk;
-      ev[k] = e;
-      lmax = __vimax_s16x2_relu(lmax, gk);
+      gv[k] = mm + ck;
+      pe[k] = e & act[k];
       ck += GE2S;
     }
+    uint32_t lmax = 0u;
+#pragma unroll
+    for (int k = 0; k < K; k += 2)
+      lmax = __vimax3_s16x2_relu(lmax, gv[k], k + 1 < K ? gv[k + 1 < K ? k + 1 : 0] : 0u);
     // Cross-lane inclusive max-scan of G per half; exclusive value per lane, then
     // the high half also sees every low-half cell (they precede it in the row).
     uint32_t v = lmax;
@@ -263,51 +273,54 @@ __device__ __forceinline__ void bsw16_group_sweep(
     ck = C0;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
+      const uint32_t up = (k & 2) ? 1u : 0u;
       const uint32_t f = run - ck + FOFS;                // max_{k<idx} G - (idx-1)*ge
       const uint32_t h = __vimax_s16x2_relu(m1[k], f);
-      const uint32_t y2 = m1[k] + 0x20002000u - f;       // bit 13: max(hm, e) >= f
-      const uint32_t ynz = h + NZC;                      // bit 15: h > 0
-      const uint32_t yfe = gp + 0x08000800u - run;       // bit 11: F not extended
-      uint32_t c = bsel(code[k], y2, 0x20002000u);
-      c = bsel(c, ynz, 0x80008000u);
-      code[k] = bsel(c, yfe, 0x08000800u);
+      const uint32_t y2 = m1[k] + (0x20002000u << up) - f;  // max(hm, e) >= f
+      const uint32_t yfe = gp + (0x08000800u << up) - run;  // F not extended
+      code[k] = bsel(bsel(code[k], y2, 0x20002000u << up), yfe, 0x08000800u << up);
       run = __vimax_s16x2_relu(run, gv[k]);
       gp = gv[k];
       ph[k] = bsel(B2, h, act[k]);
-      pe[k] = ev[k] & act[k];
       ck += GE2S;
     }
-    // Layout [row block][slab][row in block][lane] of 8-byte words: a group's
-    // lanes fill one contiguous G x 8-byte run per slab, so each store
-    // instruction writes whole sectors.
+    // 4-bit codes of words 4x .. 4x+3 in one 32-bit slab: byte (w & 1) * 2 + half
+    // holds word w's cell in its low nibble for w < 2, its high nibble for w >= 2.
+    // Layout [row block][slab][row in block][lane] of 4-byte slabs: a group's lanes
+    // fill one contiguous G x 4-byte run per slab and row.
     constexpr int R = Bsw16Shape<G, K>::kInterleave;
-    uint2* trow = reinterpret_cast<uint2*>(trace + (size_t)(i & ~(R - 1)) * S +
-                                           (size_t)(i & (R - 1)) * (G * 8)) + g;
+    uint32_t* trow = reinterpret_cast<uint32_t*>(trace + (size_t)(i & ~(R - 1)) * S +
+                                                 (size_t)(i & (R - 1)) * (G * 4)) + g;
 #pragma unroll
-    for (int x2 = 0; x2 < NS; ++x2) {
+    for (int x = 0; x < NS; ++x) {
       constexpr int kLast = K - 1;
-      const int a = 4 * x2, b = a + 1 <= kLast ? a + 1 : kLast, c = a + 2 <= kLast ? a + 2 : kLast,
+      const int a = 4 * x, b = a + 1 <= kLast ? a + 1 : kLast, c = a + 2 <= kLast ? a + 2 : kLast,
                 d = a + 3 <= kLast ? a + 3 : kLast;
-      const uint32_t w0 = prmt(code[a], code[b], 0x7531u);
-      const uint32_t w1 = 2 * x2 + 1 < NW ? prmt(code[c], code[d], 0x7531u) : 0u;
-      trow[x2 * R * G] = make_uint2(w0, w1);
+      const uint32_t lo = prmt(code[a], code[b], 0x7531u);  // flags at bits 6..3 of each byte
+      const uint32_t hi = a + 2 <= kLast ? prmt(code[c], code[d], 0x7531u) : 0u;  // bits 7..4
+      trow[x * R * G] = bsel(hi, lo >> 3, 0x0F0F0F0Fu);
     }
     if (g == 0) meta[i] = ((uint32_t)js << 11) | (uint32_t)row_len;
 
-    // Row max and its first cell: per half the first k with the max (descending
-    // scan keeps ties at the lowest k), then one 32-bit key per lane.
+    // Row max and its first cell: per half the key (h << KB) | (KM - k), whose
+    // unsigned maximum carries the lowest k holding the max; then one 32-bit key per
+    // lane (low-half cells precede high-half cells on ties).
+    constexpr int KB = Bsw16Shape<G, K>::kKeyBits;
+    constexpr uint32_t KM = (1u << KB) - 1u;
     uint32_t mx = 0u;
-    int32_t ilo = 0, ihi = 0;
 #pragma unroll
-    for (int k = K - 1; k >= 0; --k) {
-      bool phi, plo;
-      mx = __vibmax_s16x2(ph[k], mx, &phi, &plo);
-      ilo = plo ? k : ilo;
-      ihi = phi ? k : ihi;
+    for (int k = 0; k < K; k += 2) {
+      const uint32_t ka = ph[k] * (1u << KB) + (KM - (uint32_t)k) * 0x10001u;
+      const uint32_t kb = k + 1 < K ? ph[k + 1 < K ? k + 1 : 0] * (1u << KB) +
+                                          (KM - (uint32_t)(k + 1)) * 0x10001u
+                                    : 0u;
+      mx = __vimax3_u16x2(mx, ka, kb);
     }
-    const uint32_t klo = ((mx & 0xFFFFu) << 11) | (uint32_t)(2047 - (c0 + ilo));
-    const uint32_t khi = ((mx >> 16) << 11) | (uint32_t)(2047 - (H + c0 + ihi));
-    uint32_t key = max(klo, khi);
+    const uint32_t vlo = (mx & 0xFFFFu) >> KB, vhi = mx >> (16 + KB);
+    const bool lo_first = vlo >= vhi;
+    const uint32_t idx = lo_first ? (uint32_t)c0 + (KM - (mx & KM))
+                                  : (uint32_t)(H + c0) + (KM - ((mx >> 16) & KM));
+    uint32_t key = ((lo_first ? vlo : vhi) << 11) | (2047u - idx);
 #pragma unroll
     for (int off = G / 2; off > 0; off >>= 1) key = max(key, __shfl_xor_sync(gmask, key, off, G));
     const int32_t row_best = (int32_t)(key >> 11) - bias;
@@ -352,13 +365,13 @@ __device__ __forceinline__ void bsw16_group_sweep(
   cells_out = cells;
 }
 
-// Trace codes of the packed sweep (state machine of mod.rs:1581-1627). Code byte
-// of a cell: bit 7 H > 0, bit 6 diag >= E, bit 5 max(diag, E) >= F, bit 4 E
-// extended, bit 3 F NOT extended (F always closes after one cell when the gap open
-// is 0). The row holds two halves of G*K band cells; in each, lane gi keeps cells
-// gi*K .. +K-1, word kk/2 of lane gi in slab kk/4, stored as [row block][slab][row
-// in block][lane] of 8-byte words (Bsw16Shape::kInterleave rows per block).
-// Decoded into warp_walk's code layout.
+// Trace codes of the packed sweep. The 4-bit code of a cell: bit 3 diag >= E, bit
+// 2 max(diag, E) >= F, bit 1 E extended, bit 0 F NOT extended (F always closes after
+// one cell when the gap open is 0). The row holds two halves of G*K band cells; in
+// each, lane gi keeps cells gi*K .. +K-1, word kk of lane gi in slab kk/4, stored as
+// [row block][slab][row in block][lane] of 4-byte slabs (Bsw16Shape::kInterleave
+// rows per block). Decoded into warp_walk's code layout; the H move is never "stop"
+// here (the walk stops where its carried H is 0).
 template <int G, int K>
 struct Bsw16Code {
   const uint8_t* __restrict__ trace;
@@ -376,11 +389,103 @@ struct Bsw16Code {
     const uint32_t gi = c / (uint32_t)K, kk = c - gi * (uint32_t)K;
     const uint32_t ib = (uint32_t)i & (R - 1u);
     const uint32_t b = __ldg(trace + (size_t)((uint32_t)i - ib) * S +
-                             ((kk >> 2) * R + ib) * (G * 8u) + gi * 8u +
-                             ((kk >> 1) & 1u) * 4u + (kk & 1u) * 2u + hi);
-    const uint32_t h = !(b & 0x80u) ? 0u : (b & 0x60u) == 0x60u ? 1u : (b & 0x20u) ? 2u : 3u;
-    return h | ((b >> 2) & 4u) | ((go > 0 && !(b & 0x08u)) ? 8u : 0u);
+                             ((kk >> 2) * R + ib) * (G * 4u) + gi * 4u + (kk & 1u) * 2u + hi);
+    const uint32_t nib = (b >> ((kk & 2u) * 2u)) & 15u;
+    const uint32_t h = !(nib & 4u) ? 3u : (nib & 8u) ? 1u : 2u;
+    return h | ((nib & 2u) << 1) | ((go > 0 && !(nib & 1u)) ? 8u : 0u);
   }
 };
+
+// warp_walk (bsw.cuh) for codes without a stop move: the walk carries the exact
+// value of the cell it stands on -- H in the H state, E or F in a gap -- starting
+// from the end cell's score. A diagonal step from (i, j) lands on H(i, j) - s(i, j),
+// s the match / mismatch score of read[i - 1] against window[j - 1] (raw bytes); a
+// gap cell that extends adds gap_extend, the cell that opens it adds gap_open +
+// gap_extend on the way back to H. An H state on a cell whose value is 0 stops the
+// walk, as the reference's STOP move does (mod.rs:1587-1627). In a diagonal run the
+// 32 lanes take one cell each: an exclusive warp scan of their scores gives each
+// lane's H, and a ballot finds the first cell that ends the run.
+template <class Code>
+__device__ __forceinline__ uint32_t warp_walk_scored(const Code& code, int32_t& i, int32_t& j,
+                                                     int32_t v, const uint8_t* __restrict__ rd,
+                                                     const uint8_t* __restrict__ wn,
+                                                     const SwParams& sp, uint32_t* __restrict__ ops,
+                                                     uint32_t cap, uint32_t& overflow) {
+  const int32_t lane = (int32_t)(threadIdx.x & 31u);
+  uint32_t state = 0;  // 0 H, 1 E, 2 F; also the CIGAR op the state emits (M, I, D)
+  uint32_t n = 0, cur_op = 0xFFu, cur_len = 0;
+  auto push = [&](uint32_t op, uint32_t cnt) {
+    if (!cnt) return;
+    if (op == cur_op) {
+      cur_len += cnt;
+      return;
+    }
+    if (cur_len) {
+      if (n < cap) {
+        if (lane == 0) ops[n] = (cur_len << 4) | cur_op;
+      } else {
+        overflow = 1;
+      }
+      ++n;
+    }
+    cur_op = op;
+    cur_len = cnt;
+  };
+  while (i > 0 && j > 0) {
+    const int32_t di = state != 2u ? 1 : 0, dj = state != 1u ? 1 : 0;
+    const int32_t ci = i - lane * di, cj = j - lane * dj;
+    const bool inside = ci > 0 && cj > 0;
+    // A cell past row or column 0 ends the walk like the loop test does.
+    const uint32_t c = inside ? code(ci, cj) : 0xFFu;
+    bool cont;
+    int32_t vt = v, step = 0;  // this lane's value; its diagonal step's score
+    if (state == 0u) {
+      if (inside)
+        step = __ldg(rd + (ci - 1)) == __ldg(wn + (cj - 1)) ? sp.match : -sp.mismatch;
+      int32_t pre = step;  // inclusive scan of the steps, then exclusive
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int32_t x = __shfl_up_sync(0xffffffffu, pre, off);
+        if (lane >= off) pre += x;
+      }
+      vt = v - (pre - step);
+      cont = c != 0xFFu && vt != 0 && (c & 3u) == 1u;
+    } else {
+      cont = c != 0xFFu && (state == 1u ? (c & 4u) != 0u : (c & 8u) != 0u);
+    }
+    const uint32_t stop = __ballot_sync(0xffffffffu, !cont);
+    const uint32_t t = stop ? (uint32_t)(__ffs(stop) - 1) : 32u;
+    push(state, t);
+    i -= (int32_t)t * di;
+    j -= (int32_t)t * dj;
+    if (state == 0u) {
+      v = __shfl_sync(0xffffffffu, t < 32u ? vt : vt - step, t < 32u ? (int)t : 31);
+    } else {
+      v += (int32_t)t * sp.gap_extend;
+    }
+    if (t == 32u) continue;
+    const uint32_t ct = __shfl_sync(0xffffffffu, c, (int)t);
+    if (ct == 0xFFu) break;
+    if (state == 0u) {
+      if (v == 0) break;           // H == 0: the reference's STOP
+      state = (ct & 3u) - 1u;      // E or F at the same cell (the same value)
+    } else {                       // the gap's last cell, then back to H
+      push(state, 1u);
+      v += sp.gof;
+      if (state == 1u) --i;
+      else --j;
+      state = 0u;
+    }
+  }
+  if (cur_len) {
+    if (n < cap) {
+      if (lane == 0) ops[n] = (cur_len << 4) | cur_op;
+    } else {
+      overflow = 1;
+    }
+    ++n;
+  }
+  return n;
+}
 
 }  // namespace kira

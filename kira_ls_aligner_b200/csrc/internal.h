@@ -202,15 +202,16 @@ extern const int kNumBswShapes;
 
 inline int shape_cap(const BswShapeInfo& s) { return (s.packed ? 2 : 1) * s.g * s.k; }
 inline uint32_t shape_lane_bytes(const BswShapeInfo& s) {
-  // packed: one code byte per cell, in 8-byte words (two cells per 32-bit half).
-  return s.packed ? 8u * (uint32_t)(((s.k + 1) / 2 + 1) / 2) : 4u * (uint32_t)((s.k + 7) / 8);
+  // packed: a 4-bit code per cell, four words (eight cells) per 4-byte slab;
+  // int32: a 4-bit code per cell, eight cells per 4 bytes.
+  return s.packed ? 4u * (uint32_t)((s.k + 3) / 4) : 4u * (uint32_t)((s.k + 7) / 8);
 }
 inline uint32_t shape_row_stride(const BswShapeInfo& s) {
   return (uint32_t)s.g * shape_lane_bytes(s);
 }
 // Rows per interleave block of the packed trace (Bsw16Shape::kInterleave).
 inline uint32_t shape_row_interleave(const BswShapeInfo& s) {
-  return s.packed && s.g < 16 ? 16u / (uint32_t)s.g : 1u;
+  return s.packed && s.g < 32 ? 32u / (uint32_t)s.g : 1u;
 }
 // Bytes of one item's trace slot for reads of up to `max_q` bases: rows 0..max_q
 // rounded up to whole interleave blocks, then to 16 bytes.
@@ -231,14 +232,20 @@ inline int32_t packed_bias(const BswShapeInfo& s, const SwParams& sp) {
   return sp.gof + shape_cap(s) * sp.gap_extend + sp.mismatch + 1;
 }
 
-// The packed sweep is exact when every biased value stays below 2^13 and every
-// difference its flags test stays below 2^11 (the F-extend flag at bit 11).
+// Bits of the word index in the packed sweep's row-max keys (Bsw16Shape::kKeyBits).
+inline int packed_key_bits(int k) { return k <= 2 ? 1 : k <= 4 ? 2 : k <= 8 ? 3 : k <= 16 ? 4 : 5; }
+
+// The packed sweep is exact when every biased value stays below 2^13, every
+// difference its flags test stays below 2^11 (the F-extend flag at bit 11), and
+// every biased H fits a row-max key (H << key bits below 2^16).
 inline bool packed_fits(const BswShapeInfo& s, uint32_t max_q, const SwParams& sp) {
   if (!s.packed) return false;
   if (sp.match < 0 || sp.mismatch < 0 || sp.gap_open < 0 || sp.gap_extend < 0) return false;
   const int64_t top = (int64_t)max_q * sp.match;
   const int64_t cap = shape_cap(s);
   if (top + cap * sp.gap_extend + sp.gof >= 2048) return false;
+  if (top + (int64_t)packed_bias(s, sp) >= (int64_t(1) << (16 - packed_key_bits(s.k))))
+    return false;
   return top + (int64_t)packed_bias(s, sp) + cap * sp.gap_extend < 8192;
 }
 

@@ -593,7 +593,9 @@ __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
     if (outside) {
       i = j = 0;
     } else if constexpr (PACKED) {
-      n = warp_walk(Bsw16Code<G, K>{tr, mt, B.sp.gap_open}, i, j, ops, B.slot_cap, overflow);
+      n = warp_walk_scored(Bsw16Code<G, K>{tr, mt, B.sp.gap_open}, i, j, e.score,
+                           P.read_seq + P.read_off[pair], P.win_seq + P.win_off[pair], B.sp, ops,
+                           B.slot_cap, overflow);
     } else {
       n = warp_walk(BswCode<G, K>{tr, mt}, i, j, ops, B.slot_cap, overflow);
     }
@@ -942,7 +944,8 @@ const BswShapeInfo kBswShapes[] = {
     {8, 17, 128, 3, 0},  {16, 17, 128, 3, 0}, {32, 17, 128, 3, 0},
     // packed int16: K words = 2K cells per lane
     {2, 9, 256, 2, 1},   {4, 5, 256, 2, 1},   {4, 9, 256, 2, 1},  {8, 5, 256, 2, 1},
-    {8, 9, 256, 2, 1},   {16, 9, 256, 2, 1},  {32, 9, 256, 2, 1},
+    {8, 9, 256, 2, 1},   {16, 9, 256, 2, 1},  {32, 9, 256, 2, 1}, {2, 17, 128, 3, 1},
+    {2, 18, 128, 3, 1},
 };
 const int kNumBswShapes = sizeof(kBswShapes) / sizeof(kBswShapes[0]);
 
@@ -963,6 +966,8 @@ cudaError_t launch_bsw(int shape, const DevPairs& P, const BswLaunch& B, uint32_
     case 11: return launch_bsw16_shape<8, 9, 256, 2>(P, B, max_items, sms, st, between, parts);
     case 12: return launch_bsw16_shape<16, 9, 256, 2>(P, B, max_items, sms, st, between, parts);
     case 13: return launch_bsw16_shape<32, 9, 256, 2>(P, B, max_items, sms, st, between, parts);
+    case 14: return launch_bsw16_shape<2, 17, 128, 3>(P, B, max_items, sms, st, between, parts);
+    case 15: return launch_bsw16_shape<2, 18, 128, 3>(P, B, max_items, sms, st, between, parts);
     default: return cudaErrorInvalidValue;
   }
 }

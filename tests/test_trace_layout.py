@@ -1,19 +1,20 @@
-"""Packed banded-SW trace layout, restated on the CPU: rows interleave in blocks of
-16 / G ([row block][slab][row in block][lane] of 8-byte words, csrc/bsw16.cuh). For
-every packed launch shape and read length: each (row, lane, slab) word is unique
-and lies inside the item's slot (shape_slot_bytes, csrc/internal.h), and each cell
-byte the traceback decoder reads (Bsw16Code) lies in the word its lane stored for
-that cell's slab."""
+"""Packed banded-SW trace layout, restated on the CPU: a 4-bit code per cell, four
+words (eight cells) per 4-byte slab, rows interleaved in blocks of 32 / G
+([row block][slab][row in block][lane] of 4-byte slabs, csrc/bsw16.cuh). For every
+packed launch shape and read length: each (row, lane, slab) slab is unique and lies
+inside the item's slot (shape_slot_bytes, csrc/internal.h), and each cell's code
+the traceback decoder reads (Bsw16Code) lies in the slab its lane stored for that
+cell, at the byte and nibble the DP kernel packed it into."""
 import pytest
 
-PACKED_SHAPES = [(2, 9), (4, 5), (4, 9), (8, 5), (8, 9), (16, 9), (32, 9)]  # (G, K)
+PACKED_SHAPES = [(2, 9), (4, 5), (4, 9), (8, 5), (8, 9), (16, 9), (32, 9), (2, 17),
+                 (2, 18)]  # (G, K words)
 
 
 def geometry(g, k):
-    words = (k + 1) // 2              # code words per lane per row
-    slabs = (words + 1) // 2          # 8-byte stores per lane per row
-    stride = g * 8 * slabs            # bytes per row
-    inter = 1 if g >= 16 else 16 // g
+    slabs = (k + 3) // 4              # 4-byte code slabs per lane per row
+    stride = g * 4 * slabs            # bytes per row
+    inter = 1 if g >= 32 else 32 // g
     return slabs, stride, inter
 
 
@@ -24,21 +25,29 @@ def slot_bytes(g, k, max_q):
 
 
 def store_word(g, k, i, lane, slab):
-    """Byte address of lane `lane`'s slab-`slab` word of row i (the DP kernel's store)."""
+    """Byte address of lane `lane`'s slab `slab` of row i (the DP kernel's store)."""
     _, stride, r = geometry(g, k)
-    return (i & ~(r - 1)) * stride + (i & (r - 1)) * g * 8 + lane * 8 + slab * r * g * 8
+    return (i & ~(r - 1)) * stride + (i & (r - 1)) * g * 4 + lane * 4 + slab * r * g * 4
+
+
+def packed_position(kk, hi):
+    """(byte in the slab, nibble) of word kk's cell in half hi, as the DP packs it:
+    prmt of words (0, 1) and (2, 3) to the halves' high bytes, low nibbles from
+    words 0-1, high nibbles from words 2-3."""
+    w = kk & 3
+    return (w & 1) * 2 + hi, w >> 1
 
 
 def decode_byte(g, k, i, idx):
-    """Byte address the traceback reads for band cell idx of row i (Bsw16Code)."""
+    """Byte address and nibble the traceback reads for band cell idx of row i."""
     _, stride, r = geometry(g, k)
     half = g * k
     hi = 1 if idx >= half else 0
     c = idx - hi * half
     gi, kk = divmod(c, k)
     ib = i & (r - 1)
-    return ((i - ib) * stride + ((kk >> 2) * r + ib) * g * 8 + gi * 8 +
-            ((kk >> 1) & 1) * 4 + (kk & 1) * 2 + hi), gi, kk >> 2
+    addr = (i - ib) * stride + ((kk >> 2) * r + ib) * g * 4 + gi * 4 + (kk & 1) * 2 + hi
+    return addr, (kk & 2) >> 1, gi, kk >> 2, packed_position(kk, hi)
 
 
 @pytest.mark.parametrize("g,k", PACKED_SHAPES)
@@ -51,15 +60,24 @@ def test_words_unique_and_inside_the_slot(g, k, max_q):
         for lane in range(g):
             for slab in range(slabs):
                 a = store_word(g, k, i, lane, slab)
-                assert a % 8 == 0 and 0 <= a and a + 8 <= slot, (i, lane, slab, a, slot)
+                assert a % 4 == 0 and 0 <= a and a + 4 <= slot, (i, lane, slab, a, slot)
                 assert a not in seen
                 seen.add(a)
 
 
 @pytest.mark.parametrize("g,k", PACKED_SHAPES)
-def test_decoder_reads_the_stored_word(g, k):
+def test_decoder_reads_the_stored_code(g, k):
     for i in (1, 2, 3, 4, 5, 17, 150):
+        seen = set()
         for idx in range(2 * g * k):
-            a, lane, slab = decode_byte(g, k, i, idx)
+            a, nib, lane, slab, (byte, pnib) = decode_byte(g, k, i, idx)
             w = store_word(g, k, i, lane, slab)
-            assert w <= a < w + 8, (g, k, i, idx, a, w)
+            assert a == w + byte and nib == pnib, (g, k, i, idx, a, w, byte)
+            assert (a, nib) not in seen  # one cell per nibble
+            seen.add((a, nib))
+
+
+def test_every_packed_shape_of_the_library_is_covered():
+    from kira_ls_aligner_b200 import autotune
+    lib = {(g, cells // 2) for (g, cells), p in zip(autotune.shapes(), autotune.packed()) if p}
+    assert lib == set(PACKED_SHAPES)
