@@ -389,14 +389,20 @@ struct SwOut {
   bool early_abort = false;
   uint64_t cells = 0;
   Cigar cigar;
+  // Filled only on request (test of traceback forms): per row its band start and
+  // every cell's H and trace byte (test infrastructure, not the reference's output).
+  std::vector<int32_t> row_starts;
+  std::vector<std::vector<int32_t>> h_rows;
+  std::vector<std::vector<uint8_t>> trace_rows;
 };
 
 enum class TS { H, E, F };
 
 SwOut banded_sw_with(const uint8_t* read, size_t q_len, const uint8_t* reference, size_t r_len,
                      int32_t offset, const orc_cfg& cfg, int32_t abort_score, bool adaptive,
-                     int32_t drift_knob, int32_t dp_xdrop) {
+                     int32_t drift_knob, int32_t dp_xdrop, bool keep_matrix = false) {
   SwOut res;
+  if (keep_matrix) res.h_rows.resize(q_len + 1);
   const int32_t band = std::max(cfg.bandwidth, 1);
   std::vector<int32_t> prev_h, prev_e, cur_h, cur_e, cur_f;
   int32_t prev_start = 1;
@@ -498,6 +504,7 @@ SwOut banded_sw_with(const uint8_t* read, size_t q_len, const uint8_t* reference
         best_qlen_j = (size_t)j;
       }
     }
+    if (keep_matrix) res.h_rows[i] = cur_h;
     std::swap(prev_h, cur_h);
     std::swap(prev_e, cur_e);
     prev_start = j_start;
@@ -560,6 +567,10 @@ SwOut banded_sw_with(const uint8_t* read, size_t q_len, const uint8_t* reference
     }
   }
   std::reverse(cg.ops.begin(), cg.ops.end());
+  if (keep_matrix) {
+    res.row_starts = row_starts;
+    res.trace_rows = std::move(trace_rows);
+  }
   res.ref_start = (uint32_t)j;
   res.ref_end = ref_end;
   res.read_start = i;
@@ -1224,6 +1235,31 @@ int orc_banded_sw(const uint8_t* read, size_t q, const uint8_t* ref, size_t r, i
   SwOut s = banded_sw_with(read, q, ref, r, offset, *cfg, abort_score, adaptive != 0, max_drift,
                            dp_xdrop);
   emit(s, out, cigar, cap);
+  return 1;
+}
+
+// banded_sw_with plus its DP matrix: h and tr are (q + 1) x row_cap, row i holding
+// row_len[i] cells from window column row_start[i] (test infrastructure: checks of
+// traceback forms that do not store the STOP direction).
+int orc_banded_sw_matrix(const uint8_t* read, size_t q, const uint8_t* ref, size_t r,
+                         int32_t offset, const orc_cfg* cfg, int32_t abort_score, int adaptive,
+                         int32_t max_drift, int32_t dp_xdrop, orc_sw_result* out, uint32_t* cigar,
+                         uint32_t cap, int32_t* row_start, int32_t* row_len, int32_t* h,
+                         uint8_t* tr, size_t row_cap) {
+  SwOut s = banded_sw_with(read, q, ref, r, offset, *cfg, abort_score, adaptive != 0, max_drift,
+                           dp_xdrop, true);
+  emit(s, out, cigar, cap);
+  for (size_t i = 0; i <= q; ++i) {
+    const auto& hr = s.h_rows[i];
+    const auto& trr = s.trace_rows[i];
+    row_start[i] = s.row_starts[i];
+    row_len[i] = (int32_t)std::min(hr.size(), trr.size());
+    if ((size_t)row_len[i] > row_cap) return -1;
+    for (size_t c = 0; c < (size_t)row_len[i]; ++c) {
+      h[i * row_cap + c] = hr[c];
+      tr[i * row_cap + c] = trr[c];
+    }
+  }
   return 1;
 }
 

@@ -73,6 +73,14 @@ int orc_myers(const uint8_t* pat, size_t m, const uint8_t* text, size_t n, size_
 int orc_banded_sw(const uint8_t* read, size_t q, const uint8_t* ref, size_t r, int32_t offset,
                   const orc_cfg* cfg, int32_t abort_score, int adaptive, int32_t max_drift,
                   int32_t dp_xdrop, orc_sw_result* out, uint32_t* cigar, uint32_t cigar_cap);
+/* The same with the DP matrix (H and trace byte per cell, rows of row_len[i] cells
+ * from column row_start[i], stride row_cap); -1 when a row exceeds row_cap. Test
+ * infrastructure for traceback forms. */
+int orc_banded_sw_matrix(const uint8_t* read, size_t q, const uint8_t* ref, size_t r,
+                         int32_t offset, const orc_cfg* cfg, int32_t abort_score, int adaptive,
+                         int32_t max_drift, int32_t dp_xdrop, orc_sw_result* out, uint32_t* cigar,
+                         uint32_t cap, int32_t* row_start, int32_t* row_len, int32_t* h,
+                         uint8_t* tr, size_t row_cap);
 
 /* ---- mod.rs sw_batch_avx2 (16-lane i16, full window). n <= 16, equal shapes.
  * Returns 1 when the AVX2 kernel ran, 0 when the i16 fit check sent the chunk to

@@ -121,6 +121,11 @@ def lib():
         L.orc_banded_sw.argtypes = [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.c_int32,
                                     C.POINTER(OrcCfg), C.c_int32, C.c_int, C.c_int32, C.c_int32,
                                     C.POINTER(OrcSwResult), C.POINTER(C.c_uint32), C.c_uint32]
+        L.orc_banded_sw_matrix.argtypes = [
+            C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.c_int32, C.POINTER(OrcCfg),
+            C.c_int32, C.c_int, C.c_int32, C.c_int32, C.POINTER(OrcSwResult),
+            C.POINTER(C.c_uint32), C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+            C.c_size_t]
         pp = C.POINTER(C.c_char_p)
         for name in ("orc_sw_batch_avx2", "orc_sw_batch_int8"):
             f = getattr(L, name)
