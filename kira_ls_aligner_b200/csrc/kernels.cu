@@ -48,30 +48,70 @@ __global__ void __launch_bounds__(256) sieve_dropin_kernel(SieveJobsDev J,
 }
 
 // ---------------------------------------------------------------------------
-// Plane packing: one warp builds 32 plane blocks (1 KB of bases); lane i loads
-// byte 32*i + lane of the warp's span at step i (coalesced) and __ballot_sync
-// collects the bits of block i, which lane i stores.
+// Plane packing: a warp covers 512 bases (16 plane blocks); lane l loads bases
+// 16l .. 16l+15 as one 16-byte load and turns each 4-byte word into three nibbles
+// (code bit 0, code bit 1, valid) with SWAR byte arithmetic: the 2-bit code of
+// every byte is ((b >> 1) ^ (b >> 2)) & 3 (base_code), a PRMT table lookup gives
+// the letter that code stands for, and the case-folded byte equals it exactly for
+// A, C, G, T. A multiply by 0x01020408 gathers bit 0 of each byte into bits
+// 24..27. The even lane of each pair stores the block of its 32 bases.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void plane_nibbles(uint32_t w, uint32_t& n0, uint32_t& n1,
+                                              uint32_t& nv) {
+  const uint32_t x = (w >> 1) ^ (w >> 2);       // bits 0-1 of each byte: the code
+  const uint32_t y = x & 0x03030303u;
+  const uint32_t z = y | (y >> 4);              // bytes 0 and 2: two codes each
+  uint32_t sel, letter;
+  asm("prmt.b32 %0, %1, 0, 0x4420;" : "=r"(sel) : "r"(z));
+  asm("prmt.b32 %0, %1, 0, %2;" : "=r"(letter) : "r"(0x54474341u), "r"(sel));  // "ACGT"
+  const uint32_t t = (w & 0xDFDFDFDFu) ^ letter;  // zero byte: an ACGT base (any case)
+  const uint32_t ok = ~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u;
+  const uint32_t v = ok >> 7;                   // 0x01 per valid byte
+  n0 = ((x & v) * 0x01020408u) >> 24;
+  n1 = (((x >> 1) & v) * 0x01020408u) >> 24;
+  nv = (v * 0x01020408u) >> 24;
+}
+
 __global__ void __launch_bounds__(256) pack_planes_kernel(const uint8_t* __restrict__ seq,
                                                           uint64_t len, uint4* __restrict__ out,
                                                           uint64_t nblocks) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t wb = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-       wb * 32u < nblocks; wb += nwarps) {
-    const uint64_t base = wb * 1024u;
-    uint4 mine = make_uint4(0u, 0u, 0u, 0u);
-#pragma unroll 4
-    for (uint32_t i = 0; i < 32u; ++i) {
-      const uint64_t p = base + (uint64_t)i * 32u + lane;
-      const uint32_t c = p < len ? base_code(ldb(seq, p)) : 0u;
-      const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, c & 1u);
-      const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, c & 2u);
-      const uint32_t bv = __ballot_sync(0xFFFFFFFFu, c & 4u);
-      if (lane == i) mine = make_uint4(b0, b1, bv, 0u);
+  const bool aligned = ((uintptr_t)seq & 15u) == 0u;
+  for (uint64_t sp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+       sp * 16u < nblocks; sp += nwarps) {
+    const uint64_t p0 = sp * 512u + lane * 16u;
+    uint32_t w[4];
+    if (aligned && p0 + 16u <= len) {
+      const uint4 q = __ldg(reinterpret_cast<const uint4*>(seq + p0));
+      w[0] = q.x, w[1] = q.y, w[2] = q.z, w[3] = q.w;
+    } else {  // the arena's ragged end (or an unaligned arena): byte loads, zeros past len
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        uint32_t x = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const uint64_t p = p0 + 4u * k + b;
+          x |= (p < len ? ldb(seq, p) : 0u) << (8 * b);
+        }
+        w[k] = x;
+      }
     }
-    const uint64_t blk = wb * 32u + lane;
-    if (blk < nblocks) out[blk] = mine;
+    uint32_t b0 = 0, b1 = 0, bv = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      uint32_t n0, n1, nv;
+      plane_nibbles(w[k], n0, n1, nv);
+      b0 |= n0 << (4 * k);
+      b1 |= n1 << (4 * k);
+      bv |= nv << (4 * k);
+    }
+    const uint32_t o0 = __shfl_down_sync(0xFFFFFFFFu, b0, 1);
+    const uint32_t o1 = __shfl_down_sync(0xFFFFFFFFu, b1, 1);
+    const uint32_t ov = __shfl_down_sync(0xFFFFFFFFu, bv, 1);
+    const uint64_t blk = sp * 16u + (lane >> 1);
+    if (!(lane & 1u) && blk < nblocks)
+      out[blk] = make_uint4(b0 | (o0 << 16), b1 | (o1 << 16), bv | (ov << 16), 0u);
   }
 }
 
@@ -832,7 +872,7 @@ cudaError_t launch_sieve_dropin(const SieveJobsDev& J, kira_sieve_result* out, i
 
 cudaError_t launch_pack_planes(const uint8_t* seq, uint64_t len, uint4* out, uint64_t nblocks,
                                int sms, cudaStream_t st) {
-  const int blocks = grid_for((nblocks + 31) / 32, 8, sms * 16);
+  const int blocks = grid_for((nblocks + 15) / 16, 8, sms * 16);
   (pack_planes_kernel<<<blocks, 256, 0, st>>>(seq, len, out, nblocks), count_launch());
   return cudaGetLastError();
 }
