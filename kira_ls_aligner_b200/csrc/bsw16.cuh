@@ -403,8 +403,9 @@ struct Bsw16Code {
 // gap cell that extends adds gap_extend, the cell that opens it adds gap_open +
 // gap_extend on the way back to H. An H state on a cell whose value is 0 stops the
 // walk, as the reference's STOP move does (mod.rs:1587-1627). In a diagonal run the
-// 32 lanes take one cell each: an exclusive warp scan of their scores gives each
-// lane's H, and a ballot finds the first cell that ends the run.
+// 32 lanes take one cell each: a ballot of the matching cells and the popcount of
+// the lower lanes' bits give each lane's H, and a ballot finds the first cell that
+// ends the run.
 template <class Code>
 __device__ __forceinline__ uint32_t warp_walk_scored(const Code& code, int32_t& i, int32_t& j,
                                                      int32_t v, const uint8_t* __restrict__ rd,
@@ -440,15 +441,13 @@ __device__ __forceinline__ uint32_t warp_walk_scored(const Code& code, int32_t& 
     bool cont;
     int32_t vt = v, step = 0;  // this lane's value; its diagonal step's score
     if (state == 0u) {
-      if (inside)
-        step = __ldg(rd + (ci - 1)) == __ldg(wn + (cj - 1)) ? sp.match : -sp.mismatch;
-      int32_t pre = step;  // inclusive scan of the steps, then exclusive
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const int32_t x = __shfl_up_sync(0xffffffffu, pre, off);
-        if (lane >= off) pre += x;
-      }
-      vt = v - (pre - step);
+      // Steps before this lane: a ballot of the matching cells and a popcount of the
+      // lower lanes' bits (no scan): sum = matches * match - mismatches * mismatch.
+      const bool eq = inside && __ldg(rd + (ci - 1)) == __ldg(wn + (cj - 1));
+      step = eq ? sp.match : -sp.mismatch;
+      const uint32_t eqm = __ballot_sync(0xffffffffu, eq);
+      const int32_t before = __popc(eqm & ((1u << lane) - 1u));
+      vt = v - before * (sp.match + sp.mismatch) + lane * sp.mismatch;
       cont = c != 0xFFu && vt != 0 && (c & 3u) == 1u;
     } else {
       cont = c != 0xFFu && (state == 1u ? (c & 4u) != 0u : (c & 8u) != 0u);

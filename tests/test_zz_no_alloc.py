@@ -147,9 +147,11 @@ def test_noalloc_reports_pairs_beyond_the_declared_maxima():
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     cfg = AlignmentConfig(1, 4, 6, 1, 33, 100, 5, True, 16)
-    cases = sw_corpus(0x0A121, 64, qmin=30, qmax=100, pad=50, max_band=40)
+    # reads of 30-90 bases (at most 96 after the corpus's insertions), pair 17 150
+    cases = sw_corpus(0x0A121, 64, qmin=30, qmax=90, pad=50, max_band=40)
     long_read, long_win = cases[0][0] * 2, cases[0][1] * 2
     cases[17] = (long_read[:150], long_win[:220], 0, 20, O.ABORT_DISABLED)
+    assert all(len(c[0]) <= 100 for i, c in enumerate(cases) if i != 17)
     b, p, keep = _dev_batch(cases, torch, dev)
     p.max_read_len = 100  # pair 17 (150 bases) exceeds it
     with GpuContext(0) as ctx:
