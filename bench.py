@@ -252,14 +252,15 @@ def run_uneven(args, rank, local, world):
     if rank != 0:
         return None
     torch.cuda.set_device(local)
-    w = synth.uneven()
+    w = synth.uneven(resident=True)
     n = w.n_pairs
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-    batch = PairBatch(pin(w.reads), pin(w.read_off), pin(w.read_len), pin(w.wins),
+    batch = PairBatch(pin(w.reads), pin(w.read_off), pin(w.read_len), None,
                       pin(w.win_off), pin(w.win_len), pin(w.band_offset), None,
                       pin(w.bandwidth))
     cfg = AlignmentConfig(1, 4, 6, 1, 33, 100, 5, True, 16)
     ctx = GpuContext(local)
+    ctx.ref_upload(w.reference)
     L = _abi.lib()
     # Autotune the shape of each band class on a 20k-pair sample of that class
     # (DP stage time from the library's stage events).
@@ -299,7 +300,8 @@ def run_uneven(args, rank, local, world):
         "data": "synthetic (seeded)",
         "config": {"workload": w.name, "pairs": n, "read_len": "U[50,300]",
                    "band": "U{16,32,64,128}", "window": "read + 2*band", "errors": "U[0,3%] 8:1:1",
-                   "path": "host API, pinned inputs, H2D + D2H per call"},
+                   "path": "host API, pinned inputs (reads + descriptors; windows from the "
+                           "resident reference), H2D + D2H per call"},
         "bucketed": out["bucketed"], "plain": out["plain"],
         "speedup_vs_plain": out["bucketed"]["pairs_per_s"] / out["plain"]["pairs_per_s"],
         "cuda_graphs": graphs,
@@ -777,9 +779,16 @@ def run_gapfill(args, rank, local, world):
 
 
 def _subset(w, idx):
-    """A compact PairBatch of the pairs `idx` of an SwWorkload (own arenas)."""
+    """A compact PairBatch of the pairs `idx` of an SwWorkload (own read arena;
+    windows stay reference coordinates when the workload's reference is resident)."""
     from kira_ls_aligner_b200 import PairBatch
     rl, wl = w.read_len[idx], w.win_len[idx]
+    if w.wins is None:
+        reads = np.concatenate([w.reads[int(o):int(o) + int(n)]
+                                for o, n in zip(w.read_off[idx], rl)] + [np.zeros(16, np.uint8)])
+        ro = np.concatenate([[0], np.cumsum(rl[:-1], dtype=np.uint64)]).astype(np.uint64)
+        return PairBatch(reads, ro, rl.copy(), None, w.win_off[idx].copy(), wl.copy(),
+                         w.band_offset[idx].copy(), None, w.bandwidth[idx].copy())
     reads = np.concatenate([w.reads[int(o):int(o) + int(n)] for o, n in zip(w.read_off[idx], rl)]
                            + [np.zeros(16, np.uint8)])
     wins = np.concatenate([w.wins[int(o):int(o) + int(n)] for o, n in zip(w.win_off[idx], wl)]

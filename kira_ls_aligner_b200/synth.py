@@ -229,9 +229,12 @@ class SwWorkload:
 
 
 def uneven(n_pairs: int = 500_000, seed: int = 0x3E3E, q_lo: int = 50, q_hi: int = 300,
-           bands=(16, 32, 64, 128), err_hi: float = 0.03, ref_len: int = 20_000_000) -> SwWorkload:
+           bands=(16, 32, 64, 128), err_hi: float = 0.03, ref_len: int = 20_000_000,
+           resident: bool = False) -> SwWorkload:
     """Reads U[50, 300] bp, band uniform in {16, 32, 64, 128}, window = read + 2 x band
-    with the read's origin at window offset band, errors U[0, 3 %] at 8:1:1."""
+    with the read's origin at window offset band, errors U[0, 3 %] at 8:1:1. With
+    `resident` the windows stay reference coordinates (wins None, reference set: the
+    reference is device-resident), else they are copied into their own arena."""
     rng = np.random.default_rng(seed)
     ref = BASES[rng.integers(0, 4, ref_len)]
     q = rng.integers(q_lo, q_hi + 1, n_pairs).astype(np.int64)
@@ -246,6 +249,11 @@ def uneven(n_pairs: int = 500_000, seed: int = 0x3E3E, q_lo: int = 50, q_hi: int
     read_arena = reads[mask]
     read_off = np.zeros(n_pairs, np.uint64)
     read_off[1:] = np.cumsum(q[:-1])
+    if resident:
+        return SwWorkload("uneven_500k_q50-300_band16-128",
+                          np.concatenate([read_arena, np.zeros(16, np.uint8)]), read_off,
+                          q.astype(np.uint32), None, start.astype(np.uint64), w.astype(np.uint32),
+                          b.astype(np.int32), b.astype(np.int32), ref)
     win_off = np.zeros(n_pairs, np.uint64)
     win_off[1:] = np.cumsum(w[:-1])
     idx = np.repeat(start, w) + (np.arange(int(w.sum())) - np.repeat(win_off.astype(np.int64), w))
