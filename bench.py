@@ -1166,7 +1166,7 @@ def roofline_block(args, L, local, stage_ms, statuses, cells_step, n, tuning):
     probes = {}
     for op, name in enumerate(ALU_PROBES):
         v = C.c_double()
-        if L.kira_gpu_alu_probe(local, op, 200_000, C.byref(v)) == 0:
+        if L.kira_gpu_alu_probe(local, op, 40_000, C.byref(v)) == 0:
             probes[name] = v.value / 1e12
     ops_cell = 9 if packed else 18
     cell_rate = cells_step / (dp_ms / 1e3) if dp_ms > 0 else 0.0

@@ -157,8 +157,14 @@ __device__ __forceinline__ void bsw16_group_sweep(
 #pragma unroll
   for (int j = 0; j < NW; ++j) wb[j] = 0u;
 
+  // The read base of the next row is loaded a row ahead (its latency hides behind
+  // the current row's work).
+  uint32_t qb_next = q ? ldb(rd, 0) : 0u;
+  uint32_t wnext = 0u;
   for (uint32_t iu = 1; iu <= q; ++iu) {
     const int32_t i = (int32_t)iu;
+    const uint32_t qb = qb_next;
+    if (iu < q) qb_next = ldb(rd, (uint64_t)iu);
     const int32_t sc = i + offset;
     const int32_t center = sp.adaptive ? min(max(acenter, sc - drift), sc + drift) : sc;
     const int32_t js = max(center - band, 1);
@@ -176,7 +182,6 @@ __device__ __forceinline__ void bsw16_group_sweep(
     }
     const int32_t row_len = je - js + 1;
     cells += (uint32_t)row_len;
-    const uint32_t qb = ldb(rd, (uint64_t)(i - 1));
     const int32_t sft = js - prev_start - 1;
     if (sft != 0 && prev_len > 0) bsw16_realign<G, K>(ph, pe, sft, prev_len, rowbuf, c0, B2, gmask);
     if (row_len != act_len) {
@@ -193,6 +198,10 @@ __device__ __forceinline__ void bsw16_group_sweep(
       ne = prmt(ne, 0u, 0x5432u);
     }
     const uint8_t* wrow = wn + (js - 1);
+    // The next row's new window byte if its band moves one column (index in
+    // [js - 1, wl - 1]); used only by the group's last lane.
+    const uint32_t wcur = wnext;
+    if ((K & 1) && gi == G - 1) wnext = __ldg(wn + js + min(2 * H - 1, wl - js - 1));
     // Window bytes: cells past the window end repeat its last byte (never active
     // in this or a later row); cells past the row end hold real window bytes, so
     // a row whose band moved one column takes the previous row's bytes shifted by
@@ -202,9 +211,9 @@ __device__ __forceinline__ void bsw16_group_sweep(
       const uint32_t n0 = __shfl_sync(gmask, wb[0], (gi + 1) & (G - 1), G);
 #pragma unroll
       for (int j = 0; j + 1 < NW; ++j) wb[j] = prmt(wb[j], wb[j + 1], 0x5432u);
-      wb[NW - 1] = gi == G - 1
-                       ? prmt(n0, (uint32_t)__ldg(wrow + min(2 * H - 1, wlast)), 0x0041u)
-                       : n0;
+      // wcur: this row's new byte, loaded during the previous row on the guess that
+      // the band moves one column (wrow + min(2H - 1, wlast) for js = prev_start + 1).
+      wb[NW - 1] = gi == G - 1 ? prmt(n0, wcur, 0x0041u) : n0;
     } else {
 #pragma unroll
       for (int j = 0; j < NW; ++j) {

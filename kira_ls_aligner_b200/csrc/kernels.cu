@@ -986,6 +986,8 @@ const BswShapeInfo kBswShapes[] = {
     {2, 9, 256, 2, 1},   {4, 5, 256, 2, 1},   {4, 9, 256, 2, 1},  {8, 5, 256, 2, 1},
     {8, 9, 256, 2, 1},   {16, 9, 256, 2, 1},  {32, 9, 256, 2, 1}, {2, 17, 128, 3, 1},
     {2, 18, 128, 3, 1},
+    // the same packed sweeps held to more resident blocks (fewer registers, some spilled)
+    {4, 9, 256, 3, 1},   {2, 17, 128, 4, 1},
 };
 const int kNumBswShapes = sizeof(kBswShapes) / sizeof(kBswShapes[0]);
 
@@ -1008,6 +1010,8 @@ cudaError_t launch_bsw(int shape, const DevPairs& P, const BswLaunch& B, uint32_
     case 13: return launch_bsw16_shape<32, 9, 256, 2>(P, B, max_items, sms, st, between, parts);
     case 14: return launch_bsw16_shape<2, 17, 128, 3>(P, B, max_items, sms, st, between, parts);
     case 15: return launch_bsw16_shape<2, 18, 128, 3>(P, B, max_items, sms, st, between, parts);
+    case 16: return launch_bsw16_shape<4, 9, 256, 3>(P, B, max_items, sms, st, between, parts);
+    case 17: return launch_bsw16_shape<2, 17, 128, 4>(P, B, max_items, sms, st, between, parts);
     default: return cudaErrorInvalidValue;
   }
 }
