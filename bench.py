@@ -1159,7 +1159,7 @@ def roofline_block(args, L, local, stage_ms, statuses, cells_step, n, tuning):
     achieved = alg[dom] / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     per_cell = profile_figure("bsw16_dp_batched_800k.md" if packed else "bsw_dp_batched_800k.md",
                               "dram_bytes_per_cell")
-    per_pair = profile_figure("verify_sieve_batched_800k.md", "dram_bytes_per_pair")
+    per_pair = profile_figure("verify_filter_batched_800k.md", "dram_bytes_per_pair")
     traffic = {2: None if per_cell is None else per_cell * cells_step,
                0: None if per_pair is None else per_pair * n}.get(dom)
     dp_ms = stage_ms[2] / args.steps
