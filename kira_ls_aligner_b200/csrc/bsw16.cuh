@@ -264,17 +264,25 @@ __device__ __forceinline__ void bsw16_group_sweep(
       lmax = __vimax3_s16x2_relu(lmax, gv[k], k + 1 < K ? gv[k + 1 < K ? k + 1 : 0] : 0u);
     // Cross-lane inclusive max-scan of G per half; exclusive value per lane, then
     // the high half also sees every low-half cell (they precede it in the row).
-    uint32_t v = lmax;
+    uint32_t excl, tot, gp;
+    if constexpr (G == 2) {  // two lanes: one exchange gives both the prefix and the total
+      const uint32_t other = __shfl_xor_sync(gmask, lmax, 1, G);
+      gp = __shfl_xor_sync(gmask, gv[K - 1], 1, G);
+      tot = __vimax_s16x2_relu(lmax, other);
+      excl = gi == 0 ? 0u : other;
+    } else {
+      uint32_t v = lmax;
 #pragma unroll
-    for (int off = 1; off < G; off <<= 1) {
-      const uint32_t tt = __shfl_up_sync(gmask, v, off, G);
-      if (gi >= off) v = __vimax_s16x2_relu(v, tt);
+      for (int off = 1; off < G; off <<= 1) {
+        const uint32_t tt = __shfl_up_sync(gmask, v, off, G);
+        if (gi >= off) v = __vimax_s16x2_relu(v, tt);
+      }
+      excl = __shfl_up_sync(gmask, v, 1, G);
+      if (gi == 0) excl = 0u;
+      tot = __shfl_sync(gmask, v, G - 1, G);
+      gp = __shfl_sync(gmask, gv[K - 1], (gi + G - 1) & (G - 1), G);
     }
-    uint32_t excl = __shfl_up_sync(gmask, v, 1, G);
-    if (gi == 0) excl = 0u;
-    const uint32_t tot = __shfl_sync(gmask, v, G - 1, G);
     excl = __vimax_s16x2_relu(excl, prmt(tot, 0u, 0x1054u));
-    uint32_t gp = __shfl_sync(gmask, gv[K - 1], (gi + G - 1) & (G - 1), G);
     if (gi == 0) gp = prmt(gp, 0u, 0x1054u);
 
     // Pass 2: F, H, the remaining flags; neutralise inactive cells.
