@@ -389,15 +389,15 @@ __device__ __forceinline__ void bsw16_group_sweep(
 // [row block][slab][row in block][lane] of 4-byte slabs (Bsw16Shape::kInterleave
 // rows per block). Decoded into warp_walk's code layout; the H move is never "stop"
 // here (the walk stops where its carried H is 0).
-template <int G, int K>
+template <int G, int K, bool STAGED_META = false>
 struct Bsw16Code {
   const uint8_t* __restrict__ trace;
-  const uint32_t* __restrict__ meta;
+  const uint32_t* __restrict__ meta;  // global, or the walk's shared-memory copy
   int32_t go;
   __device__ __forceinline__ uint32_t operator()(int32_t i, int32_t j) const {
     constexpr uint32_t H = Bsw16Shape<G, K>::kHalf, S = Bsw16Shape<G, K>::kRowStride;
     constexpr uint32_t R = Bsw16Shape<G, K>::kInterleave;
-    const uint32_t m = __ldg(meta + i);
+    const uint32_t m = STAGED_META ? meta[i] : __ldg(meta + i);
     const int32_t rs = (int32_t)(m >> 11), rl = (int32_t)(m & 2047u);
     const int32_t idx = j - rs;
     if (idx < 0 || idx >= rl) return 0xFFu;
@@ -413,7 +413,8 @@ struct Bsw16Code {
   }
 };
 
-// warp_walk (bsw.cuh) for codes without a stop move: the walk carries the exact
+// warp_walk (bsw.cuh) for codes without a stop move (rd / wn: the pair's read and
+// window, in global or shared memory): the walk carries the exact
 // value of the cell it stands on -- H in the H state, E or F in a gap -- starting
 // from the end cell's score. A diagonal step from (i, j) lands on H(i, j) - s(i, j),
 // s the match / mismatch score of read[i - 1] against window[j - 1] (raw bytes); a
@@ -460,7 +461,7 @@ __device__ __forceinline__ uint32_t warp_walk_scored(const Code& code, int32_t& 
     if (state == 0u) {
       // Steps before this lane: a ballot of the matching cells and a popcount of the
       // lower lanes' bits (no scan): sum = matches * match - mismatches * mismatch.
-      const bool eq = inside && __ldg(rd + (ci - 1)) == __ldg(wn + (cj - 1));
+      const bool eq = inside && rd[ci - 1] == wn[cj - 1];
       step = eq ? sp.match : -sp.mismatch;
       const uint32_t eqm = __ballot_sync(0xffffffffu, eq);
       const int32_t before = __popc(eqm & ((1u << lane) - 1u));

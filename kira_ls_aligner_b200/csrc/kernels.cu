@@ -613,8 +613,11 @@ __global__ void __launch_bounds__(T, MINB) bsw16_dp_kernel(DevPairs P, BswLaunch
 
 // One warp per item (warp_walk over the trace of shape <G, K>, packed or int32);
 // lane 0 writes the item's result row.
+constexpr uint32_t kTbStageBytes = 4096;  // per warp: metadata + read + window of a walk
+
 template <int G, int K, bool PACKED>
 __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
+  __shared__ uint32_t tb_stage[PACKED ? 4 : 1][PACKED ? kTbStageBytes / 4 : 1];
   const uint32_t count = bsw_round_end(B);
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
   const bool lead = (threadIdx.x & 31u) == 0u;
@@ -633,9 +636,27 @@ __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
     if (outside) {
       i = j = 0;
     } else if constexpr (PACKED) {
-      n = warp_walk_scored(Bsw16Code<G, K>{tr, mt, B.sp.gap_open}, i, j, e.score,
-                           P.read_seq + P.read_off[pair], P.win_seq + P.win_off[pair], B.sp, ops,
-                           B.slot_cap, overflow);
+      // The walk's row metadata, read and window go to this warp's shared-memory
+      // strip when they fit (one coalesced pass), so each round of the walk waits on
+      // one global load (its codes) instead of a metadata load and then the codes.
+      const uint32_t q = P.read_len[pair], w = P.win_len[pair];
+      const uint8_t* rd = P.read_seq + P.read_off[pair];
+      const uint8_t* wn = P.win_seq + P.win_off[pair];
+      if (4u * (q + 1u) + q + w <= kTbStageBytes) {
+        uint32_t* smeta = tb_stage[threadIdx.x >> 5];
+        uint8_t* sseq = reinterpret_cast<uint8_t*>(smeta + q + 1u);
+        const uint32_t ln = threadIdx.x & 31u;
+        for (uint32_t t = ln; t <= q; t += 32u) smeta[t] = __ldg(mt + t);
+        for (uint32_t t = ln; t < q; t += 32u) sseq[t] = __ldg(rd + t);
+        for (uint32_t t = ln; t < w; t += 32u) sseq[q + t] = __ldg(wn + t);
+        __syncwarp();
+        n = warp_walk_scored(Bsw16Code<G, K, true>{tr, smeta, B.sp.gap_open}, i, j, e.score,
+                             sseq, sseq + q, B.sp, ops, B.slot_cap, overflow);
+        __syncwarp();
+      } else {
+        n = warp_walk_scored(Bsw16Code<G, K>{tr, mt, B.sp.gap_open}, i, j, e.score, rd, wn,
+                             B.sp, ops, B.slot_cap, overflow);
+      }
     } else {
       n = warp_walk(BswCode<G, K>{tr, mt}, i, j, ops, B.slot_cap, overflow);
     }
