@@ -141,6 +141,8 @@ struct kira_ctx {
   uint64_t graph_replays = 0, graph_captures = 0;
   unsigned long long graph_kernels = 0;  // kernels in the cached graph (launch accounting)
   uint32_t last_rounds = 0;              // trace rounds of the last kira_gpu_bsw_batch
+  cudaStream_t aux = nullptr;            // second half of a split banded-SW stage
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaStream_t h2d = nullptr, d2h = nullptr;   // copy streams of the chunked host path
   int64_t chunk_pairs = -1;                    // chunked host path: -1 auto, 0 off, else pairs
   int wfa_lanes = 0;                           // WFA lanes per pair: 0 auto, else 8 / 16 / 32
@@ -530,6 +532,9 @@ void mark(kira_ctx* ctx, int i, cudaStream_t st) {
   ctx->ev_recorded = i + 1;
 }
 
+// Batches of at least this many pairs split their banded-SW stage over two streams.
+constexpr uint32_t kSplitPairs = 1u << 16;
+
 // How one call of the composed path fits into a chunked batch: planes already
 // built by the caller, whether the flag word is reset, and whether CIGAR offsets
 // continue from the running total in total_dev.
@@ -606,8 +611,26 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
   B.out = out;
   B.ncig = ncig;
   B.flags = counters + 2;
-  KIRA_CUDA(launch_bsw_rounds(shape, D, B, n, per_round, ctx->sms, st,
-                              ctx->profile ? ctx->ev[3] : nullptr));
+  if (per_round >= n && n >= kSplitPairs && !ctx->profile) {
+    // One trace round: the two halves of the banded-SW items (split on the device
+    // by the Myers stage's count) run on two streams, so one half's DP fills the
+    // SMs the other's last wave leaves idle and its traceback overlaps that DP.
+    if (!ctx->aux) KIRA_CUDA(cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking));
+    if (!ctx->ev_fork) KIRA_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    if (!ctx->ev_join) KIRA_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+    KIRA_CUDA(cudaEventRecord(ctx->ev_fork, st));
+    KIRA_CUDA(cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
+    BswLaunch B1 = B, B2 = B;
+    B1.split = 1u;
+    B2.split = 2u;
+    KIRA_CUDA(launch_bsw(shape, D, B1, n, ctx->sms, st));
+    KIRA_CUDA(launch_bsw(shape, D, B2, n, ctx->sms, ctx->aux));
+    KIRA_CUDA(cudaEventRecord(ctx->ev_join, ctx->aux));
+    KIRA_CUDA(cudaStreamWaitEvent(st, ctx->ev_join, 0));
+  } else {
+    KIRA_CUDA(launch_bsw_rounds(shape, D, B, n, per_round, ctx->sms, st,
+                                ctx->profile ? ctx->ev[3] : nullptr));
+  }
   if (ctx->profile) ctx->ev_recorded = 4;
   mark(ctx, 4, st);
   if (cm.before_scan) KIRA_CUDA(cudaStreamWaitEvent(st, cm.before_scan, 0));
@@ -1535,6 +1558,12 @@ void kira_gpu_destroy(kira_ctx* ctx) {
   for (auto e : ctx->ev_scan) cudaEventDestroy(e);
   if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
   if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
+  if (ctx->aux) {
+    cudaStreamSynchronize(ctx->aux);
+    cudaStreamDestroy(ctx->aux);
+  }
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->stage) cudaFreeHost(ctx->stage);
   cudaStreamDestroy(ctx->stream);
   delete ctx;

@@ -90,6 +90,9 @@ struct BswLaunch {
   // bound); trace slots and row metadata are indexed by item - item_lo, every
   // other per-item array by the item itself.
   uint32_t item_lo, item_hi;
+  // 1 / 2: the first / second half of the item count (device-side), for the two
+  // halves of a one-round batch run on two streams at once; 0: the round above.
+  uint32_t split;
 };
 
 struct CompactLaunch {

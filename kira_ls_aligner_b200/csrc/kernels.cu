@@ -505,10 +505,18 @@ __global__ void __launch_bounds__(128) myers_kernel(DevPairs P, MyersLaunch M) {
 // ---------------------------------------------------------------------------
 // Banded SW: DP sweep (group of G lanes per item) and traceback (thread per item)
 // ---------------------------------------------------------------------------
-// One past the last item of a launch's trace round.
-__device__ __forceinline__ uint32_t bsw_round_end(const BswLaunch& B) {
+// The items [lo, end) of a launch: its trace round, or with B.split one of the two
+// halves of the (device-side) item count that run on two streams at once.
+__device__ __forceinline__ void bsw_range(const BswLaunch& B, uint32_t& lo, uint32_t& end) {
   const uint32_t count = B.count_dev ? *B.count_dev : B.count;
-  return B.item_hi ? min(count, B.item_hi) : count;
+  if (B.split) {
+    const uint32_t mid = (count + 1u) / 2u;
+    lo = B.split == 1u ? 0u : mid;
+    end = B.split == 1u ? mid : count;
+    return;
+  }
+  lo = B.item_lo;
+  end = B.item_hi ? min(count, B.item_hi) : count;
 }
 
 template <int G, int K, int T, int MINB, bool FULL>
@@ -522,13 +530,14 @@ __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B
   const uint32_t groups_per_block = blockDim.x / G;
   const uint32_t group_in_block = threadIdx.x / G;
   int32_t* rowbuf = bsw_smem + (size_t)(threadIdx.x >> 5) * 2u * K * 32u;  // per warp
-  const uint32_t count = bsw_round_end(B);
+  uint32_t lo, count;
+  bsw_range(B, lo, count);
   const uint32_t ngroups = gridDim.x * groups_per_block;
-  uint32_t item = B.item_lo + blockIdx.x * groups_per_block + group_in_block;
+  uint32_t item = lo + blockIdx.x * groups_per_block + group_in_block;
   for (;;) {
     if (B.work) {  // dynamic fetch: the group leader takes the next item
       uint32_t t = 0;
-      if (g == 0) t = B.item_lo + atomicAdd(B.work, 1u);
+      if (g == 0) t = lo + atomicAdd(B.work, 1u);
       item = __shfl_sync(gmask, t, gw * G);
     }
     if (item >= count) break;
@@ -573,13 +582,14 @@ __global__ void __launch_bounds__(T, MINB) bsw16_dp_kernel(DevPairs P, BswLaunch
   const uint32_t groups_per_block = blockDim.x / G;
   const uint32_t group_in_block = threadIdx.x / G;
   uint16_t* rowbuf = bsw16_smem + (size_t)group_in_block * 4u * G * K;  // per group
-  const uint32_t count = bsw_round_end(B);
+  uint32_t lo, count;
+  bsw_range(B, lo, count);
   const uint32_t ngroups = gridDim.x * groups_per_block;
-  uint32_t item = B.item_lo + blockIdx.x * groups_per_block + group_in_block;
+  uint32_t item = lo + blockIdx.x * groups_per_block + group_in_block;
   for (;;) {
     if (B.work) {
       uint32_t t = 0;
-      if (g == 0) t = B.item_lo + atomicAdd(B.work, 1u);
+      if (g == 0) t = lo + atomicAdd(B.work, 1u);
       item = __shfl_sync(gmask, t, gw * G);
     }
     if (item >= count) break;
@@ -618,10 +628,11 @@ constexpr uint32_t kTbStageBytes = 4096;  // per warp: metadata + read + window 
 template <int G, int K, bool PACKED>
 __global__ void __launch_bounds__(128) bsw_tb_kernel(DevPairs P, BswLaunch B) {
   __shared__ uint32_t tb_stage[PACKED ? 4 : 1][PACKED ? kTbStageBytes / 4 : 1];
-  const uint32_t count = bsw_round_end(B);
+  uint32_t lo, count;
+  bsw_range(B, lo, count);
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
   const bool lead = (threadIdx.x & 31u) == 0u;
-  for (uint32_t item = B.item_lo + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  for (uint32_t item = lo + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
        item < count; item += warps) {
     const uint32_t pair = B.list ? B.list[item] : item;
     const DpEnd e = B.ends[item];
