@@ -931,7 +931,6 @@ def run_ours(args, rank, local, world, dist):
     else:
         tuning = autotune.tune_bsw_shape(ctx, 33, run_sync,
                                          device_name=torch.cuda.get_device_name(dev))
-    L.kira_gpu_profile(ctx.handle, 1)
     stage_ms = np.zeros(len(_abi.STAGES))
     sampler = ClockSampler(local)
     sampler.start()
@@ -955,16 +954,22 @@ def run_ours(args, rank, local, world, dist):
         launches += L.kira_gpu_launch_count() - c0
         e1.synchronize()
         total_ms += e0.elapsed_time(e1)
-        buf = (C.c_float * 8)()
-        k = L.kira_gpu_stage_times(ctx.handle, buf, 8)
-        stage_ms[:k] += np.array(buf[:k])
     torch.cuda.synchronize(dev)
     if dist is not None:
         dist.barrier()
     clocks = sampler.stop()
-    L.kira_gpu_profile(ctx.handle, 0)
     cells = int(t_cells.item())
     cells_step = cells // max(args.steps, 1)
+    # Stage times from the library's stage events, on separate steps after the timed
+    # ones (stage timing runs the stages one after another on one stream).
+    L.kira_gpu_profile(ctx.handle, 1)
+    for _ in range(PROFILED_STEPS):
+        flush.zero_()
+        step()
+        buf = (C.c_float * 8)()
+        k = L.kira_gpu_stage_times(ctx.handle, buf, 8)
+        stage_ms[:k] += np.array(buf[:k]) * args.steps / PROFILED_STEPS
+    L.kira_gpu_profile(ctx.handle, 0)
     total_ms = _max_over_ranks(total_ms, dist, dev)
     ms_per_step = total_ms / args.steps
     value = n * world * args.steps / (total_ms / 1e3)
@@ -1133,6 +1138,7 @@ def profile_figure(name: str, key: str):
         return None
 
 
+PROFILED_STEPS = 5
 ALU_PROBES = ("dpx_s16x2_addmax", "iadd3", "lop3", "imad", "lop3+imad", "dpx+imad")
 
 
