@@ -54,6 +54,7 @@ struct Bsw16Shape {
   static constexpr int kInterleave = G >= 32 ? 1 : 32 / G;
   // Bits of the word index in a row-max key ((h << kKeyBits) | (max - k) per half).
   static constexpr int kKeyBits = K <= 2 ? 1 : K <= 4 ? 2 : K <= 8 ? 3 : K <= 16 ? 4 : 5;
+  static_assert(K <= 32, "a row-max key holds 5 bits of word index");
 };
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
@@ -107,14 +108,19 @@ __device__ __forceinline__ void bsw16_realign(uint32_t (&ph)[K], uint32_t (&pe)[
   __syncwarp(gmask);
 }
 
-// Activity masks for a row of `row_len` cells: 0xFFFF per active half.
-template <int G, int K>
-__device__ __forceinline__ void bsw16_act(uint32_t (&act)[K], int32_t row_len, int32_t c0) {
-  constexpr int H = G * K;
-#pragma unroll
-  for (int k = 0; k < K; ++k)
-    act[k] = (c0 + k < row_len ? 0x0000FFFFu : 0u) | (H + c0 + k < row_len ? 0xFFFF0000u : 0u);
+// Activity mask of word k (0xFFFF per active half) from d0 = (2^15 + row_len - 1 -
+// cell) per half of word 0: bit 15 of a half is set while its cell is inside the
+// row, and PRMT replicates it over the half.
+__device__ __forceinline__ uint32_t bsw16_act(uint32_t d0, int k) {
+  uint32_t r;
+  asm("prmt.b32 %0, %1, 0, 0xBB99;" : "=r"(r) : "r"(d0 - (uint32_t)k * 0x10001u));
+  return r;
 }
+
+template <bool B>
+struct BoolTag {
+  static constexpr bool value = B;
+};
 
 template <int G, int K>
 __device__ __forceinline__ void bsw16_group_sweep(
@@ -136,20 +142,21 @@ __device__ __forceinline__ void bsw16_group_sweep(
   const uint32_t FOFS = isum(ge - gof, ge - gof);              // f = run - C_k + (ge - gof)
   const uint32_t C0 = isum(c0 * ge - gof, (H + c0) * ge - gof);  // C_k = idx*ge - gof
   const uint32_t GE2S = isum(ge, ge);
+  // Per-half cell index of word 0 under 2^15 (the activity masks' d0 less row_len - 1).
+  const uint32_t D0B = isum(0x8000 - 1 - c0, 0x8000 - 1 - H - c0);
 
-  int32_t prev_start = 1, prev_len = 0, act_len = -1;
+  int32_t prev_start = 1, prev_len = 0;
   int32_t best = 0, bi = 0, bj = 0, bq = 0, bqj = 0;
   uint32_t early = 0;
   uint32_t cells = 0;  // < 2^32: read_len * row length
   const int32_t drift = sp.adaptive ? sp.max_drift : 0;
   int32_t acenter = 1 + offset;
   const int32_t wl = (int32_t)w;
-  uint32_t ph[K], pe[K], act[K];
+  uint32_t ph[K], pe[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     ph[k] = B2;
     pe[k] = 0u;
-    act[k] = 0u;
   }
   // Window bytes of this lane's cells, four per word: word j holds cells 2j (low
   // half, high half) and 2j+1 (low, high) as bytes 0..3.
@@ -184,10 +191,6 @@ __device__ __forceinline__ void bsw16_group_sweep(
     cells += (uint32_t)row_len;
     const int32_t sft = js - prev_start - 1;
     if (sft != 0 && prev_len > 0) bsw16_realign<G, K>(ph, pe, sft, prev_len, rowbuf, c0, B2, gmask);
-    if (row_len != act_len) {
-      bsw16_act<G, K>(act, row_len, c0);
-      act_len = row_len;
-    }
     // Upper neighbours of the last word: the next lane's first word; for the last
     // lane the low half continues into cell H (lane 0's high half) and the high
     // half runs past the capacity (neutral).
@@ -201,19 +204,23 @@ __device__ __forceinline__ void bsw16_group_sweep(
     // The next row's new window byte if its band moves one column (index in
     // [js - 1, wl - 1]); used only by the group's last lane.
     const uint32_t wcur = wnext;
-    if ((K & 1) && gi == G - 1) wnext = __ldg(wn + js + min(2 * H - 1, wl - js - 1));
+    if (gi == G - 1) wnext = __ldg(wn + js + min(2 * H - 1, wl - js - 1));
     // Window bytes: cells past the window end repeat its last byte (never active
     // in this or a later row); cells past the row end hold real window bytes, so
     // a row whose band moved one column takes the previous row's bytes shifted by
     // one cell (the group's last lane fetches the one new byte).
     const int32_t wlast = wl - js;
-    if ((K & 1) && sft == 0 && prev_len > 0) {
+    if (sft == 0 && prev_len > 0) {
       const uint32_t n0 = __shfl_sync(gmask, wb[0], (gi + 1) & (G - 1), G);
 #pragma unroll
       for (int j = 0; j + 1 < NW; ++j) wb[j] = prmt(wb[j], wb[j + 1], 0x5432u);
-      // wcur: this row's new byte, loaded during the previous row on the guess that
-      // the band moves one column (wrow + min(2H - 1, wlast) for js = prev_start + 1).
-      wb[NW - 1] = gi == G - 1 ? prmt(n0, wcur, 0x0041u) : n0;
+      // The cell after this lane's last: the next lane's first (for the last lane,
+      // cell H in the low half and wcur in the high half). wcur: this row's new
+      // byte, loaded during the previous row on the guess that the band moves one
+      // column (wrow + min(2H - 1, wlast) for js = prev_start + 1).
+      const uint32_t nx = gi == G - 1 ? prmt(n0, wcur, 0x0041u) : n0;
+      // Odd K: the last word holds cell K - 1 alone; even K: cells K - 2 and K - 1.
+      wb[NW - 1] = (K & 1) ? nx : prmt(wb[NW - 1], nx, 0x5432u);
     } else {
 #pragma unroll
       for (int j = 0; j < NW; ++j) {
@@ -225,82 +232,99 @@ __device__ __forceinline__ void bsw16_group_sweep(
         wb[j] = prmt(prmt(b0, b1, 0x0040u), prmt(b2, b3, 0x0040u), 0x5410u);
       }
     }
-    // Pass 1: E (+ extend flag), H_diag + s, the diag-vs-E flag, max(Hdiag+s, E)
-    // and the F-scan operand G = max(Hdiag+s, E, 0) - gof + idx*ge. E is final
-    // here, so the previous row's E of word k is replaced at once (word k reads
-    // only words k and k + 1 of the previous row).
-    // Bit 7 of each byte of z: that cell's window base differs from the read base.
-    const uint32_t qb4 = qb * 0x01010101u;
-    uint32_t m1[K], gv[K], code[K];
-    uint32_t ck = C0, z = 0u;
+    // Activity: a row of at least 2H - 1 cells leaves at most its last cell (the
+    // last lane's high half of word K - 1) outside, masked by `lm`; shorter rows
+    // (band starts and ends, bands narrower than the shape) mask every word.
+    const uint32_t d0 = D0B + isum(row_len, row_len);
+    const uint32_t lm = (gi == G - 1 && row_len < 2 * H) ? 0x0000FFFFu : 0xFFFFFFFFu;
+    uint32_t m1[K], code[K];
+    auto sweep = [&](auto masked) {
+      constexpr bool MASKED = decltype(masked)::value;
+      // Pass 1: E (+ extend flag), H_diag + s, the diag-vs-E flag, max(Hdiag+s, E)
+      // and the F-scan operand G = max(Hdiag+s, E, 0) - gof + idx*ge (its lane
+      // maximum). E is final here, so the previous row's E of word k is replaced at
+      // once (word k reads only words k and k + 1 of the previous row).
+      // Bit 7 of each byte of z: that cell's window base differs from the read base.
+      const uint32_t qb4 = qb * 0x01010101u;
+      uint32_t z = 0u, lmax = 0u, gprev = 0u, glast = 0u;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      if ((k & 1) == 0) {
-        const uint32_t x = wb[k >> 1] ^ qb4;
-        z = x | ((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu);
+      for (int k = 0; k < K; ++k) {
+        if ((k & 1) == 0) {
+          const uint32_t x = wb[k >> 1] ^ qb4;
+          z = x | ((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu);
+        }
+        const uint32_t uh = k + 1 < K ? ph[k + 1 < K ? k + 1 : 0] : nh;
+        const uint32_t ue = k + 1 < K ? pe[k + 1 < K ? k + 1 : 0] : ne;
+        // Flag bits: 14..11 for words 0-1 of each group of four, 15..12 for words 2-3.
+        const uint32_t up = (k & 2) ? 1u : 0u;
+        const uint32_t t = uh - GOFS;                      // H_up - gof
+        const uint32_t e = __viaddmax_s16x2(ue, NGE2, t);  // max(E_up - ge, H_up - gof)
+        const uint32_t yee = e + (0x0FFF0FFFu << up | (up ? 0x00010001u : 0u)) - t;  // e > t
+        // 0xFFFF per mismatching half (sign of the cell's byte replicated).
+        const uint32_t ms = prmt(z, 0u, (k & 1) ? 0xBBAAu : 0x9988u);
+        const uint32_t s2 = bsel(MAT2, MIS2, ms);
+        const uint32_t hm = __viaddmax_s16x2(ph[k], s2, B2);     // max(Hdiag + s, 0)
+        const uint32_t y1 = hm + (0x40004000u << up) - e;  // hm >= e
+        const uint32_t mm = __vimax_s16x2_relu(hm, e);
+        code[k] = bsel(y1, yee, 0x10001000u << up);
+        m1[k] = mm;
+        const uint32_t gv = mm + C0 + (uint32_t)k * GE2S;
+        if (k & 1)
+          lmax = __vimax3_s16x2_relu(lmax, gprev, gv);
+        else if (k == K - 1)
+          lmax = __vimax_s16x2_relu(lmax, gv);
+        gprev = gv;
+        if (k == K - 1) glast = gv;
+        pe[k] = MASKED ? (e & bsw16_act(d0, k)) : k == K - 1 ? (e & lm) : e;
       }
-      const uint32_t uh = k + 1 < K ? ph[k + 1 < K ? k + 1 : 0] : nh;
-      const uint32_t ue = k + 1 < K ? pe[k + 1 < K ? k + 1 : 0] : ne;
-      // Flag bits: 14..11 for words 0-1 of each group of four, 15..12 for words 2-3.
-      const uint32_t up = (k & 2) ? 1u : 0u;
-      const uint32_t t = uh - GOFS;                      // H_up - gof
-      const uint32_t e = __viaddmax_s16x2(ue, NGE2, t);  // max(E_up - ge, H_up - gof)
-      const uint32_t yee = e + (0x0FFF0FFFu << up | (up ? 0x00010001u : 0u)) - t;  // e > t
-      // 0xFFFF per mismatching half (sign of the cell's byte replicated).
-      const uint32_t ms = prmt(z, 0u, (k & 1) ? 0xBBAAu : 0x9988u);
-      const uint32_t s2 = bsel(MAT2, MIS2, ms);
-      const uint32_t hm = __viaddmax_s16x2(ph[k], s2, B2);     // max(Hdiag + s, 0)
-      const uint32_t y1 = hm + (0x40004000u << up) - e;  // hm >= e
-      const uint32_t mm = __vimax_s16x2_relu(hm, e);
-      code[k] = bsel(y1, yee, 0x10001000u << up);
-      m1[k] = mm;
-      gv[k] = mm + ck;
-      pe[k] = e & act[k];
-      ck += GE2S;
-    }
-    uint32_t lmax = 0u;
+      // Cross-lane inclusive max-scan of G per half; exclusive value per lane, then
+      // the high half also sees every low-half cell (they precede it in the row).
+      uint32_t excl, tot, gp;
+      if constexpr (G == 2) {  // two lanes: one exchange gives both the prefix and the total
+        const uint32_t other = __shfl_xor_sync(gmask, lmax, 1, G);
+        gp = __shfl_xor_sync(gmask, glast, 1, G);
+        tot = __vimax_s16x2_relu(lmax, other);
+        excl = gi == 0 ? 0u : other;
+      } else {
+        uint32_t v = lmax;
 #pragma unroll
-    for (int k = 0; k < K; k += 2)
-      lmax = __vimax3_s16x2_relu(lmax, gv[k], k + 1 < K ? gv[k + 1 < K ? k + 1 : 0] : 0u);
-    // Cross-lane inclusive max-scan of G per half; exclusive value per lane, then
-    // the high half also sees every low-half cell (they precede it in the row).
-    uint32_t excl, tot, gp;
-    if constexpr (G == 2) {  // two lanes: one exchange gives both the prefix and the total
-      const uint32_t other = __shfl_xor_sync(gmask, lmax, 1, G);
-      gp = __shfl_xor_sync(gmask, gv[K - 1], 1, G);
-      tot = __vimax_s16x2_relu(lmax, other);
-      excl = gi == 0 ? 0u : other;
-    } else {
-      uint32_t v = lmax;
-#pragma unroll
-      for (int off = 1; off < G; off <<= 1) {
-        const uint32_t tt = __shfl_up_sync(gmask, v, off, G);
-        if (gi >= off) v = __vimax_s16x2_relu(v, tt);
+        for (int off = 1; off < G; off <<= 1) {
+          const uint32_t tt = __shfl_up_sync(gmask, v, off, G);
+          if (gi >= off) v = __vimax_s16x2_relu(v, tt);
+        }
+        excl = __shfl_up_sync(gmask, v, 1, G);
+        if (gi == 0) excl = 0u;
+        tot = __shfl_sync(gmask, v, G - 1, G);
+        gp = __shfl_sync(gmask, glast, (gi + G - 1) & (G - 1), G);
       }
-      excl = __shfl_up_sync(gmask, v, 1, G);
-      if (gi == 0) excl = 0u;
-      tot = __shfl_sync(gmask, v, G - 1, G);
-      gp = __shfl_sync(gmask, gv[K - 1], (gi + G - 1) & (G - 1), G);
-    }
-    excl = __vimax_s16x2_relu(excl, prmt(tot, 0u, 0x1054u));
-    if (gi == 0) gp = prmt(gp, 0u, 0x1054u);
+      excl = __vimax_s16x2_relu(excl, prmt(tot, 0u, 0x1054u));
+      if (gi == 0) gp = prmt(gp, 0u, 0x1054u);
 
-    // Pass 2: F, H, the remaining flags; neutralise inactive cells.
-    uint32_t run = excl;
-    ck = C0;
+      // Pass 2: F word by word (F' = max(F - ge, max(Hdiag+s, E) - gof), from the
+      // scan's value for word 0), H, the remaining flags; neutralise inactive cells.
+      uint32_t f = excl - C0 + FOFS;  // max over the row's earlier G - (idx - 1)*ge
+      uint32_t tprev = 0u;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const uint32_t up = (k & 2) ? 1u : 0u;
-      const uint32_t f = run - ck + FOFS;                // max_{k<idx} G - (idx-1)*ge
-      const uint32_t h = __vimax_s16x2_relu(m1[k], f);
-      const uint32_t y2 = m1[k] + (0x20002000u << up) - f;  // max(hm, e) >= f
-      const uint32_t yfe = gp + (0x08000800u << up) - run;  // F not extended
-      code[k] = bsel(bsel(code[k], y2, 0x20002000u << up), yfe, 0x08000800u << up);
-      run = __vimax_s16x2_relu(run, gv[k]);
-      gp = gv[k];
-      ph[k] = bsel(B2, h, act[k]);
-      ck += GE2S;
-    }
+      for (int k = 0; k < K; ++k) {
+        const uint32_t up = (k & 2) ? 1u : 0u;
+        const uint32_t h = __vimax_s16x2_relu(m1[k], f);
+        const uint32_t y2 = m1[k] + (0x20002000u << up) - f;  // max(hm, e) >= f
+        // F not extended: word 0 by the scan (the previous cell's operand reaches
+        // the running maximum), later words by F == max(hm, e)_prev - gof (F is
+        // never below it).
+        const uint32_t yfe = k == 0 ? gp + (0x08000800u << up) - excl
+                                    : tprev + (0x08000800u << up) - f;
+        code[k] = bsel(bsel(code[k], y2, 0x20002000u << up), yfe, 0x08000800u << up);
+        const uint32_t t = m1[k] - GOFS;
+        f = __viaddmax_s16x2(f, NGE2, t);
+        tprev = t;
+        ph[k] = MASKED ? bsel(B2, h, bsw16_act(d0, k)) : k == K - 1 ? bsel(B2, h, lm) : h;
+      }
+    };
+    if (row_len >= 2 * H - 1)
+      sweep(BoolTag<false>{});
+    else
+      sweep(BoolTag<true>{});
     // 4-bit codes of words 4x .. 4x+3 in one 32-bit slab: byte (w & 1) * 2 + half
     // holds word w's cell in its low nibble for w < 2, its high nibble for w >= 2.
     // Layout [row block][slab][row in block][lane] of 4-byte slabs: a group's lanes
