@@ -122,16 +122,62 @@ struct BoolTag {
   static constexpr bool value = B;
 };
 
+// Trace rows go to global memory in whole interleave blocks. A group stages the
+// slabs of its current block (kInterleave rows, kSlabs * 128 bytes, laid out exactly
+// as in global memory) in its own shared-memory strip and, once the block is complete
+// (or the sweep ends), one lane copies the strip out with one bulk asynchronous copy
+// (cp.async.bulk shared -> global): every DRAM sector is written whole, once, and the
+// per-row stores stay in shared memory. The strip is reused after the copy has read
+// it (wait_group.read before the next block's first store).
+struct TraceStage {
+  uint32_t* strip;    // this group's shared-memory strip (16-byte aligned)
+  uint8_t* gtrace;    // the item's trace slot in global memory
+  uint32_t bytes;     // kSlabs * 128: one interleave block
+  bool dirty = false;     // rows staged since the last copy
+  bool inflight = false;  // a copy of the strip may still be reading it
+  int32_t blk = 0;        // block the staged rows belong to
+
+  // Before a store into the strip: the previous copy has finished reading it.
+  __device__ __forceinline__ void ready(uint32_t g, uint32_t gmask) {
+    if (inflight) {
+      if (g == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+      __syncwarp(gmask);
+      inflight = false;
+    }
+  }
+  // Copies the staged block out (the group's stores are made visible to the async
+  // proxy first; lane 0 issues the copy).
+  __device__ __forceinline__ void flush(uint32_t g, uint32_t gmask) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp(gmask);
+    if (g == 0) {
+      const uint32_t src = (uint32_t)__cvta_generic_to_shared(strip);
+      const uint8_t* dst = gtrace + (size_t)blk * bytes;
+      asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                   :: "l"(dst), "r"(src), "r"(bytes) : "memory");
+      asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    }
+    inflight = true;
+    dirty = false;
+  }
+};
+
+// Waits until every bulk copy this thread issued has completed (end of a kernel).
+__device__ __forceinline__ void bulk_copies_done() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 template <int G, int K>
 __device__ __forceinline__ void bsw16_group_sweep(
     const uint8_t* __restrict__ rd, uint32_t q, const uint8_t* __restrict__ wn, uint32_t w,
     int32_t band, int32_t offset, int32_t abort_score, const SwParams& sp, int32_t bias,
-    uint16_t* rowbuf, uint8_t* __restrict__ trace, uint32_t* __restrict__ meta, uint32_t g,
-    uint32_t gmask, DpEnd& out, uint64_t& cells_out) {
+    uint16_t* rowbuf, uint32_t* strip, uint8_t* __restrict__ trace, uint32_t* __restrict__ meta,
+    uint32_t g, uint32_t gmask, DpEnd& out, uint64_t& cells_out) {
   constexpr int H = G * K;
   constexpr int NW = Bsw16Shape<G, K>::kWords;
   constexpr int NS = Bsw16Shape<G, K>::kSlabs;
-  constexpr int S = Bsw16Shape<G, K>::kRowStride;
+  constexpr int R = Bsw16Shape<G, K>::kInterleave;
+  TraceStage ts{strip, trace, (uint32_t)(NS * 128)};
   const int32_t gi = (int32_t)g;
   const int32_t c0 = gi * K;
   const int32_t match = sp.match, mism = sp.mismatch, gof = sp.gof, ge = sp.gap_extend;
@@ -178,6 +224,7 @@ __device__ __forceinline__ void bsw16_group_sweep(
     const int32_t je = min(center + band, wl);
     if (js > je) {  // mod.rs:1437-1444: row skipped, no centre / x-drop update
       if (g == 0) meta[i] = (1u << 11);
+      if (ts.dirty && (i & (R - 1)) == R - 1) ts.flush(g, gmask);
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         ph[k] = B2;
@@ -328,10 +375,11 @@ __device__ __forceinline__ void bsw16_group_sweep(
     // 4-bit codes of words 4x .. 4x+3 in one 32-bit slab: byte (w & 1) * 2 + half
     // holds word w's cell in its low nibble for w < 2, its high nibble for w >= 2.
     // Layout [row block][slab][row in block][lane] of 4-byte slabs: a group's lanes
-    // fill one contiguous G x 4-byte run per slab and row.
-    constexpr int R = Bsw16Shape<G, K>::kInterleave;
-    uint32_t* trow = reinterpret_cast<uint32_t*>(trace + (size_t)(i & ~(R - 1)) * S +
-                                                 (size_t)(i & (R - 1)) * (G * 4)) + g;
+    // fill one contiguous G x 4-byte run per slab and row. The block is staged in
+    // the group's strip and copied out whole (TraceStage).
+    ts.ready(g, gmask);
+    ts.blk = i / R;
+    uint32_t* trow = ts.strip + (i & (R - 1)) * G + g;
 #pragma unroll
     for (int x = 0; x < NS; ++x) {
       constexpr int kLast = K - 1;
@@ -341,6 +389,8 @@ __device__ __forceinline__ void bsw16_group_sweep(
       const uint32_t hi = a + 2 <= kLast ? prmt(code[c], code[d], 0x7531u) : 0u;  // bits 7..4
       trow[x * R * G] = bsel(hi, lo >> 3, 0x0F0F0F0Fu);
     }
+    ts.dirty = true;
+    if ((i & (R - 1)) == R - 1) ts.flush(g, gmask);
     if (g == 0) meta[i] = ((uint32_t)js << 11) | (uint32_t)row_len;
 
     // Row max and its first cell: per half the key (h << KB) | (KM - k), whose
@@ -394,6 +444,9 @@ __device__ __forceinline__ void bsw16_group_sweep(
       }
     }
   }
+  // The last (partial) block, then the strip is free for the group's next item.
+  if (ts.dirty) ts.flush(g, gmask);
+  ts.ready(g, gmask);
   if (bq > 0 && sat_add(bq, sp.clip) > best) {  // mod.rs:1575-1579
     best = bq;
     bi = (int32_t)q;

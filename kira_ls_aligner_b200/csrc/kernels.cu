@@ -573,15 +573,20 @@ __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B
 // Packed int16 sweep (bsw16.cuh); same item loop and outputs as bsw_dp_kernel.
 template <int G, int K, int T, int MINB>
 __global__ void __launch_bounds__(T, MINB) bsw16_dp_kernel(DevPairs P, BswLaunch B) {
-  extern __shared__ uint16_t bsw16_smem[];
+  // Dynamic shared memory: each group's trace strip (one interleave block,
+  // kSlabs * 128 bytes), then each group's realignment buffer (4 * G * K halves).
+  extern __shared__ __align__(128) uint32_t bsw16_smem[];
   constexpr int CAP = 2 * G * K;
+  constexpr uint32_t kStripWords = Bsw16Shape<G, K>::kSlabs * 32u;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t g = lane % G;
   const uint32_t gw = lane / G;
   const uint32_t gmask = (G == 32) ? 0xFFFFFFFFu : (((1u << G) - 1u) << (gw * G));
   const uint32_t groups_per_block = blockDim.x / G;
   const uint32_t group_in_block = threadIdx.x / G;
-  uint16_t* rowbuf = bsw16_smem + (size_t)group_in_block * 4u * G * K;  // per group
+  uint32_t* strip = bsw16_smem + (size_t)group_in_block * kStripWords;
+  uint16_t* rowbuf = reinterpret_cast<uint16_t*>(bsw16_smem + (size_t)(T / G) * kStripWords) +
+                     (size_t)group_in_block * 4u * G * K;  // per group
   uint32_t lo, count;
   bsw_range(B, lo, count);
   const uint32_t ngroups = gridDim.x * groups_per_block;
@@ -610,7 +615,7 @@ __global__ void __launch_bounds__(T, MINB) bsw16_dp_kernel(DevPairs P, BswLaunch
       continue;
     }
     bsw16_group_sweep<G, K>(P.read_seq + P.read_off[pair], q, P.win_seq + P.win_off[pair], w,
-                            band, offset, abort_score, B.sp, B.bias, rowbuf,
+                            band, offset, abort_score, B.sp, B.bias, rowbuf, strip,
                             B.tg.trace + (size_t)slot_item * B.tg.slot_bytes,
                             B.tg.meta + (size_t)slot_item * B.tg.meta_stride, g, gmask, end, cells);
     if (g == 0) {
@@ -619,6 +624,7 @@ __global__ void __launch_bounds__(T, MINB) bsw16_dp_kernel(DevPairs P, BswLaunch
     }
     if (!B.work) item += ngroups;
   }
+  if (g == 0) bulk_copies_done();  // the trace copies this lane issued
 }
 
 // One warp per item (warp_walk over the trace of shape <G, K>, packed or int32);
@@ -988,7 +994,8 @@ static cudaError_t launch_bsw16_shape(const DevPairs& P, const BswLaunch& B, uin
                                       int sms, cudaStream_t st, cudaEvent_t between, int parts) {
   cudaError_t e = cudaSuccess;
   if (parts & kBswPartDp) {
-    const size_t smem = (size_t)T * 8u * K;  // per group 4 * G * K halves
+    // per group: a trace strip of kSlabs * 128 bytes and 4 * G * K halves
+    const size_t smem = (size_t)(T / G) * Bsw16Shape<G, K>::kSlabs * 128u + (size_t)T * 8u * K;
     auto kern = bsw16_dp_kernel<G, K, T, MINB>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
