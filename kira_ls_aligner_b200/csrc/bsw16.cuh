@@ -108,6 +108,49 @@ __device__ __forceinline__ void bsw16_realign(uint32_t (&ph)[K], uint32_t (&pe)[
   __syncwarp(gmask);
 }
 
+// Realignment by one cell in registers (the band stayed, or moved two columns):
+// cell c <- old cell c - 1 (DOWN) or old cell c + 1 (up). The cells of the previous
+// row at and beyond its length are already neutral, so only the cells shifted in
+// from outside the row capacity (cell -1, cell 2H) need the neutral value: H = the
+// bias, E = 0. Word k's halves hold cells g*K + k and H + g*K + k, so the cell
+// before a lane's word 0 is the previous lane's word K - 1 (for lane 0: none in
+// the low half, cell H - 1 = the last lane's low half in the high half), and the
+// cell after its word K - 1 the next lane's word 0 (for the last lane: cell H =
+// lane 0's high half in the low half, none in the high half).
+template <int G, int K, bool DOWN>
+__device__ __forceinline__ void bsw16_shift1(uint32_t (&ph)[K], uint32_t (&pe)[K], uint32_t b2,
+                                             int32_t gi, uint32_t gmask) {
+  if constexpr (DOWN) {
+    uint32_t h = __shfl_sync(gmask, ph[K - 1], (gi + G - 1) & (G - 1), G);
+    uint32_t e = __shfl_sync(gmask, pe[K - 1], (gi + G - 1) & (G - 1), G);
+    if (gi == 0) {
+      h = prmt(b2, h, 0x5410u);
+      e = prmt(0u, e, 0x5410u);
+    }
+#pragma unroll
+    for (int k = K - 1; k > 0; --k) {
+      ph[k] = ph[k - 1];
+      pe[k] = pe[k - 1];
+    }
+    ph[0] = h;
+    pe[0] = e;
+  } else {
+    uint32_t h = __shfl_sync(gmask, ph[0], (gi + 1) & (G - 1), G);
+    uint32_t e = __shfl_sync(gmask, pe[0], (gi + 1) & (G - 1), G);
+    if (gi == G - 1) {
+      h = prmt(h, b2, 0x5432u);
+      e = prmt(e, 0u, 0x5432u);
+    }
+#pragma unroll
+    for (int k = 0; k + 1 < K; ++k) {
+      ph[k] = ph[k + 1];
+      pe[k] = pe[k + 1];
+    }
+    ph[K - 1] = h;
+    pe[K - 1] = e;
+  }
+}
+
 // Activity mask of word k (0xFFFF per active half) from d0 = (2^15 + row_len - 1 -
 // cell) per half of word 0: bit 15 of a half is set while its cell is inside the
 // row, and PRMT replicates it over the half.
@@ -116,11 +159,6 @@ __device__ __forceinline__ uint32_t bsw16_act(uint32_t d0, int k) {
   asm("prmt.b32 %0, %1, 0, 0xBB99;" : "=r"(r) : "r"(d0 - (uint32_t)k * 0x10001u));
   return r;
 }
-
-template <bool B>
-struct BoolTag {
-  static constexpr bool value = B;
-};
 
 // Trace rows go to global memory in whole interleave blocks. A group stages the
 // slabs of its current block (kInterleave rows, kSlabs * 128 bytes, laid out exactly
@@ -237,7 +275,14 @@ __device__ __forceinline__ void bsw16_group_sweep(
     const int32_t row_len = je - js + 1;
     cells += (uint32_t)row_len;
     const int32_t sft = js - prev_start - 1;
-    if (sft != 0 && prev_len > 0) bsw16_realign<G, K>(ph, pe, sft, prev_len, rowbuf, c0, B2, gmask);
+    if (sft != 0 && prev_len > 0) {
+      if (sft == -1)
+        bsw16_shift1<G, K, true>(ph, pe, B2, gi, gmask);
+      else if (sft == 1)
+        bsw16_shift1<G, K, false>(ph, pe, B2, gi, gmask);
+      else
+        bsw16_realign<G, K>(ph, pe, sft, prev_len, rowbuf, c0, B2, gmask);
+    }
     // Upper neighbours of the last word: the next lane's first word; for the last
     // lane the low half continues into cell H (lane 0's high half) and the high
     // half runs past the capacity (neutral).
@@ -268,7 +313,7 @@ __device__ __forceinline__ void bsw16_group_sweep(
       const uint32_t nx = gi == G - 1 ? prmt(n0, wcur, 0x0041u) : n0;
       // Odd K: the last word holds cell K - 1 alone; even K: cells K - 2 and K - 1.
       wb[NW - 1] = (K & 1) ? nx : prmt(wb[NW - 1], nx, 0x5432u);
-    } else {
+    } else if (sft != -1 || prev_len == 0) {  // (the band stayed: same window bytes)
 #pragma unroll
       for (int j = 0; j < NW; ++j) {
         const int ka = 2 * j, kb = 2 * j + 1 < K ? 2 * j + 1 : K - 1;
@@ -279,14 +324,12 @@ __device__ __forceinline__ void bsw16_group_sweep(
         wb[j] = prmt(prmt(b0, b1, 0x0040u), prmt(b2, b3, 0x0040u), 0x5410u);
       }
     }
-    // Activity: a row of at least 2H - 1 cells leaves at most its last cell (the
-    // last lane's high half of word K - 1) outside, masked by `lm`; shorter rows
-    // (band starts and ends, bands narrower than the shape) mask every word.
+    // Activity: every word is masked in every row. (Groups of a warp sweep
+    // different pairs; a separate unmasked form for full rows made the warp run
+    // both forms whenever any of its groups had a short row at a band edge.)
     const uint32_t d0 = D0B + isum(row_len, row_len);
-    const uint32_t lm = (gi == G - 1 && row_len < 2 * H) ? 0x0000FFFFu : 0xFFFFFFFFu;
     uint32_t m1[K], code[K];
-    auto sweep = [&](auto masked) {
-      constexpr bool MASKED = decltype(masked)::value;
+    {
       // Pass 1: E (+ extend flag), H_diag + s, the diag-vs-E flag, max(Hdiag+s, E)
       // and the F-scan operand G = max(Hdiag+s, E, 0) - gof + idx*ge (its lane
       // maximum). E is final here, so the previous row's E of word k is replaced at
@@ -322,7 +365,7 @@ __device__ __forceinline__ void bsw16_group_sweep(
           lmax = __vimax_s16x2_relu(lmax, gv);
         gprev = gv;
         if (k == K - 1) glast = gv;
-        pe[k] = MASKED ? (e & bsw16_act(d0, k)) : k == K - 1 ? (e & lm) : e;
+        pe[k] = e & bsw16_act(d0, k);
       }
       // Cross-lane inclusive max-scan of G per half; exclusive value per lane, then
       // the high half also sees every low-half cell (they precede it in the row).
@@ -365,13 +408,9 @@ __device__ __forceinline__ void bsw16_group_sweep(
         const uint32_t t = m1[k] - GOFS;
         f = __viaddmax_s16x2(f, NGE2, t);
         tprev = t;
-        ph[k] = MASKED ? bsel(B2, h, bsw16_act(d0, k)) : k == K - 1 ? bsel(B2, h, lm) : h;
+        ph[k] = bsel(B2, h, bsw16_act(d0, k));
       }
-    };
-    if (row_len >= 2 * H - 1)
-      sweep(BoolTag<false>{});
-    else
-      sweep(BoolTag<true>{});
+    }
     // 4-bit codes of words 4x .. 4x+3 in one 32-bit slab: byte (w & 1) * 2 + half
     // holds word w's cell in its low nibble for w < 2, its high nibble for w >= 2.
     // Layout [row block][slab][row in block][lane] of 4-byte slabs: a group's lanes
