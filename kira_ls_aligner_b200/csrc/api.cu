@@ -143,6 +143,10 @@ struct kira_ctx {
   uint32_t last_rounds = 0;              // trace rounds of the last kira_gpu_bsw_batch
   cudaStream_t aux = nullptr;            // second half of a split banded-SW stage
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // Bucketed banded SW: one stream per band class (DP then traceback), forked from
+  // and joined back into the context's stream.
+  cudaStream_t cls_st[kBandClasses] = {};
+  cudaEvent_t ev_cls_fork = nullptr, ev_cls_join[kBandClasses] = {};
   cudaStream_t h2d = nullptr, d2h = nullptr;   // copy streams of the chunked host path
   int64_t chunk_pairs = -1;                    // chunked host path: -1 auto, 0 off, else pairs
   int wfa_lanes = 0;                           // WFA lanes per pair: 0 auto, else 8 / 16 / 32
@@ -660,6 +664,31 @@ cudaError_t enqueue_bucketed(kira_ctx* ctx, const DevPairs& D, const BucketRun& 
   cudaError_t e = cudaMemsetAsync(R.work, 0, 4ull * R.nwork, st);
   if (e != cudaSuccess) return e;
   mark(ctx, 2, st);
+  int classes = 0;
+  for (int c = 0; c < kBandClasses; ++c) classes += R.cnt[c] ? 1 : 0;
+  if (R.one_round && !ctx->profile && classes > 1) {
+    // Every class on its own stream, widest first on the context's stream: the
+    // classes' DP sweeps fill each other's last partial waves, and each class's
+    // traceback overlaps the others' sweeps. (Their trace slots, ends, CIGAR slots
+    // and work counters are disjoint.) Stage timing keeps the serial form below.
+    if ((e = cudaEventRecord(ctx->ev_cls_fork, st)) != cudaSuccess) return e;
+    bool first = true;
+    for (int c = kBandClasses - 1; c >= 0; --c) {
+      if (!R.cnt[c]) continue;
+      cudaStream_t s = first ? st : ctx->cls_st[c];
+      if (!first && (e = cudaStreamWaitEvent(s, ctx->ev_cls_fork, 0)) != cudaSuccess) return e;
+      if ((e = launch_bsw(R.shape[c], D, R.L[c], R.cnt[c], ctx->sms, s)) != cudaSuccess) return e;
+      if (!first && (e = cudaEventRecord(ctx->ev_cls_join[c], s)) != cudaSuccess) return e;
+      first = false;
+    }
+    first = true;
+    for (int c = kBandClasses - 1; c >= 0; --c) {
+      if (!R.cnt[c]) continue;
+      if (!first && (e = cudaStreamWaitEvent(st, ctx->ev_cls_join[c], 0)) != cudaSuccess) return e;
+      first = false;
+    }
+    return cudaSuccess;
+  }
   if (R.one_round) {
     // Widest class first (longest rows), then the narrower ones fill in behind it.
     for (int c = kBandClasses - 1; c >= 0; --c)
@@ -690,31 +719,64 @@ int plan_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const k
   cudaError_t cerr = cudaSuccess;
   const uint32_t n = P.n;
   std::vector<uint8_t> cls(n);
+  // Classes and per-class maxima, part by part on the context's host threads.
+  struct ClassPart {
+    uint32_t cnt[kBandClasses], qmax[kBandClasses], bmax[kBandClasses], q, w;
+  };
+  const uint32_t nparts = host_parts(n);
+  std::vector<ClassPart> cp(nparts);
+  host_for(ctx, n, [&](uint32_t lo, uint32_t hi, uint32_t k) {
+    ClassPart x{};
+    for (uint32_t i = lo; i < hi; ++i) {
+      const uint32_t b = (uint32_t)std::max(P.bandwidth ? P.bandwidth[i] : cfg.bandwidth, 1);
+      const int c = band_class(b);
+      cls[i] = (uint8_t)c;
+      ++x.cnt[c];
+      x.qmax[c] = std::max(x.qmax[c], P.read_len[i]);
+      x.bmax[c] = std::max(x.bmax[c], b);
+      x.q = std::max(x.q, P.read_len[i]);
+      x.w = std::max(x.w, P.win_len[i]);
+    }
+    cp[k] = x;
+  });
   uint32_t cnt[kBandClasses] = {}, qmax[kBandClasses] = {}, bmax[kBandClasses] = {};
   uint32_t qall = 0, wall = 0;
-  for (uint32_t i = 0; i < n; ++i) {
-    const uint32_t b = (uint32_t)std::max(P.bandwidth ? P.bandwidth[i] : cfg.bandwidth, 1);
-    const int c = band_class(b);
-    cls[i] = (uint8_t)c;
-    ++cnt[c];
-    qmax[c] = std::max(qmax[c], P.read_len[i]);
-    bmax[c] = std::max(bmax[c], b);
-    qall = std::max(qall, P.read_len[i]);
-    wall = std::max(wall, P.win_len[i]);
+  for (const ClassPart& x : cp) {
+    for (int c = 0; c < kBandClasses; ++c) {
+      cnt[c] += x.cnt[c];
+      qmax[c] = std::max(qmax[c], x.qmax[c]);
+      bmax[c] = std::max(bmax[c], x.bmax[c]);
+    }
+    qall = std::max(qall, x.q);
+    wall = std::max(wall, x.w);
   }
   uint32_t base[kBandClasses + 1] = {};
   for (int c = 0; c < kBandClasses; ++c) base[c + 1] = base[c] + cnt[c];
   // Order: band class, then read length descending (the tail of a launch is
   // short), stable. Counting sort on (class, qall - q) when the key range is
-  // modest, else a comparison sort.
+  // modest (per-part histograms, then each part scatters from its own offsets,
+  // which keeps the order stable), else a comparison sort.
   std::vector<uint32_t> list(n);
   const uint64_t nkeys = (uint64_t)kBandClasses * (qall + 1);
-  if (nkeys <= 4ull * n + (1u << 16)) {
-    std::vector<uint32_t> at(nkeys + 1, 0);
+  if (nkeys <= 4ull * n + (1u << 16) && nkeys * nparts <= (64ull << 20)) {
+    std::vector<uint32_t> at(nkeys * nparts, 0);  // [part][key]: counts, then offsets
     auto key = [&](uint32_t i) { return (uint64_t)cls[i] * (qall + 1) + (qall - P.read_len[i]); };
-    for (uint32_t i = 0; i < n; ++i) ++at[key(i) + 1];
-    for (uint64_t k = 0; k < nkeys; ++k) at[k + 1] += at[k];
-    for (uint32_t i = 0; i < n; ++i) list[at[key(i)]++] = i;
+    host_for(ctx, n, [&](uint32_t lo, uint32_t hi, uint32_t k) {
+      uint32_t* h = at.data() + (uint64_t)k * nkeys;
+      for (uint32_t i = lo; i < hi; ++i) ++h[key(i)];
+    });
+    uint32_t run = 0;
+    for (uint64_t kk = 0; kk < nkeys; ++kk)
+      for (uint32_t part = 0; part < nparts; ++part) {
+        uint32_t& v = at[(uint64_t)part * nkeys + kk];
+        const uint32_t c = v;
+        v = run;
+        run += c;
+      }
+    host_for(ctx, n, [&](uint32_t lo, uint32_t hi, uint32_t k) {
+      uint32_t* h = at.data() + (uint64_t)k * nkeys;
+      for (uint32_t i = lo; i < hi; ++i) list[h[key(i)]++] = i;
+    });
   } else {
     uint32_t at[kBandClasses];
     for (int c = 0; c < kBandClasses; ++c) at[c] = base[c];
@@ -768,6 +830,17 @@ int plan_bucketed(kira_ctx* ctx, const kira_pairs& P, const DevPairs& D, const k
   }
   const uint32_t nwork = std::max<uint32_t>(rounds_before[kBandClasses], 1);
   ctx->last_rounds = rounds_before[kBandClasses];
+  if (one_round) {  // the class streams of enqueue_bucketed (created outside any capture)
+    if (!ctx->ev_cls_fork)
+      KIRA_CUDA(cudaEventCreateWithFlags(&ctx->ev_cls_fork, cudaEventDisableTiming));
+    for (int c = 0; c < kBandClasses; ++c) {
+      if (!cnt[c]) continue;
+      if (!ctx->cls_st[c])
+        KIRA_CUDA(cudaStreamCreateWithFlags(&ctx->cls_st[c], cudaStreamNonBlocking));
+      if (!ctx->ev_cls_join[c])
+        KIRA_CUDA(cudaEventCreateWithFlags(&ctx->ev_cls_join[c], cudaEventDisableTiming));
+    }
+  }
   const uint32_t cap = qall + wall + 2;
   KIRA_DBUF(dlist, uint32_t, B_SW_LIST, n);
   KIRA_DBUF(trace, uint8_t, B_TRACE, tbytes);
@@ -1564,6 +1637,14 @@ void kira_gpu_destroy(kira_ctx* ctx) {
   }
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  for (int c = 0; c < kBandClasses; ++c) {
+    if (ctx->cls_st[c]) {
+      cudaStreamSynchronize(ctx->cls_st[c]);
+      cudaStreamDestroy(ctx->cls_st[c]);
+    }
+    if (ctx->ev_cls_join[c]) cudaEventDestroy(ctx->ev_cls_join[c]);
+  }
+  if (ctx->ev_cls_fork) cudaEventDestroy(ctx->ev_cls_fork);
   if (ctx->stage) cudaFreeHost(ctx->stage);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
