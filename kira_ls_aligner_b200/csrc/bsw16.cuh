@@ -50,11 +50,16 @@ struct Bsw16Shape {
   static constexpr int kRowStride = G * kLaneBytes;
   // Rows interleave in blocks of kInterleave: a block stores slab by slab, and in
   // each slab row by row, so one 128-byte line holds one slab of kInterleave
-  // consecutive rows (the cells a diagonal traceback run reads next).
-  static constexpr int kInterleave = G >= 32 ? 1 : 32 / G;
+  // consecutive rows (the cells a diagonal traceback run reads next). One lane per
+  // pair interleaves 8 rows (a 32-byte sector per slab), which keeps its
+  // shared-memory staging strip (one block) small.
+  static constexpr int kInterleave = G == 1 ? 8 : G >= 32 ? 1 : 32 / G;
+  // Bytes of one interleave block of a group (its shared-memory staging strip).
+  static constexpr int kStripBytes = kSlabs * kInterleave * G * 4;
   // Bits of the word index in a row-max key ((h << kKeyBits) | (max - k) per half).
-  static constexpr int kKeyBits = K <= 2 ? 1 : K <= 4 ? 2 : K <= 8 ? 3 : K <= 16 ? 4 : 5;
-  static_assert(K <= 32, "a row-max key holds 5 bits of word index");
+  static constexpr int kKeyBits =
+      K <= 2 ? 1 : K <= 4 ? 2 : K <= 8 ? 3 : K <= 16 ? 4 : K <= 32 ? 5 : 6;
+  static_assert(K <= 64, "a row-max key holds 6 bits of word index");
 };
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
@@ -77,6 +82,45 @@ __host__ __device__ __forceinline__ uint32_t pk2(int32_t v) {
 // half when both halves' results stay inside [0, 2^16).
 __host__ __device__ __forceinline__ uint32_t isum(int32_t lo, int32_t hi) {
   return (uint32_t)hi * 65536u + (uint32_t)lo;
+}
+
+// __shfl_sync within a group of G lanes (a group of one lane reads itself).
+template <int G>
+__device__ __forceinline__ uint32_t gshfl(uint32_t gmask, uint32_t v, int src) {
+  if constexpr (G == 1) return v;
+  else return __shfl_sync(gmask, v, src, G);
+}
+
+// Window bytes of a lane's cells as the sweep keeps them (word j: bytes of cells 2j
+// and 2j + 1 of the low half and of the high half, in the order lo 2j, hi 2j,
+// lo 2j+1, hi 2j+1), from the two runs of bytes starting at `a` (low-half cells) and
+// `b` (high-half cells). Aligned 4-byte loads and funnel shifts: no word loaded
+// lies past the one holding the window's last byte `last`, so bytes past the window
+// end are whatever that word holds (those cells are never active).
+template <int K>
+__device__ __forceinline__ void bsw16_window_words(uint32_t (&wb)[(K + 1) / 2],
+                                                   const uint8_t* a, const uint8_t* b,
+                                                   const uint8_t* last) {
+  constexpr int NW = (K + 1) / 2;
+  constexpr int NU = (K + 3) / 4;  // 4-byte runs per half: words 2m and 2m + 1
+  const uintptr_t la = reinterpret_cast<uintptr_t>(last) & ~static_cast<uintptr_t>(3);
+  const uintptr_t a0 = reinterpret_cast<uintptr_t>(a) & ~static_cast<uintptr_t>(3);
+  const uintptr_t b0 = reinterpret_cast<uintptr_t>(b) & ~static_cast<uintptr_t>(3);
+  const uint32_t sa = (static_cast<uint32_t>(reinterpret_cast<uintptr_t>(a)) & 3u) * 8u;
+  const uint32_t sb = (static_cast<uint32_t>(reinterpret_cast<uintptr_t>(b)) & 3u) * 8u;
+  auto at = [la](uintptr_t x) {
+    return __ldg(reinterpret_cast<const uint32_t*>(x < la ? x : la));
+  };
+  uint32_t wa = at(a0), wv = at(b0);
+#pragma unroll
+  for (int m = 0; m < NU; ++m) {
+    const uint32_t na = at(a0 + 4u * (m + 1)), nb = at(b0 + 4u * (m + 1));
+    const uint32_t ua = __funnelshift_r(wa, na, sa), ub = __funnelshift_r(wv, nb, sb);
+    wb[2 * m] = prmt(ua, ub, 0x5140u);
+    if (2 * m + 1 < NW) wb[2 * m + 1 < NW ? 2 * m + 1 : 0] = prmt(ua, ub, 0x7362u);
+    wa = na;
+    wv = nb;
+  }
 }
 
 // Realign the packed previous row by `s` cells (cell c <- old cell c + s); old
@@ -121,8 +165,8 @@ template <int G, int K, bool DOWN>
 __device__ __forceinline__ void bsw16_shift1(uint32_t (&ph)[K], uint32_t (&pe)[K], uint32_t b2,
                                              int32_t gi, uint32_t gmask) {
   if constexpr (DOWN) {
-    uint32_t h = __shfl_sync(gmask, ph[K - 1], (gi + G - 1) & (G - 1), G);
-    uint32_t e = __shfl_sync(gmask, pe[K - 1], (gi + G - 1) & (G - 1), G);
+    uint32_t h = gshfl<G>(gmask, ph[K - 1], (gi + G - 1) & (G - 1));
+    uint32_t e = gshfl<G>(gmask, pe[K - 1], (gi + G - 1) & (G - 1));
     if (gi == 0) {
       h = prmt(b2, h, 0x5410u);
       e = prmt(0u, e, 0x5410u);
@@ -135,8 +179,8 @@ __device__ __forceinline__ void bsw16_shift1(uint32_t (&ph)[K], uint32_t (&pe)[K
     ph[0] = h;
     pe[0] = e;
   } else {
-    uint32_t h = __shfl_sync(gmask, ph[0], (gi + 1) & (G - 1), G);
-    uint32_t e = __shfl_sync(gmask, pe[0], (gi + 1) & (G - 1), G);
+    uint32_t h = gshfl<G>(gmask, ph[0], (gi + 1) & (G - 1));
+    uint32_t e = gshfl<G>(gmask, pe[0], (gi + 1) & (G - 1));
     if (gi == G - 1) {
       h = prmt(h, b2, 0x5432u);
       e = prmt(e, 0u, 0x5432u);
@@ -161,7 +205,7 @@ __device__ __forceinline__ uint32_t bsw16_act(uint32_t d0, int k) {
 }
 
 // Trace rows go to global memory in whole interleave blocks. A group stages the
-// slabs of its current block (kInterleave rows, kSlabs * 128 bytes, laid out exactly
+// slabs of its current block (kInterleave rows, kStripBytes, laid out exactly
 // as in global memory) in its own shared-memory strip and, once the block is complete
 // (or the sweep ends), one lane copies the strip out with one bulk asynchronous copy
 // (cp.async.bulk shared -> global): every DRAM sector is written whole, once, and the
@@ -170,7 +214,7 @@ __device__ __forceinline__ uint32_t bsw16_act(uint32_t d0, int k) {
 struct TraceStage {
   uint32_t* strip;    // this group's shared-memory strip (16-byte aligned)
   uint8_t* gtrace;    // the item's trace slot in global memory
-  uint32_t bytes;     // kSlabs * 128: one interleave block
+  uint32_t bytes;     // kStripBytes: one interleave block
   bool dirty = false;     // rows staged since the last copy
   bool inflight = false;  // a copy of the strip may still be reading it
   int32_t blk = 0;        // block the staged rows belong to
@@ -215,7 +259,7 @@ __device__ __forceinline__ void bsw16_group_sweep(
   constexpr int NW = Bsw16Shape<G, K>::kWords;
   constexpr int NS = Bsw16Shape<G, K>::kSlabs;
   constexpr int R = Bsw16Shape<G, K>::kInterleave;
-  TraceStage ts{strip, trace, (uint32_t)(NS * 128)};
+  TraceStage ts{strip, trace, (uint32_t)Bsw16Shape<G, K>::kStripBytes};
   const int32_t gi = (int32_t)g;
   const int32_t c0 = gi * K;
   const int32_t match = sp.match, mism = sp.mismatch, gof = sp.gof, ge = sp.gap_extend;
@@ -286,8 +330,8 @@ __device__ __forceinline__ void bsw16_group_sweep(
     // Upper neighbours of the last word: the next lane's first word; for the last
     // lane the low half continues into cell H (lane 0's high half) and the high
     // half runs past the capacity (neutral).
-    uint32_t nh = __shfl_sync(gmask, ph[0], (gi + 1) & (G - 1), G);
-    uint32_t ne = __shfl_sync(gmask, pe[0], (gi + 1) & (G - 1), G);
+    uint32_t nh = gshfl<G>(gmask, ph[0], (gi + 1) & (G - 1));
+    uint32_t ne = gshfl<G>(gmask, pe[0], (gi + 1) & (G - 1));
     if (gi == G - 1) {
       nh = prmt(nh, B2, 0x5432u);
       ne = prmt(ne, 0u, 0x5432u);
@@ -297,32 +341,24 @@ __device__ __forceinline__ void bsw16_group_sweep(
     // [js - 1, wl - 1]); used only by the group's last lane.
     const uint32_t wcur = wnext;
     if (gi == G - 1) wnext = __ldg(wn + js + min(2 * H - 1, wl - js - 1));
-    // Window bytes: cells past the window end repeat its last byte (never active
+    // Window bytes: cells past the window end hold any byte (they are never active
     // in this or a later row); cells past the row end hold real window bytes, so
     // a row whose band moved one column takes the previous row's bytes shifted by
-    // one cell (the group's last lane fetches the one new byte).
-    const int32_t wlast = wl - js;
+    // one cell (the group's last lane fetches the one new byte), and a row whose
+    // band stayed keeps them.
     if (sft == 0 && prev_len > 0) {
-      const uint32_t n0 = __shfl_sync(gmask, wb[0], (gi + 1) & (G - 1), G);
+      const uint32_t n0 = gshfl<G>(gmask, wb[0], (gi + 1) & (G - 1));
 #pragma unroll
       for (int j = 0; j + 1 < NW; ++j) wb[j] = prmt(wb[j], wb[j + 1], 0x5432u);
       // The cell after this lane's last: the next lane's first (for the last lane,
       // cell H in the low half and wcur in the high half). wcur: this row's new
       // byte, loaded during the previous row on the guess that the band moves one
-      // column (wrow + min(2H - 1, wlast) for js = prev_start + 1).
+      // column (wrow + min(2H - 1, wl - js) for js = prev_start + 1).
       const uint32_t nx = gi == G - 1 ? prmt(n0, wcur, 0x0041u) : n0;
       // Odd K: the last word holds cell K - 1 alone; even K: cells K - 2 and K - 1.
       wb[NW - 1] = (K & 1) ? nx : prmt(wb[NW - 1], nx, 0x5432u);
     } else if (sft != -1 || prev_len == 0) {  // (the band stayed: same window bytes)
-#pragma unroll
-      for (int j = 0; j < NW; ++j) {
-        const int ka = 2 * j, kb = 2 * j + 1 < K ? 2 * j + 1 : K - 1;
-        const uint32_t b0 = __ldg(wrow + min(c0 + ka, wlast));
-        const uint32_t b1 = __ldg(wrow + min(H + c0 + ka, wlast));
-        const uint32_t b2 = __ldg(wrow + min(c0 + kb, wlast));
-        const uint32_t b3 = __ldg(wrow + min(H + c0 + kb, wlast));
-        wb[j] = prmt(prmt(b0, b1, 0x0040u), prmt(b2, b3, 0x0040u), 0x5410u);
-      }
+      bsw16_window_words<K>(wb, wrow + c0, wrow + H + c0, wn + (wl - 1));
     }
     // Activity: every word is masked in every row. (Groups of a warp sweep
     // different pairs; a separate unmasked form for full rows made the warp run
@@ -336,7 +372,8 @@ __device__ __forceinline__ void bsw16_group_sweep(
       // once (word k reads only words k and k + 1 of the previous row).
       // Bit 7 of each byte of z: that cell's window base differs from the read base.
       const uint32_t qb4 = qb * 0x01010101u;
-      uint32_t z = 0u, lmax = 0u, gprev = 0u, glast = 0u;
+      // Two running maxima (alternate word pairs) halve the dependent chain.
+      uint32_t z = 0u, lmax = 0u, lmax1 = 0u, gprev = 0u, glast = 0u;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if ((k & 1) == 0) {
@@ -359,10 +396,13 @@ __device__ __forceinline__ void bsw16_group_sweep(
         code[k] = bsel(y1, yee, 0x10001000u << up);
         m1[k] = mm;
         const uint32_t gv = mm + C0 + (uint32_t)k * GE2S;
-        if (k & 1)
+        if ((k & 1) && (k & 2))
+          lmax1 = __vimax3_s16x2_relu(lmax1, gprev, gv);
+        else if (k & 1)
           lmax = __vimax3_s16x2_relu(lmax, gprev, gv);
         else if (k == K - 1)
-          lmax = __vimax_s16x2_relu(lmax, gv);
+          lmax = __vimax3_s16x2_relu(lmax, lmax1, gv);
+        if (k == K - 1 && (k & 1)) lmax = __vimax_s16x2_relu(lmax, lmax1);
         gprev = gv;
         if (k == K - 1) glast = gv;
         pe[k] = e & bsw16_act(d0, k);
@@ -370,7 +410,11 @@ __device__ __forceinline__ void bsw16_group_sweep(
       // Cross-lane inclusive max-scan of G per half; exclusive value per lane, then
       // the high half also sees every low-half cell (they precede it in the row).
       uint32_t excl, tot, gp;
-      if constexpr (G == 2) {  // two lanes: one exchange gives both the prefix and the total
+      if constexpr (G == 1) {  // one lane: nothing before it, the total is its own
+        excl = 0u;
+        tot = lmax;
+        gp = glast;
+      } else if constexpr (G == 2) {  // two lanes: one exchange gives both the prefix and the total
         const uint32_t other = __shfl_xor_sync(gmask, lmax, 1, G);
         gp = __shfl_xor_sync(gmask, glast, 1, G);
         tot = __vimax_s16x2_relu(lmax, other);
@@ -437,15 +481,19 @@ __device__ __forceinline__ void bsw16_group_sweep(
     // lane (low-half cells precede high-half cells on ties).
     constexpr int KB = Bsw16Shape<G, K>::kKeyBits;
     constexpr uint32_t KM = (1u << KB) - 1u;
-    uint32_t mx = 0u;
+    uint32_t mx = 0u, mx1 = 0u;  // two running maxima (alternate word pairs)
 #pragma unroll
     for (int k = 0; k < K; k += 2) {
       const uint32_t ka = ph[k] * (1u << KB) + (KM - (uint32_t)k) * 0x10001u;
       const uint32_t kb = k + 1 < K ? ph[k + 1 < K ? k + 1 : 0] * (1u << KB) +
                                           (KM - (uint32_t)(k + 1)) * 0x10001u
                                     : 0u;
-      mx = __vimax3_u16x2(mx, ka, kb);
+      if (k & 2)
+        mx1 = __vimax3_u16x2(mx1, ka, kb);
+      else
+        mx = __vimax3_u16x2(mx, ka, kb);
     }
+    mx = __vimax3_u16x2(mx, mx1, 0u);
     const uint32_t vlo = (mx & 0xFFFFu) >> KB, vhi = mx >> (16 + KB);
     const bool lo_first = vlo >= vhi;
     const uint32_t idx = lo_first ? (uint32_t)c0 + (KM - (mx & KM))

@@ -214,7 +214,8 @@ inline uint32_t shape_row_stride(const BswShapeInfo& s) {
 }
 // Rows per interleave block of the packed trace (Bsw16Shape::kInterleave).
 inline uint32_t shape_row_interleave(const BswShapeInfo& s) {
-  return s.packed && s.g < 32 ? 32u / (uint32_t)s.g : 1u;
+  if (!s.packed) return 1u;
+  return s.g == 1 ? 8u : s.g < 32 ? 32u / (uint32_t)s.g : 1u;
 }
 // Bytes of one item's trace slot for reads of up to `max_q` bases: rows 0..max_q
 // rounded up to whole interleave blocks, then to 16 bytes.
@@ -236,7 +237,9 @@ inline int32_t packed_bias(const BswShapeInfo& s, const SwParams& sp) {
 }
 
 // Bits of the word index in the packed sweep's row-max keys (Bsw16Shape::kKeyBits).
-inline int packed_key_bits(int k) { return k <= 2 ? 1 : k <= 4 ? 2 : k <= 8 ? 3 : k <= 16 ? 4 : 5; }
+inline int packed_key_bits(int k) {
+  return k <= 2 ? 1 : k <= 4 ? 2 : k <= 8 ? 3 : k <= 16 ? 4 : k <= 32 ? 5 : 6;
+}
 
 // The packed sweep is exact when every biased value stays below 2^13, every
 // difference its flags test stays below 2^11 (the F-extend flag at bit 11), and

@@ -574,10 +574,10 @@ __global__ void __launch_bounds__(T, MINB) bsw_dp_kernel(DevPairs P, BswLaunch B
 template <int G, int K, int T, int MINB>
 __global__ void __launch_bounds__(T, MINB) bsw16_dp_kernel(DevPairs P, BswLaunch B) {
   // Dynamic shared memory: each group's trace strip (one interleave block,
-  // kSlabs * 128 bytes), then each group's realignment buffer (4 * G * K halves).
+  // kStripBytes), then each group's realignment buffer (4 * G * K halves).
   extern __shared__ __align__(128) uint32_t bsw16_smem[];
   constexpr int CAP = 2 * G * K;
-  constexpr uint32_t kStripWords = Bsw16Shape<G, K>::kSlabs * 32u;
+  constexpr uint32_t kStripWords = Bsw16Shape<G, K>::kStripBytes / 4u;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t g = lane % G;
   const uint32_t gw = lane / G;
@@ -994,8 +994,8 @@ static cudaError_t launch_bsw16_shape(const DevPairs& P, const BswLaunch& B, uin
                                       int sms, cudaStream_t st, cudaEvent_t between, int parts) {
   cudaError_t e = cudaSuccess;
   if (parts & kBswPartDp) {
-    // per group: a trace strip of kSlabs * 128 bytes and 4 * G * K halves
-    const size_t smem = (size_t)(T / G) * Bsw16Shape<G, K>::kSlabs * 128u + (size_t)T * 8u * K;
+    // per group: a trace strip of kStripBytes and 4 * G * K halves
+    const size_t smem = (size_t)(T / G) * Bsw16Shape<G, K>::kStripBytes + (size_t)T * 8u * K;
     auto kern = bsw16_dp_kernel<G, K, T, MINB>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
@@ -1027,6 +1027,8 @@ const BswShapeInfo kBswShapes[] = {
     {2, 18, 128, 3, 1},
     // the same packed sweeps held to more resident blocks (fewer registers, some spilled)
     {4, 9, 256, 3, 1},   {2, 17, 128, 4, 1},
+    // one lane per pair: no cross-lane exchange, a row's scalar work done once
+    {1, 34, 128, 2, 1},
 };
 const int kNumBswShapes = sizeof(kBswShapes) / sizeof(kBswShapes[0]);
 
@@ -1051,6 +1053,7 @@ cudaError_t launch_bsw(int shape, const DevPairs& P, const BswLaunch& B, uint32_
     case 15: return launch_bsw16_shape<2, 18, 128, 3>(P, B, max_items, sms, st, between, parts);
     case 16: return launch_bsw16_shape<4, 9, 256, 3>(P, B, max_items, sms, st, between, parts);
     case 17: return launch_bsw16_shape<2, 17, 128, 4>(P, B, max_items, sms, st, between, parts);
+    case 18: return launch_bsw16_shape<1, 34, 128, 2>(P, B, max_items, sms, st, between, parts);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -1,5 +1,5 @@
 """Packed banded-SW trace layout, restated on the CPU: a 4-bit code per cell, four
-words (eight cells) per 4-byte slab, rows interleaved in blocks of 32 / G
+words (eight cells) per 4-byte slab, rows interleaved in blocks of 32 / G (8 for G = 1)
 ([row block][slab][row in block][lane] of 4-byte slabs, csrc/bsw16.cuh). For every
 packed launch shape and read length: each (row, lane, slab) slab is unique and lies
 inside the item's slot (shape_slot_bytes, csrc/internal.h), and each cell's code
@@ -8,13 +8,13 @@ cell, at the byte and nibble the DP kernel packed it into."""
 import pytest
 
 PACKED_SHAPES = [(2, 9), (4, 5), (4, 9), (8, 5), (8, 9), (16, 9), (32, 9), (2, 17),
-                 (2, 18)]  # (G, K words)
+                 (2, 18), (1, 34)]  # (G, K words)
 
 
 def geometry(g, k):
     slabs = (k + 3) // 4              # 4-byte code slabs per lane per row
     stride = g * 4 * slabs            # bytes per row
-    inter = 1 if g >= 32 else 32 // g
+    inter = 8 if g == 1 else 1 if g >= 32 else 32 // g
     return slabs, stride, inter
 
 
