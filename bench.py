@@ -269,14 +269,27 @@ def run_uneven(args, rank, local, world):
         sub = _subset(w, np.nonzero(w.bandwidth == band)[0][:20000])
         tuned[band] = autotune.tune_bsw_shape(
             ctx, band, lambda: ctx.bsw_batch(sub, cfg), device_name=torch.cuda.get_device_name(local))
+    # Both forms through the C entry point on the same preallocated pinned host
+    # outputs (result rows and CIGAR ops), as the e2e verification call does.
+    from kira_ls_aligner_b200.runtime import default_sw_cigar_cap
+    res_h = torch.empty(n * 32, dtype=torch.uint8).pin_memory()
+    ops_cap = default_sw_cigar_cap(batch)
+    ops_h = torch.empty(ops_cap, dtype=torch.int32).pin_memory()
+    cb = _abi.CigarBuf(ops_h.data_ptr(), ops_cap, 0)
+    pc, cc, cells_h = batch.to_c(), cfg.to_c(), C.c_uint64()
+
+    def call():
+        ctx.check(L.kira_gpu_bsw_batch(ctx.handle, C.byref(pc), C.byref(cc), res_h.data_ptr(),
+                                       C.byref(cb), C.byref(cells_h)))
+
     out = {}
     for mode in ("plain", "bucketed"):
         ctx.check(L.kira_gpu_set_plain(ctx.handle, 1 if mode == "plain" else 0))
         # The bucketed form replays its per-class launches from a CUDA graph.
         ctx.check(L.kira_gpu_set_graphs(ctx.handle, 0 if mode == "plain" else 1, None, None))
         for _ in range(args.warmup):
-            res, ops, cells = ctx.bsw_batch(batch, cfg)
-        ts = [_timed(lambda: ctx.bsw_batch(batch, cfg)) for _ in range(args.steps)]
+            call()
+        ts = [_timed(call) for _ in range(args.steps)]
         res, ops, cells = ctx.bsw_batch(batch, cfg)
         ctx.check(L.kira_gpu_profile(ctx.handle, 1))
         ctx.bsw_batch(batch, cfg)
@@ -300,8 +313,9 @@ def run_uneven(args, rank, local, world):
         "data": "synthetic (seeded)",
         "config": {"workload": w.name, "pairs": n, "read_len": "U[50,300]",
                    "band": "U{16,32,64,128}", "window": "read + 2*band", "errors": "U[0,3%] 8:1:1",
-                   "path": "host API, pinned inputs (reads + descriptors; windows from the "
-                           "resident reference), H2D + D2H per call"},
+                   "path": "host API (kira_gpu_bsw_batch), pinned inputs (reads + "
+                           "descriptors; windows from the resident reference) and pinned "
+                           "outputs (rows + CIGAR ops), H2D + D2H per call"},
         "bucketed": out["bucketed"], "plain": out["plain"],
         "speedup_vs_plain": out["bucketed"]["pairs_per_s"] / out["plain"]["pairs_per_s"],
         "cuda_graphs": graphs,

@@ -1027,8 +1027,9 @@ const BswShapeInfo kBswShapes[] = {
     {2, 18, 128, 3, 1},
     // the same packed sweeps held to more resident blocks (fewer registers, some spilled)
     {4, 9, 256, 3, 1},   {2, 17, 128, 4, 1},
-    // one lane per pair: no cross-lane exchange, a row's scalar work done once
-    {1, 34, 128, 2, 1},
+    // 34 words a lane: one lane per pair (no cross-lane exchange, a row's scalar
+    // work done once), and 2 / 4 lanes for bands up to 67 / 135
+    {1, 34, 128, 2, 1},  {2, 34, 128, 2, 1},  {4, 34, 128, 2, 1},
 };
 const int kNumBswShapes = sizeof(kBswShapes) / sizeof(kBswShapes[0]);
 
@@ -1054,6 +1055,8 @@ cudaError_t launch_bsw(int shape, const DevPairs& P, const BswLaunch& B, uint32_
     case 16: return launch_bsw16_shape<4, 9, 256, 3>(P, B, max_items, sms, st, between, parts);
     case 17: return launch_bsw16_shape<2, 17, 128, 4>(P, B, max_items, sms, st, between, parts);
     case 18: return launch_bsw16_shape<1, 34, 128, 2>(P, B, max_items, sms, st, between, parts);
+    case 19: return launch_bsw16_shape<2, 34, 128, 2>(P, B, max_items, sms, st, between, parts);
+    case 20: return launch_bsw16_shape<4, 34, 128, 2>(P, B, max_items, sms, st, between, parts);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -8,7 +8,7 @@ cell, at the byte and nibble the DP kernel packed it into."""
 import pytest
 
 PACKED_SHAPES = [(2, 9), (4, 5), (4, 9), (8, 5), (8, 9), (16, 9), (32, 9), (2, 17),
-                 (2, 18), (1, 34)]  # (G, K words)
+                 (2, 18), (1, 34), (2, 34), (4, 34)]  # (G, K words)
 
 
 def geometry(g, k):
