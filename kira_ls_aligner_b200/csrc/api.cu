@@ -35,7 +35,7 @@ enum BufId {
   B_ROWKEYS, B_DONE_ROW, B_WORK, B_WFA_MAXS, B_WFA_TBF, B_WFA_OUT, B_WFA_NCIG, B_WFA_SLOTS,
   B_WFA_SCRATCH, B_WFA_FLAGS, B_PF_CHAINS, B_PF_TOP1, B_PF_MARGIN, B_PF_OUT, B_PF_NCIG,
   B_PF_MDLEN, B_PF_MDOFF, B_PF_MD, B_PF_EXACT, B_WFA_FB, B_WFA_WHIST, B_SIEVE_LIST, B_PACKED, B_STATUS, B_KEEP, B_ROW_OFF,
-  B_ROWS, B_ROW_SUMS, B_ROW_TOTAL, B_COUNT
+  B_ROWS, B_ROW_SUMS, B_ROW_TOTAL, B_SW_GROUPS, B_COUNT
 };
 
 struct DevBuf {
@@ -550,11 +550,24 @@ struct ChunkMode {
   cudaEvent_t after_scan = nullptr;   // recorded once this chunk's CIGARs are placed
 };
 
-// The composed path on device buffers, enqueued on `st`.
+// The banded-SW stage of a chunk deferred to a launch over several chunks' items:
+// the batch-wide per-pair arrays the front stages write, and the item list (with
+// its count word) the Myers stage appends the chunk's SW pairs to as batch indices.
+struct DeferSw {
+  uint32_t* ncig;   // batch-wide, pair index = base + the chunk's pair
+  int32_t* swoff;   // batch-wide band offsets
+  uint32_t* slist;  // item list of the chunk's group
+  uint32_t* count;  // its count word
+  uint32_t base;    // batch index of the chunk's pair 0
+};
+
+// The composed path on device buffers, enqueued on `st`. With `df` only the stages
+// up to Myers run (sieve, certificate, Myers; the SW pairs are listed in df).
 int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verify_params& p,
                     uint64_t read_bytes, uint64_t win_bytes, bool resident, kira_sw_result* out,
                     uint32_t* ops, uint64_t cap, uint64_t* total_dev, kira_verify_detail* detail,
-                    unsigned long long* cells_dev, cudaStream_t st, ChunkMode cm = ChunkMode()) {
+                    unsigned long long* cells_dev, cudaStream_t st, ChunkMode cm = ChunkMode(),
+                    const DeferSw* df = nullptr) {
   cudaError_t cerr = cudaSuccess;
   const uint32_t n = D.n;
   if (n == 0) return KIRA_OK;
@@ -564,10 +577,18 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
   const SwParams sp = resolve(p.sw);
   const int shape = pick_shape(ctx, mx.band, mx.q, sp);
   if (shape < 0) return fail(ctx, KIRA_ERR_INVALID, "no banded-SW shape for band %u", mx.band);
-  KIRA_DBUF(ncig, uint32_t, B_NCIG, n);
-  KIRA_DBUF(swoff, int32_t, B_SW_OFFSET, n);
+  uint32_t* ncig = df ? df->ncig + df->base : nullptr;
+  int32_t* swoff = df ? df->swoff + df->base : nullptr;
+  uint32_t* slist = df ? df->slist : nullptr;
+  if (!df) {
+    KIRA_DBUF(a, uint32_t, B_NCIG, n);
+    KIRA_DBUF(b, int32_t, B_SW_OFFSET, n);
+    KIRA_DBUF(c, uint32_t, B_SW_LIST, n);
+    ncig = a;
+    swoff = b;
+    slist = c;
+  }
   KIRA_DBUF(mlist, uint32_t, B_MYERS_LIST, n);
-  KIRA_DBUF(slist, uint32_t, B_SW_LIST, n);
   KIRA_DBUF(counters, uint32_t, B_COUNTERS, 4);
   KIRA_CUDA(cudaMemsetAsync(counters, 0, cm.first ? 16 : 8, st));
   VerifyDev V{p.sieve_threshold, p.cert_strict, sp,       out,       detail, ncig,
@@ -600,7 +621,12 @@ int verify_pipeline(kira_ctx* ctx, DevPairs D, const Maxes& mx, const kira_verif
   M.sw_list = slist;
   M.counters = counters;
   M.flags = counters + 2;
+  if (df) {
+    M.sw_count = df->count;
+    M.sw_base = df->base;
+  }
   KIRA_CUDA(launch_myers(D, M, n, ctx->sms, st));
+  if (df) return KIRA_OK;  // the SW stage runs over the group's items later
   BswLaunch B{};
   const uint32_t per_round = round_items(ctx, n, shape, mx.q);
   rc = prepare_bsw(ctx, n, n, per_round, mx, shape, B);
@@ -1165,6 +1191,88 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
   // (measured: the 2M-pair compact call 3.8 -> 3.6 ms); on the copy, compute and
   // download streams of this path the later uploads were not held up behind the
   // kernels' waits.
+  // Grouped banded SW (three or more chunks): each chunk runs only the stages up to
+  // Myers, which list its SW pairs (batch indices) in its group's item list; the
+  // chunks form two groups (the first ending at about 55 % of the pairs), and each
+  // group's DP + traceback run once over the group's items on two side streams
+  // while the later chunks' uploads and front stages go on. One SW launch per chunk
+  // was a small partial wave each (a chunk of 250k-500k pairs has 12k-25k items
+  // against 38k resident one-lane groups). Scratch: group 0 in this context, group
+  // 1 in the twin; the CIGAR scan and compaction run once over the batch.
+  const bool grouped = nch >= 3;
+  uint32_t gsplit = nch;  // first chunk of group 1
+  DeferSw dfs{};
+  if (grouped) {
+    gsplit = 1;
+    while (gsplit + 1 < nch && (uint64_t)bounds[gsplit] * 100 < (uint64_t)n * 55) ++gsplit;
+    KIRA_DBUF(gn, uint32_t, B_NCIG, n);
+    KIRA_DBUF(gs, int32_t, B_SW_OFFSET, n);
+    KIRA_DBUF(gl, uint32_t, B_SW_LIST, n);
+    KIRA_DBUF(gc, uint32_t, B_SW_GROUPS, 2);
+    KIRA_CUDA(cudaMemsetAsync(gc, 0, 8, st));
+    dfs = DeferSw{gn, gs, gl, gc, 0};
+    for (int k = 0; k < 4; ++k)
+      if (!ctx->cls_st[k]) KIRA_CUDA(cudaStreamCreateWithFlags(&ctx->cls_st[k], cudaStreamNonBlocking));
+    for (int k = 0; k < kBandClasses; ++k)
+      if (!ctx->ev_cls_join[k])
+        KIRA_CUDA(cudaEventCreateWithFlags(&ctx->ev_cls_join[k], cudaEventDisableTiming));
+    if (!ctx->ev_cls_fork)
+      KIRA_CUDA(cudaEventCreateWithFlags(&ctx->ev_cls_fork, cudaEventDisableTiming));
+  }
+  const SwParams gsp = resolve(p.sw);
+  BswLaunch gB[2] = {};
+  // DP + traceback of group g (chunks [c0, c1)) on side streams 2g and 2g + 1,
+  // behind the group's front stages; ev_cls_join[g] marks the end.
+  auto run_group_sw = [&](int g, uint32_t c0, uint32_t c1) -> int {
+    kira_ctx* gx = g == 0 ? ctx : twin;
+    cudaStream_t s1 = ctx->cls_st[2 * g], s2 = ctx->cls_st[2 * g + 1];
+    Maxes gm;
+    for (uint32_t c = c0; c < c1; ++c) {
+      gm.q = std::max(gm.q, scans[c].mx.q);
+      gm.w = std::max(gm.w, scans[c].mx.w);
+      gm.band = std::max(gm.band, scans[c].mx.band);
+    }
+    const int shape = pick_shape(ctx, gm.band, gm.q, gsp);
+    if (shape < 0) return fail(ctx, KIRA_ERR_INVALID, "no banded-SW shape for band %u", gm.band);
+    const uint32_t lo = bounds[c0], ng = bounds[c1] - lo;
+    const uint32_t per_round = round_items(gx, ng, shape, gm.q);
+    BswLaunch& B = gB[g];
+    int rc = prepare_bsw(gx, n, ng, per_round, gm, shape, B);
+    if (rc) {
+      if (gx != ctx) ctx->last_error = gx->last_error;
+      return rc;
+    }
+    B.list = dfs.slist + lo;
+    B.count_dev = dfs.count + g;
+    B.sp = gsp;
+    B.bias = packed_bias(kBswShapes[shape], gsp);
+    B.offset = dfs.swoff;
+    B.cells = cells_dev;
+    B.out = dout;
+    B.ncig = dfs.ncig;
+    B.flags = static_cast<uint32_t*>(gx->bufs[B_COUNTERS].p) + 2;
+    // The group's scratch was (re)sized on gx's stream; its chunks' fronts ran on
+    // both compute streams.
+    KIRA_CUDA(cudaEventRecord(ctx->ev_cls_join[2 + g], gx->stream));
+    KIRA_CUDA(cudaStreamWaitEvent(s1, ctx->ev_cls_join[2 + g], 0));
+    for (uint32_t c = c0; c < c1; ++c) KIRA_CUDA(cudaStreamWaitEvent(s1, ctx->ev_comp[c], 0));
+    const DevPairs Dg{n,  rs, ro, rl, ws, wo, wl, bo, ab, bw, rp, wp};
+    if (per_round >= ng && ng >= kSplitPairs) {
+      KIRA_CUDA(cudaEventRecord(ctx->ev_cls_join[4 + g], s1));
+      KIRA_CUDA(cudaStreamWaitEvent(s2, ctx->ev_cls_join[4 + g], 0));
+      BswLaunch B1 = B, B2 = B;
+      B1.split = 1u;
+      B2.split = 2u;
+      KIRA_CUDA(launch_bsw(shape, Dg, B1, ng, ctx->sms, s1));
+      KIRA_CUDA(launch_bsw(shape, Dg, B2, ng, ctx->sms, s2));
+      KIRA_CUDA(cudaEventRecord(ctx->ev_cls_join[4 + g], s2));
+      KIRA_CUDA(cudaStreamWaitEvent(s1, ctx->ev_cls_join[4 + g], 0));
+    } else {
+      KIRA_CUDA(launch_bsw_rounds(shape, Dg, B, ng, per_round, ctx->sms, s1, nullptr));
+    }
+    KIRA_CUDA(cudaEventRecord(ctx->ev_cls_join[g], s1));
+    return KIRA_OK;
+  };
   std::vector<uint64_t> r_from(nch), r_to(nch), w_from(nch), w_to(nch);
   uint64_t rdone = 0, wdone = 0;
   cudaStream_t up = ctx->h2d;
@@ -1231,18 +1339,49 @@ int verify_batch_chunked(kira_ctx* ctx, const kira_pairs& P, const kira_verify_p
     cm.accumulate = true;
     cm.before_scan = c ? ctx->ev_scan[c - 1] : nullptr;
     cm.after_scan = ctx->ev_scan[c];
+    DeferSw df = dfs;
+    df.slist = dfs.slist + bounds[c < gsplit ? 0 : gsplit];
+    df.count = dfs.count + (c < gsplit ? 0 : 1);
+    df.base = lo;
     int rc = verify_pipeline(cx, D, scans[c].mx, p, P.read_seq_bytes, P.win_seq_bytes, !host_w,
                              dout + lo, ops, cigar->cap, total_dev, ddet ? ddet + lo : nullptr,
-                             cells_dev, cs, cm);
+                             cells_dev, cs, cm, grouped ? &df : nullptr);
+    if (!rc && co && !grouped)
+      rc = launch_status_keep(dout + lo, m, dstat + lo, keep + lo, ctx->sms, cs) == cudaSuccess
+               ? KIRA_OK
+               : cuda_fail(ctx, cudaGetLastError(), "status bytes");
+    if (!rc) KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], cs));
+    if (!rc && grouped && c + 1 == gsplit) {
+      // Group 0's SW needs its chunks' maxima (checked) and their fronts (enqueued).
+      rc = run_group_sw(0, 0, gsplit);
+    }
+    if (!rc && grouped && c + 1 == nch) rc = run_group_sw(1, gsplit, nch);
     if (rc) {
-      if (cx != ctx) ctx->last_error = cx->last_error;
+      if (cx != ctx && cx->last_error.size()) ctx->last_error = cx->last_error;
       cudaStreamSynchronize(up);
       cudaStreamSynchronize(st);
       cudaStreamSynchronize(twin->stream);
+      for (int k = 0; k < 4; ++k)
+        if (ctx->cls_st[k]) cudaStreamSynchronize(ctx->cls_st[k]);
       return rc;
     }
-    if (co) KIRA_CUDA(launch_status_keep(dout + lo, m, dstat + lo, keep + lo, ctx->sms, cs));
-    KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], cs));
+  }
+  if (grouped) {
+    // Both groups' SW done: one CIGAR scan over the batch, then each group's
+    // compaction from its own slots, then the status bytes.
+    KIRA_CUDA(cudaStreamWaitEvent(st, ctx->ev_cls_join[0], 0));
+    KIRA_CUDA(cudaStreamWaitEvent(st, ctx->ev_cls_join[1], 0));
+    KIRA_DBUF(off, uint32_t, B_CIG_OFF, n);
+    KIRA_DBUF(sums, uint32_t, B_CHUNK_SUMS, n / 4096 + 2);
+    KIRA_CUDA(launch_cigar_scan(dfs.ncig, n, off, sums, total_dev, st));
+    for (int g = 0; g < 2; ++g) {
+      const uint32_t lo = bounds[g ? gsplit : 0], hi = bounds[g ? nch : gsplit];
+      CompactLaunch CL{hi - lo, dout + lo, dfs.ncig + lo, off + lo, gB[g].item_of_pair + lo,
+                       gB[g].cig_slots, gB[g].slot_cap, ops, cigar->cap};
+      KIRA_CUDA(launch_cigar_compact(CL, ctx->sms, st));
+    }
+    if (co) KIRA_CUDA(launch_status_keep(dout, n, dstat, keep, ctx->sms, st));
+    for (uint32_t c = 0; c < nch; ++c) KIRA_CUDA(cudaEventRecord(ctx->ev_comp[c], st));
   }
   for (uint32_t c = 0; c < nch; ++c) {
     const uint32_t lo = bounds[c], m = bounds[c + 1] - lo;

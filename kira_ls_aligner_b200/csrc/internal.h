@@ -59,6 +59,10 @@ struct MyersLaunch {
   uint32_t* sw_list;
   uint32_t* counters;
   uint32_t* flags;            // bit 2: pattern longer than the kernel supports
+  // Banded-SW items of several calls gathered into one list: its count word (null:
+  // counters[1]) and the batch index of this call's pair 0 (added to each entry).
+  uint32_t* sw_count;
+  uint32_t sw_base;
 };
 
 struct BswLaunch {

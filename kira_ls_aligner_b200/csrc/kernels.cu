@@ -422,7 +422,8 @@ __device__ void myers_warp(const DevPairs& P, const MyersLaunch& M, uint32_t bas
   if (M.cascade) {
     const uint32_t hits = __ballot_sync(0xFFFFFFFFu, valid && hit);
     uint32_t base_slot = 0;
-    if (lane == 0 && hits) base_slot = atomicAdd(M.counters + 1, (uint32_t)__popc(hits));
+    if (lane == 0 && hits)
+      base_slot = atomicAdd(M.sw_count ? M.sw_count : M.counters + 1, (uint32_t)__popc(hits));
     base_slot = __shfl_sync(0xFFFFFFFFu, base_slot, 0);
     if (valid) {
       if (M.detail) {
@@ -431,7 +432,7 @@ __device__ void myers_warp(const DevPairs& P, const MyersLaunch& M, uint32_t bas
       }
       if (hit) {
         const uint32_t rank = (uint32_t)__popc(hits & ((1u << lane) - 1u));
-        M.sw_list[base_slot + rank] = pair;
+        M.sw_list[base_slot + rank] = M.sw_base + pair;
       } else {
         kira_sw_result r;
         r.score = 0;
