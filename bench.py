@@ -724,7 +724,7 @@ def run_gapfill(args, rank, local, world):
     A sample of segments is checked against the oracle outside the timed region."""
     import torch
 
-    from kira_ls_aligner_b200 import AlignmentConfig, GpuContext, PairBatch, _abi, synth
+    from kira_ls_aligner_b200 import AlignmentConfig, GpuContext, PairBatch, _abi, autotune, synth
     if rank != 0:
         return
     torch.cuda.set_device(local)
@@ -738,6 +738,15 @@ def run_gapfill(args, rank, local, world):
     ctx = GpuContext(local)
     ctx.ref_upload(g.reference)
     L = _abi.lib()
+    # Launch shape of the band-256 class: installed, or autotuned on 4,000 segments
+    # drawn across the batch (DP stage time from the library's stage events).
+    if args.shape >= 0:
+        ctx.check(L.kira_gpu_set_bsw_shape(ctx.handle, 256, args.shape))
+        tuned = {"best": args.shape, "shape": autotune.shapes()[args.shape], "dp_ms": None}
+    else:
+        sub = _subset(g, np.linspace(0, g.n_pairs - 1, 4000).astype(np.int64))
+        tuned = autotune.tune_bsw_shape(ctx, 256, lambda: ctx.bsw_batch(sub, cfg),
+                                        device_name=torch.cuda.get_device_name(local))
     for _ in range(args.warmup):
         res, ops, cells = ctx.bsw_batch(b, cfg)
     ts = [_timed(lambda: ctx.bsw_batch(b, cfg)) for _ in range(args.steps)]
@@ -787,6 +796,7 @@ def run_gapfill(args, rank, local, world):
                    "path": "resident reference, host API (H2D segments + descriptors, "
                            "D2H rows + CIGARs per call)", "generate_s": round(gen_s, 1)},
         "gcups": cells / (ms / 1e3) / 1e9, "cells": int(cells), "trace_rounds": rounds,
+        "autotune": tuned,
         "reads_per_s": g.n_reads / (ms / 1e3), "stage_ms": stage, "parity": parity,
         "checksum": int(res["score"].astype(np.int64).sum())}))
     ctx.close()

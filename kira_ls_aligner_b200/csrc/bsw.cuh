@@ -33,6 +33,7 @@ namespace kira {
 
 template <int G, int K>
 struct BswShape {
+  static_assert(K <= 32, "the E-extend flags of a lane's cells are one 32-bit mask");
   static constexpr int kCap = G * K;                    // cells per row
   static constexpr int kWords = (K + 7) / 8;            // trace words per lane per row
   static constexpr int kLaneBytes = 4 * kWords;         // nibble k at byte k/2, half k&1
