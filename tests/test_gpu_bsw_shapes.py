@@ -44,7 +44,7 @@ def _shapes():
     return list(enumerate(autotune.shapes()))
 
 
-@pytest.mark.parametrize("shape", range(14))
+@pytest.mark.parametrize("shape", range(24))
 @pytest.mark.parametrize("scoring", [(1, 4, 6, 1, True, 16), (2, 3, 5, 2, False, 16),
                                      (1, 1, 0, 1, True, 4), (3, 2, 4, 0, True, 16)])
 def test_forced_shape(ctx, shape, scoring):
