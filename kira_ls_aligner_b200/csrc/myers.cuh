@@ -84,23 +84,36 @@ __device__ __forceinline__ bool myers_lane(uint32_t m, uint32_t n, uint32_t max_
   }
   const uint32_t* peq = sm.peq + lane;
   uint32_t err = m, best = m, pos = 0;
-  uint32_t t0 = 0, t1 = 0, tv = 0;
+  // Software pipelined over the text: the Peq words of column j + 1 are loaded while
+  // column j is computed, and the text plane word of the next 32 columns one block
+  // ahead, so neither load's latency sits on the column-to-column chain.
+  // Column code: 0-3 for ACGT, 4 (an all-zero Peq row) for any other base.
+  auto code_at = [](uint32_t bit, const PlaneWord& w) {
+    return ((w.v >> bit) & 1u) ? (((w.b0 >> bit) & 1u) | (((w.b1 >> bit) & 1u) << 1)) : 4u;
+  };
+  PlaneWord cw = plane_word_at(tplanes, tpos);
+  PlaneWord nw = n > 32u ? plane_word_at(tplanes, tpos + 32u) : cw;
+  uint32_t eqn[L];
+  {
+    const uint32_t* pc = peq + code_at(0u, cw) * 32u;
+#pragma unroll
+    for (int k = 0; k < L; ++k) eqn[k] = pc[k * 160];
+  }
   for (uint32_t j = 0; j < n; ++j) {
-    const uint32_t bit = j & 31u;
-    if (bit == 0u) {
-      const PlaneWord pw = plane_word_at(tplanes, tpos + j);
-      t0 = pw.b0;
-      t1 = pw.b1;
-      tv = pw.v;
-    }
-    const uint32_t code = ((tv >> bit) & 1u) ? (((t0 >> bit) & 1u) | (((t1 >> bit) & 1u) << 1))
-                                             : 4u;
-    const uint32_t* pc = peq + code * 32u;
     uint32_t eq[L], av[L], sum[L];
 #pragma unroll
     for (int k = 0; k < L; ++k) {
-      eq[k] = pc[k * 160];
+      eq[k] = eqn[k];
       av[k] = eq[k] & vp[k];
+    }
+    if ((j & 31u) == 31u) {  // column j + 1 opens the next block of 32
+      cw = nw;
+      if (j + 33u < n) nw = plane_word_at(tplanes, tpos + j + 33u);
+    }
+    if (j + 1u < n) {
+      const uint32_t* pc = peq + code_at((j + 1u) & 31u, cw) * 32u;
+#pragma unroll
+      for (int k = 0; k < L; ++k) eqn[k] = pc[k * 160];
     }
     add_chain<L>(av, vp, sum);
     uint32_t hp_prev = 0, hn_prev = 0, hp_top = 0, hn_top = 0;
