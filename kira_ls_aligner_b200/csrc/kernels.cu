@@ -1031,6 +1031,9 @@ const BswShapeInfo kBswShapes[] = {
     // 34 words a lane: one lane per pair (no cross-lane exchange, a row's scalar
     // work done once), and 2 / 4 lanes for bands up to 67 / 135
     {1, 34, 128, 2, 1},  {2, 34, 128, 2, 1},  {4, 34, 128, 2, 1},
+    // one lane per pair in smaller blocks (a block's SMs free up at a finer grain
+    // at the end of a launch)
+    {1, 34, 64, 4, 1},   {1, 34, 32, 8, 1},
 };
 const int kNumBswShapes = sizeof(kBswShapes) / sizeof(kBswShapes[0]);
 
@@ -1058,6 +1061,8 @@ cudaError_t launch_bsw(int shape, const DevPairs& P, const BswLaunch& B, uint32_
     case 18: return launch_bsw16_shape<1, 34, 128, 2>(P, B, max_items, sms, st, between, parts);
     case 19: return launch_bsw16_shape<2, 34, 128, 2>(P, B, max_items, sms, st, between, parts);
     case 20: return launch_bsw16_shape<4, 34, 128, 2>(P, B, max_items, sms, st, between, parts);
+    case 21: return launch_bsw16_shape<1, 34, 64, 4>(P, B, max_items, sms, st, between, parts);
+    case 22: return launch_bsw16_shape<1, 34, 32, 8>(P, B, max_items, sms, st, between, parts);
     default: return cudaErrorInvalidValue;
   }
 }
