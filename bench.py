@@ -629,9 +629,12 @@ def run_serving(args, rank, local, world):
     def serve(open_loop: bool):
         srv = Server(local, slots=args.slots, max_batch_pairs=1 << 20)
         srv.ref_upload(pool.reference)
-        for _ in range(2):  # warm-up: every slot grows its arenas on full batches
+        # Warm-up (untimed): the whole request stream submitted at once, twice, so that
+        # every slot has run full-size batches of both kinds (arenas, pinned staging,
+        # the chunked path's twin context and side streams) before the timed run.
+        for _ in range(2):
             warm = [srv.submit_verify(b, vp) if kind == "short" else srv.submit_bsw(b, cfg)
-                    for _, kind, b in reqs[:12 * args.slots]]
+                    for _, kind, b in reqs]
             for t in warm:
                 t.wait(600)
         b0 = srv.stats()["batches"]
