@@ -661,6 +661,12 @@ def run_serving(args, rank, local, world):
                "p50_long_ms": pct([i.latency_s for k, i in infos if k == "long"], 50),
                "p99_long_ms": pct([i.latency_s for k, i in infos if k == "long"], 99),
                "batches": srv.stats()["batches"] - b0,
+               # where the slowest requests spent their time: queued (submit to batch
+               # start) and in their batch (start to done)
+               "queue_ms_p50_p99": [pct([(i.t_start_ns - i.t_submit_ns) / 1e9 for _, i in infos], q)
+                                    for q in (50, 99)],
+               "batch_ms_p50_p99": [pct([(i.t_done_ns - i.t_start_ns) / 1e9 for _, i in infos], q)
+                                    for q in (50, 99)],
                "host_ms": srv.stats()["host_ms"], "submit_s": t_sub,
                "mean_requests_per_batch": float(np.mean([i.batch_requests for _, i in infos]))}
         srv.close()
