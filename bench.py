@@ -7,10 +7,14 @@ pairs, 150 bp reads, 250 bp windows, 8 candidates per read, band 33, scoring
 
 One JSON line on rank 0. `value` = pairs/s with inputs resident in HBM
 (kira_gpu_verify_dev, CUDA events on the launching stream, L2 flushed between
-steps); `e2e` = pairs/s through the host API (kira_gpu_verify_batch) with pinned
-host inputs, H2D + D2H inside the timed region. Multi-GPU: one process per GPU,
-each rank verifies its own 2M-pair shard (weak scaling, no data-path collective),
-time = max over ranks.
+steps); `e2e` = pairs/s through the host API (kira_gpu_verify_batch_compact: a
+status byte per pair, rows and CIGARs of the aligned pairs; kira_gpu_verify_batch
+with a row per pair beside it) with pinned host inputs and outputs, H2D + D2H inside
+the timed region. After the timed steps the line's `parity` block checks every pair's
+row and CIGAR against the oracle. Multi-GPU: one process per GPU, one job sharded into
+contiguous ranges (weak scaling, no data-path collective), time = max over ranks.
+The line also folds in a short uneven-batch run (`uneven`) and a serving run
+(`serving`); `--workload` runs the other configurations on their own.
 """
 from __future__ import annotations
 
